@@ -1,0 +1,168 @@
+"""Zel'dovich initial conditions in CUBE's particle format (utilities/ic.f90).
+
+Steps, as in ic.f90 for one image (nn=1):
+  noise U[0,1) on the (nic*ng)^3 grid (ic.f90:262-268; here a seeded Philox stream)
+  -> Box-Muller pairs along x (:289-299)
+  -> forward FFT, multiply by sqrt(P(k) (nw/box)^3), zero mode (:363-385)
+  -> potential kernel -4 pi / k_discrete^2 (:415-437) and inverse FFT
+  -> 2x2x2 corner gradient at the particle lattice, displacement -grad/(8 nic pi ratio_cs)
+     in coarse cells and velocity -grad/(8 pi nic)*vfactor(a) (:665-722)
+  -> ZIPX encode floor(xq/x_resolution) with integer wrap (:717-719), PID (:723-729),
+     cell order with the reference's arrival order (tile-major, spine index).
+The FFTs run in numpy (small grids) or torch on a GPU (large grids); the IC is an
+input to the timed step, not part of it.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import cosmology
+from .params import Params
+
+
+def noise_field(n: int, seed: int) -> np.ndarray:
+    """Uniform [0,1) float32 noise, Fortran order (x fastest) as noise_<img>.bin stores it.
+    Returned as array[z, y, x]."""
+    rng = np.random.Generator(np.random.Philox(key=seed))
+    return rng.random((n, n, n), dtype=np.float32)
+
+
+def box_muller(u: np.ndarray) -> np.ndarray:
+    """ic.f90:289-299: pairs (i, i+1) along x."""
+    th = 2 * np.pi * u[..., 0::2].astype(np.float64)
+    r = np.sqrt(-2 * np.log(1 - u[..., 1::2].astype(np.float64)))
+    g = np.empty(u.shape, dtype=np.float32)
+    g[..., 0::2] = (r * np.cos(th)).astype(np.float32)
+    g[..., 1::2] = (r * np.sin(th)).astype(np.float32)
+    return g
+
+
+def _kgrid(n: int):
+    k = np.fft.fftfreq(n, d=1.0 / n)  # integer wavenumbers, Nyquist negative
+    kx = np.arange(n // 2 + 1, dtype=np.float64)
+    return k, kx
+
+
+def potential_field(p: Params, a: float, seed: int, use_torch: bool = False) -> np.ndarray:
+    """phi on the (nic*ng)^3 IC grid, array[z, y, x] float32."""
+    nw = p.nic * p.ng
+    g = box_muller(noise_field(nw, seed))
+    k1, kx = _kgrid(nw)
+    kz = k1[:, None, None]
+    ky = k1[None, :, None]
+    kxx = kx[None, None, :]
+    kr = 2 * math.pi * np.sqrt(kxx ** 2 + ky ** 2 + kz ** 2) / p.box
+    tf = np.sqrt(cosmology.linear_power(kr, a, p) * (nw / p.box) ** 3)
+    s = np.sin(np.pi * np.arange(nw) / nw)
+    kdisc = (2 * s[None, None, : nw // 2 + 1]) ** 2 + (2 * np.sin(np.pi * k1 / nw))[None, :, None] ** 2 \
+        + (2 * np.sin(np.pi * k1 / nw))[:, None, None] ** 2
+    kdisc = np.maximum(kdisc, 1.0 / nw ** 2)
+    kern = -4 * np.pi / kdisc
+    kern[0, 0, 0] = 0.0
+    mult = (tf * kern).astype(np.float64)
+    mult[0, 0, 0] = 0.0
+    if use_torch:
+        import torch
+
+        dev = torch.device("cuda")
+        gt = torch.from_numpy(g).to(dev)
+        ck = torch.fft.rfftn(gt.double(), dim=(0, 1, 2))
+        ck *= torch.from_numpy(mult).to(dev)
+        phi = torch.fft.irfftn(ck, s=(nw, nw, nw), dim=(0, 1, 2)).float().cpu().numpy()
+        del gt, ck
+        torch.cuda.empty_cache()
+        return phi
+    ck = np.fft.rfftn(g.astype(np.float64))
+    ck *= mult
+    return np.fft.irfftn(ck, s=(nw, nw, nw)).astype(np.float32)
+
+
+def zeldovich(p: Params, z_i: float = 49.0, seed: int = 1, use_torch: bool = False):
+    """Particles (xp, vp, pid, rhoc) in the reference checkpoint layout, plus header info.
+
+    Returns a dict with keys xp (N,3) int8/int16, vp (N,3) float32, pid (N,) int64,
+    rhoc (nnt^3 * nt^3,) int32, a, mass_p_cdm, vz_max, dt_vmax.
+    """
+    p.validate()
+    a = 1.0 / (1.0 + z_i)
+    nic, rcs, npnc = p.nic, p.ratio_cs, p.np_nc
+    nw = nic * p.ng
+    phi = potential_field(p, a, seed, use_torch)
+    nlat = p.nc * npnc  # particles per dimension
+    step = rcs * nic // npnc  # IC cells per lattice spacing
+    idx = (np.arange(nlat) * step)  # 0-based IC index ii-1 of lattice point
+    # corner gradient gradphi(d) = 0.5*sum over the 2x2x2 block of +/- phi (ic.f90:665-667)
+    im = (idx - 1) % nw
+    i0 = idx % nw
+    P = phi  # [z,y,x]
+
+    def blk(zs, ys, xs):
+        return P[np.ix_(zs, ys, xs)].astype(np.float64)
+
+    c = {}
+    for bz, zs in ((0, im), (1, i0)):
+        for by, ys in ((0, im), (1, i0)):
+            for bx, xs in ((0, im), (1, i0)):
+                c[(bz, by, bx)] = blk(zs, ys, xs)
+    gx = sum(0.5 * (1 if bx else -1) * v for (bz, by, bx), v in c.items())
+    gy = sum(0.5 * (1 if by else -1) * v for (bz, by, bx), v in c.items())
+    gz = sum(0.5 * (1 if bz else -1) * v for (bz, by, bx), v in c.items())
+    del c
+    grad = np.stack([gx, gy, gz], axis=-1).astype(np.float32)  # [z,y,x,3] real4 gradphi
+    del gx, gy, gz
+    vf = cosmology.vfactor(a, p.omega_m, p.omega_l)
+    # Lagrangian position in coarse units (0-based global), ic.f90:700
+    lat = np.arange(nlat, dtype=np.float64) / npnc + (0.5 / nic) / rcs
+    disp = -grad.astype(np.float64) / (8 * nic * math.pi * rcs)
+    X = np.empty((nlat, nlat, nlat, 3), dtype=np.float64)
+    X[..., 0] = lat[None, None, :] + disp[..., 0]
+    X[..., 1] = lat[None, :, None] + disp[..., 1]
+    X[..., 2] = lat[:, None, None] + disp[..., 2]
+    vel = (-grad / np.float32(8 * math.pi * nic) * np.float32(vf)).astype(np.float32)
+    # max displacement gradient for nlayer and vz_max (ic.f90:575-590)
+    grad_max = np.abs(grad).max(axis=(0, 1, 2)) * 2.0
+    vmax3 = grad_max / (8 * nic * math.pi) * vf
+    # cells (global 0-based), wrapped
+    X = X.reshape(-1, 3)
+    vel = vel.reshape(-1, 3)
+    cell = np.floor(X).astype(np.int64)  # g = ceiling(xq) in 1-based == floor + 1 for non-integers
+    cellw = cell % p.nc
+    # PID (ic.f90:723-729): lattice coords of the particle
+    lz, ly, lx = np.meshgrid(np.arange(nlat), np.arange(nlat), np.arange(nlat), indexing="ij")
+    lat_idx = np.stack([lx.ravel(), ly.ravel(), lz.ravel()], axis=-1)
+    iq = (lat_idx * (rcs // npnc)) % p.ng
+    pid = (iq[:, 0] + p.ng * iq[:, 1] + p.ng * p.ng * iq[:, 2] + 1).astype(np.int64)
+    # destination tile and arrival key (ilayer, k, j, i) in the destination tile frame
+    nt = p.nt
+    npt = nt * npnc
+    npb = npnc
+    tile = cellw // nt
+    lat_loc = lat_idx - tile * npt  # local lattice index (0-based), wrap into [-npb, npt+npb)
+    lat_loc = (lat_loc + npb) % (nlat) - npb
+    nlayer = 2 * int(math.ceil(float(np.float32(grad_max[2])) * npnc / (8 * nic * math.pi * rcs))) + 3
+    kk = lat_loc[:, 2] + npb  # 0-based from 1-npb
+    ilayer = kk % nlayer
+    span = npt + 2 * npb
+    key = ((ilayer * span + kk) * span + (lat_loc[:, 1] + npb)) * span + (lat_loc[:, 0] + npb)
+    loc = cellw - tile * nt
+    order_cell = ((((tile[:, 2] * p.nnt + tile[:, 1]) * p.nnt + tile[:, 0]) * nt + loc[:, 2]) * nt
+                  + loc[:, 1]) * nt + loc[:, 0]
+    perm = np.lexsort((key, order_cell))
+    xres = 2.0 ** (-8 * p.izipx)
+    frac_code = np.floor(X / xres).astype(np.int64)  # floor(xq/x_resolution) in any frame: same low bits
+    mod = 1 << (8 * p.izipx)
+    code = frac_code % mod
+    code = np.where(code >= mod // 2, code - mod, code).astype(p.xdtype)
+    rhoc = np.bincount(order_cell, minlength=p.ncells).astype(np.int32)
+    return {
+        "xp": np.ascontiguousarray(code[perm]),
+        "vp": np.ascontiguousarray(vel[perm]),
+        "pid": np.ascontiguousarray(pid[perm]),
+        "rhoc": rhoc,
+        "a": a,
+        "mass_p_cdm": float(p.ng) ** 3 / float(nlat ** 3),
+        "vz_max": float(vmax3[2]),
+        "dt_vmax": float(np.float32(0.9) * 16.0 / np.float32(max(vmax3.max(), 1e-30))),
+    }

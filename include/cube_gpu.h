@@ -1,0 +1,148 @@
+/*
+ * cube_gpu.h -- C ABI of the B200 P3M gravity step for one CUBE image (nn=1).
+ *
+ * The reference drives its step with zero-argument Fortran subroutines that share
+ * module globals (main.f90:33-38: timestep, drift, buffer_grid, buffer_x, kick,
+ * buffer_v).  This header replaces that sequence with explicit calls on an opaque
+ * context.  Every entry point returns 0 on success or a negative CUBE_E_* code;
+ * cube_gpu_last_error() gives the text.  A Fortran host binds these through an
+ * ISO_C_BINDING interface module (see the integration notes); a Python host binds
+ * them with ctypes (cube_nu_b200/_lib.py).
+ *
+ * Conventions
+ *  - Arrays cross the boundary in the reference's own memory layout: xp(3,np) and
+ *    vp(3,np) are Fortran column-major, i.e. three consecutive values per particle;
+ *    rhoc(nt,nt,nt,nnt,nnt,nnt) is the physical coarse-cell count array of the
+ *    checkpoint file `np` (checkpoint.f90:30), x fastest.
+ *  - Particles are ordered as the reference stores them: tile (z,y,x outer), then
+ *    coarse cell in the tile (x fastest), then arrival order (drift.f90:96-136).
+ *  - Between cube_gpu_upload and cube_gpu_download the device owns the particle
+ *    state; host buffers are only borrowed during those calls.
+ *  - One host thread per context; never call from inside an OpenMP region.
+ */
+#ifndef CUBE_GPU_H
+#define CUBE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes (negative). */
+#define CUBE_OK 0
+#define CUBE_E_ARG (-1)        /* bad argument / inconsistent geometry                     */
+#define CUBE_E_CUDA (-2)       /* CUDA runtime error                                       */
+#define CUBE_E_CAPACITY (-3)   /* particle capacity or per-cell segment limit exceeded     */
+#define CUBE_E_RANGE (-4)      /* particle moved beyond the ghost depth (drift.f90:64-73)  */
+#define CUBE_E_COUNT (-5)      /* particle count not conserved (drift.f90:139-143)         */
+#define CUBE_E_STATE (-6)      /* call out of order (e.g. step before upload)              */
+#define CUBE_E_TIMEOUT (-7)    /* a bounded device-side wait gave up                       */
+
+/* Device error-word bits (set by kernels, read back by the host after a step). */
+#define CUBE_DEVERR_DRIFT_RANGE 0x1u
+#define CUBE_DEVERR_DEPOSIT_RANGE 0x2u
+#define CUBE_DEVERR_INTERP_RANGE 0x4u
+#define CUBE_DEVERR_SEGMENT 0x8u
+#define CUBE_DEVERR_CAPACITY 0x10u
+#define CUBE_DEVERR_FIXED_OVERFLOW 0x20u
+
+/* Deposit arithmetic. */
+#define CUBE_DEPOSIT_FP32 0  /* plain form: FP32 atomics (order-dependent rounding)           */
+#define CUBE_DEPOSIT_FIXED 1 /* chosen form: int64 fixed-point atomics (deterministic)         */
+
+/*
+ * Run parameters.  Names and meanings follow parameters.f90; derived sizes
+ * (nc, nt, ntt, ngp, ngt, nfp, nfb, nft; parameters.f90:57-69) are computed by the
+ * library from these.  cube_params_default() fills the reference defaults.
+ */
+typedef struct cube_params {
+  int64_t ng;        /* fine cells per dimension of the image (parameters.f90:24)       */
+  int64_t ratio_cs;  /* fine cells per coarse cell, 4 (parameters.f90:25)               */
+  int64_t nnt;       /* tiles per image per dimension (parameters.f90:28)               */
+  int64_t nns;       /* subtiles per tile per dimension (parameters.f90:29)             */
+  int64_t np_nc;     /* particles per coarse cell per dimension at the IC (:32)         */
+  int64_t ncb;       /* coarse ghost depth, 4 (parameters.f90:81)                       */
+  int64_t ngb;       /* PM2 tile buffer in fine cells, 16 (parameters.f90:61)           */
+  int32_t izipx;     /* bytes per compressed coordinate: 1 (int8) or 2 (int16)          */
+  int32_t pm3_on;    /* PM3 switch (kick.f90:9)                                         */
+  int32_t pp_on;     /* PP switch (kick.f90:10)                                         */
+  int32_t deposit_mode; /* CUBE_DEPOSIT_FP32 or CUBE_DEPOSIT_FIXED                     */
+  float box;         /* box size in Mpc/h (parameters.f90:23)                           */
+  float app;         /* PP softening in fine cells, 0.06 (parameters.f90:46)            */
+  float apm1c;       /* PM1 softening in coarse cells, 3.5 (parameters.f90:38)          */
+  float apm2;        /* PM2 softening in fine cells, 3.5 (parameters.f90:40)            */
+  float apm3f;       /* PM3 softening in refined cells, 3.5 (parameters.f90:42)         */
+  float mass_p_cdm;  /* particle mass in fine-cell units (ic.f90:839)                   */
+  float f_nu;        /* neutrino mass fraction for the linear-response rescale (0: CDM) */
+  int64_t np_capacity; /* particle capacity on device (0: derive from ng, np_nc)        */
+  int32_t max_segment; /* largest destination cell the drift sorts (0: default 16384)   */
+  int32_t reserved;
+} cube_params;
+
+/* Per-step scalars chosen by the host timestep (timestep.f90:4-110). */
+typedef struct cube_step_in {
+  float dt;      /* kick step (timestep.f90:267)                  */
+  float dt_old;  /* previous dt; drift uses (dt_old+dt)/2 (drift.f90:21) */
+  float a_mid;   /* a at mid step (timestep.f90:297)              */
+  float vz_max;  /* sim%vz_max from the previous kick (drift.f90:26)  */
+} cube_step_in;
+
+/* Per-step results that the reference writes into sim and tcat. */
+typedef struct cube_step_out {
+  float dt_pm1, dt_pm2, dt_pm3, dt_pp, dt_vmax; /* kick.f90:39,69,239,298,314 */
+  float vmax[3];                                /* final |v| maxima              */
+  float vz_max;                                 /* kick.f90:315                   */
+  float f2max_pm1, f2max_pm2, f2max_pm3, f2max_pp;
+  int32_t napm[8];                              /* PM3 class histogram, index 2..5 (kick.f90:132) */
+  int64_t nplocal;
+  int64_t pp_pairs;                             /* in-range PP pairs evaluated (both orders)  */
+  float tcat[16];                               /* stage times in ms: 0 drift,1 PM1,2 PM2,3 PM3,4 PP,5 whole */
+} cube_step_out;
+
+typedef struct cube_ctx cube_ctx;
+
+/* Fill the reference defaults of parameters.f90 for a given ng. */
+void cube_params_default(cube_params* p, int64_t ng);
+
+/* Create a context on CUDA device `device`: derives sizes, builds the FP64 Green
+ * tables on the device (Green/Green.f90:1-80, initialize.f90:247-334) and allocates
+ * particle and mesh buffers.  Replaces initialize + create_cubefft_plan. */
+int cube_gpu_create(const cube_params* p, int device, cube_ctx** out);
+int cube_gpu_destroy(cube_ctx* ctx);
+
+/* Copy particles in (particle_initialization.f90:77-90 after the checkpoint read). */
+int cube_gpu_upload(cube_ctx* ctx, const void* xp, const float* vp, const int64_t* pid,
+                    const int32_t* rhoc, int64_t nplocal);
+/* Copy particles out (checkpoint.f90:24-33). `nplocal` receives the count. */
+int cube_gpu_download(cube_ctx* ctx, void* xp, float* vp, int64_t* pid, int32_t* rhoc,
+                      int64_t* nplocal);
+
+/* drift.f90:1-233 with dt_mid=(dt_old+dt)/2; bit-exact arrival order and ZIPX update. */
+int cube_gpu_drift(cube_ctx* ctx, const cube_step_in* in);
+/* kick.f90:1-353: PM1 + PM2 + PM3 + PP velocity updates and dt criteria. */
+int cube_gpu_kick(cube_ctx* ctx, const cube_step_in* in, cube_step_out* out);
+/* One loop body of main.f90:36-38 (drift, ghosts, kick, ghosts). */
+int cube_gpu_step(cube_ctx* ctx, const cube_step_in* in, cube_step_out* out);
+
+/* Inspection for tests: download the last PM level field.
+ * level 1: PM1 density (nc^3) / potential, 2: PM2 tile `box`, 3: PM3 subtile `box`.
+ * what 0: density (mass units), 1: potential phi after normalisation,
+ *      2: force (3 components interleaved) on cells 0..nforce+1.
+ * Fields are written x fastest in the reference index ranges. */
+int cube_gpu_debug_field(cube_ctx* ctx, int level, int box, int what, float* out, int64_t n);
+/* Download the Green table of a level (1, 2, or 3 with class iapm 2..5). */
+int cube_gpu_green_table(cube_ctx* ctx, int level, int iapm, float* out, int64_t n);
+/* Download per-subtile PM3 class (ires, kick.f90:108-133), ns3 entries. */
+int cube_gpu_subtile_class(cube_ctx* ctx, int32_t* ires, int64_t n);
+
+/* Text of the last error on this thread. */
+int cube_gpu_last_error(char* buf, size_t n);
+/* Library build string. */
+const char* cube_gpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUBE_GPU_H */

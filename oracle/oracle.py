@@ -1,0 +1,149 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes front end of the CPU oracle (oracle/liboracle.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import this
+module.  It is the checker, never the product: the product library
+(cube_nu_b200/libcube_gpu.so) does not load it.
+
+Parity status: unpinned (no reference golden data exists; see cube_oracle.cpp).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from cube_nu_b200.params import CParams, Params
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+class KickOut(ctypes.Structure):
+    _fields_ = [
+        ("f2max_pm1", ctypes.c_double), ("f2max_pm2", ctypes.c_double), ("f2max_pm3", ctypes.c_double),
+        ("f2max_pp", ctypes.c_double), ("vmax", ctypes.c_double * 3),
+        ("dt_pm1", ctypes.c_float), ("dt_pm2", ctypes.c_float), ("dt_pm3", ctypes.c_float),
+        ("dt_pp", ctypes.c_float), ("dt_vmax", ctypes.c_float), ("vz_max", ctypes.c_float),
+        ("napm", ctypes.c_int32 * 8), ("pp_pairs", ctypes.c_int64), ("err", ctypes.c_int64),
+    ]
+
+
+def build(force: bool = False) -> str:
+    path = os.path.join(_HERE, "liboracle.so")
+    if force or not os.path.exists(path):
+        subprocess.check_call(["make", "-s", "-C", _HERE])
+    return path
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = build()
+        L = ctypes.CDLL(path)
+        P = ctypes.POINTER(CParams)
+        vp = ctypes.c_void_p
+        L.oracle_set_threads.argtypes = [ctypes.c_int]
+        L.oracle_green.argtypes = [P, ctypes.c_int, ctypes.c_int, vp]
+        L.oracle_rfft3.argtypes = [ctypes.c_int, vp, vp]
+        L.oracle_irfft3.argtypes = [ctypes.c_int, vp, vp]
+        L.oracle_drift.restype = ctypes.c_int64
+        L.oracle_drift.argtypes = [P, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                   vp, vp, vp, vp]
+        L.oracle_drift64.restype = ctypes.c_int64
+        L.oracle_drift64.argtypes = L.oracle_drift.argtypes
+        L.oracle_kick.argtypes = [P, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_double, ctypes.POINTER(KickOut), ctypes.c_int, ctypes.c_int64,
+                                  ctypes.c_int, vp, ctypes.c_int64]
+        L.oracle_kick64.argtypes = [P, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                    ctypes.POINTER(KickOut), ctypes.c_int, ctypes.c_int64, ctypes.c_int, vp,
+                                    ctypes.c_int64]
+        L.oracle_classify.argtypes = [P, vp, vp, vp]
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def set_threads(n: int) -> int:
+    return lib().oracle_set_threads(n)
+
+
+def green(p: Params, level: int, iapm: int = 2) -> np.ndarray:
+    n = {1: p.nc, 2: p.ngt}.get(level) or p.nft(iapm)
+    out = np.zeros((n, n, n // 2 + 1), dtype=np.float32)
+    cp = p.to_c()
+    rc = lib().oracle_green(ctypes.byref(cp), level, iapm, _ptr(out))
+    if rc:
+        raise RuntimeError("oracle_green failed %d" % rc)
+    return out
+
+
+def rfft3(r: np.ndarray) -> np.ndarray:
+    n = r.shape[0]
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    c = np.zeros((n, n, n // 2 + 1), dtype=np.complex128)
+    lib().oracle_rfft3(n, _ptr(r), _ptr(c))
+    return c
+
+
+def irfft3(c: np.ndarray) -> np.ndarray:
+    n = c.shape[0]
+    c = np.ascontiguousarray(c, dtype=np.complex128).copy()
+    r = np.zeros((n, n, n), dtype=np.float64)
+    lib().oracle_irfft3(n, _ptr(c), _ptr(r))
+    return r
+
+
+def drift(p: Params, xp, vp, pid, rhoc, dt_old: float, dt: float, vz_max: float):
+    """drift.f90; returns (xp, vp, pid, rhoc) in the new order."""
+    n = xp.shape[0]
+    fp64 = vp.dtype == np.float64
+    xo = np.zeros_like(xp)
+    vo = np.zeros_like(vp)
+    po = np.zeros_like(pid)
+    ro = np.zeros_like(rhoc)
+    cp = p.to_c()
+    fn = lib().oracle_drift64 if fp64 else lib().oracle_drift
+    m = fn(ctypes.byref(cp), _ptr(np.ascontiguousarray(xp)), _ptr(np.ascontiguousarray(vp)),
+           _ptr(np.ascontiguousarray(pid)), _ptr(np.ascontiguousarray(rhoc)), dt_old, dt, vz_max,
+           _ptr(xo), _ptr(vo), _ptr(po), _ptr(ro))
+    if m < 0:
+        raise RuntimeError("oracle drift failed: %d" % m)
+    if m != n:
+        raise RuntimeError("particle count not conserved: %d -> %d" % (n, m))
+    return xo, vo, po, ro
+
+
+def kick(p: Params, xp, vp, rhoc, dt: float, a_mid: float, fixed: bool = False, only: int = 15,
+         boxes_frac: float = 0.0, debug=None):
+    """kick.f90 in FP32 (vp float32, updated in place) or FP64 (vp float64).
+
+    debug=(level, box, what, n) returns the requested field as the 2nd value."""
+    out = KickOut()
+    cp = p.to_c()
+    dbg = np.zeros(debug[3], dtype=np.float32) if debug else None
+    dl, db, dw, dn = (debug[0], debug[1], debug[2], debug[3]) if debug else (0, -1, -1, 0)
+    xp = np.ascontiguousarray(xp)
+    rhoc = np.ascontiguousarray(rhoc)
+    if vp.dtype == np.float64:
+        rc = lib().oracle_kick64(ctypes.byref(cp), _ptr(xp), _ptr(vp), _ptr(rhoc), dt, a_mid, only,
+                                 ctypes.byref(out), dl, db, dw, _ptr(dbg) if dbg is not None else None, dn)
+    else:
+        rc = lib().oracle_kick(ctypes.byref(cp), _ptr(xp), _ptr(vp), _ptr(rhoc), dt, a_mid, int(fixed), only,
+                               boxes_frac, ctypes.byref(out), dl, db, dw,
+                               _ptr(dbg) if dbg is not None else None, dn)
+    if rc:
+        raise RuntimeError("oracle kick failed: %d (err bits %d)" % (rc, out.err))
+    return (out, dbg) if debug else out
+
+
+def classify(p: Params, rhoc):
+    ires = np.zeros(p.ns3, dtype=np.int32)
+    napm = np.zeros(8, dtype=np.int32)
+    cp = p.to_c()
+    lib().oracle_classify(ctypes.byref(cp), _ptr(np.ascontiguousarray(rhoc)), _ptr(ires), _ptr(napm))
+    return ires, napm
