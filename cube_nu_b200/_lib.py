@@ -1,0 +1,176 @@
+"""ctypes binding of the C ABI in include/cube_gpu.h (libcube_gpu.so, built in-tree).
+
+There is no CPU fallback: if the library is missing, importing the GPU context
+raises.  Build it with ``python -m cube_nu_b200.build`` (or ``__graft_entry__.build()``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .params import CParams, Params
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcube_gpu.so")
+
+EXPORTS = (
+    "cube_params_default", "cube_gpu_create", "cube_gpu_destroy", "cube_gpu_upload", "cube_gpu_download",
+    "cube_gpu_drift", "cube_gpu_kick", "cube_gpu_step", "cube_gpu_capture", "cube_gpu_captured",
+    "cube_gpu_green_table", "cube_gpu_subtile_class", "cube_gpu_last_error", "cube_gpu_version",
+)
+
+
+class StepIn(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_float), ("dt_old", ctypes.c_float), ("a_mid", ctypes.c_float),
+                ("vz_max", ctypes.c_float)]
+
+
+class StepOut(ctypes.Structure):
+    _fields_ = [
+        ("dt_pm1", ctypes.c_float), ("dt_pm2", ctypes.c_float), ("dt_pm3", ctypes.c_float), ("dt_pp", ctypes.c_float),
+        ("dt_vmax", ctypes.c_float), ("vmax", ctypes.c_float * 3), ("vz_max", ctypes.c_float),
+        ("f2max_pm1", ctypes.c_float), ("f2max_pm2", ctypes.c_float), ("f2max_pm3", ctypes.c_float),
+        ("f2max_pp", ctypes.c_float), ("napm", ctypes.c_int32 * 8), ("nplocal", ctypes.c_int64),
+        ("pp_pairs", ctypes.c_int64), ("tcat", ctypes.c_float * 16),
+    ]
+
+
+_LIB = None
+
+
+def load():
+    """Load libcube_gpu.so; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libcube_gpu.so not built (%s); run python -m cube_nu_b200.build" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    P = ctypes.POINTER(CParams)
+    L.cube_params_default.argtypes = [P, ctypes.c_int64]
+    L.cube_params_default.restype = None
+    L.cube_gpu_create.argtypes = [P, ctypes.c_int, ctypes.POINTER(vp)]
+    L.cube_gpu_destroy.argtypes = [vp]
+    L.cube_gpu_upload.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int64]
+    L.cube_gpu_download.argtypes = [vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int64)]
+    L.cube_gpu_drift.argtypes = [vp, ctypes.POINTER(StepIn)]
+    L.cube_gpu_kick.argtypes = [vp, ctypes.POINTER(StepIn), ctypes.POINTER(StepOut)]
+    L.cube_gpu_step.argtypes = [vp, ctypes.POINTER(StepIn), ctypes.POINTER(StepOut)]
+    L.cube_gpu_capture.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.cube_gpu_captured.argtypes = [vp, vp, ctypes.c_int64]
+    L.cube_gpu_green_table.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int64]
+    L.cube_gpu_subtile_class.argtypes = [vp, vp, ctypes.c_int64]
+    L.cube_gpu_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+    L.cube_gpu_version.restype = ctypes.c_char_p
+    _LIB = L
+    return L
+
+
+class CubeError(RuntimeError):
+    pass
+
+
+def _check(rc: int, what: str) -> int:
+    if rc < 0:
+        buf = ctypes.create_string_buffer(512)
+        load().cube_gpu_last_error(buf, 512)
+        raise CubeError("%s failed (%d): %s" % (what, rc, buf.value.decode(errors="replace")))
+    return rc
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Context:
+    """One image's device state; mirrors the reference's step subroutines."""
+
+    def __init__(self, params: Params, device: int = 0):
+        self.params = params
+        self._cp = params.to_c()
+        self._lib = load()
+        h = ctypes.c_void_p()
+        _check(self._lib.cube_gpu_create(ctypes.byref(self._cp), device, ctypes.byref(h)), "cube_gpu_create")
+        self._h = h
+        self.np = 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.cube_gpu_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, xp, vp, pid, rhoc) -> None:
+        p = self.params
+        xp = np.ascontiguousarray(xp, dtype=p.xdtype)
+        vp = np.ascontiguousarray(vp, dtype=np.float32)
+        pid = np.ascontiguousarray(pid, dtype=np.int64)
+        rhoc = np.ascontiguousarray(rhoc, dtype=np.int32)
+        n = xp.shape[0]
+        _check(self._lib.cube_gpu_upload(self._h, _ptr(xp), _ptr(vp), _ptr(pid), _ptr(rhoc), n), "cube_gpu_upload")
+        self.np = n
+
+    def download(self):
+        p = self.params
+        xp = np.empty((self.np, 3), dtype=p.xdtype)
+        vp = np.empty((self.np, 3), dtype=np.float32)
+        pid = np.empty(self.np, dtype=np.int64)
+        rhoc = np.empty(p.ncells, dtype=np.int32)
+        n = ctypes.c_int64()
+        _check(self._lib.cube_gpu_download(self._h, _ptr(xp), _ptr(vp), _ptr(pid), _ptr(rhoc), ctypes.byref(n)),
+               "cube_gpu_download")
+        return xp, vp, pid, rhoc
+
+    def drift(self, dt: float, dt_old: float, vz_max: float) -> None:
+        si = StepIn(dt, dt_old, 0.0, vz_max)
+        _check(self._lib.cube_gpu_drift(self._h, ctypes.byref(si)), "cube_gpu_drift")
+
+    def kick(self, dt: float, a_mid: float) -> StepOut:
+        si = StepIn(dt, 0.0, a_mid, 0.0)
+        so = StepOut()
+        _check(self._lib.cube_gpu_kick(self._h, ctypes.byref(si), ctypes.byref(so)), "cube_gpu_kick")
+        return so
+
+    def step(self, dt: float, dt_old: float, a_mid: float, vz_max: float) -> StepOut:
+        si = StepIn(dt, dt_old, a_mid, vz_max)
+        so = StepOut()
+        _check(self._lib.cube_gpu_step(self._h, ctypes.byref(si), ctypes.byref(so)), "cube_gpu_step")
+        return so
+
+    def capture(self, level: int, box: int, what: int) -> None:
+        _check(self._lib.cube_gpu_capture(self._h, level, box, what), "cube_gpu_capture")
+
+    def captured(self, n: int) -> np.ndarray:
+        out = np.empty(n, dtype=np.float32)
+        m = _check(self._lib.cube_gpu_captured(self._h, _ptr(out), n), "cube_gpu_captured")
+        return out[:m]
+
+    def green(self, level: int, iapm: int = 2) -> np.ndarray:
+        p = self.params
+        n = {1: p.nc, 2: p.ngt}.get(level) or p.nft(iapm)
+        out = np.empty((n, n, n // 2 + 1), dtype=np.float32)
+        _check(self._lib.cube_gpu_green_table(self._h, level, iapm, _ptr(out), out.size), "cube_gpu_green_table")
+        return out
+
+    def subtile_class(self) -> np.ndarray:
+        out = np.empty(self.params.ns3, dtype=np.int32)
+        _check(self._lib.cube_gpu_subtile_class(self._h, _ptr(out), out.size), "cube_gpu_subtile_class")
+        return out
+
+
+def version() -> str:
+    return load().cube_gpu_version().decode()

@@ -1,0 +1,99 @@
+// Device-side geometry and helpers shared by the CUBE step kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/cube_gpu.h"
+
+namespace cube {
+
+// ratio_sf, parameters.f90:26 (1-based; class iapm uses RSF[iapm]).
+__host__ __device__ inline int rsf_of(int iapm) {
+  const int t[8] = {0, 1, 2, 4, 6, 8, 12, 16};
+  return t[iapm & 7];
+}
+
+// Geometry derived from cube_params (parameters.f90:57-82).  Plain struct passed to
+// kernels by value.
+struct Geo {
+  int ng, rcs, nnt, nns, ncb, ngb, nc, nt, ntt, ngp, ngt;
+  int izipx;
+  int nfp[8], nfb[8], nft[8];
+  float app, apm1c, apm2, apm3f, mass_p, f_nu;
+  double x_res;      // 2^(-8 izipx) coarse cells per code unit
+  double inv_step;   // 1/(x_res*ratio_cs): code units per fine cell
+  uint32_t zmask;    // 0xff or 0xffff
+  int64_t ncells;    // nc^3
+};
+
+__host__ __device__ inline int wrapi(int a, int n) {
+  a %= n;
+  return a < 0 ? a + n : a;
+}
+
+// Storage index of global coarse cell (gx,gy,gz) in the reference order
+// rhoc(nt,nt,nt,nnt,nnt,nnt): tile z,y,x outer, then cell z,y,x (x fastest).
+__host__ __device__ inline int64_t cell_index(const Geo& G, int gx, int gy, int gz) {
+  gx = wrapi(gx, G.nc);
+  gy = wrapi(gy, G.nc);
+  gz = wrapi(gz, G.nc);
+  const int tx = gx / G.nt, ty = gy / G.nt, tz = gz / G.nt;
+  const int lx = gx - tx * G.nt, ly = gy - ty * G.nt, lz = gz - tz * G.nt;
+  return ((((int64_t)(tz * G.nnt + ty) * G.nnt + tx) * G.nt + lz) * G.nt + ly) * G.nt + lx;
+}
+
+// Inverse of cell_index: global coarse cell coordinates (0-based).
+__host__ __device__ inline void cell_coords(const Geo& G, int64_t c, int& gx, int& gy, int& gz) {
+  const int64_t nt3 = (int64_t)G.nt * G.nt * G.nt;
+  const int64_t t = c / nt3, r = c - t * nt3;
+  const int lz = (int)(r / (G.nt * G.nt)), ly = (int)((r / G.nt) % G.nt), lx = (int)(r % G.nt);
+  const int tx = (int)(t % G.nnt), ty = (int)((t / G.nnt) % G.nnt), tz = (int)(t / (G.nnt * G.nnt));
+  gx = tx * G.nt + lx;
+  gy = ty * G.nt + ly;
+  gz = tz * G.nt + lz;
+}
+
+// ZIPX decode, kick.f90:627-628: (int(xp+ishift,izipx)+rshift)*x_resolution equals
+// ((unsigned)xp + 0.5) * 2^(-8 izipx), an exact double.
+__device__ __forceinline__ double zfrac(int code, const Geo& G) {
+  return ((double)((uint32_t)code & G.zmask) + 0.5) * G.x_res;
+}
+
+__device__ __forceinline__ int load_code(const void* xp, int izipx, int64_t i) {
+  return izipx == 1 ? (int)((const int8_t*)xp)[i] : (int)((const int16_t*)xp)[i];
+}
+
+__device__ __forceinline__ void store_code(void* xp, int izipx, int64_t i, int v) {
+  if (izipx == 1) ((int8_t*)xp)[i] = (int8_t)v;
+  else ((int16_t*)xp)[i] = (int16_t)v;
+}
+
+// TSC weights with the reference's FP32 arithmetic (particle_mesh.f90:56-62):
+// dx1=(1-l)^2/2, dx3=l^2/2, dx2=1-dx1-dx3 with l=xpos-floor(xpos).
+__device__ __forceinline__ int tsc_weights(double xpos, float w[3]) {
+  const double fl = floor(xpos);
+  const float l = (float)(xpos - fl);
+  const float a = __fsub_rn(1.f, l);
+  w[0] = __fmul_rn(__fmul_rn(a, a), 0.5f);
+  w[2] = __fmul_rn(__fmul_rn(l, l), 0.5f);
+  w[1] = __fsub_rn(__fsub_rn(1.f, w[0]), w[2]);
+  return (int)fl + 1;  // idx(:,2), 1-based
+}
+
+// vp + dv*a_mid*dt/6/pi with the last division by real(8) pi (kick.f90:797).
+__device__ __forceinline__ float kick_add(float v, float dv, float a_mid, float dt) {
+  const float t = __fdiv_rn(__fmul_rn(__fmul_rn(dv, a_mid), dt), 6.f);
+  return (float)__dadd_rn((double)v, __ddiv_rn((double)t, 3.141592653589793));
+}
+
+// Non-negative float max through integer atomics.
+__device__ __forceinline__ void atomic_max_pos(float* addr, float v) {
+  atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
+}
+
+__device__ __forceinline__ void set_err(unsigned* err, unsigned bit) { atomicOr(err, bit); }
+
+// Gradient weights (parameters.f90:53-54), real4.
+#define CUBE_W_ALPHA (4.f / 3.f)
+
+}  // namespace cube

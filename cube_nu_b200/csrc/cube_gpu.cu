@@ -1,0 +1,740 @@
+// C ABI and step orchestration for one CUBE image on one B200.
+//
+// Replaces the reference's zero-argument step subroutines (main.f90:33-38; drift.f90,
+// kick.f90, particle_mesh.f90) with explicit calls on a context that owns the
+// device-resident particle state between cube_gpu_upload and cube_gpu_download.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/cube_gpu.h"
+#include "common.cuh"
+#include "fft.cuh"
+#include "kernels.cuh"
+
+using namespace cube;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(CUBE_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));           \
+  } while (0)
+
+bool smooth23(int n) {
+  if (n <= 0) return false;
+  while (n % 2 == 0) n /= 2;
+  while (n % 3 == 0) n /= 3;
+  return n == 1;
+}
+
+struct FFTTable {
+  int n = 0;
+  float2* tw = nullptr;
+  FFTDesc desc;
+};
+
+}  // namespace
+
+struct cube_ctx {
+  cube_params P;
+  Geo G;
+  int device = 0;
+  cudaStream_t s = nullptr;
+  bool loaded = false;
+  int64_t np = 0, cap = 0;
+  int xbytes = 1;
+  int ns3 = 0, ntiles = 0;
+  // particles (current and drift output)
+  void *xp = nullptr, *xp2 = nullptr;
+  float *vp = nullptr, *vp2 = nullptr;
+  int64_t *pid = nullptr, *pid2 = nullptr;
+  int32_t *pcell = nullptr, *pcell2 = nullptr;
+  // cells
+  int32_t *rhoc = nullptr, *rhoc2 = nullptr, *fill = nullptr, *biglist = nullptr, *nbig = nullptr;
+  int64_t *cstart = nullptr, *cstart2 = nullptr, *scan_tmp = nullptr;
+  // drift scratch
+  int32_t* dest = nullptr;
+  uint64_t *key = nullptr, *skey = nullptr;
+  uint32_t* ssrc = nullptr;
+  // reductions: f2max[4] (pm1, pm2, pm3, pp), vmax[3][3] (pm2, pm3, pp)
+  float* red = nullptr;
+  unsigned long long* pairs = nullptr;
+  unsigned* err = nullptr;
+  int32_t *ires = nullptr, *napm = nullptr;
+  int32_t* box_slot = nullptr;  // [nchunk][ns3]
+  int32_t* h_slots = nullptr;   // pinned host copy
+  int64_t slot_chunks = 0;
+  // meshes
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  float* green1 = nullptr;
+  float* green2 = nullptr;
+  float* green3[8] = {nullptr};
+  std::vector<FFTTable> ffts;
+  // capture for tests
+  int cap_level = 0, cap_box = -1, cap_what = -1;
+  float* cap_buf = nullptr;
+  int64_t cap_n = 0;
+  // timing
+  cudaEvent_t ev[8];
+};
+
+namespace {
+
+const FFTDesc* fft_desc(cube_ctx* c, int n) {
+  for (auto& t : c->ffts)
+    if (t.n == n) return &t.desc;
+  return nullptr;
+}
+
+int add_fft(cube_ctx* c, int n) {
+  if (fft_desc(c, n)) return 0;
+  if (!smooth23(n)) return fail(CUBE_E_ARG, "FFT size " + std::to_string(n) + " is not of the form 2^a 3^b");
+  FFTTable t;
+  t.n = n;
+  std::vector<float2> h(n);
+  for (int k = 0; k < n; ++k) {
+    const double a = -2.0 * M_PI * (double)k / (double)n;
+    h[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  CK(cudaMalloc(&t.tw, n * sizeof(float2)));
+  CK(cudaMemcpy(t.tw, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+  t.desc.n = n;
+  t.desc.tw = t.tw;
+  int m = n, k = 0;
+  while (m % 4 == 0 && k < 15) { t.desc.rad[k++] = 4; m /= 4; }
+  while (m % 2 == 0 && k < 15) { t.desc.rad[k++] = 2; m /= 2; }
+  while (m % 3 == 0 && k < 15) { t.desc.rad[k++] = 3; m /= 3; }
+  if (m != 1) return fail(CUBE_E_ARG, "FFT size too large");
+  t.desc.nrad = k;
+  c->ffts.push_back(t);
+  return 0;
+}
+
+Geo make_geo(const cube_params& p) {
+  Geo g;
+  memset(&g, 0, sizeof(g));
+  g.ng = (int)p.ng;
+  g.rcs = (int)p.ratio_cs;
+  g.nnt = (int)p.nnt;
+  g.nns = (int)p.nns;
+  g.ncb = (int)p.ncb;
+  g.ngb = (int)p.ngb;
+  g.nc = g.ng / g.rcs;
+  g.nt = g.nc / g.nnt;
+  g.ntt = g.nt / g.nns;
+  g.ngp = g.ng / g.nnt;
+  g.ngt = g.ngp + 2 * g.ngb;
+  g.izipx = p.izipx;
+  for (int i = 1; i <= 7; ++i) {
+    g.nfp[i] = (g.ngp / g.nns) * rsf_of(i);
+    g.nfb[i] = g.rcs * rsf_of(i);
+    g.nft[i] = g.nfp[i] + 2 * g.nfb[i];
+  }
+  g.app = p.app;
+  g.apm1c = p.apm1c;
+  g.apm2 = p.apm2;
+  g.apm3f = p.apm3f;
+  g.mass_p = p.mass_p_cdm;
+  g.f_nu = p.f_nu;
+  g.x_res = std::ldexp(1.0, -8 * g.izipx);
+  g.inv_step = 1.0 / (g.x_res * (double)g.rcs);
+  g.zmask = (g.izipx == 1) ? 0xffu : 0xffffu;
+  g.ncells = (int64_t)g.nc * g.nc * g.nc;
+  return g;
+}
+
+// Mesh bytes for nbox boxes of side n: real (4 or 8 B), half spectrum (8 B).
+size_t mesh_bytes(int n, int64_t nbox, bool fixed) {
+  const size_t n3 = (size_t)n * n * n, nh = (size_t)n * n * (n / 2 + 1);
+  return (size_t)nbox * (n3 * (fixed ? 8 : 4) + nh * 8 + 256);
+}
+
+struct MeshPtrs {
+  void* real;
+  float2* ck;
+};
+MeshPtrs mesh_ptrs(cube_ctx* c, int n, int64_t nbox, bool fixed) {
+  const size_t n3 = (size_t)n * n * n;
+  MeshPtrs m;
+  m.real = c->arena;
+  size_t off = ((size_t)nbox * n3 * (fixed ? 8 : 4) + 255) & ~(size_t)255;
+  m.ck = reinterpret_cast<float2*>((char*)c->arena + off);
+  return m;
+}
+
+// How many boxes of side n fit in the arena.
+int64_t boxes_fit(cube_ctx* c, int n, bool fixed) {
+  const size_t per = mesh_bytes(n, 1, fixed);
+  return std::max<int64_t>(1, (int64_t)(c->arena_bytes / per));
+}
+
+void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out,
+                float2* ck, const float* green, float norm, int reps) {
+  const FFTDesc& D = *fft_desc(c, n);
+  const int nh = n / 2 + 1;
+  const int64_t nrows = nbox * (int64_t)n * n;
+  const int rpb = std::max(1, 2048 / n);
+  const size_t smx = (size_t)(n + 2 * rpb * n) * sizeof(float2);
+  const unsigned gx = (unsigned)((nrows + rpb - 1) / rpb);
+  if (fixed)
+    k_fft_x_r2c<long long><<<gx, 256, smx, c->s>>>((const long long*)real_in, ck, nrows, D, rpb, scale);
+  else
+    k_fft_x_r2c<float><<<gx, 256, smx, c->s>>>((const float*)real_in, ck, nrows, D, rpb, scale);
+  const int W = (n <= 256) ? 16 : (n <= 512 ? 8 : 4);
+  const size_t smy = (size_t)(n + 2 * W * n) * sizeof(float2);
+  dim3 gy((unsigned)(nbox * n), (unsigned)((nh + W - 1) / W));
+  k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1);
+  k_fft_z_green<<<gy, 256, smy, c->s>>>(ck, green, D, W);
+  k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1);
+  k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, norm, reps);
+}
+
+inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+
+int build_green(cube_ctx* c, float** dst, int n, float soft, float range, float gs) {
+  if (*dst) return 0;
+  const int64_t m = (int64_t)n * n * (n / 2 + 1);
+  CK(cudaMalloc(dst, m * sizeof(float)));
+  k_green<<<nblk(m, 128), 128, 0, c->s>>>(*dst, n, soft, range, gs);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+float* green3(cube_ctx* c, int iapm) {
+  const Geo& G = c->G;
+  if (build_green(c, &c->green3[iapm], G.nft[iapm], G.apm3f, G.apm2 * (float)rsf_of(iapm), 1.f / (float)rsf_of(iapm)))
+    return nullptr;
+  return c->green3[iapm];
+}
+
+// Copy a box field into the capture buffer when it is the one requested.
+void maybe_capture(cube_ctx* c, int level, int64_t box, int what, const void* src, int64_t n, bool fixed_int) {
+  if (c->cap_level != level || c->cap_box != box || c->cap_what != what) return;
+  cudaFree(c->cap_buf);
+  c->cap_buf = nullptr;
+  c->cap_n = n;
+  if (cudaMalloc(&c->cap_buf, n * (fixed_int ? 8 : 4)) != cudaSuccess) return;
+  cudaMemcpyAsync(c->cap_buf, src, n * (fixed_int ? 8 : 4), cudaMemcpyDeviceToDevice, c->s);
+  if (fixed_int) c->cap_n = -n;  // marks int64 content
+}
+
+}  // namespace
+
+// =================================================================================
+extern "C" {
+
+void cube_params_default(cube_params* p, int64_t ng) {
+  memset(p, 0, sizeof(*p));
+  p->ng = ng;
+  p->ratio_cs = 4;
+  p->nnt = 4;
+  p->nns = 4;
+  p->np_nc = 4;
+  p->ncb = 4;
+  p->ngb = 16;
+  p->izipx = 2;
+  p->pm3_on = 1;
+  p->pp_on = 1;
+  p->deposit_mode = CUBE_DEPOSIT_FP32;
+  p->box = 600.f;
+  p->app = 0.06f;
+  p->apm1c = 3.5f;
+  p->apm2 = 3.5f;
+  p->apm3f = 3.5f;
+  p->mass_p_cdm = 0.f;
+}
+
+const char* cube_gpu_version(void) { return "cube-b200 0.1 (sm_100a)"; }
+
+int cube_gpu_last_error(char* buf, size_t n) {
+  if (!buf || n == 0) return CUBE_E_ARG;
+  snprintf(buf, n, "%s", g_last_error.c_str());
+  return 0;
+}
+
+int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
+  if (!p || !out) return fail(CUBE_E_ARG, "null argument");
+  *out = nullptr;
+  if (p->ratio_cs <= 0 || p->ng % p->ratio_cs || (p->ng / p->ratio_cs) % p->nnt ||
+      ((p->ng / p->ratio_cs) / p->nnt) % p->nns)
+    return fail(CUBE_E_ARG, "ng, nnt, nns must divide evenly (parameters.f90:57-59)");
+  if (p->izipx != 1 && p->izipx != 2) return fail(CUBE_E_ARG, "izipx must be 1 or 2");
+  if (p->mass_p_cdm <= 0.f) return fail(CUBE_E_ARG, "mass_p_cdm must be positive");
+  cube_ctx* c = new cube_ctx();
+  c->P = *p;
+  c->G = make_geo(*p);
+  const Geo& G = c->G;
+  if (G.nt < 2 * G.ncb) {
+    delete c;
+    return fail(CUBE_E_ARG, "tiles must be at least 2*ncb coarse cells wide");
+  }
+  if (G.nt + 2 * G.ncb > 256 || G.ntt < 2) {
+    delete c;
+    return fail(CUBE_E_ARG, "unsupported tile geometry (nt+2ncb<=256, ntt>=2)");
+  }
+  c->device = device;
+  c->ns3 = (int)((int64_t)G.nnt * G.nnt * G.nnt * G.nns * G.nns * G.nns);
+  c->ntiles = G.nnt * G.nnt * G.nnt;
+  c->xbytes = G.izipx;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking));
+  for (int i = 0; i < 8; ++i) CK(cudaEventCreate(&c->ev[i]));
+  int rc = add_fft(c, G.nc);
+  if (!rc) rc = add_fft(c, G.ngt);
+  for (int i = 2; i <= 5 && !rc; ++i) rc = add_fft(c, G.nft[i]);
+  if (rc) {
+    cube_gpu_destroy(c);
+    return rc;
+  }
+  const size_t big = 200 * 1024;
+  CK(cudaFuncSetAttribute(k_fft_x_r2c<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  CK(cudaFuncSetAttribute(k_fft_x_r2c<long long>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  CK(cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  CK(cudaFuncSetAttribute(k_fft_z_green, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  CK(cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  CK(cudaFuncSetAttribute(k_drift_sort_big, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+  // cells
+  const int64_t nc3 = G.ncells;
+  CK(cudaMalloc(&c->rhoc, nc3 * 4));
+  CK(cudaMalloc(&c->rhoc2, nc3 * 4));
+  CK(cudaMalloc(&c->fill, nc3 * 4));
+  CK(cudaMalloc(&c->biglist, nc3 * 4));
+  CK(cudaMalloc(&c->nbig, 4));
+  CK(cudaMalloc(&c->cstart, (nc3 + 1) * 8));
+  CK(cudaMalloc(&c->cstart2, (nc3 + 1) * 8));
+  CK(cudaMalloc(&c->scan_tmp, ((nc3 + 2047) / 2048 + 2) * 8));
+  CK(cudaMalloc(&c->red, 64 * sizeof(float)));
+  CK(cudaMalloc(&c->pairs, 8));
+  CK(cudaMalloc(&c->err, 4));
+  CK(cudaMemset(c->err, 0, 4));
+  CK(cudaMalloc(&c->ires, c->ns3 * 4));
+  CK(cudaMalloc(&c->napm, 8 * 4));
+  // Green tables of PM1 and PM2 (initialize.f90:247-258); PM3 classes on first use.
+  rc = build_green(c, &c->green1, G.nc, G.apm1c, 0.f, (float)G.rcs);
+  if (!rc) rc = build_green(c, &c->green2, G.ngt, G.apm2, G.apm1c * (float)G.rcs, 1.f);
+  if (rc) {
+    cube_gpu_destroy(c);
+    return rc;
+  }
+  CK(cudaStreamSynchronize(c->s));
+  *out = c;
+  return 0;
+}
+
+int cube_gpu_destroy(cube_ctx* c) {
+  if (!c) return 0;
+  cudaSetDevice(c->device);
+  if (c->s) cudaStreamSynchronize(c->s);
+  void* bufs[] = {c->xp, c->xp2, c->vp, c->vp2, c->pid, c->pid2, c->pcell, c->pcell2, c->rhoc, c->rhoc2,
+                  c->fill, c->biglist, c->nbig, c->cstart, c->cstart2, c->scan_tmp, c->dest, c->key, c->skey,
+                  c->ssrc, c->red, c->pairs, c->err, c->ires, c->napm, c->box_slot, c->arena, c->green1,
+                  c->green2, c->cap_buf};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  for (int i = 0; i < 8; ++i)
+    if (c->green3[i]) cudaFree(c->green3[i]);
+  for (auto& t : c->ffts) cudaFree(t.tw);
+  if (c->h_slots) cudaFreeHost(c->h_slots);
+  for (int i = 0; i < 8; ++i)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->s) cudaStreamDestroy(c->s);
+  delete c;
+  return 0;
+}
+
+static int alloc_particles(cube_ctx* c, int64_t np) {
+  if (np <= c->cap) return 0;
+  const int64_t cap = std::max<int64_t>(np, c->P.np_capacity);
+  void** ps[] = {&c->xp, &c->xp2, (void**)&c->vp, (void**)&c->vp2, (void**)&c->pid, (void**)&c->pid2,
+                 (void**)&c->pcell, (void**)&c->pcell2, (void**)&c->dest, (void**)&c->key, (void**)&c->skey,
+                 (void**)&c->ssrc};
+  const size_t sz[] = {(size_t)cap * 3 * c->xbytes, (size_t)cap * 3 * c->xbytes, (size_t)cap * 12, (size_t)cap * 12,
+                       (size_t)cap * 8, (size_t)cap * 8, (size_t)cap * 4, (size_t)cap * 4, (size_t)cap * 4,
+                       (size_t)cap * 8, (size_t)cap * 8, (size_t)cap * 4};
+  for (int i = 0; i < 12; ++i) {
+    if (*ps[i]) cudaFree(*ps[i]);
+    *ps[i] = nullptr;
+    CK(cudaMalloc(ps[i], sz[i] + 16));
+  }
+  c->cap = cap;
+  // mesh arena: everything that fits of what the largest level needs, within 70% of free memory
+  const Geo& G = c->G;
+  const bool fixed = c->P.deposit_mode == CUBE_DEPOSIT_FIXED;
+  size_t need = std::max(mesh_bytes(G.nc, 1, fixed), mesh_bytes(G.ngt, c->ntiles, fixed));
+  for (int i = 2; i <= 5; ++i) need = std::max(need, mesh_bytes(G.nft[i], c->ns3, fixed) / 4);
+  size_t fre = 0, tot = 0;
+  CK(cudaMemGetInfo(&fre, &tot));
+  size_t budget = (size_t)(0.7 * (double)fre);
+  size_t want = std::min(need, budget);
+  want = std::max(want, std::max(mesh_bytes(G.nc, 1, fixed), mesh_bytes(G.nft[5], 1, fixed)));
+  if (c->arena) cudaFree(c->arena);
+  c->arena = nullptr;
+  CK(cudaMalloc(&c->arena, want));
+  c->arena_bytes = want;
+  return 0;
+}
+
+int cube_gpu_upload(cube_ctx* c, const void* xp, const float* vp, const int64_t* pid, const int32_t* rhoc,
+                    int64_t nplocal) {
+  if (!c || !xp || !vp || !pid || !rhoc || nplocal <= 0) return fail(CUBE_E_ARG, "bad upload arguments");
+  CK(cudaSetDevice(c->device));
+  const Geo& G = c->G;
+  int64_t sum = 0;
+  for (int64_t i = 0; i < G.ncells; ++i) {
+    if (rhoc[i] < 0) return fail(CUBE_E_ARG, "negative rhoc");
+    sum += rhoc[i];
+  }
+  if (sum != nplocal) return fail(CUBE_E_COUNT, "sum(rhoc) != nplocal");
+  int rc = alloc_particles(c, nplocal);
+  if (rc) return rc;
+  c->np = nplocal;
+  CK(cudaMemcpyAsync(c->xp, xp, (size_t)nplocal * 3 * c->xbytes, cudaMemcpyHostToDevice, c->s));
+  CK(cudaMemcpyAsync(c->vp, vp, (size_t)nplocal * 12, cudaMemcpyHostToDevice, c->s));
+  CK(cudaMemcpyAsync(c->pid, pid, (size_t)nplocal * 8, cudaMemcpyHostToDevice, c->s));
+  CK(cudaMemcpyAsync(c->rhoc, rhoc, (size_t)G.ncells * 4, cudaMemcpyHostToDevice, c->s));
+  exclusive_scan(c->rhoc, c->cstart, G.ncells, c->scan_tmp, c->s);
+  k_fill_pcell<<<nblk(G.ncells), 256, 0, c->s>>>(c->cstart, G.ncells, c->pcell);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->s));
+  c->loaded = true;
+  return 0;
+}
+
+int cube_gpu_download(cube_ctx* c, void* xp, float* vp, int64_t* pid, int32_t* rhoc, int64_t* nplocal) {
+  if (!c || !c->loaded) return fail(CUBE_E_STATE, "no particles on device");
+  CK(cudaSetDevice(c->device));
+  if (xp) CK(cudaMemcpyAsync(xp, c->xp, (size_t)c->np * 3 * c->xbytes, cudaMemcpyDeviceToHost, c->s));
+  if (vp) CK(cudaMemcpyAsync(vp, c->vp, (size_t)c->np * 12, cudaMemcpyDeviceToHost, c->s));
+  if (pid) CK(cudaMemcpyAsync(pid, c->pid, (size_t)c->np * 8, cudaMemcpyDeviceToHost, c->s));
+  if (rhoc) CK(cudaMemcpyAsync(rhoc, c->rhoc, (size_t)c->G.ncells * 4, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  if (nplocal) *nplocal = c->np;
+  return 0;
+}
+
+static int check_err(cube_ctx* c) {
+  unsigned e = 0;
+  CK(cudaMemcpyAsync(&e, c->err, 4, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  if (e) {
+    CK(cudaMemsetAsync(c->err, 0, 4, c->s));
+    CK(cudaStreamSynchronize(c->s));
+    if (e & CUBE_DEVERR_DRIFT_RANGE) return fail(CUBE_E_RANGE, "drift: particle moved beyond the ghost depth");
+    if (e & CUBE_DEVERR_SEGMENT) return fail(CUBE_E_CAPACITY, "drift: destination cell exceeds max_segment");
+    if (e & CUBE_DEVERR_DEPOSIT_RANGE) return fail(CUBE_E_RANGE, "mass assignment out of range");
+    if (e & CUBE_DEVERR_INTERP_RANGE) return fail(CUBE_E_RANGE, "update velocity out of range");
+    return fail(CUBE_E_RANGE, "device error word " + std::to_string(e));
+  }
+  return 0;
+}
+
+// drift.f90.  Enqueues the drift; returns after the error word is checked.
+static int drift_enqueue(cube_ctx* c, const cube_step_in* in) {
+  const Geo& G = c->G;
+  const float dt_mid = (in->dt_old + in->dt) / 2.f;
+  const int nlayer = 2 * (int)std::ceil(dt_mid * in->vz_max / (float)G.rcs) + 2;
+  if (nlayer <= 0 || nlayer > 65535) return fail(CUBE_E_ARG, "bad nlayer from dt_mid*vz_max");
+  const int64_t np = c->np;
+  CK(cudaMemsetAsync(c->rhoc2, 0, G.ncells * 4, c->s));
+  CK(cudaMemsetAsync(c->fill, 0, G.ncells * 4, c->s));
+  CK(cudaMemsetAsync(c->nbig, 0, 4, c->s));
+  k_drift_dest<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->vp, c->pcell, c->cstart, dt_mid, nlayer, c->dest, c->key,
+                                           c->rhoc2, c->err);
+  exclusive_scan(c->rhoc2, c->cstart2, G.ncells, c->scan_tmp, c->s);
+  k_drift_scatter<<<nblk(np), 256, 0, c->s>>>(np, c->dest, c->key, c->cstart2, c->fill, c->skey, c->ssrc);
+  k_drift_sort_small<<<nblk(G.ncells * 32), 256, 0, c->s>>>(G.ncells, c->rhoc2, c->cstart2, c->skey, c->ssrc,
+                                                            c->biglist, c->nbig);
+  const int max_seg = c->P.max_segment > 0 ? std::min(c->P.max_segment, 16384) : 16384;
+  // One block per listed long segment; the grid is bounded by the cell count.
+  int nb_host = 0;
+  CK(cudaMemcpyAsync(&nb_host, c->nbig, 4, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  if (nb_host > 0)
+    k_drift_sort_big<<<nb_host, 512, (size_t)max_seg * 12, c->s>>>(c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey,
+                                                                    c->ssrc, max_seg, c->err);
+  k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp, c->pid, dt_mid, c->xp2, c->vp2,
+                                             c->pid2, c->pcell2);
+  CK(cudaGetLastError());
+  int rc = check_err(c);
+  if (rc) return rc;
+  int64_t total = 0;
+  CK(cudaMemcpyAsync(&total, c->cstart2 + G.ncells, 8, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  if (total != np) return fail(CUBE_E_COUNT, "drift: particle count not conserved");
+  std::swap(c->xp, c->xp2);
+  std::swap(c->vp, c->vp2);
+  std::swap(c->pid, c->pid2);
+  std::swap(c->pcell, c->pcell2);
+  std::swap(c->rhoc, c->rhoc2);
+  std::swap(c->cstart, c->cstart2);
+  return 0;
+}
+
+int cube_gpu_drift(cube_ctx* c, const cube_step_in* in) {
+  if (!c || !in) return fail(CUBE_E_ARG, "null argument");
+  if (!c->loaded) return fail(CUBE_E_STATE, "drift before upload");
+  CK(cudaSetDevice(c->device));
+  return drift_enqueue(c, in);
+}
+
+static float dt_crit(float coef, float f2max, float a_mid) {
+  const float G_grid = (float)((double)(1.0f / 6.0f) / M_PI);  // variables.f90:28
+  return coef * std::sqrt(1.f / (std::sqrt(f2max) * a_mid * G_grid));
+}
+
+int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
+  if (!c || !in) return fail(CUBE_E_ARG, "null argument");
+  if (!c->loaded) return fail(CUBE_E_STATE, "kick before upload");
+  CK(cudaSetDevice(c->device));
+  const Geo& G = c->G;
+  const int64_t np = c->np;
+  const bool fixed = c->P.deposit_mode == CUBE_DEPOSIT_FIXED;
+  const float a_mid = in->a_mid, dt = in->dt;
+  float* f2 = c->red;        // [0..3]
+  float* vm = c->red + 8;    // [pm2 0..2][pm3 3..5][pp 6..8]
+  CK(cudaMemsetAsync(c->red, 0, 64 * sizeof(float), c->s));
+  CK(cudaMemsetAsync(c->pairs, 0, 8, c->s));
+  CK(cudaEventRecord(c->ev[0], c->s));
+  // ---------------- PM1 (particle_mesh.f90) ----------------
+  {
+    const int n = G.nc;
+    MeshPtrs m = mesh_ptrs(c, n, 1, fixed);
+    const int64_t n3 = (int64_t)n * n * n;
+    CK(cudaMemsetAsync(m.real, 0, n3 * (fixed ? 8 : 4), c->s));
+    if (fixed) k_deposit_pm1<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real);
+    else k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real);
+    maybe_capture(c, 1, 0, 0, m.real, n3, fixed);
+    float* phi = reinterpret_cast<float*>(m.real);
+    launch_fft(c, n, 1, m.real, fixed, G.mass_p, phi, m.ck, c->green1, (float)n, 3);
+    maybe_capture(c, 1, 0, 1, phi, n3, false);
+    k_f2max_periodic<<<nblk(n3), 256, 0, c->s>>>(phi, n, f2 + 0);
+    k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, a_mid, dt);
+  }
+  CK(cudaEventRecord(c->ev[1], c->s));
+  // ---------------- PM2 (kick.f90:47-77) ----------------
+  {
+    const int n = G.ngt;
+    const int64_t n3 = (int64_t)n * n * n;
+    const int64_t per = std::min<int64_t>(c->ntiles, boxes_fit(c, n, fixed));
+    for (int t0 = 0; t0 < c->ntiles; t0 += (int)per) {
+      const int nb = (int)std::min<int64_t>(per, c->ntiles - t0);
+      MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
+      CK(cudaMemsetAsync(m.real, 0, nb * n3 * (fixed ? 8 : 4), c->s));
+      if (fixed) k_deposit_pm2<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb);
+      else k_deposit_pm2<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb);
+      if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
+        maybe_capture(c, 2, c->cap_box, 0, (char*)m.real + (c->cap_box - t0) * n3 * (fixed ? 8 : 4), n3, fixed);
+      float* phi = reinterpret_cast<float*>(m.real);
+      launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, c->green2, (float)n * (float)n * (float)n, 1);
+      if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
+        maybe_capture(c, 2, c->cap_box, 1, phi + (c->cap_box - t0) * n3, n3, false);
+      k_f2max_box<<<nblk((int64_t)G.ngp * G.ngp * G.ngp * nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1);
+      k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, a_mid, dt, vm + 0, c->err);
+    }
+  }
+  CK(cudaEventRecord(c->ev[2], c->s));
+  // ---------------- subtile classes (kick.f90:108-138) ----------------
+  CK(cudaMemsetAsync(c->napm, 0, 32, c->s));
+  k_classify<<<nblk(c->ns3), 256, 0, c->s>>>(G, c->rhoc, c->ns3, c->ires, c->napm);
+  std::vector<int32_t> ires(c->ns3);
+  int32_t napm[8];
+  CK(cudaMemcpyAsync(ires.data(), c->ires, c->ns3 * 4, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(napm, c->napm, 32, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  // ---------------- PM3 (kick.f90:203-276) ----------------
+  if (c->P.pm3_on) {
+    // chunks per class
+    struct Chunk { int iapm; int64_t first; int nb; };
+    std::vector<Chunk> chunks;
+    std::vector<std::vector<int>> lists(8);
+    for (int s = 0; s < c->ns3; ++s) lists[ires[s]].push_back(s);
+    for (int cl = 2; cl <= 5; ++cl) {
+      if (lists[cl].empty()) continue;
+      const int64_t per = std::min<int64_t>((int64_t)lists[cl].size(), boxes_fit(c, G.nft[cl], fixed));
+      for (int64_t f = 0; f < (int64_t)lists[cl].size(); f += per)
+        chunks.push_back({cl, f, (int)std::min<int64_t>(per, (int64_t)lists[cl].size() - f)});
+    }
+    const int64_t nch = (int64_t)chunks.size();
+    if (nch > c->slot_chunks) {
+      if (c->box_slot) cudaFree(c->box_slot);
+      if (c->h_slots) cudaFreeHost(c->h_slots);
+      c->box_slot = nullptr;
+      c->h_slots = nullptr;
+      CK(cudaMalloc(&c->box_slot, nch * c->ns3 * 4));
+      CK(cudaMallocHost(&c->h_slots, nch * c->ns3 * 4));
+      c->slot_chunks = nch;
+    }
+    for (int64_t k = 0; k < nch; ++k) {
+      int32_t* hs = c->h_slots + k * c->ns3;
+      std::fill(hs, hs + c->ns3, -1);
+      for (int j = 0; j < chunks[k].nb; ++j) hs[lists[chunks[k].iapm][chunks[k].first + j]] = j;
+    }
+    if (nch) CK(cudaMemcpyAsync(c->box_slot, c->h_slots, nch * c->ns3 * 4, cudaMemcpyHostToDevice, c->s));
+    for (int64_t k = 0; k < nch; ++k) {
+      const int cl = chunks[k].iapm, nb = chunks[k].nb;
+      const int n = G.nft[cl];
+      const int64_t n3 = (int64_t)n * n * n;
+      const float* g3 = green3(c, cl);
+      if (!g3) return CUBE_E_CUDA;
+      const int32_t* slots = c->box_slot + k * c->ns3;
+      MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
+      CK(cudaMemsetAsync(m.real, 0, nb * n3 * (fixed ? 8 : 4), c->s));
+      if (fixed) k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err);
+      else k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err);
+      int cap_slot = -1;
+      if (c->cap_level == 3 && c->cap_box >= 0 && c->cap_box < c->ns3 && ires[c->cap_box] == cl)
+        cap_slot = c->h_slots[k * c->ns3 + c->cap_box];
+      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 0, (char*)m.real + cap_slot * n3 * (fixed ? 8 : 4), n3, fixed);
+      float* phi = reinterpret_cast<float*>(m.real);
+      launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, g3, (float)n * (float)n * (float)n, 1);
+      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 1, phi + cap_slot * n3, n3, false);
+      const int nf = G.nfp[cl];
+      k_f2max_box<<<nblk((int64_t)nf * nf * nf * nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2);
+      k_interp_pm3<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp, a_mid, dt, vm + 3,
+                                                c->err);
+    }
+  }
+  CK(cudaEventRecord(c->ev[3], c->s));
+  // ---------------- PP (kick.f90:280-311) ----------------
+  if (c->P.pp_on) {
+    const float mass_scale = (G.f_nu > 0.f)
+                                 ? (float)((double)G.mass_p * ((1.0 - (double)G.f_nu) * (1.0 - (double)G.f_nu)))
+                                 : G.mass_p;
+    const float v_scale = (float)((double)(a_mid * dt / 6.f) / M_PI);
+    k_pp<<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->xp, c->pcell, c->cstart, c->ires, c->vp, mass_scale, v_scale,
+                                          f2 + 3, vm + 6, c->pairs);
+  }
+  CK(cudaEventRecord(c->ev[4], c->s));
+  CK(cudaGetLastError());
+  float red[64];
+  unsigned long long pairs = 0;
+  CK(cudaMemcpyAsync(red, c->red, sizeof(red), cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(&pairs, c->pairs, 8, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  int rc = check_err(c);
+  if (rc) return rc;
+  if (out) {
+    memset(out, 0, sizeof(*out));
+    out->f2max_pm1 = red[0];
+    out->f2max_pm2 = red[1];
+    out->f2max_pm3 = red[2];
+    out->f2max_pp = red[3];
+    out->dt_pm1 = dt_crit(0.5f, red[0], a_mid);  // kick.f90:39
+    out->dt_pm2 = dt_crit(0.5f, red[1], a_mid);  // kick.f90:69
+    out->dt_pm3 = dt_crit(0.5f, red[2], a_mid);  // kick.f90:239
+    out->dt_pp = dt_crit(0.05f, red[3], a_mid);  // kick.f90:298
+    const float* v = c->P.pp_on ? (red + 14) : (c->P.pm3_on ? red + 11 : red + 8);
+    for (int d = 0; d < 3; ++d) out->vmax[d] = v[d];
+    const float vmx = std::max(v[0], std::max(v[1], v[2]));
+    out->dt_vmax = 0.9f * 14 / vmx;  // kick.f90:314
+    out->vz_max = v[2];
+    for (int i = 0; i < 8; ++i) out->napm[i] = napm[i];
+    out->nplocal = np;
+    out->pp_pairs = (int64_t)pairs;
+    float ms;
+    for (int i = 0; i < 4; ++i) {
+      cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]);
+      out->tcat[1 + i] = ms;
+    }
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[4]);
+    out->tcat[5] = ms;
+  }
+  return 0;
+}
+
+int cube_gpu_step(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
+  if (!c || !in) return fail(CUBE_E_ARG, "null argument");
+  if (!c->loaded) return fail(CUBE_E_STATE, "step before upload");
+  CK(cudaSetDevice(c->device));
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, c->s));
+  int rc = drift_enqueue(c, in);
+  CK(cudaEventRecord(b, c->s));
+  if (!rc) rc = cube_gpu_kick(c, in, out);
+  if (!rc && out) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    out->tcat[0] = ms;
+    out->tcat[5] += ms;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
+}
+
+int cube_gpu_capture(cube_ctx* c, int level, int box, int what) {
+  if (!c) return fail(CUBE_E_ARG, "null context");
+  c->cap_level = level;
+  c->cap_box = box;
+  c->cap_what = what;
+  return 0;
+}
+
+int cube_gpu_captured(cube_ctx* c, float* out, int64_t n) {
+  if (!c || !out) return fail(CUBE_E_ARG, "null argument");
+  if (!c->cap_buf) return fail(CUBE_E_STATE, "nothing captured");
+  CK(cudaSetDevice(c->device));
+  const bool is_int = c->cap_n < 0;
+  const int64_t m = is_int ? -c->cap_n : c->cap_n;
+  if (n < m) return fail(CUBE_E_ARG, "capture buffer too small");
+  if (is_int) {
+    std::vector<long long> h(m);
+    CK(cudaMemcpy(h.data(), c->cap_buf, m * 8, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < m; ++i) out[i] = (float)std::ldexp((double)h[i], -40) * c->G.mass_p;
+  } else {
+    std::vector<float> h(m);
+    CK(cudaMemcpy(h.data(), c->cap_buf, m * 4, cudaMemcpyDeviceToHost));
+    // density captures hold unscaled weights; phi captures are final
+    const float sc = (c->cap_what == 0) ? c->G.mass_p : 1.f;
+    for (int64_t i = 0; i < m; ++i) out[i] = (c->cap_what == 0) ? h[i] * sc : h[i];
+  }
+  return (int)m;
+}
+
+int cube_gpu_green_table(cube_ctx* c, int level, int iapm, float* out, int64_t n) {
+  if (!c || !out) return fail(CUBE_E_ARG, "null argument");
+  CK(cudaSetDevice(c->device));
+  const Geo& G = c->G;
+  float* src = nullptr;
+  int m = 0;
+  if (level == 1) { src = c->green1; m = G.nc; }
+  else if (level == 2) { src = c->green2; m = G.ngt; }
+  else if (level == 3 && iapm >= 2 && iapm <= 5) { src = green3(c, iapm); m = G.nft[iapm]; }
+  if (!src) return fail(CUBE_E_ARG, "bad level/iapm");
+  const int64_t cnt = (int64_t)m * m * (m / 2 + 1);
+  if (n < cnt) return fail(CUBE_E_ARG, "buffer too small");
+  CK(cudaStreamSynchronize(c->s));
+  CK(cudaMemcpy(out, src, cnt * 4, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int cube_gpu_subtile_class(cube_ctx* c, int32_t* ires, int64_t n) {
+  if (!c || !ires || n < c->ns3) return fail(CUBE_E_ARG, "bad argument");
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemsetAsync(c->napm, 0, 32, c->s));
+  k_classify<<<nblk(c->ns3), 256, 0, c->s>>>(c->G, c->rhoc, c->ns3, c->ires, c->napm);
+  CK(cudaMemcpyAsync(ires, c->ires, c->ns3 * 4, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  return 0;
+}
+
+}  // extern "C"

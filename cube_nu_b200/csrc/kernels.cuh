@@ -1,0 +1,826 @@
+// Step kernels (header-only, included once by cube_gpu.cu) for one CUBE image on one B200 (sm_100a).
+//
+// All particle data stays in the reference's order (tile z,y,x; coarse cell z,y,x;
+// arrival).  Ghost cells of the reference (buffer_grid.f90, buffer_particle.f90) are
+// periodic copies when nn=1, so every kernel reads neighbour cells through periodic
+// cell indexing instead of materialised ghost copies.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace cube {
+
+// =================================================================================
+// Exclusive scan int32 -> int64 (cell starts); out has n+1 entries.
+// =================================================================================
+static constexpr int SCAN_T = 256, SCAN_I = 8, SCAN_TILE = SCAN_T * SCAN_I;
+
+__device__ __forceinline__ int64_t warp_incl_scan(int64_t v) {
+  for (int o = 1; o < 32; o <<= 1) {
+    int64_t u = __shfl_up_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) >= o) v += u;
+  }
+  return v;
+}
+
+// Block-wide exclusive scan of one value per thread; returns exclusive prefix, total in *tot.
+__device__ int64_t block_excl_scan(int64_t v, int64_t* tot) {
+  __shared__ int64_t ws[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int64_t inc = warp_incl_scan(v);
+  if (lane == 31) ws[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    int64_t s = (lane < nw) ? ws[lane] : 0;
+    s = warp_incl_scan(s);
+    if (lane < nw) ws[lane] = s;
+  }
+  __syncthreads();
+  const int64_t base = (wid > 0) ? ws[wid - 1] : 0;
+  *tot = ws[nw - 1];
+  __syncthreads();
+  return base + inc - v;
+}
+
+__global__ void k_scan_tiles(const int32_t* __restrict__ in, int64_t n, int64_t* __restrict__ tile_sums) {
+  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_I;
+  int64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < SCAN_I; ++i)
+    if (base + i < n) s += in[base + i];
+  int64_t tot;
+  block_excl_scan(s, &tot);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_sums(int64_t* __restrict__ sums, int64_t nt) {
+  // single block: exclusive scan of nt tile sums in place
+  __shared__ int64_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int64_t b0 = 0; b0 < nt; b0 += blockDim.x) {
+    const int64_t i = b0 + threadIdx.x;
+    const int64_t v = (i < nt) ? sums[i] : 0;
+    int64_t tot;
+    const int64_t ex = block_excl_scan(v, &tot);
+    if (i < nt) sums[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sums[nt] = carry;
+}
+
+__global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n, const int64_t* __restrict__ tile_sums,
+                             int64_t* __restrict__ out, int64_t ntiles) {
+  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_I;
+  int64_t v[SCAN_I];
+  int64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < SCAN_I; ++i) {
+    v[i] = (base + i < n) ? in[base + i] : 0;
+    s += v[i];
+  }
+  int64_t tot;
+  int64_t ex = block_excl_scan(s, &tot) + tile_sums[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < SCAN_I; ++i) {
+    if (base + i < n) out[base + i] = ex;
+    ex += v[i];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tile_sums[ntiles];
+}
+
+inline void exclusive_scan(const int32_t* in, int64_t* out, int64_t n, int64_t* tmp, cudaStream_t s) {
+  const int64_t nt = (n + SCAN_TILE - 1) / SCAN_TILE;
+  k_scan_tiles<<<(unsigned)nt, SCAN_T, 0, s>>>(in, n, tmp);
+  k_scan_sums<<<1, 1024, 0, s>>>(tmp, nt);
+  k_scan_apply<<<(unsigned)nt, SCAN_T, 0, s>>>(in, n, tmp, out, nt);
+}
+
+// Particle -> storage cell index, from the cell starts.
+__global__ void k_fill_pcell(const int64_t* __restrict__ cstart, int64_t ncells, int32_t* __restrict__ pcell) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  for (int64_t i = cstart[c]; i < cstart[c + 1]; ++i) pcell[i] = (int32_t)c;
+}
+
+// =================================================================================
+// Drift (drift.f90:1-233), bit-exact.
+// =================================================================================
+// Destination cell, arrival key and count.  The reference scans, per destination
+// tile, source cells of the tile's ncb-deep extended region in order
+// (ilayer, k, j, i, l) with ilayer=(k-(1-ncb)) mod nlayer (drift.f90:96-115).  The key
+// packs that order relative to the destination tile:
+//   ilayer:16 | k+ncb-1:8 | j+ncb-1:8 | i+ncb-1:8 | l:24.
+__global__ void k_drift_dest(Geo G, int64_t np, const void* __restrict__ xp, const float* __restrict__ vp,
+                             const int32_t* __restrict__ pcell, const int64_t* __restrict__ cstart, float dt_mid,
+                             int nlayer, int32_t* __restrict__ dest, uint64_t* __restrict__ key,
+                             int32_t* __restrict__ count_new, unsigned* err) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= np) return;
+  const int c = pcell[ip];
+  int g[3];
+  cell_coords(G, c, g[0], g[1], g[2]);
+  const int64_t l = ip - cstart[c];
+  int dn[3];
+  bool bad = false;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int code = load_code(xp, G.izipx, 3 * ip + d);
+    const float p = __fmul_rn(dt_mid, vp[3 * ip + d]);
+    const double deltax = (double)__fdiv_rn(p, (float)G.rcs);       // drift.f90:57
+    const int li = g[d] % G.nt;                                      // i-1 in the source tile
+    const double xq = (double)li + zfrac(code, G);                   // drift.f90:59
+    const double ig = ceil(__dadd_rn(xq, deltax));                   // drift.f90:63
+    if (!(ig >= (double)(1 - 2 * G.ncb) && ig <= (double)(G.nt + 2 * G.ncb))) bad = true;
+    dn[d] = bad ? 0 : (int)ig - (li + 1);
+  }
+  int dst[3], rel[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    dst[d] = wrapi(g[d] + dn[d], G.nc);
+    const int torg = (dst[d] / G.nt) * G.nt;
+    rel[d] = wrapi(g[d] - torg + G.ncb, G.nc) - G.ncb;  // source coordinate (i-1) in the dest tile
+    if (rel[d] >= G.nt + G.ncb) bad = true;             // outside the dest tile's ghost region
+  }
+  if (bad || l >= (1 << 24)) {
+    set_err(err, CUBE_DEVERR_DRIFT_RANGE);
+    dest[ip] = -1;
+    return;
+  }
+  const int64_t dc = cell_index(G, dst[0], dst[1], dst[2]);
+  const uint64_t kz = (uint64_t)(rel[2] + G.ncb), ky = (uint64_t)(rel[1] + G.ncb), kx = (uint64_t)(rel[0] + G.ncb);
+  const uint64_t il = kz % (uint64_t)nlayer;
+  key[ip] = (il << 48) | (kz << 40) | (ky << 32) | (kx << 24) | (uint64_t)l;
+  dest[ip] = (int32_t)dc;
+  atomicAdd(&count_new[dc], 1);
+}
+
+__global__ void k_drift_scatter(int64_t np, const int32_t* __restrict__ dest, const uint64_t* __restrict__ key,
+                                const int64_t* __restrict__ cstart_new, int32_t* __restrict__ fill,
+                                uint64_t* __restrict__ skey, uint32_t* __restrict__ ssrc) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= np) return;
+  const int dc = dest[ip];
+  if (dc < 0) return;
+  const int slot = atomicAdd(&fill[dc], 1);
+  const int64_t pos = cstart_new[dc] + slot;
+  skey[pos] = key[ip];
+  ssrc[pos] = (uint32_t)ip;
+}
+
+// Warp per destination cell: segments of <=32 sorted in registers (bitonic over
+// the warp); longer ones are listed for the block sorter.
+__global__ void k_drift_sort_small(int64_t ncells, const int32_t* __restrict__ count_new,
+                                   const int64_t* __restrict__ cstart_new, uint64_t* __restrict__ skey,
+                                   uint32_t* __restrict__ ssrc, int32_t* __restrict__ biglist,
+                                   int32_t* __restrict__ nbig) {
+  const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (c >= ncells) return;
+  const int n = count_new[c];
+  if (n <= 1) return;
+  if (n > 32) {
+    if (lane == 0) biglist[atomicAdd(nbig, 1)] = (int32_t)c;
+    return;
+  }
+  const int64_t base = cstart_new[c];
+  uint64_t k = (lane < n) ? skey[base + lane] : ~0ull;
+  uint32_t v = (lane < n) ? ssrc[base + lane] : 0u;
+  for (int size = 2; size <= 32; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, stride);
+      const uint32_t ov = __shfl_xor_sync(0xffffffffu, v, stride);
+      const bool up = ((lane & size) == 0);
+      const bool lower = ((lane & stride) == 0);
+      const bool take = lower ? (up ? (ok < k) : (ok > k)) : (up ? (ok > k) : (ok < k));
+      if (take) { k = ok; v = ov; }
+    }
+  if (lane < n) {
+    skey[base + lane] = k;
+    ssrc[base + lane] = v;
+  }
+}
+
+// Block per long segment: bitonic sort in shared memory (keys are unique).
+__global__ void k_drift_sort_big(const int32_t* __restrict__ biglist, const int32_t* __restrict__ nbig,
+                                 const int32_t* __restrict__ count_new, const int64_t* __restrict__ cstart_new,
+                                 uint64_t* __restrict__ skey, uint32_t* __restrict__ ssrc, int max_seg,
+                                 unsigned* err) {
+  extern __shared__ uint64_t smk[];
+  if ((int)blockIdx.x >= *nbig) return;
+  const int c = biglist[blockIdx.x];
+  const int n = count_new[c];
+  if (n > max_seg) {
+    if (threadIdx.x == 0) set_err(err, CUBE_DEVERR_SEGMENT);
+    return;
+  }
+  int m = 1;
+  while (m < n) m <<= 1;
+  uint32_t* smv = reinterpret_cast<uint32_t*>(smk + max_seg);
+  const int64_t base = cstart_new[c];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    smk[i] = (i < n) ? skey[base + i] : ~0ull;
+    smv[i] = (i < n) ? ssrc[base + i] : 0u;
+  }
+  __syncthreads();
+  for (int size = 2; size <= m; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool up = ((i & size) == 0);
+          const uint64_t a = smk[i], b = smk[j];
+          if ((a > b) == up) {
+            smk[i] = b;
+            smk[j] = a;
+            const uint32_t t = smv[i];
+            smv[i] = smv[j];
+            smv[j] = t;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    skey[base + i] = smk[i];
+    ssrc[base + i] = smv[i];
+  }
+}
+
+// New arrays in the sorted order, with the ZIPX update xp+nint(dt_mid*vp/(x_res*ratio_cs))
+// in the integer kind (drift.f90:117).
+__global__ void k_drift_gather(Geo G, int64_t np, const uint32_t* __restrict__ ssrc, const int32_t* __restrict__ dest,
+                               const void* __restrict__ xp, const float* __restrict__ vp,
+                               const int64_t* __restrict__ pid, float dt_mid, void* __restrict__ xo,
+                               float* __restrict__ vo, int64_t* __restrict__ po, int32_t* __restrict__ pcell_o) {
+  const int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos >= np) return;
+  const int64_t src = ssrc[pos];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float v = vp[3 * src + d];
+    const int code = load_code(xp, G.izipx, 3 * src + d);
+    const long long dn = llround(__dmul_rn((double)__fmul_rn(dt_mid, v), G.inv_step));
+    store_code(xo, G.izipx, 3 * pos + d, (int)(code + (int)dn));
+    vo[3 * pos + d] = v;
+  }
+  po[pos] = pid[src];
+  pcell_o[pos] = dest[src];
+}
+
+// =================================================================================
+// Deposit (particle_mesh.f90:20-109, kick.f90:611-691).
+// =================================================================================
+static constexpr float FIXED_SCALE = 1099511627776.f;  // 2^40
+
+template <bool FIXED>
+__device__ __forceinline__ void dep_add(void* rho, int64_t i, float w) {
+  if (FIXED) {
+    const long long q = __float2ll_rn(__fmul_rn(w, FIXED_SCALE));
+    atomicAdd(reinterpret_cast<unsigned long long*>(rho) + i, (unsigned long long)q);
+  } else {
+    atomicAdd(reinterpret_cast<float*>(rho) + i, w);
+  }
+}
+
+template <bool FIXED>
+__global__ void k_deposit_pm1(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+                              void* __restrict__ rho) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= np) return;
+  int g[3];
+  cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+  int i2[3];
+  float w[3][3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double xpos = (double)g[d] + zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
+    i2[d] = tsc_weights(xpos, w[d]);  // xpos*ratio_cs/gridsize with gridsize=ratio_cs is exact
+  }
+  const int nc = G.nc;
+#pragma unroll
+  for (int a3 = 0; a3 < 3; ++a3) {
+    const int z = wrapi(i2[2] - 2 + a3, nc);
+#pragma unroll
+    for (int a2 = 0; a2 < 3; ++a2) {
+      const int y = wrapi(i2[1] - 2 + a2, nc);
+#pragma unroll
+      for (int a1 = 0; a1 < 3; ++a1) {
+        const int x = wrapi(i2[0] - 2 + a1, nc);
+        const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
+        dep_add<FIXED>(rho, ((int64_t)z * nc + y) * nc + x, ww);
+      }
+    }
+  }
+}
+
+// Candidate tiles along one dimension for a particle with global cell g: its own tile
+// and, within ncb of a tile face, the neighbour whose ghost region holds it.
+// Writes (tile, local coordinate i-1 in that tile) pairs; returns the count (1 or 2).
+__device__ __forceinline__ int tile_cands(const Geo& G, int g, int* t, int* li) {
+  const int tt = g / G.nt, l = g - tt * G.nt;
+  int n = 0;
+  t[n] = tt; li[n] = l; ++n;
+  if (l < G.ncb) { t[n] = wrapi(tt - 1, G.nnt); li[n] = l + G.nt; ++n; }
+  else if (l >= G.nt - G.ncb) { t[n] = wrapi(tt + 1, G.nnt); li[n] = l - G.nt; ++n; }
+  return n;
+}
+
+// PM2 tile meshes [tile - tile0][ngt^3]; fine index i maps to array i-(1-ngb).
+template <bool FIXED>
+__global__ void k_deposit_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+                              void* __restrict__ rho, int tile0, int ntile) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= np) return;
+  int g[3];
+  cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+  int tc[3][2], lc[3][2], nca[3];
+  double f[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    nca[d] = tile_cands(G, g[d], tc[d], lc[d]);
+    f[d] = zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
+  }
+  const int ngt = G.ngt;
+  const int64_t ngt3 = (int64_t)ngt * ngt * ngt;
+  for (int cz = 0; cz < nca[2]; ++cz)
+    for (int cy = 0; cy < nca[1]; ++cy)
+      for (int cx = 0; cx < nca[0]; ++cx) {
+        const int T = (tc[2][cz] * G.nnt + tc[1][cy]) * G.nnt + tc[0][cx];
+        if (T < tile0 || T >= tile0 + ntile) continue;
+        const int l[3] = {lc[0][cx], lc[1][cy], lc[2][cz]};
+        int i2[3];
+        float w[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double xpos = ((double)l[d] + f[d]) * (double)G.rcs;  // /gridsize(=1)
+          i2[d] = tsc_weights(xpos, w[d]);
+        }
+        char* base = (char*)rho + (int64_t)(T - tile0) * ngt3 * (FIXED ? 8 : 4);
+#pragma unroll
+        for (int a3 = 0; a3 < 3; ++a3) {
+          const int z = i2[2] - 1 + a3 - (1 - G.ngb);
+          if (z < 0 || z >= ngt) continue;
+#pragma unroll
+          for (int a2 = 0; a2 < 3; ++a2) {
+            const int y = i2[1] - 1 + a2 - (1 - G.ngb);
+            if (y < 0 || y >= ngt) continue;
+#pragma unroll
+            for (int a1 = 0; a1 < 3; ++a1) {
+              const int x = i2[0] - 1 + a1 - (1 - G.ngb);
+              if (x < 0 || x >= ngt) continue;
+              const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
+              dep_add<FIXED>(base, ((int64_t)z * ngt + y) * ngt + x, ww);
+            }
+          }
+        }
+      }
+}
+
+// Candidate subtiles along one dimension (PM3 nloop=1): own subtile and, in the
+// first/last coarse cell of a subtile, the neighbour subtile (possibly in the
+// neighbour tile).  Returns count; writes tile, subtile, and local coordinate (i-1)
+// in that tile.
+__device__ __forceinline__ int sub_cands(const Geo& G, int g, int* t, int* u, int* li) {
+  const int tt = g / G.nt, l = g - tt * G.nt;
+  const int uu = l / G.ntt, r = l - uu * G.ntt;
+  int n = 0;
+  t[n] = tt; u[n] = uu; li[n] = l; ++n;
+  if (r == 0) {
+    if (uu > 0) { t[n] = tt; u[n] = uu - 1; li[n] = l; }
+    else { t[n] = wrapi(tt - 1, G.nnt); u[n] = G.nns - 1; li[n] = l + G.nt; }
+    ++n;
+  }
+  if (r == G.ntt - 1) {
+    if (uu < G.nns - 1) { t[n] = tt; u[n] = uu + 1; li[n] = l; }
+    else { t[n] = wrapi(tt + 1, G.nnt); u[n] = 0; li[n] = l - G.nt; }
+    ++n;
+  }
+  return n;
+}
+
+__device__ __forceinline__ int subtile_id(const Geo& G, const int t[3], const int u[3]) {
+  const int T = (t[2] * G.nnt + t[1]) * G.nnt + t[0];
+  return ((T * G.nns + u[2]) * G.nns + u[1]) * G.nns + u[0];
+}
+
+// PM3 meshes of one class: slot = box_slot[subtile] (or -1), mesh [slot][nft^3];
+// refined index i maps to array i-(1-nfb).
+template <bool FIXED>
+__global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+                              const int32_t* __restrict__ box_slot, int iapm, void* __restrict__ rho,
+                              unsigned* err) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= np) return;
+  int g[3];
+  cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+  int tc[3][3], uc[3][3], lc[3][3], nca[3];
+  double f[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    nca[d] = sub_cands(G, g[d], tc[d], uc[d], lc[d]);
+    f[d] = zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
+  }
+  const int nft = G.nft[iapm], nfp = G.nfp[iapm], nfb = G.nfb[iapm];
+  const int64_t nft3 = (int64_t)nft * nft * nft;
+  const double gs = (double)(1.f / (float)rsf_of(iapm));  // pm%gridsize, real4
+  for (int cz = 0; cz < nca[2]; ++cz)
+    for (int cy = 0; cy < nca[1]; ++cy)
+      for (int cx = 0; cx < nca[0]; ++cx) {
+        const int t[3] = {tc[0][cx], tc[1][cy], tc[2][cz]};
+        const int u[3] = {uc[0][cx], uc[1][cy], uc[2][cz]};
+        const int slot = box_slot[subtile_id(G, t, u)];
+        if (slot < 0) continue;
+        const int l[3] = {lc[0][cx], lc[1][cy], lc[2][cz]};
+        int i2[3];
+        float w[3][3];
+        bool oob = false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double xpos = ((double)l[d] + f[d]) * (double)G.rcs / gs - (double)(u[d] * nfp);  // kick.f90:628-629
+          i2[d] = tsc_weights(xpos, w[d]);
+          if (i2[d] - 1 < -nfb || i2[d] + 1 > nfp + nfb + 1) oob = true;
+        }
+        if (oob) {
+          set_err(err, CUBE_DEVERR_DEPOSIT_RANGE);
+          continue;
+        }
+        char* base = (char*)rho + (int64_t)slot * nft3 * (FIXED ? 8 : 4);
+#pragma unroll
+        for (int a3 = 0; a3 < 3; ++a3) {
+          const int z = i2[2] - 1 + a3 - (1 - nfb);
+          if (z < 0 || z >= nft) continue;
+#pragma unroll
+          for (int a2 = 0; a2 < 3; ++a2) {
+            const int y = i2[1] - 1 + a2 - (1 - nfb);
+            if (y < 0 || y >= nft) continue;
+#pragma unroll
+            for (int a1 = 0; a1 < 3; ++a1) {
+              const int x = i2[0] - 1 + a1 - (1 - nfb);
+              if (x < 0 || x >= nft) continue;
+              const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
+              dep_add<FIXED>(base, ((int64_t)z * nft + y) * nft + x, ww);
+            }
+          }
+        }
+      }
+}
+
+// =================================================================================
+// Force from potential (particle_mesh.f90:224-247, kick.f90:839-862) and max |F|^2.
+// =================================================================================
+__device__ __forceinline__ float grad4(float pm2, float pm1, float pp1, float pp2) {
+  const float w0 = (CUBE_W_ALPHA - 1.f) / 4.f, w1 = -CUBE_W_ALPHA / 2.f, w2 = CUBE_W_ALPHA / 2.f,
+              w3 = (1.f - CUBE_W_ALPHA) / 4.f;
+  float s = __fmul_rn(pm2, w0);
+  s = __fadd_rn(s, __fmul_rn(pm1, w1));
+  s = __fadd_rn(s, __fmul_rn(pp1, w2));
+  s = __fadd_rn(s, __fmul_rn(pp2, w3));
+  return s;
+}
+
+__device__ __forceinline__ float sumsq3(float a, float b, float c) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
+}
+
+__device__ __forceinline__ void block_max_to(float v, float* out) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) atomic_max_pos(out, v);
+}
+
+// PM1: periodic nc^3 phi[z][y][x].
+__global__ void k_f2max_periodic(const float* __restrict__ phi, int nc, float* __restrict__ f2out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float v = 0.f;
+  if (i < (int64_t)nc * nc * nc) {
+    const int x = (int)(i % nc), y = (int)((i / nc) % nc), z = (int)(i / ((int64_t)nc * nc));
+    auto P = [&](int a, int b, int c) {
+      return phi[((int64_t)wrapi(c, nc) * nc + wrapi(b, nc)) * nc + wrapi(a, nc)];
+    };
+    const float fx = grad4(P(x - 2, y, z), P(x - 1, y, z), P(x + 1, y, z), P(x + 2, y, z));
+    const float fy = grad4(P(x, y - 2, z), P(x, y - 1, z), P(x, y + 1, z), P(x, y + 2, z));
+    const float fz = grad4(P(x, y, z - 2), P(x, y, z - 1), P(x, y, z + 1), P(x, y, z + 2));
+    v = sumsq3(fx, fy, fz);
+  }
+  block_max_to(v, f2out);
+}
+
+// Box meshes: phi[b][n^3] with index i mapping to array i-m1phi; physical 1..nforce.
+__global__ void k_f2max_box(const float* __restrict__ phi, int n, int nforce, int m1phi, int nbox,
+                            float* __restrict__ f2out) {
+  const int64_t nf3 = (int64_t)nforce * nforce * nforce;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float v = 0.f;
+  if (i < nf3 * nbox) {
+    const int64_t b = i / nf3;
+    const int64_t r = i - b * nf3;
+    const int x = (int)(r % nforce) + 1, y = (int)((r / nforce) % nforce) + 1, z = (int)(r / ((int64_t)nforce * nforce)) + 1;
+    const float* pb = phi + b * (int64_t)n * n * n;
+    auto P = [&](int a, int bb, int c) { return pb[((int64_t)(c - m1phi) * n + (bb - m1phi)) * n + (a - m1phi)]; };
+    const float fx = grad4(P(x - 2, y, z), P(x - 1, y, z), P(x + 1, y, z), P(x + 2, y, z));
+    const float fy = grad4(P(x, y - 2, z), P(x, y - 1, z), P(x, y + 1, z), P(x, y + 2, z));
+    const float fz = grad4(P(x, y, z - 2), P(x, y, z - 1), P(x, y, z + 1), P(x, y, z + 2));
+    v = sumsq3(fx, fy, fz);
+  }
+  block_max_to(v, f2out);
+}
+
+// =================================================================================
+// Interpolation and kick (particle_mesh.f90:148-217, kick.f90:745-834).  The force
+// at each of the 27 TSC cells is differenced from phi on the fly; the values equal
+// those of a stored force grid because each uses the same four phi values.
+// =================================================================================
+template <class PhiFn>
+__device__ __forceinline__ void tsc_gather_force(const int i2[3], const float w[3][3], PhiFn P, float dv[3]) {
+  dv[0] = dv[1] = dv[2] = 0.f;
+#pragma unroll
+  for (int a3 = 0; a3 < 3; ++a3) {
+    const int z = i2[2] - 1 + a3;
+#pragma unroll
+    for (int a2 = 0; a2 < 3; ++a2) {
+      const int y = i2[1] - 1 + a2;
+#pragma unroll
+      for (int a1 = 0; a1 < 3; ++a1) {
+        const int x = i2[0] - 1 + a1;
+        const float F0 = grad4(P(x - 2, y, z), P(x - 1, y, z), P(x + 1, y, z), P(x + 2, y, z));
+        const float F1 = grad4(P(x, y - 2, z), P(x, y - 1, z), P(x, y + 1, z), P(x, y + 2, z));
+        const float F2 = grad4(P(x, y, z - 2), P(x, y, z - 1), P(x, y, z + 1), P(x, y, z + 2));
+        const float wa = w[0][a1], wb = w[1][a2], wc = w[2][a3];
+        dv[0] = __fadd_rn(dv[0], __fmul_rn(__fmul_rn(__fmul_rn(F0, wa), wb), wc));
+        dv[1] = __fadd_rn(dv[1], __fmul_rn(__fmul_rn(__fmul_rn(F1, wa), wb), wc));
+        dv[2] = __fadd_rn(dv[2], __fmul_rn(__fmul_rn(__fmul_rn(F2, wa), wb), wc));
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void apply_kick(float* vp, int64_t ip, const float dv[3], float a_mid, float dt,
+                                           float* vmax) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float v = kick_add(vp[3 * ip + d], dv[d], a_mid, dt);
+    vp[3 * ip + d] = v;
+    if (vmax) atomic_max_pos(vmax + d, fabsf(v));
+  }
+}
+
+__global__ void k_interp_pm1(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+                             const float* __restrict__ phi, float* __restrict__ vp, float a_mid, float dt) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= np) return;
+  int g[3];
+  cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+  int i2[3];
+  float w[3][3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double xpos = (double)g[d] + zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
+    i2[d] = tsc_weights(xpos, w[d]);
+  }
+  const int nc = G.nc;
+  // force index i (1-based, periodic) reads phi(i-2..i+2); array index (i-1) mod nc
+  auto P = [&](int a, int b, int c) {
+    return __ldg(&phi[((int64_t)wrapi(c - 1, nc) * nc + wrapi(b - 1, nc)) * nc + wrapi(a - 1, nc)]);
+  };
+  float dv[3];
+  tsc_gather_force(i2, w, P, dv);
+  apply_kick(vp, ip, dv, a_mid, dt, nullptr);
+}
+
+__global__ void k_interp_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+                             const float* __restrict__ phi, int tile0, int ntile, float* __restrict__ vp, float a_mid,
+                             float dt, float* vmax, unsigned* err) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= np) return;
+  int g[3];
+  cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+  const int T = ((g[2] / G.nt) * G.nnt + g[1] / G.nt) * G.nnt + g[0] / G.nt;
+  if (T < tile0 || T >= tile0 + ntile) return;
+  int i2[3];
+  float w[3][3];
+  bool oob = false;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double xpos = ((double)(g[d] % G.nt) + zfrac(load_code(xp, G.izipx, 3 * ip + d), G)) * (double)G.rcs;
+    i2[d] = tsc_weights(xpos, w[d]);
+    if (i2[d] - 1 < 0 || i2[d] + 1 > G.ngp + 1) oob = true;
+  }
+  if (oob) {
+    set_err(err, CUBE_DEVERR_INTERP_RANGE);
+    return;
+  }
+  const int n = G.ngt, m1 = 1 - G.ngb;
+  const float* pb = phi + (int64_t)(T - tile0) * n * n * n;
+  auto P = [&](int a, int b, int c) { return __ldg(&pb[((int64_t)(c - m1) * n + (b - m1)) * n + (a - m1)]); };
+  float dv[3];
+  tsc_gather_force(i2, w, P, dv);
+  apply_kick(vp, ip, dv, a_mid, dt, vmax);
+}
+
+__global__ void k_interp_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+                             const float* __restrict__ phi, const int32_t* __restrict__ box_slot, int iapm,
+                             float* __restrict__ vp, float a_mid, float dt, float* vmax, unsigned* err) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= np) return;
+  int g[3];
+  cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+  int t[3], u[3], l[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    t[d] = g[d] / G.nt;
+    l[d] = g[d] - t[d] * G.nt;
+    u[d] = l[d] / G.ntt;
+  }
+  const int slot = box_slot[subtile_id(G, t, u)];
+  if (slot < 0) return;
+  const int nft = G.nft[iapm], nfp = G.nfp[iapm], nfb = G.nfb[iapm];
+  const double gs = (double)(1.f / (float)rsf_of(iapm));
+  int i2[3];
+  float w[3][3];
+  bool oob = false;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double xpos =
+        ((double)l[d] + zfrac(load_code(xp, G.izipx, 3 * ip + d), G)) * (double)G.rcs / gs - (double)(u[d] * nfp);
+    i2[d] = tsc_weights(xpos, w[d]);
+    if (i2[d] - 1 < 0 || i2[d] + 1 > nfp + 1) oob = true;
+  }
+  if (oob) {
+    set_err(err, CUBE_DEVERR_INTERP_RANGE);
+    return;
+  }
+  const int m1 = 1 - nfb;
+  const float* pb = phi + (int64_t)slot * nft * nft * nft;
+  auto P = [&](int a, int b, int c) { return __ldg(&pb[((int64_t)(c - m1) * nft + (b - m1)) * nft + (a - m1)]); };
+  float dv[3];
+  tsc_gather_force(i2, w, P, dv);
+  apply_kick(vp, ip, dv, a_mid, dt, vmax);
+}
+
+// =================================================================================
+// Subtile classes (kick.f90:108-133) and the box slot map of one class.
+// =================================================================================
+__global__ void k_classify(Geo G, const int32_t* __restrict__ rhoc, int ns3, int32_t* __restrict__ ires,
+                           int32_t* __restrict__ napm) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns3) return;
+  const int nns3 = G.nns * G.nns * G.nns;
+  const int T = s / nns3, f = s - T * nns3;
+  const int tx = T % G.nnt, ty = (T / G.nnt) % G.nnt, tz = T / (G.nnt * G.nnt);
+  const int ux = f % G.nns, uy = (f / G.nns) % G.nns, uz = f / (G.nns * G.nns);
+  int mx = 0;
+  for (int k = 0; k < G.ntt; ++k)
+    for (int j = 0; j < G.ntt; ++j)
+      for (int i = 0; i < G.ntt; ++i) {
+        const int64_t c = cell_index(G, tx * G.nt + ux * G.ntt + i, ty * G.nt + uy * G.ntt + j, tz * G.nt + uz * G.ntt + k);
+        mx = max(mx, rhoc[c]);
+      }
+  const float npc = (float)mx / 64.f;
+  const int r = (npc < 24.f) ? 2 : (npc < 114.f) ? 3 : (npc < 320.f) ? 4 : 5;
+  ires[s] = r;
+  atomicAdd(&napm[r], 1);
+}
+
+// =================================================================================
+// PP (kick.f90:376-588).  Each physical particle sums 0<r^2<range^2 pairs over the
+// coarse cells its range can reach; equivalent to the reference's PP-cell lists
+// (the PP cell 4/rsf fine cells is wider than the range 3.5/rsf).
+// =================================================================================
+__device__ __forceinline__ float F_ra(float r, float apm) {
+  const float ep = __fdiv_rn(2.f * r, apm);
+  if (apm == 0.f || ep > 2.f) return __fdiv_rn(1.f, __fmul_rn(r, r));
+  const float c = __fdiv_rn(__fdiv_rn(1.f, 35.f), __fmul_rn(apm, apm));
+  const float e2 = ep * ep, e3 = e2 * ep, e4 = e3 * ep, e5 = e4 * ep, e6 = e5 * ep;
+  if (ep > 1.f) return c * (12.f * (1.f / e2) - 224.f + 896.f * ep - 840.f * e2 + 224.f * e3 + 70.f * e4 - 48.f * e5 + 7.f * e6);
+  if (ep > 0.f) return c * (224.f * ep - 224.f * e3 + 70.f * e4 + 48.f * e5 - 21.f * e6);
+  return 0.f;
+}
+
+__global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+                     const int64_t* __restrict__ cstart, const int32_t* __restrict__ ires, float* __restrict__ vp,
+                     float mass_scale, float v_scale, float* f2max, float* vmax,
+                     unsigned long long* npairs) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= np) return;
+  int g[3];
+  cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+  int t[3], u[3], l[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    t[d] = g[d] / G.nt;
+    l[d] = g[d] - t[d] * G.nt;
+    u[d] = l[d] / G.ntt;
+  }
+  const int iapm = ires[subtile_id(G, t, u)];
+  const float range = __fdiv_rn(3.5f, (float)rsf_of(iapm));  // apm3(iapm)
+  const float range2 = __fmul_rn(range, range);
+  float xf[3], fin[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double fr = zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
+    xf[d] = __fmul_rn((float)((double)l[d] + fr), (float)G.rcs);  // xvec*ratio_cs (kick.f90:424)
+    fin[d] = __fmul_rn((float)fr, (float)G.rcs);                  // offset inside the coarse cell, fine units
+  }
+  int lo[3], hi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = (fin[d] < range) ? -1 : 0;
+    hi[d] = ((float)G.rcs - fin[d] < range) ? 1 : 0;
+  }
+  float acc[3] = {0.f, 0.f, 0.f};
+  unsigned long long cnt = 0;
+  for (int dz = lo[2]; dz <= hi[2]; ++dz)
+    for (int dy = lo[1]; dy <= hi[1]; ++dy)
+      for (int dx = lo[0]; dx <= hi[0]; ++dx) {
+        const int64_t c = cell_index(G, g[0] + dx, g[1] + dy, g[2] + dz);
+        const int64_t s = cstart[c], e = cstart[c + 1];
+        const int lq[3] = {l[0] + dx, l[1] + dy, l[2] + dz};
+        for (int64_t q = s; q < e; ++q) {
+          float rv[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const float xq = __fmul_rn((float)((double)lq[d] + zfrac(load_code(xp, G.izipx, 3 * q + d), G)), (float)G.rcs);
+            rv[d] = __fsub_rn(xq, xf[d]);
+          }
+          const float r2 = sumsq3(rv[0], rv[1], rv[2]);
+          if (r2 > 0.f && r2 < range2) {
+            const float rm = __fsqrt_rn(r2);
+            const float sc = F_ra(rm, G.app) - F_ra(rm, range);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) acc[d] += __fdiv_rn(rv[d], rm) * sc;
+            ++cnt;
+          }
+        }
+      }
+  float f1[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) f1[d] = __fmul_rn(acc[d], mass_scale);
+  atomic_max_pos(f2max, sumsq3(f1[0], f1[1], f1[2]));
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float v = __fadd_rn(vp[3 * ip + d], __fmul_rn(f1[d], v_scale));
+    vp[3 * ip + d] = v;
+    atomic_max_pos(vmax + d, fabsf(v));
+  }
+  if (cnt) atomicAdd(npairs, cnt);
+}
+
+// =================================================================================
+// Green's function (Green/Green.f90:1-80) in FP64, stored real32.
+// =================================================================================
+__global__ void k_green(float* __restrict__ Gk, int n, float apm_soft, float apm_range, float gridsize) {
+  const int nh = n / 2 + 1;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)nh * n * n) return;
+  const int k1 = (int)(i % nh), k2 = (int)((i / nh) % n), k3 = (int)(i / ((int64_t)nh * n));
+  const float inv_n = 1.f / (float)n;
+  const double PI = 3.141592653589793;
+  auto fs = [&](int k) {  // fftspace(k+1)
+    const int m = ((k + 1 + n / 2 - 1) % n) - n / 2;
+    return (2.0 * PI) * (double)inv_n * (double)m;
+  };
+  const double kv[3] = {fs(k1), fs(k2), fs(k3)};
+  const float alpha = 4.f / 3.f;
+  double Dv[3], ur[3] = {0, 0, 0};
+  for (int d = 0; d < 3; ++d) Dv[d] = (double)alpha * sin(kv[d]) + (double)(1.f - alpha) * sin(2 * kv[d]) / 2;
+  for (int i3 = -2; i3 <= 2; ++i3)
+    for (int i2 = -2; i2 <= 2; ++i2)
+      for (int i1 = -2; i1 <= 2; ++i1) {
+        const double kn[3] = {kv[0] + 2 * PI * i1, kv[1] + 2 * PI * i2, kv[2] + 2 * PI * i3};
+        const double kmag = sqrt(kn[0] * kn[0] + kn[1] * kn[1] + kn[2] * kn[2]);
+        if (kmag == 0) continue;  // only k=0, zeroed below
+        double prod = 1;
+        for (int d = 0; d < 3; ++d) prod *= (kn[d] == 0) ? 1.0 : sin(kn[d] / 2) / (kn[d] / 2);
+        const double p2 = prod * prod;
+        const double Uk2 = p2 * p2 * p2;
+        double y = (double)apm_soft * kmag / 2;
+        const double Ss = 12 / (y * y * y * y) * (2 - 2 * cos(y) - y * sin(y));
+        double Sr;
+        if (apm_range == 0.f) Sr = 0;
+        else {
+          y = (double)apm_range * kmag / 2;
+          Sr = 12 / (y * y * y * y) * (2 - 2 * cos(y) - y * sin(y));
+        }
+        for (int d = 0; d < 3; ++d) ur[d] += Uk2 * (kn[d] * (Ss * Ss - Sr * Sr) / (kmag * kmag));
+      }
+  double u2n = 1;
+  const double two15 = (double)(2.f / 15.f);
+  for (int d = 0; d < 3; ++d) {
+    const double s = sin(kv[d] / 2);
+    u2n *= 1 - s * s + two15 * s * s * s * s;
+  }
+  const double num = Dv[0] * ur[0] + Dv[1] * ur[1] + Dv[2] * ur[2];
+  const double den = Dv[0] * Dv[0] + Dv[1] * Dv[1] + Dv[2] * Dv[2];
+  const float gs2 = gridsize * gridsize;
+  double val = (den == 0) ? 0.0 : 4 * PI * num / den / (u2n * u2n) / (double)gs2;
+  const int h = n / 2;
+  if ((k1 % h == 0) && (k2 % h == 0) && (k3 % h == 0)) val = 0.0;  // Green.f90:71
+  Gk[i] = (float)val;
+}
+
+}  // namespace cube

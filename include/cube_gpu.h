@@ -126,12 +126,14 @@ int cube_gpu_kick(cube_ctx* ctx, const cube_step_in* in, cube_step_out* out);
 /* One loop body of main.f90:36-38 (drift, ghosts, kick, ghosts). */
 int cube_gpu_step(cube_ctx* ctx, const cube_step_in* in, cube_step_out* out);
 
-/* Inspection for tests: download the last PM level field.
- * level 1: PM1 density (nc^3) / potential, 2: PM2 tile `box`, 3: PM3 subtile `box`.
- * what 0: density (mass units), 1: potential phi after normalisation,
- *      2: force (3 components interleaved) on cells 0..nforce+1.
- * Fields are written x fastest in the reference index ranges. */
-int cube_gpu_debug_field(cube_ctx* ctx, int level, int box, int what, float* out, int64_t n);
+/* Inspection for tests.  cube_gpu_capture arms a capture: during the next kick the
+ * field `what` (0: density = deposited mass per cell, 1: potential phi after the
+ * inverse FFT and normalisation) of PM level `level` (1: the nc^3 mesh, 2: PM2 tile
+ * `box`, 3: PM3 subtile `box` in initialize.f90:351-367 numbering) is copied aside.
+ * cube_gpu_captured downloads it (x fastest, array index = reference index - m1)
+ * and returns the number of values. */
+int cube_gpu_capture(cube_ctx* ctx, int level, int box, int what);
+int cube_gpu_captured(cube_ctx* ctx, float* out, int64_t n);
 /* Download the Green table of a level (1, 2, or 3 with class iapm 2..5). */
 int cube_gpu_green_table(cube_ctx* ctx, int level, int iapm, float* out, int64_t n);
 /* Download per-subtile PM3 class (ires, kick.f90:108-133), ns3 entries. */

@@ -1,0 +1,172 @@
+"""Parity of the CUDA path (through the C ABI) against the CPU oracle.
+
+Tolerances:
+  * drift (cell sort, arrival order, ZIPX update): bit-exact.
+  * fixed-point deposit (chosen form): bit-exact density.
+  * FP32 deposit: per-cell relative 1e-5 (atomics change the summation order).
+  * potential: max |diff| <= 2e-5 * max |phi| (FP32 FFT rounding vs the oracle's FFT).
+  * velocities after a kick: max |dv_gpu - dv_oracle| <= 2e-4 * max |dv_oracle|.
+"""
+import numpy as np
+import pytest
+
+from cube_nu_b200.params import DEPOSIT_FIXED, DEPOSIT_FP32, config_small
+from tests.helpers import clustered_state, lattice_state, uniform_state
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(izipx=1, fixed=False, n=None, **kw):
+    p = config_small(ng=64, nnt=2, nns=2, np_nc=2, izipx=izipx)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    p.deposit_mode = DEPOSIT_FIXED if fixed else DEPOSIT_FP32
+    p.mass_p_cdm = float(p.ng) ** 3 / float(n if n else p.npglobal)
+    return p
+
+
+def _ctx(p, st):
+    from cube_nu_b200._lib import Context
+
+    ctx = Context(p)
+    ctx.upload(*st)
+    return ctx
+
+
+@pytest.mark.parametrize("level,iapm", [(1, 2), (2, 2), (3, 2), (3, 3), (3, 4), (3, 5)])
+def test_green_tables(oracle_lib, level, iapm):
+    p = _params()
+    st = lattice_state(p, seed=1)
+    with _ctx(p, st) as ctx:
+        g = ctx.green(level, iapm)
+    ref = oracle_lib.green(p, level, iapm)
+    assert g.shape == ref.shape
+    scale = np.abs(ref).max()
+    assert np.abs(g - ref).max() <= 1e-6 * scale
+    assert g.flat[0] == 0.0
+
+
+@pytest.mark.parametrize("izipx", [1, 2])
+@pytest.mark.parametrize("kind", ["uniform", "clustered"])
+def test_drift_bitexact(oracle_lib, izipx, kind):
+    p = _params(izipx=izipx)
+    n = 20000
+    st = uniform_state(p, n, seed=3, vscale=2.0) if kind == "uniform" else clustered_state(p, n, seed=4, vscale=2.0)
+    p.mass_p_cdm = float(p.ng) ** 3 / n
+    vz = float(np.abs(st[1][:, 2]).max())
+    with _ctx(p, st) as ctx:
+        cur = st
+        for step, (dt_old, dt) in enumerate([(0.0, 1.0), (1.0, 0.7), (0.7, 1.3)]):
+            ref = oracle_lib.drift(p, *cur, dt_old, dt, vz)
+            ctx.drift(dt, dt_old, vz)
+            got = ctx.download()
+            for a, b, name in zip(got, ref, ("xp", "vp", "pid", "rhoc")):
+                assert np.array_equal(a, b), "step %d: %s differs at %d entries" % (step, name, int((a != b).sum()))
+            cur = ref
+
+
+def test_drift_long_segments(oracle_lib):
+    """Destination cells with more than 32 arrivals go through the block sorter."""
+    p = _params()
+    n = 30000
+    st = clustered_state(p, n, seed=5, nblob=2, sigma=0.3, frac=0.8, vscale=1.0)
+    assert st[3].max() > 32
+    p.mass_p_cdm = float(p.ng) ** 3 / n
+    vz = float(np.abs(st[1][:, 2]).max())
+    ref = oracle_lib.drift(p, *st, 0.5, 0.5, vz)
+    with _ctx(p, st) as ctx:
+        ctx.drift(0.5, 0.5, vz)
+        got = ctx.download()
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
+
+
+def _field_cases(p):
+    return [(1, 0, p.nc ** 3), (2, 0, p.ngt ** 3), (2, 7, p.ngt ** 3), (3, 0, None), (3, 37, None)]
+
+
+@pytest.mark.parametrize("fixed", [False, True])
+def test_density_and_potential(oracle_lib, fixed):
+    p = _params(fixed=fixed)
+    n = 24000
+    st = clustered_state(p, n, seed=7)
+    p.mass_p_cdm = float(p.ng) ** 3 / n
+    ires, _ = oracle_lib.classify(p, st[3])
+    for level, box, size in _field_cases(p):
+        if size is None:
+            size = p.nft(int(ires[box])) ** 3
+        for what in (0, 1):
+            _, ref = oracle_lib.kick(p, st[0], st[1].copy(), st[3], 0.1, 0.05, fixed=fixed,
+                                     debug=(level, box, what, size))
+            with _ctx(p, st) as ctx:
+                ctx.capture(level, box, what)
+                ctx.kick(0.1, 0.05)
+                got = ctx.captured(size)
+            assert got.size == size
+            if what == 0:
+                if fixed:
+                    assert np.array_equal(got, ref), "fixed-point density differs (level %d box %d)" % (level, box)
+                else:
+                    np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-5 * np.abs(ref).max())
+                assert abs(got.sum() - ref.sum()) <= 1e-5 * abs(ref.sum()) + 1e-3
+            else:
+                err = np.abs(got - ref).max() / np.abs(ref).max()
+                assert err < 2e-5, "phi rel err %.3g (level %d box %d)" % (err, level, box)
+
+
+@pytest.mark.parametrize("izipx,fixed,kind", [(1, False, "lattice"), (2, True, "lattice"), (1, False, "clustered"),
+                                              (2, True, "clustered")])
+def test_kick_matches_oracle(oracle_lib, izipx, fixed, kind):
+    p = _params(izipx=izipx, fixed=fixed)
+    if kind == "lattice":
+        st = lattice_state(p, seed=11, disp=0.3)
+    else:
+        st = clustered_state(p, 30000, seed=12, sigma=0.4)
+    n = st[0].shape[0]
+    p.mass_p_cdm = float(p.ng) ** 3 / n
+    dt, a_mid = 0.2, 0.05
+    v_ref = st[1].copy()
+    out = oracle_lib.kick(p, st[0], v_ref, st[3], dt, a_mid, fixed=fixed)
+    v64 = st[1].astype(np.float64)
+    oracle_lib.kick(p, st[0], v64, st[3], dt, a_mid)
+    with _ctx(p, st) as ctx:
+        so = ctx.kick(dt, a_mid)
+        _, v_gpu, _, _ = ctx.download()
+    dref = v_ref - st[1]
+    scale = np.abs(dref).max()
+    err = np.abs((v_gpu - st[1]) - dref).max() / scale
+    assert err < 2e-4, "kick rel err vs FP32 oracle %.3g" % err
+    err64 = np.abs((v_gpu - st[1]) - (v64 - st[1])).max() / scale
+    assert err64 < 2e-4, "kick rel err vs FP64 oracle %.3g" % err64
+    assert list(so.napm) == list(out.napm)
+    for a, b in ((so.f2max_pm1, out.f2max_pm1), (so.f2max_pm2, out.f2max_pm2), (so.f2max_pm3, out.f2max_pm3)):
+        assert abs(a - b) <= 1e-4 * abs(b)
+    assert abs(so.f2max_pp - out.f2max_pp) <= 1e-3 * abs(out.f2max_pp) + 1e-12
+    assert so.pp_pairs == out.pp_pairs * 2 or out.pp_pairs == 0 or abs(so.pp_pairs - 2 * out.pp_pairs) <= 4
+
+
+def test_step_sequence(oracle_lib):
+    """Three drift+kick steps; positions agree exactly except where a rounded
+    displacement flips because the FP32 kicks differ in their last bits."""
+    p = _params(izipx=2)
+    st = lattice_state(p, seed=21, disp=0.3, vscale=0.5)
+    n = st[0].shape[0]
+    p.mass_p_cdm = float(p.ng) ** 3 / n
+    cur = st
+    vz = float(np.abs(st[1][:, 2]).max())
+    dt_old = 0.0
+    with _ctx(p, st) as ctx:
+        for k in range(3):
+            dt, a_mid = 0.3, 0.05 + 0.01 * k
+            cur = oracle_lib.drift(p, *cur, dt_old, dt, vz)
+            vref = cur[1].copy()
+            out = oracle_lib.kick(p, cur[0], vref, cur[3], dt, a_mid)
+            cur = (cur[0], vref, cur[2], cur[3])
+            so = ctx.step(dt, dt_old, a_mid, vz)
+            vz = out.vz_max
+            dt_old = dt
+        xg, vg, pg, rg = ctx.download()
+    same = np.mean(np.all(xg == cur[0], axis=1))
+    assert same > 0.999
+    assert np.array_equal(rg, cur[3]) or np.abs(rg - cur[3]).sum() <= 0.002 * n
+    assert abs(so.vz_max - out.vz_max) <= 1e-4 * out.vz_max
