@@ -1,0 +1,434 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the P3M KDK step (drift + PM1 + PM2 + PM3 + PP).
+
+Default workload: 512^3 CDM particles in a 1000 Mpc/h box, fine mesh 1024^3
+(PM1 256^3, PM2 64 tiles of 288^3, PM3 subtile meshes of 144^3 and up), int16
+compressed coordinates, Zel'dovich ICs at z=49 (EH no-wiggle, A_s), reference
+adaptive timestep.  One JSON line on rank 0.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload 512|128] [--deposit fixed|plain]
+
+--impl reference times the CPU restatement of the reference path (oracle/, the
+reference Fortran cannot be built here) on the host cores over a bounded sample of
+the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from cube_nu_b200 import cosmology  # noqa: E402
+from cube_nu_b200.params import DEPOSIT_FIXED, DEPOSIT_FP32, config_512, config_plain_128  # noqa: E402
+
+METRIC = "particle-steps/s P3M KDK @512^3"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def workload(name: str):
+    if name == "512":
+        p = config_512()
+        desc = "512^3 CDM, 1000 Mpc/h, fine mesh 1024^3 (PM1 256^3, PM2 64x288^3, PM3 4096 subtiles), int16 ZIPX"
+    else:
+        p = config_plain_128()
+        p.nic = 1
+        desc = "128^3 CDM, 200 Mpc/h, fine mesh 256^3 (PM1 64^3, PM2 64x96^3, PM3 4096 subtiles), int8 ZIPX"
+    return p, desc
+
+
+# ------------------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# ------------------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------
+# algorithmic bytes per kernel launch (roofline numerators)
+# ------------------------------------------------------------------------------------
+def kernel_bytes(p, name: str, n_particles: int, napm, fixed: bool):
+    """Algorithmic HBM bytes one launch of a kernel class must move (documented in DESIGN.md)."""
+    bx = 3 * p.izipx
+    rb = 8 if fixed else 4
+
+    def mesh(n, nbox, what):
+        n3 = n ** 3 * nbox
+        nh = n * n * (n // 2 + 1) * nbox
+        return {"x": n3 * rb + nh * 8, "y": 2 * nh * 8, "z": 2 * nh * 8 + n * n * (n // 2 + 1) * 4,
+                "c": nh * 8 + n3 * 4}[what]
+
+    if name.startswith("fft_") and name.endswith("_pm3"):
+        # one launch per class chunk; use the dominant class (2) with all its subtiles
+        n = p.nft(2)
+        nb = int(napm[2]) if napm is not None else p.ns3
+        what = {"fft_x_pm3": "x", "fft_y_pm3": "y", "fft_z_green_pm3": "z", "fft_c2r_pm3": "c"}[name]
+        return mesh(n, nb, what)
+    if name.startswith("fft_") and name.endswith("_pm2"):
+        what = {"fft_x_pm2": "x", "fft_y_pm2": "y", "fft_z_green_pm2": "z", "fft_c2r_pm2": "c"}[name]
+        return mesh(p.ngt, p.ntiles, what)
+    if name in ("deposit_pm1", "deposit_pm2", "deposit_pm3"):
+        # read position code + cell index per particle, one read-modify-write of 27 cells
+        boxes = {"deposit_pm1": 1.0, "deposit_pm2": (1 + 2 * p.ncb / p.nt) ** 3, "deposit_pm3": (1 + 2 / p.ntt) ** 3}[name]
+        return int(n_particles * (bx + 4 + boxes * 27 * 2 * rb))
+    if name in ("interp_pm1", "interp_pm2", "interp_pm3"):
+        # position code + cell, velocity read+write, 27 force points x 3 (from phi)
+        return int(n_particles * (bx + 4 + 24 + 27 * 4))
+    if name == "pp":
+        return int(n_particles * (bx + 4 + 24))
+    if name in ("drift_dest",):
+        return int(n_particles * (bx + 12 + 4 + 8 + 4 + 4))
+    if name in ("drift_gather",):
+        return int(n_particles * (2 * bx + 24 + 16 + 8))
+    return None
+
+
+# ------------------------------------------------------------------------------------
+# CPU baseline (oracle on the host cores, bounded sample)
+# ------------------------------------------------------------------------------------
+def cpu_baseline(p, st, dt, dt_old, a_mid, vz, frac_tiles=1 / 64):
+    """Time the oracle restatement on a bounded sample of the workload and scale it
+    to one full step.  Returns (particle-steps/s, cores, sample description, seconds)."""
+    from oracle import oracle as O
+
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    xp, vp, pid, rhoc = st
+    n = xp.shape[0]
+    ntiles = p.ntiles
+    tiles = max(1, int(round(ntiles * frac_tiles)))
+    t0 = time.perf_counter()
+    O.drift_sample(p, xp, vp, pid, rhoc, dt_old, dt, vz, tiles)
+    t_drift = time.perf_counter() - t0
+    v = vp.copy()
+    t0 = time.perf_counter()
+    out = O.kick(p, xp, v, rhoc, dt, a_mid, fixed=False, boxes_frac=tiles / ntiles)
+    t_kick = time.perf_counter() - t0
+    scale = ntiles / tiles
+    t_full = t_drift * scale + out.t_pm1 + (out.t_pm2 + out.t_pm3 + out.t_pp) * scale
+    sample = ("oracle FP32 restatement: drift of %d/%d tiles, PM1 full, PM2 %d/%d tiles, PM3+PP %d/%d subtiles; "
+              "scaled to one full step (%.1f s measured)" % (tiles, ntiles, tiles, ntiles, tiles * p.nns ** 3,
+                                                              p.ns3, t_drift + t_kick))
+    return n / t_full, cores, sample, t_drift + t_kick
+
+
+def make_ic(p, seed, device):
+    from cube_nu_b200 import ic
+
+    if p.ng >= 256:
+        d = ic.zeldovich_torch(p, z_i=49.0, seed=seed, device=device)
+    else:
+        d = ic.zeldovich(p, z_i=49.0, seed=seed)
+    p.mass_p_cdm = d["mass_p_cdm"]
+    return d
+
+
+def pinned_like(a):
+    import torch
+
+    t = torch.empty(a.shape, dtype={np.int8: torch.int8, np.int16: torch.int16, np.float32: torch.float32,
+                                    np.int64: torch.int64, np.int32: torch.int32}[a.dtype.type], pin_memory=True)
+    out = t.numpy()
+    out[...] = a
+    return out, t
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="512", choices=["512", "128"])
+    ap.add_argument("--deposit", default="fixed", choices=["fixed", "plain"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-json", default="")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    p, desc = workload(args.workload)
+    fixed = args.deposit == "fixed"
+    p.deposit_mode = DEPOSIT_FIXED if fixed else DEPOSIT_FP32
+
+    import torch
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        run_reference(args, p, desc)
+        return 0
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    d = make_ic(p, seed=1 + rank, device="cuda:%d" % local)
+    n = d["xp"].shape[0]
+    st = (d["xp"], d["vp"], d["pid"], d["rhoc"])
+    from cube_nu_b200._lib import Context
+
+    ctx = Context(p, device=local)
+    ctx.upload(*st)
+    tab = cosmology.expansion_table(p.h0, p.omega_m, p.omega_r)
+    bg = cosmology.Background.from_table(tab)
+    S = cosmology.StepState(a=d["a"], dt_vmax=d["dt_vmax"], vz_max=d["vz_max"])
+    bg.init_cursor(S.a)
+    zck = [49.0, 0.0]
+
+    def one_step():
+        cosmology.timestep(bg, S, zck)
+        so = ctx.step(S.dt, S.dt_old, S.a_mid, S.vz_max)
+        S.dt_pm1, S.dt_pm2, S.dt_pm3, S.dt_pp, S.dt_vmax = so.dt_pm1, so.dt_pm2, so.dt_pm3, so.dt_pp, so.dt_vmax
+        S.vz_max = so.vz_max
+        return so
+
+    first = None
+    for _ in range(args.warmup):
+        so = one_step()
+        first = first or (S.dt, S.dt_old, S.a_mid, S.vz_max)
+    # state at the start of the timed region (for the CPU baseline sample)
+    base_state = ctx.download() if (rank == 0 and not args.no_cpu_baseline) else None
+    base_args = (S.dt, S.dt, S.a_mid, S.vz_max)
+
+    ctx.profile(True)
+    launches0 = ctx.launches()
+    clocks = Clocks(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_wall = time.perf_counter()
+    dev_ms = 0.0
+    stage = np.zeros(7)
+    sos = []
+    for _ in range(args.steps):
+        so = one_step()
+        dev_ms += so.tcat[6]
+        stage += np.array(list(so.tcat)[:7])
+        sos.append(so)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = ctx.launches() - launches0
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    # max over ranks of the device time
+    dev_s = dev_ms / 1e3
+    if dist:
+        tt = torch.tensor([dev_s, t_wall], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dev_s, t_wall = float(tt[0]), float(tt[1])
+    total_particles = n * world
+    value = total_particles * args.steps / dev_s
+
+    # ---------------- end to end through the C ABI with pinned host buffers ----------------
+    xh, xt = pinned_like(st[0])
+    vh, vt = pinned_like(st[1])
+    ph, pt = pinned_like(st[2])
+    rh, rt = pinned_like(st[3])
+    cur = ctx.download()
+    xh[...] = cur[0]
+    vh[...] = cur[1]
+    ph[...] = cur[2]
+    rh[...] = cur[3]
+    from cube_nu_b200._lib import _check, _ptr
+    import ctypes
+
+    lib = ctx._lib
+    nplocal = ctypes.c_int64()
+    e2e_steps = args.steps
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter()
+    for _ in range(e2e_steps):
+        _check(lib.cube_gpu_upload(ctx._h, _ptr(xh), _ptr(vh), _ptr(ph), _ptr(rh), n), "upload")
+        one_step()
+        _check(lib.cube_gpu_download(ctx._h, _ptr(xh), _ptr(vh), _ptr(ph), _ptr(rh), ctypes.byref(nplocal)), "download")
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t_e2e
+    if dist:
+        tt = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt[0])
+    io_bytes = n * (3 * p.izipx + 12 + 8) + p.ncells * 4
+    e2e_value = total_particles * e2e_steps / t_e2e
+
+    if rank == 0:
+        peaks, peak_kind = load_peaks()
+        napm = list(sos[-1].napm)
+        # roofline of the dominant kernel class
+        rows = []
+        for name, (ms, cnt) in prof.items():
+            if cnt == 0:
+                continue
+            b = kernel_bytes(p, name, n, napm, fixed)
+            avg = ms / cnt
+            rows.append((ms, name, cnt, avg, b))
+        rows.sort(reverse=True)
+        dom = next((r for r in rows if r[4] is not None), None)
+        hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+        roof = None
+        if dom:
+            ach = dom[4] / (dom[3] / 1e3) / 1e9
+            roof = {"kernel": dom[1], "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                    "frac": round(ach / hbm, 4), "traffic": None, "peak_kind": peak_kind,
+                    "avg_launch_ms": round(dom[3], 4), "algorithmic_bytes_per_launch": dom[4]}
+        cpu = None
+        if base_state is not None:
+            v, cores, sample, secs = cpu_baseline(p, base_state, *base_args)
+            cpu = {"value": round(v, 1), "unit": "particle-steps/s", "cores": cores, "kind": "port",
+                   "sample": sample}
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_s * 1e3 / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic (Zel'dovich ICs z=49, EH no-wiggle, seeded)",
+            "config": {"workload": desc, "particles_per_gpu": n, "ng": p.ng, "box": p.box,
+                       "deposit": "int64 fixed-point" if fixed else "fp32 atomics",
+                       "timestep": "reference adaptive (timestep.f90)", "parallelism": "replicas x%d" % world,
+                       "l2": "inputs larger than L2 (%.1f GB particle state)" % (n * 26 / 1e9),
+                       "pm3_classes": napm[2:6], "a_end": S.a},
+            "e2e": {"value": round(e2e_value, 1), "unit": "particle-steps/s", "h2d_bytes_per_step": io_bytes,
+                    "d2h_bytes_per_step": io_bytes},
+            "gpu_launches": int(launches),
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "wall_s": round(t_wall, 3),
+            "stage_ms_per_step": {k: round(float(v) / args.steps, 3) for k, v in
+                                  zip(("drift", "pm1", "pm2", "pm3", "pp", "kick", "step"), stage)},
+        }
+        if args.profile_json:
+            with open(args.profile_json, "w") as f:
+                json.dump({"kernels": [{"name": r[1], "total_ms": r[0], "launches": r[2], "avg_ms": r[3],
+                                        "alg_bytes": r[4]} for r in rows], "steps": args.steps}, f, indent=1)
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_reference(args, p, desc):
+    """--impl reference: the CPU restatement timed on the host cores."""
+    import torch
+
+    dev = "cuda:0" if torch.cuda.is_available() else None
+    if dev:
+        d = make_ic(p, seed=1, device=dev)
+    else:
+        from cube_nu_b200 import ic
+
+        d = ic.zeldovich(p, z_i=49.0, seed=1)
+        p.mass_p_cdm = d["mass_p_cdm"]
+    st = (d["xp"], d["vp"], d["pid"], d["rhoc"])
+    n = st[0].shape[0]
+    tab = cosmology.expansion_table(p.h0, p.omega_m, p.omega_r)
+    bg = cosmology.Background.from_table(tab)
+    S = cosmology.StepState(a=d["a"], dt_vmax=d["dt_vmax"], vz_max=d["vz_max"])
+    bg.init_cursor(S.a)
+    cosmology.timestep(bg, S, [49.0, 0.0])
+    rates = []
+    cores = os.cpu_count() or 1
+    sample = ""
+    for i in range(args.warmup + args.steps):
+        v, cores, sample, secs = cpu_baseline(p, st, S.dt, S.dt_old, S.a_mid, S.vz_max)
+        if i >= args.warmup:
+            rates.append(v)
+        if i == 0 and secs * (args.warmup + args.steps) > 240:
+            # keep the whole run within a few minutes: one warm-up, one timed sample
+            args.warmup, args.steps = 0, 1
+            rates.append(v)
+            break
+    value = float(np.mean(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": "particle-steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(n / value * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic (Zel'dovich ICs z=49, EH no-wiggle, seeded)",
+        "config": {"workload": desc, "particles_per_gpu": n, "ng": p.ng, "box": p.box,
+                   "timestep": "reference adaptive (timestep.f90)",
+                   "reference": "CPU restatement of the reference Fortran path (gfortran/FFTW absent)"},
+        "cpu_baseline": {"value": round(value, 1), "unit": "particle-steps/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(value, 1), "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

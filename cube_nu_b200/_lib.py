@@ -19,6 +19,7 @@ EXPORTS = (
     "cube_params_default", "cube_gpu_create", "cube_gpu_destroy", "cube_gpu_upload", "cube_gpu_download",
     "cube_gpu_drift", "cube_gpu_kick", "cube_gpu_step", "cube_gpu_capture", "cube_gpu_captured",
     "cube_gpu_green_table", "cube_gpu_subtile_class", "cube_gpu_last_error", "cube_gpu_version",
+    "cube_gpu_profile", "cube_gpu_profile_read", "cube_gpu_profile_name", "cube_gpu_kernel_launches",
 )
 
 
@@ -65,6 +66,12 @@ def load():
     L.cube_gpu_subtile_class.argtypes = [vp, vp, ctypes.c_int64]
     L.cube_gpu_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     L.cube_gpu_version.restype = ctypes.c_char_p
+    L.cube_gpu_profile.argtypes = [vp, ctypes.c_int]
+    L.cube_gpu_profile_read.argtypes = [vp, vp, vp, ctypes.c_int]
+    L.cube_gpu_profile_name.argtypes = [ctypes.c_int]
+    L.cube_gpu_profile_name.restype = ctypes.c_char_p
+    L.cube_gpu_kernel_launches.argtypes = [vp]
+    L.cube_gpu_kernel_launches.restype = ctypes.c_int64
     _LIB = L
     return L
 
@@ -165,6 +172,19 @@ class Context:
         out = np.empty((n, n, n // 2 + 1), dtype=np.float32)
         _check(self._lib.cube_gpu_green_table(self._h, level, iapm, _ptr(out), out.size), "cube_gpu_green_table")
         return out
+
+    def profile(self, enable: bool = True) -> None:
+        _check(self._lib.cube_gpu_profile(self._h, int(enable)), "cube_gpu_profile")
+
+    def profile_read(self) -> dict:
+        """{kernel class: (total ms, launches)} since profile(True)."""
+        ms = np.zeros(64, dtype=np.float64)
+        cnt = np.zeros(64, dtype=np.int64)
+        k = _check(self._lib.cube_gpu_profile_read(self._h, _ptr(ms), _ptr(cnt), 64), "cube_gpu_profile_read")
+        return {self._lib.cube_gpu_profile_name(i).decode(): (float(ms[i]), int(cnt[i])) for i in range(k)}
+
+    def launches(self) -> int:
+        return int(self._lib.cube_gpu_kernel_launches(self._h))
 
     def subtile_class(self) -> np.ndarray:
         out = np.empty(self.params.ns3, dtype=np.int32)

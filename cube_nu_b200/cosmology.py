@@ -48,18 +48,17 @@ def expansion_table(h0: float, om: float, orad: float, n: int = ISTEP_MAX, a_sto
         if a[i + 1] <= a_stop:
             i_end = i + 1
             break
-    # conformal time tau(a) = int_0^a da / (a^2 H), units of Mpc/(km/s)
-    tau = np.zeros(n)
+    # conformal time tau(a) = int_0^a da / (a^2 H) in Mpc/(km/s): analytic below the last
+    # table entry (radiation + matter), cumulative trapezoid along the table above it
     aa = a[: i_end + 1]
-    grid = np.linspace(0, 1, 20001) ** 2
-    for i, ai in enumerate(aa):
-        x = grid * ai
-        y = np.zeros_like(x)
-        m = x > 0
-        y[m] = 1.0 / (x[m] ** 2 * hubble(x[m], h0, om, orad, ol))
-        # integrand ~ 1/sqrt(orad) H0 near 0 (finite)
-        y[~m] = 1.0 / (100.0 * h0 * math.sqrt(orad))
-        tau[i] = np.trapezoid(y, x)
+    H0 = 100.0 * h0
+    a_last = aa[-1]
+    tau_last = 2.0 / (H0 * om) * (math.sqrt(orad + om * a_last) - math.sqrt(orad))
+    integ = 1.0 / (aa ** 2 * hubble(aa, h0, om, orad, ol))
+    seg = 0.5 * (integ[1:] + integ[:-1]) * (aa[:-1] - aa[1:])
+    cum = np.concatenate([[0.0], np.cumsum(seg[::-1])])[::-1]
+    tau = np.full(n, 0.0)
+    tau[: i_end + 1] = tau_last + cum
     tau[i_end + 1:] = tau[0]
     return np.array([t, a, tau, H], dtype=np.float64)
 
@@ -136,7 +135,7 @@ class StepState:
     dt_vmax: float = 1e3
     vz_max: float = 0.0
     a_mid: float = 0.0
-    cur_checkpoint: int = 1
+    cur_checkpoint: int = 2  # next target; main.f90:19 steps past the checkpoint it resumed from
     checkpoint_step: bool = False
     final_step: bool = False
 

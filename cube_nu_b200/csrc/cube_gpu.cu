@@ -49,6 +49,23 @@ struct FFTTable {
   FFTDesc desc;
 };
 
+// Kernel classes for the opt-in event timers (cube_gpu_profile).
+enum KClass {
+  K_DRIFT_DEST, K_DRIFT_SCATTER, K_DRIFT_SORT, K_DRIFT_GATHER, K_SCAN, K_DEP_PM1, K_FFT_PM1, K_F2_PM1, K_INT_PM1,
+  K_DEP_PM2, K_FFTX_PM2, K_FFTY_PM2, K_FFTZ_PM2, K_FFTC_PM2, K_F2_PM2, K_INT_PM2, K_DEP_PM3, K_FFTX_PM3, K_FFTY_PM3,
+  K_FFTZ_PM3, K_FFTC_PM3, K_F2_PM3, K_INT_PM3, K_PP, K_CLASSIFY, K_GREEN, K_FILL, K_NCLASS
+};
+const char* const KNAMES[K_NCLASS] = {
+    "drift_dest", "drift_scatter", "drift_sort", "drift_gather", "scan", "deposit_pm1", "fft_pm1", "f2max_pm1",
+    "interp_pm1", "deposit_pm2", "fft_x_pm2", "fft_y_pm2", "fft_z_green_pm2", "fft_c2r_pm2", "f2max_pm2",
+    "interp_pm2", "deposit_pm3", "fft_x_pm3", "fft_y_pm3", "fft_z_green_pm3", "fft_c2r_pm3", "f2max_pm3",
+    "interp_pm3", "pp", "classify", "green", "fill_pcell"};
+
+struct ProfRec {
+  int cls;
+  int a, b;  // event pool indices
+};
+
 }  // namespace
 
 struct cube_ctx {
@@ -93,9 +110,63 @@ struct cube_ctx {
   int64_t cap_n = 0;
   // timing
   cudaEvent_t ev[8];
+  // opt-in per-kernel timers and the launch counter
+  bool prof = false;
+  std::vector<cudaEvent_t> pool;
+  int pool_used = 0;
+  std::vector<ProfRec> pending;
+  double prof_ms[K_NCLASS] = {0};
+  int64_t prof_n[K_NCLASS] = {0};
+  int64_t launches = 0;
 };
 
 namespace {
+
+int pool_event(cube_ctx* c) {
+  if (c->pool_used == (int)c->pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c->pool.push_back(e);
+  }
+  return c->pool_used++;
+}
+
+void prof_begin(cube_ctx* c, int cls, int nlaunch, int& a) {
+  c->launches += nlaunch;
+  a = -1;
+  if (!c->prof) return;
+  a = pool_event(c);
+  cudaEventRecord(c->pool[a], c->s);
+  (void)cls;
+}
+
+void prof_end(cube_ctx* c, int cls, int a) {
+  if (!c->prof || a < 0) return;
+  const int b = pool_event(c);
+  cudaEventRecord(c->pool[b], c->s);
+  c->pending.push_back({cls, a, b});
+}
+
+// After a stream synchronisation: fold the pending event pairs into the totals.
+void prof_collect(cube_ctx* c) {
+  for (const ProfRec& r : c->pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c->pool[r.a], c->pool[r.b]) == cudaSuccess) {
+      c->prof_ms[r.cls] += ms;
+      c->prof_n[r.cls] += 1;
+    }
+  }
+  c->pending.clear();
+  c->pool_used = 0;
+}
+
+#define LAUNCH(c, cls, nl, ...)     \
+  do {                              \
+    int a_;                         \
+    prof_begin((c), (cls), (nl), a_); \
+    __VA_ARGS__;                    \
+    prof_end((c), (cls), a_);       \
+  } while (0)
 
 const FFTDesc* fft_desc(cube_ctx* c, int n) {
   for (auto& t : c->ffts)
@@ -186,7 +257,11 @@ int64_t boxes_fit(cube_ctx* c, int n, bool fixed) {
 }
 
 void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out,
-                float2* ck, const float* green, float norm, int reps) {
+                float2* ck, const float* green, float norm, int reps, int level) {
+  const int kx = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTX_PM2 : K_FFTX_PM3;
+  const int ky = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTY_PM2 : K_FFTY_PM3;
+  const int kz = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTZ_PM2 : K_FFTZ_PM3;
+  const int kc = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTC_PM2 : K_FFTC_PM3;
   const FFTDesc& D = *fft_desc(c, n);
   const int nh = n / 2 + 1;
   const int64_t nrows = nbox * (int64_t)n * n;
@@ -194,16 +269,16 @@ void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixe
   const size_t smx = (size_t)(n + 2 * rpb * n) * sizeof(float2);
   const unsigned gx = (unsigned)((nrows + rpb - 1) / rpb);
   if (fixed)
-    k_fft_x_r2c<long long><<<gx, 256, smx, c->s>>>((const long long*)real_in, ck, nrows, D, rpb, scale);
+    LAUNCH(c, kx, 1, k_fft_x_r2c<long long><<<gx, 256, smx, c->s>>>((const long long*)real_in, ck, nrows, D, rpb, scale));
   else
-    k_fft_x_r2c<float><<<gx, 256, smx, c->s>>>((const float*)real_in, ck, nrows, D, rpb, scale);
+    LAUNCH(c, kx, 1, k_fft_x_r2c<float><<<gx, 256, smx, c->s>>>((const float*)real_in, ck, nrows, D, rpb, scale));
   const int W = (n <= 256) ? 16 : (n <= 512 ? 8 : 4);
   const size_t smy = (size_t)(n + 2 * W * n) * sizeof(float2);
   dim3 gy((unsigned)(nbox * n), (unsigned)((nh + W - 1) / W));
-  k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1);
-  k_fft_z_green<<<gy, 256, smy, c->s>>>(ck, green, D, W);
-  k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1);
-  k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, norm, reps);
+  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1));
+  LAUNCH(c, kz, 1, k_fft_z_green<<<gy, 256, smy, c->s>>>(ck, green, D, W));
+  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1));
+  LAUNCH(c, kc, 1, k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, norm, reps));
 }
 
 inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
@@ -212,7 +287,7 @@ int build_green(cube_ctx* c, float** dst, int n, float soft, float range, float 
   if (*dst) return 0;
   const int64_t m = (int64_t)n * n * (n / 2 + 1);
   CK(cudaMalloc(dst, m * sizeof(float)));
-  k_green<<<nblk(m, 128), 128, 0, c->s>>>(*dst, n, soft, range, gs);
+  LAUNCH(c, K_GREEN, 1, k_green<<<nblk(m, 128), 128, 0, c->s>>>(*dst, n, soft, range, gs));
   CK(cudaGetLastError());
   return 0;
 }
@@ -354,6 +429,7 @@ int cube_gpu_destroy(cube_ctx* c) {
   if (c->h_slots) cudaFreeHost(c->h_slots);
   for (int i = 0; i < 8; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
   if (c->s) cudaStreamDestroy(c->s);
   delete c;
   return 0;
@@ -409,8 +485,8 @@ int cube_gpu_upload(cube_ctx* c, const void* xp, const float* vp, const int64_t*
   CK(cudaMemcpyAsync(c->vp, vp, (size_t)nplocal * 12, cudaMemcpyHostToDevice, c->s));
   CK(cudaMemcpyAsync(c->pid, pid, (size_t)nplocal * 8, cudaMemcpyHostToDevice, c->s));
   CK(cudaMemcpyAsync(c->rhoc, rhoc, (size_t)G.ncells * 4, cudaMemcpyHostToDevice, c->s));
-  exclusive_scan(c->rhoc, c->cstart, G.ncells, c->scan_tmp, c->s);
-  k_fill_pcell<<<nblk(G.ncells), 256, 0, c->s>>>(c->cstart, G.ncells, c->pcell);
+  LAUNCH(c, K_SCAN, 3, exclusive_scan(c->rhoc, c->cstart, G.ncells, c->scan_tmp, c->s));
+  LAUNCH(c, K_FILL, 1, k_fill_pcell<<<nblk(G.ncells), 256, 0, c->s>>>(c->cstart, G.ncells, c->pcell));
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->s));
   c->loaded = true;
@@ -455,28 +531,29 @@ static int drift_enqueue(cube_ctx* c, const cube_step_in* in) {
   CK(cudaMemsetAsync(c->rhoc2, 0, G.ncells * 4, c->s));
   CK(cudaMemsetAsync(c->fill, 0, G.ncells * 4, c->s));
   CK(cudaMemsetAsync(c->nbig, 0, 4, c->s));
-  k_drift_dest<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->vp, c->pcell, c->cstart, dt_mid, nlayer, c->dest, c->key,
-                                           c->rhoc2, c->err);
-  exclusive_scan(c->rhoc2, c->cstart2, G.ncells, c->scan_tmp, c->s);
-  k_drift_scatter<<<nblk(np), 256, 0, c->s>>>(np, c->dest, c->key, c->cstart2, c->fill, c->skey, c->ssrc);
-  k_drift_sort_small<<<nblk(G.ncells * 32), 256, 0, c->s>>>(G.ncells, c->rhoc2, c->cstart2, c->skey, c->ssrc,
-                                                            c->biglist, c->nbig);
+  LAUNCH(c, K_DRIFT_DEST, 1, k_drift_dest<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->vp, c->pcell, c->cstart, dt_mid, nlayer, c->dest, c->key,
+                                           c->rhoc2, c->err));
+  LAUNCH(c, K_SCAN, 3, exclusive_scan(c->rhoc2, c->cstart2, G.ncells, c->scan_tmp, c->s));
+  LAUNCH(c, K_DRIFT_SCATTER, 1, k_drift_scatter<<<nblk(np), 256, 0, c->s>>>(np, c->dest, c->key, c->cstart2, c->fill, c->skey, c->ssrc));
+  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_small<<<nblk(G.ncells * 32), 256, 0, c->s>>>(G.ncells, c->rhoc2, c->cstart2, c->skey, c->ssrc,
+                                                            c->biglist, c->nbig));
   const int max_seg = c->P.max_segment > 0 ? std::min(c->P.max_segment, 16384) : 16384;
   // One block per listed long segment; the grid is bounded by the cell count.
   int nb_host = 0;
   CK(cudaMemcpyAsync(&nb_host, c->nbig, 4, cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
   if (nb_host > 0)
-    k_drift_sort_big<<<nb_host, 512, (size_t)max_seg * 12, c->s>>>(c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey,
-                                                                    c->ssrc, max_seg, c->err);
-  k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp, c->pid, dt_mid, c->xp2, c->vp2,
-                                             c->pid2, c->pcell2);
+    LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nb_host, 512, (size_t)max_seg * 12, c->s>>>(c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey,
+                                                                    c->ssrc, max_seg, c->err));
+  LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp, c->pid, dt_mid, c->xp2, c->vp2,
+                                             c->pid2, c->pcell2));
   CK(cudaGetLastError());
   int rc = check_err(c);
   if (rc) return rc;
   int64_t total = 0;
   CK(cudaMemcpyAsync(&total, c->cstart2 + G.ncells, 8, cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
+  prof_collect(c);
   if (total != np) return fail(CUBE_E_COUNT, "drift: particle count not conserved");
   std::swap(c->xp, c->xp2);
   std::swap(c->vp, c->vp2);
@@ -518,14 +595,14 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     MeshPtrs m = mesh_ptrs(c, n, 1, fixed);
     const int64_t n3 = (int64_t)n * n * n;
     CK(cudaMemsetAsync(m.real, 0, n3 * (fixed ? 8 : 4), c->s));
-    if (fixed) k_deposit_pm1<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real);
-    else k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real);
+    if (fixed) LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real));
+    else LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real));
     maybe_capture(c, 1, 0, 0, m.real, n3, fixed);
     float* phi = reinterpret_cast<float*>(m.real);
-    launch_fft(c, n, 1, m.real, fixed, G.mass_p, phi, m.ck, c->green1, (float)n, 3);
+    launch_fft(c, n, 1, m.real, fixed, G.mass_p, phi, m.ck, c->green1, (float)n, 3, 1);
     maybe_capture(c, 1, 0, 1, phi, n3, false);
-    k_f2max_periodic<<<nblk(n3), 256, 0, c->s>>>(phi, n, f2 + 0);
-    k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, a_mid, dt);
+    LAUNCH(c, K_F2_PM1, 1, k_f2max_periodic<<<nblk(n3), 256, 0, c->s>>>(phi, n, f2 + 0));
+    LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, a_mid, dt));
   }
   CK(cudaEventRecord(c->ev[1], c->s));
   // ---------------- PM2 (kick.f90:47-77) ----------------
@@ -537,22 +614,22 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       const int nb = (int)std::min<int64_t>(per, c->ntiles - t0);
       MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
       CK(cudaMemsetAsync(m.real, 0, nb * n3 * (fixed ? 8 : 4), c->s));
-      if (fixed) k_deposit_pm2<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb);
-      else k_deposit_pm2<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb);
+      if (fixed) LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb));
+      else LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb));
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
         maybe_capture(c, 2, c->cap_box, 0, (char*)m.real + (c->cap_box - t0) * n3 * (fixed ? 8 : 4), n3, fixed);
       float* phi = reinterpret_cast<float*>(m.real);
-      launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, c->green2, (float)n * (float)n * (float)n, 1);
+      launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, c->green2, (float)n * (float)n * (float)n, 1, 2);
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
         maybe_capture(c, 2, c->cap_box, 1, phi + (c->cap_box - t0) * n3, n3, false);
-      k_f2max_box<<<nblk((int64_t)G.ngp * G.ngp * G.ngp * nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1);
-      k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, a_mid, dt, vm + 0, c->err);
+      LAUNCH(c, K_F2_PM2, 1, k_f2max_box<<<nblk((int64_t)G.ngp * G.ngp * G.ngp * nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1));
+      LAUNCH(c, K_INT_PM2, 1, k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, a_mid, dt, vm + 0, c->err));
     }
   }
   CK(cudaEventRecord(c->ev[2], c->s));
   // ---------------- subtile classes (kick.f90:108-138) ----------------
   CK(cudaMemsetAsync(c->napm, 0, 32, c->s));
-  k_classify<<<nblk(c->ns3), 256, 0, c->s>>>(G, c->rhoc, c->ns3, c->ires, c->napm);
+  LAUNCH(c, K_CLASSIFY, 1, k_classify<<<nblk(c->ns3), 256, 0, c->s>>>(G, c->rhoc, c->ns3, c->ires, c->napm));
   std::vector<int32_t> ires(c->ns3);
   int32_t napm[8];
   CK(cudaMemcpyAsync(ires.data(), c->ires, c->ns3 * 4, cudaMemcpyDeviceToHost, c->s));
@@ -596,19 +673,19 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       const int32_t* slots = c->box_slot + k * c->ns3;
       MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
       CK(cudaMemsetAsync(m.real, 0, nb * n3 * (fixed ? 8 : 4), c->s));
-      if (fixed) k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err);
-      else k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err);
+      if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err));
+      else LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err));
       int cap_slot = -1;
       if (c->cap_level == 3 && c->cap_box >= 0 && c->cap_box < c->ns3 && ires[c->cap_box] == cl)
         cap_slot = c->h_slots[k * c->ns3 + c->cap_box];
       if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 0, (char*)m.real + cap_slot * n3 * (fixed ? 8 : 4), n3, fixed);
       float* phi = reinterpret_cast<float*>(m.real);
-      launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, g3, (float)n * (float)n * (float)n, 1);
+      launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, g3, (float)n * (float)n * (float)n, 1, 3);
       if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 1, phi + cap_slot * n3, n3, false);
       const int nf = G.nfp[cl];
-      k_f2max_box<<<nblk((int64_t)nf * nf * nf * nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2);
-      k_interp_pm3<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp, a_mid, dt, vm + 3,
-                                                c->err);
+      LAUNCH(c, K_F2_PM3, 1, k_f2max_box<<<nblk((int64_t)nf * nf * nf * nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2));
+      LAUNCH(c, K_INT_PM3, 1, k_interp_pm3<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp, a_mid, dt, vm + 3,
+                                                c->err));
     }
   }
   CK(cudaEventRecord(c->ev[3], c->s));
@@ -618,8 +695,8 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
                                  ? (float)((double)G.mass_p * ((1.0 - (double)G.f_nu) * (1.0 - (double)G.f_nu)))
                                  : G.mass_p;
     const float v_scale = (float)((double)(a_mid * dt / 6.f) / M_PI);
-    k_pp<<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->xp, c->pcell, c->cstart, c->ires, c->vp, mass_scale, v_scale,
-                                          f2 + 3, vm + 6, c->pairs);
+    LAUNCH(c, K_PP, 1, k_pp<<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->xp, c->pcell, c->cstart, c->ires, c->vp, mass_scale, v_scale,
+                                          f2 + 3, vm + 6, c->pairs));
   }
   CK(cudaEventRecord(c->ev[4], c->s));
   CK(cudaGetLastError());
@@ -628,6 +705,7 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
   CK(cudaMemcpyAsync(red, c->red, sizeof(red), cudaMemcpyDeviceToHost, c->s));
   CK(cudaMemcpyAsync(&pairs, c->pairs, 8, cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
+  prof_collect(c);
   int rc = check_err(c);
   if (rc) return rc;
   if (out) {
@@ -663,23 +741,48 @@ int cube_gpu_step(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
   if (!c || !in) return fail(CUBE_E_ARG, "null argument");
   if (!c->loaded) return fail(CUBE_E_STATE, "step before upload");
   CK(cudaSetDevice(c->device));
-  cudaEvent_t a, b;
-  CK(cudaEventCreate(&a));
-  CK(cudaEventCreate(&b));
-  CK(cudaEventRecord(a, c->s));
+  // ev[5]: step start, ev[6]: drift end, ev[7]: step end (all on the context stream)
+  CK(cudaEventRecord(c->ev[5], c->s));
   int rc = drift_enqueue(c, in);
-  CK(cudaEventRecord(b, c->s));
+  CK(cudaEventRecord(c->ev[6], c->s));
   if (!rc) rc = cube_gpu_kick(c, in, out);
+  CK(cudaEventRecord(c->ev[7], c->s));
+  CK(cudaEventSynchronize(c->ev[7]));
   if (!rc && out) {
     float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
+    cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]);
     out->tcat[0] = ms;
     out->tcat[5] += ms;
+    cudaEventElapsedTime(&ms, c->ev[5], c->ev[7]);
+    out->tcat[6] = ms;  // whole step on the device, host gaps included
   }
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
   return rc;
 }
+
+int cube_gpu_profile(cube_ctx* c, int enable) {
+  if (!c) return fail(CUBE_E_ARG, "null context");
+  CK(cudaStreamSynchronize(c->s));
+  prof_collect(c);
+  c->prof = enable != 0;
+  for (int i = 0; i < K_NCLASS; ++i) {
+    c->prof_ms[i] = 0;
+    c->prof_n[i] = 0;
+  }
+  return 0;
+}
+
+int cube_gpu_profile_read(cube_ctx* c, double* ms, int64_t* count, int n) {
+  if (!c) return fail(CUBE_E_ARG, "null context");
+  for (int i = 0; i < n && i < K_NCLASS; ++i) {
+    if (ms) ms[i] = c->prof_ms[i];
+    if (count) count[i] = c->prof_n[i];
+  }
+  return K_NCLASS;
+}
+
+const char* cube_gpu_profile_name(int i) { return (i >= 0 && i < K_NCLASS) ? KNAMES[i] : ""; }
+
+int64_t cube_gpu_kernel_launches(cube_ctx* c) { return c ? c->launches : -1; }
 
 int cube_gpu_capture(cube_ctx* c, int level, int box, int what) {
   if (!c) return fail(CUBE_E_ARG, "null context");
@@ -731,7 +834,7 @@ int cube_gpu_subtile_class(cube_ctx* c, int32_t* ires, int64_t n) {
   if (!c || !ires || n < c->ns3) return fail(CUBE_E_ARG, "bad argument");
   CK(cudaSetDevice(c->device));
   CK(cudaMemsetAsync(c->napm, 0, 32, c->s));
-  k_classify<<<nblk(c->ns3), 256, 0, c->s>>>(c->G, c->rhoc, c->ns3, c->ires, c->napm);
+  LAUNCH(c, K_CLASSIFY, 1, k_classify<<<nblk(c->ns3), 256, 0, c->s>>>(c->G, c->rhoc, c->ns3, c->ires, c->napm));
   CK(cudaMemcpyAsync(ires, c->ires, c->ns3 * 4, cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
   return 0;

@@ -166,3 +166,111 @@ def zeldovich(p: Params, z_i: float = 49.0, seed: int = 1, use_torch: bool = Fal
         "vz_max": float(vmax3[2]),
         "dt_vmax": float(np.float32(0.9) * 16.0 / np.float32(max(vmax3.max(), 1e-30))),
     }
+
+
+def zeldovich_torch(p: Params, z_i: float = 49.0, seed: int = 1, device: str = "cuda"):
+    """The same recipe as :func:`zeldovich`, computed with torch on a GPU for large
+    grids (FP32 FFTs).  Noise comes from torch's seeded Philox generator, so the
+    realisation differs from the numpy path.  Returns host numpy arrays."""
+    import torch
+
+    p.validate()
+    a = 1.0 / (1.0 + z_i)
+    nic, rcs, npnc = p.nic, p.ratio_cs, p.np_nc
+    nw = nic * p.ng
+    dev = torch.device(device)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(int(seed))
+    with torch.no_grad():
+        u = torch.rand((nw, nw, nw), generator=gen, device=dev, dtype=torch.float32)
+        th = 2 * math.pi * u[..., 0::2]
+        r = torch.sqrt(-2 * torch.log1p(-u[..., 1::2]))
+        g = torch.empty_like(u)
+        g[..., 0::2] = r * torch.cos(th)
+        g[..., 1::2] = r * torch.sin(th)
+        del u, th, r
+        ck = torch.fft.rfftn(g, dim=(0, 1, 2))
+        del g
+        k1 = torch.fft.fftfreq(nw, d=1.0 / nw, device=dev, dtype=torch.float64)
+        kx = torch.arange(nw // 2 + 1, device=dev, dtype=torch.float64)
+        s1 = (2 * torch.sin(math.pi * k1 / nw)) ** 2
+        sx = (2 * torch.sin(math.pi * kx / nw)) ** 2
+        for iz in range(nw):  # plane by plane to bound memory
+            kr = 2 * math.pi * torch.sqrt(kx[None, :] ** 2 + k1[:, None] ** 2 + k1[iz] ** 2) / p.box
+            P = torch.from_numpy(cosmology.linear_power(kr.cpu().numpy(), a, p)).to(dev)
+            tf = torch.sqrt(P * (nw / p.box) ** 3)
+            kd = torch.clamp(sx[None, :] + s1[:, None] + s1[iz], min=1.0 / nw ** 2)
+            mult = tf * (-4 * math.pi / kd)
+            if iz == 0:
+                mult[0, 0] = 0.0
+            ck[iz] *= mult.to(torch.float32)
+        phi = torch.fft.irfftn(ck, s=(nw, nw, nw), dim=(0, 1, 2))
+        del ck
+        nlat = p.nc * npnc
+        step = rcs * nic // npnc
+        idx = torch.arange(nlat, device=dev) * step
+        im = (idx - 1) % nw
+        i0 = idx % nw
+        grad = torch.zeros((nlat, nlat, nlat, 3), device=dev, dtype=torch.float32)
+        for bz, zs in ((0, im), (1, i0)):
+            for by, ys in ((0, im), (1, i0)):
+                for bx, xs in ((0, im), (1, i0)):
+                    blk = phi.index_select(0, zs).index_select(1, ys).index_select(2, xs)
+                    grad[..., 0] += 0.5 * (1 if bx else -1) * blk
+                    grad[..., 1] += 0.5 * (1 if by else -1) * blk
+                    grad[..., 2] += 0.5 * (1 if bz else -1) * blk
+                    del blk
+        del phi
+        vf = cosmology.vfactor(a, p.omega_m, p.omega_l)
+        grad_max = (grad.abs().amax(dim=(0, 1, 2)) * 2.0).cpu().numpy()
+        vmax3 = grad_max / (8 * nic * math.pi) * vf
+        lat = torch.arange(nlat, device=dev, dtype=torch.float64) / npnc + (0.5 / nic) / rcs
+        X = torch.empty((nlat, nlat, nlat, 3), device=dev, dtype=torch.float64)
+        X[..., 0] = lat[None, None, :]
+        X[..., 1] = lat[None, :, None]
+        X[..., 2] = lat[:, None, None]
+        X -= grad.double() / (8 * nic * math.pi * rcs)
+        vel = (-grad / (8 * math.pi * nic) * vf).reshape(-1, 3)
+        del grad
+        X = X.reshape(-1, 3)
+        cell = torch.floor(X).long()
+        cellw = cell % p.nc
+        li = torch.arange(nlat, device=dev)
+        lz, ly, lx = torch.meshgrid(li, li, li, indexing="ij")
+        lat_idx = torch.stack([lx.reshape(-1), ly.reshape(-1), lz.reshape(-1)], dim=-1)
+        del lz, ly, lx
+        iq = (lat_idx * (rcs // npnc)) % p.ng
+        pid = iq[:, 0] + p.ng * iq[:, 1] + p.ng * p.ng * iq[:, 2] + 1
+        nt = p.nt
+        npt = nt * npnc
+        npb = npnc
+        tile = cellw // nt
+        lat_loc = (lat_idx - tile * npt + npb) % nlat - npb
+        nlayer = 2 * int(math.ceil(float(grad_max[2]) * npnc / (8 * nic * math.pi * rcs))) + 3
+        kk = lat_loc[:, 2] + npb
+        span = npt + 2 * npb
+        key = (((kk % nlayer) * span + kk) * span + (lat_loc[:, 1] + npb)) * span + (lat_loc[:, 0] + npb)
+        loc = cellw - tile * nt
+        order_cell = ((((tile[:, 2] * p.nnt + tile[:, 1]) * p.nnt + tile[:, 0]) * nt + loc[:, 2]) * nt
+                      + loc[:, 1]) * nt + loc[:, 0]
+        kmax = int(key.max().item()) + 1
+        perm = torch.argsort(order_cell * kmax + key)
+        xres = 2.0 ** (-8 * p.izipx)
+        mod = 1 << (8 * p.izipx)
+        code = torch.floor(X / xres).long() % mod
+        code = torch.where(code >= mod // 2, code - mod, code)
+        rhoc = torch.bincount(order_cell, minlength=p.ncells).int()
+        xdt = torch.int8 if p.izipx == 1 else torch.int16
+        out = {
+            "xp": code[perm].to(xdt).cpu().numpy(),
+            "vp": vel[perm].cpu().numpy(),
+            "pid": pid[perm].cpu().numpy(),
+            "rhoc": rhoc.cpu().numpy(),
+            "a": a,
+            "mass_p_cdm": float(p.ng) ** 3 / float(nlat ** 3),
+            "vz_max": float(vmax3[2]),
+            "dt_vmax": float(np.float32(0.9) * 16.0 / np.float32(max(vmax3.max(), 1e-30))),
+        }
+    del X, vel, cell, cellw, lat_idx, iq, pid, tile, lat_loc, kk, key, loc, order_cell, perm, code, rhoc
+    torch.cuda.empty_cache()
+    return out

@@ -98,7 +98,7 @@ typedef struct cube_step_out {
   int32_t napm[8];                              /* PM3 class histogram, index 2..5 (kick.f90:132) */
   int64_t nplocal;
   int64_t pp_pairs;                             /* in-range PP pairs evaluated (both orders)  */
-  float tcat[16];                               /* stage times in ms: 0 drift,1 PM1,2 PM2,3 PM3,4 PP,5 whole */
+  float tcat[16];                               /* stage ms: 0 drift,1 PM1,2 PM2,3 PM3,4 PP,5 sum, 6 step wall on device */
 } cube_step_out;
 
 typedef struct cube_ctx cube_ctx;
@@ -134,6 +134,16 @@ int cube_gpu_step(cube_ctx* ctx, const cube_step_in* in, cube_step_out* out);
  * and returns the number of values. */
 int cube_gpu_capture(cube_ctx* ctx, int level, int box, int what);
 int cube_gpu_captured(cube_ctx* ctx, float* out, int64_t n);
+/* Opt-in per-kernel timers: CUDA events around every kernel launch on the context's
+ * stream.  cube_gpu_profile(ctx, 1) resets and enables them; cube_gpu_profile_read
+ * fills accumulated milliseconds and launch counts per kernel class (names from
+ * cube_gpu_profile_name) and returns the number of classes. */
+int cube_gpu_profile(cube_ctx* ctx, int enable);
+int cube_gpu_profile_read(cube_ctx* ctx, double* ms, int64_t* count, int n);
+const char* cube_gpu_profile_name(int i);
+/* Number of kernels this context has launched since creation. */
+int64_t cube_gpu_kernel_launches(cube_ctx* ctx);
+
 /* Download the Green table of a level (1, 2, or 3 with class iapm 2..5). */
 int cube_gpu_green_table(cube_ctx* ctx, int level, int iapm, float* out, int64_t n);
 /* Download per-subtile PM3 class (ires, kick.f90:108-133), ns3 entries. */

@@ -183,13 +183,13 @@ static void green_3d(float* Gk, int64_t nglobal, float apm_soft, float apm_range
 template <class XT, class VT>
 static int64_t drift_impl(const Geo& G, const XT* xp, const VT* vp, const int64_t* pid,
                           const int32_t* rhoc, float dt_old, float dt, float vz_max, XT* xo, VT* vo,
-                          int64_t* po, int32_t* rhoc_o) {
+                          int64_t* po, int32_t* rhoc_o, int64_t tile_limit = -1) {
   Cells C(G, rhoc);
   const float dt_mid = (dt_old + dt) / 2;                  // drift.f90:21
   const int nlayer = 2 * (int)std::ceil(dt_mid * vz_max / (float)G.rcs) + 2;  // drift.f90:26
   const double inv = 1.0 / (G.x_res * (double)G.rcs);
   const int64_t nt = G.nt, ncb = G.ncb;
-  const int64_t ntiles = G.nnt * G.nnt * G.nnt;
+  const int64_t ntiles = (tile_limit > 0) ? std::min<int64_t>(tile_limit, G.nnt * G.nnt * G.nnt) : G.nnt * G.nnt * G.nnt;
   // per tile: destination lists (physical cells only)
   std::vector<int64_t> tile_count(ntiles, 0);
   std::vector<std::vector<std::vector<int64_t>>> dest(ntiles);
@@ -786,6 +786,7 @@ using namespace oracle;
 extern "C" {
 
 typedef struct oracle_kick_out {
+  double t_pm1, t_pm2, t_pm3, t_pp;  // wall seconds per stage
   double f2max_pm1, f2max_pm2, f2max_pm3, f2max_pp;
   double vmax[3];
   float dt_pm1, dt_pm2, dt_pm3, dt_pp, dt_vmax, vz_max;
@@ -829,6 +830,19 @@ int64_t oracle_drift(const cube_params* p, const void* xp, const float* vp, cons
     return drift_impl<int8_t, float>(G, (const int8_t*)xp, vp, pid, rhoc, dt_old, dt, vz_max, (int8_t*)xo, vo, po, rhoc_o);
   return drift_impl<int16_t, float>(G, (const int16_t*)xp, vp, pid, rhoc, dt_old, dt, vz_max, (int16_t*)xo, vo, po, rhoc_o);
 }
+// drift.f90 restricted to the first `tiles` tiles (CPU-baseline timing sample): returns
+// the number of particles those tiles receive.
+int64_t oracle_drift_sample(const cube_params* p, const void* xp, const float* vp, const int64_t* pid,
+                            const int32_t* rhoc, float dt_old, float dt, float vz_max, void* xo, float* vo, int64_t* po,
+                            int32_t* rhoc_o, int64_t tiles) {
+  Geo G = make_geo(p);
+  if (G.izipx == 1)
+    return drift_impl<int8_t, float>(G, (const int8_t*)xp, vp, pid, rhoc, dt_old, dt, vz_max, (int8_t*)xo, vo, po, rhoc_o,
+                                     tiles);
+  return drift_impl<int16_t, float>(G, (const int16_t*)xp, vp, pid, rhoc, dt_old, dt, vz_max, (int16_t*)xo, vo, po,
+                                    rhoc_o, tiles);
+}
+
 int64_t oracle_drift64(const cube_params* p, const void* xp, const double* vp, const int64_t* pid, const int32_t* rhoc,
                        float dt_old, float dt, float vz_max, void* xo, double* vo, int64_t* po, int32_t* rhoc_o) {
   Geo G = make_geo(p);
@@ -860,6 +874,7 @@ static int kick_impl(const Geo& G, const XT* xp, T* vp, const int32_t* rhoc, flo
     for (int64_t i = 0; i < n; ++i) dbg_out[i] = (float)v[i];
   };
   T vmax[3] = {0, 0, 0};
+  double t0 = omp_get_wtime();
   // PM1
   T f2 = 0;
   if (only & 1) {
@@ -871,6 +886,8 @@ static int kick_impl(const Geo& G, const XT* xp, T* vp, const int32_t* rhoc, flo
   }
   out->f2max_pm1 = (double)f2;
   out->dt_pm1 = dt_crit(0.5f, (float)f2, a_mid);
+  out->t_pm1 = omp_get_wtime() - t0;
+  t0 = omp_get_wtime();
   // PM2
   const int64_t ntiles = G.nnt * G.nnt * G.nnt;
   const int64_t ntile_run = boxes_frac > 0 ? std::max<int64_t>(1, (int64_t)(ntiles * boxes_frac)) : ntiles;
@@ -901,6 +918,8 @@ static int kick_impl(const Geo& G, const XT* xp, T* vp, const int32_t* rhoc, flo
     vmax[0] = vm0; vmax[1] = vm1; vmax[2] = vm2;
   }
   out->dt_pm2 = dt_crit(0.5f, (float)out->f2max_pm2, a_mid);
+  out->t_pm2 = omp_get_wtime() - t0;
+  t0 = omp_get_wtime();
   // classification (kick.f90:108-138)
   std::vector<int> ires;
   classify(G, rhoc, ires, out->napm);
@@ -937,6 +956,8 @@ static int kick_impl(const Geo& G, const XT* xp, T* vp, const int32_t* rhoc, flo
     vmax[0] = vm0; vmax[1] = vm1; vmax[2] = vm2;
   }
   out->dt_pm3 = dt_crit(0.5f, (float)out->f2max_pm3, a_mid);
+  out->t_pm3 = omp_get_wtime() - t0;
+  t0 = omp_get_wtime();
   if (G.pp_on && (only & 8)) {
     T f2m = 0, vm0 = 0, vm1 = 0, vm2 = 0;
     int64_t e = 0, npairs = 0;
@@ -956,6 +977,7 @@ static int kick_impl(const Geo& G, const XT* xp, T* vp, const int32_t* rhoc, flo
     vmax[0] = vm0; vmax[1] = vm1; vmax[2] = vm2;
   }
   out->dt_pp = dt_crit(0.05f, (float)out->f2max_pp, a_mid);
+  out->t_pp = omp_get_wtime() - t0;
   for (int d = 0; d < 3; ++d) out->vmax[d] = (double)vmax[d];
   const float vm = (float)std::max({vmax[0], vmax[1], vmax[2]});
   out->dt_vmax = 0.9f * 14 / vm;  // kick.f90:314

@@ -22,6 +22,7 @@ _LIB = None
 
 class KickOut(ctypes.Structure):
     _fields_ = [
+        ("t_pm1", ctypes.c_double), ("t_pm2", ctypes.c_double), ("t_pm3", ctypes.c_double), ("t_pp", ctypes.c_double),
         ("f2max_pm1", ctypes.c_double), ("f2max_pm2", ctypes.c_double), ("f2max_pm3", ctypes.c_double),
         ("f2max_pp", ctypes.c_double), ("vmax", ctypes.c_double * 3),
         ("dt_pm1", ctypes.c_float), ("dt_pm2", ctypes.c_float), ("dt_pm3", ctypes.c_float),
@@ -51,6 +52,9 @@ def lib():
         L.oracle_drift.restype = ctypes.c_int64
         L.oracle_drift.argtypes = [P, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                    vp, vp, vp, vp]
+        L.oracle_drift_sample.restype = ctypes.c_int64
+        L.oracle_drift_sample.argtypes = [P, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                          vp, vp, vp, vp, ctypes.c_int64]
         L.oracle_drift64.restype = ctypes.c_int64
         L.oracle_drift64.argtypes = L.oracle_drift.argtypes
         L.oracle_kick.argtypes = [P, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int,
@@ -116,6 +120,22 @@ def drift(p: Params, xp, vp, pid, rhoc, dt_old: float, dt: float, vz_max: float)
     if m != n:
         raise RuntimeError("particle count not conserved: %d -> %d" % (n, m))
     return xo, vo, po, ro
+
+
+def drift_sample(p: Params, xp, vp, pid, rhoc, dt_old: float, dt: float, vz_max: float, tiles: int) -> int:
+    """drift.f90 over the first `tiles` tiles only (CPU-baseline sample); returns the
+    number of particles placed."""
+    xo = np.zeros_like(xp)
+    vo = np.zeros_like(vp)
+    po = np.zeros_like(pid)
+    ro = np.zeros_like(rhoc)
+    cp = p.to_c()
+    m = lib().oracle_drift_sample(ctypes.byref(cp), _ptr(np.ascontiguousarray(xp)), _ptr(np.ascontiguousarray(vp)),
+                                  _ptr(np.ascontiguousarray(pid)), _ptr(np.ascontiguousarray(rhoc)), dt_old, dt,
+                                  vz_max, _ptr(xo), _ptr(vo), _ptr(po), _ptr(ro), tiles)
+    if m < 0:
+        raise RuntimeError("oracle drift failed: %d" % m)
+    return int(m)
 
 
 def kick(p: Params, xp, vp, rhoc, dt: float, a_mid: float, fixed: bool = False, only: int = 15,

@@ -142,7 +142,9 @@ def test_kick_matches_oracle(oracle_lib, izipx, fixed, kind):
     for a, b in ((so.f2max_pm1, out.f2max_pm1), (so.f2max_pm2, out.f2max_pm2), (so.f2max_pm3, out.f2max_pm3)):
         assert abs(a - b) <= 1e-4 * abs(b)
     assert abs(so.f2max_pp - out.f2max_pp) <= 1e-3 * abs(out.f2max_pp) + 1e-12
-    assert so.pp_pairs == out.pp_pairs * 2 or out.pp_pairs == 0 or abs(so.pp_pairs - 2 * out.pp_pairs) <= 4
+    # the oracle counts a pair once per subtile that evaluates it (kick.f90:516-566), the
+    # GPU once per physical particle: out <= gpu <= 2*out
+    assert out.pp_pairs <= so.pp_pairs <= 2 * out.pp_pairs
 
 
 def test_step_sequence(oracle_lib):
