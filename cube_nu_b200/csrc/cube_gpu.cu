@@ -268,17 +268,32 @@ void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixe
   const int rpb = std::max(1, 2048 / n);
   const size_t smx = (size_t)(n + 2 * rpb * n) * sizeof(float2);
   const unsigned gx = (unsigned)((nrows + rpb - 1) / rpb);
-  if (fixed)
+  const int nhh = n / 2 + 1;
+  const size_t smxy = (size_t)(n + nhh * (n + 1)) * sizeof(float2);
+  // butterflies per thread: y-FFT / unpack (nh*n/2), row packing (n*n/2 over 2*MAXB)
+  const bool fused = (n <= 160) && ((int64_t)nhh * (n / 2) <= (int64_t)XY_MAXB * 512) &&
+                     ((int64_t)(n / 2) * n <= (int64_t)2 * XY_MAXB * 512) && smxy <= 200 * 1024;
+  if (fused) {
+    const unsigned planes = (unsigned)(nbox * n);
+    if (fixed)
+      LAUNCH(c, kx, 1, k_fft_xy_r2c<long long><<<planes, 512, smxy, c->s>>>((const long long*)real_in, ck, D, scale));
+    else
+      LAUNCH(c, kx, 1, k_fft_xy_r2c<float><<<planes, 512, smxy, c->s>>>((const float*)real_in, ck, D, scale));
+  } else if (fixed)
     LAUNCH(c, kx, 1, k_fft_x_r2c<long long><<<gx, 256, smx, c->s>>>((const long long*)real_in, ck, nrows, D, rpb, scale));
   else
     LAUNCH(c, kx, 1, k_fft_x_r2c<float><<<gx, 256, smx, c->s>>>((const float*)real_in, ck, nrows, D, rpb, scale));
   const int W = (n <= 256) ? 16 : (n <= 512 ? 8 : 4);
   const size_t smy = (size_t)(n + 2 * W * n) * sizeof(float2);
   dim3 gy((unsigned)(nbox * n), (unsigned)((nh + W - 1) / W));
-  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1));
+  if (!fused) LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1));
   LAUNCH(c, kz, 1, k_fft_z_green<<<gy, 256, smy, c->s>>>(ck, green, D, W));
-  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1));
-  LAUNCH(c, kc, 1, k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, norm, reps));
+  if (fused) {
+    LAUNCH(c, kc, 1, k_fft_yx_c2r<<<(unsigned)(nbox * n), 512, smxy, c->s>>>(ck, phi_out, D, norm, reps));
+  } else {
+    LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1));
+    LAUNCH(c, kc, 1, k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, norm, reps));
+  }
 }
 
 inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
@@ -384,6 +399,9 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
   CK(cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   CK(cudaFuncSetAttribute(k_fft_z_green, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   CK(cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  CK(cudaFuncSetAttribute(k_fft_xy_r2c<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  CK(cudaFuncSetAttribute(k_fft_xy_r2c<long long>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  CK(cudaFuncSetAttribute(k_fft_yx_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   CK(cudaFuncSetAttribute(k_drift_sort_big, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
   // cells
   const int64_t nc3 = G.ncells;
@@ -601,7 +619,7 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     float* phi = reinterpret_cast<float*>(m.real);
     launch_fft(c, n, 1, m.real, fixed, G.mass_p, phi, m.ck, c->green1, (float)n, 3, 1);
     maybe_capture(c, 1, 0, 1, phi, n3, false);
-    LAUNCH(c, K_F2_PM1, 1, k_f2max_periodic<<<nblk(n3), 256, 0, c->s>>>(phi, n, f2 + 0));
+    LAUNCH(c, K_F2_PM1, 1, k_f2max_periodic<<<(unsigned)std::min<int64_t>(1184, (int64_t)n * n / 8 + 1), 256, 0, c->s>>>(phi, n, f2 + 0));
     LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, a_mid, dt));
   }
   CK(cudaEventRecord(c->ev[1], c->s));
@@ -622,7 +640,7 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, c->green2, (float)n * (float)n * (float)n, 1, 2);
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
         maybe_capture(c, 2, c->cap_box, 1, phi + (c->cap_box - t0) * n3, n3, false);
-      LAUNCH(c, K_F2_PM2, 1, k_f2max_box<<<nblk((int64_t)G.ngp * G.ngp * G.ngp * nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1));
+      LAUNCH(c, K_F2_PM2, 1, k_f2max_box<<<1184, 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1));
       LAUNCH(c, K_INT_PM2, 1, k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, a_mid, dt, vm + 0, c->err));
     }
   }
@@ -683,7 +701,7 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, g3, (float)n * (float)n * (float)n, 1, 3);
       if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 1, phi + cap_slot * n3, n3, false);
       const int nf = G.nfp[cl];
-      LAUNCH(c, K_F2_PM3, 1, k_f2max_box<<<nblk((int64_t)nf * nf * nf * nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2));
+      LAUNCH(c, K_F2_PM3, 1, k_f2max_box<<<1184, 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2));
       LAUNCH(c, K_INT_PM3, 1, k_interp_pm3<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp, a_mid, dt, vm + 3,
                                                 c->err));
     }

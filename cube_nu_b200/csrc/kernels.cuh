@@ -488,44 +488,72 @@ __device__ __forceinline__ float sumsq3(float a, float b, float c) {
   return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
 }
 
-__device__ __forceinline__ void block_max_to(float v, float* out) {
+__device__ __forceinline__ float warp_max(float v) {
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  if ((threadIdx.x & 31) == 0) atomic_max_pos(out, v);
+  return v;
 }
 
-// PM1: periodic nc^3 phi[z][y][x].
+// Block-wide max of non-negative values; one atomic per block.  Every thread of the
+// block must call it (no early returns before it).
+__device__ __forceinline__ void block_max_to(float v, float* out) {
+  __shared__ float sm[32];
+  v = warp_max(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sm[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (lane < (int)(blockDim.x >> 5)) ? sm[lane] : 0.f;
+    v = warp_max(v);
+    if (lane == 0 && v > 0.f) atomic_max_pos(out, v);
+  }
+}
+
+// PM1: periodic nc^3 phi[z][y][x].  One warp per x-row, grid-stride over rows.
 __global__ void k_f2max_periodic(const float* __restrict__ phi, int nc, float* __restrict__ f2out) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
   float v = 0.f;
-  if (i < (int64_t)nc * nc * nc) {
-    const int x = (int)(i % nc), y = (int)((i / nc) % nc), z = (int)(i / ((int64_t)nc * nc));
-    auto P = [&](int a, int b, int c) {
-      return phi[((int64_t)wrapi(c, nc) * nc + wrapi(b, nc)) * nc + wrapi(a, nc)];
-    };
-    const float fx = grad4(P(x - 2, y, z), P(x - 1, y, z), P(x + 1, y, z), P(x + 2, y, z));
-    const float fy = grad4(P(x, y - 2, z), P(x, y - 1, z), P(x, y + 1, z), P(x, y + 2, z));
-    const float fz = grad4(P(x, y, z - 2), P(x, y, z - 1), P(x, y, z + 1), P(x, y, z + 2));
-    v = sumsq3(fx, fy, fz);
+  const int nrows = nc * nc;
+  for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < nrows; row += gridDim.x * wpb) {
+    const int z = row / nc, y = row - z * nc;
+    const int zm2 = wrapi(z - 2, nc), zm1 = wrapi(z - 1, nc), zp1 = wrapi(z + 1, nc), zp2 = wrapi(z + 2, nc);
+    const int ym2 = wrapi(y - 2, nc), ym1 = wrapi(y - 1, nc), yp1 = wrapi(y + 1, nc), yp2 = wrapi(y + 2, nc);
+    auto R = [&](int zz, int yy) { return phi + ((size_t)zz * nc + yy) * nc; };
+    const float* r0 = R(z, y);
+    for (int x = lane; x < nc; x += 32) {
+      const int xm2 = wrapi(x - 2, nc), xm1 = wrapi(x - 1, nc), xp1 = wrapi(x + 1, nc), xp2 = wrapi(x + 2, nc);
+      const float fx = grad4(r0[xm2], r0[xm1], r0[xp1], r0[xp2]);
+      const float fy = grad4(R(z, ym2)[x], R(z, ym1)[x], R(z, yp1)[x], R(z, yp2)[x]);
+      const float fz = grad4(R(zm2, y)[x], R(zm1, y)[x], R(zp1, y)[x], R(zp2, y)[x]);
+      v = fmaxf(v, sumsq3(fx, fy, fz));
+    }
   }
   block_max_to(v, f2out);
 }
 
-// Box meshes: phi[b][n^3] with index i mapping to array i-m1phi; physical 1..nforce.
+// Box meshes phi[b][n^3], index i at array i-m1phi; physical cells 1..nforce.  One warp
+// per x-row of physical cells, grid-stride over (box, z, y) rows.
 __global__ void k_f2max_box(const float* __restrict__ phi, int n, int nforce, int m1phi, int nbox,
                             float* __restrict__ f2out) {
-  const int64_t nf3 = (int64_t)nforce * nforce * nforce;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
   float v = 0.f;
-  if (i < nf3 * nbox) {
-    const int64_t b = i / nf3;
-    const int64_t r = i - b * nf3;
-    const int x = (int)(r % nforce) + 1, y = (int)((r / nforce) % nforce) + 1, z = (int)(r / ((int64_t)nforce * nforce)) + 1;
-    const float* pb = phi + b * (int64_t)n * n * n;
-    auto P = [&](int a, int bb, int c) { return pb[((int64_t)(c - m1phi) * n + (bb - m1phi)) * n + (a - m1phi)]; };
-    const float fx = grad4(P(x - 2, y, z), P(x - 1, y, z), P(x + 1, y, z), P(x + 2, y, z));
-    const float fy = grad4(P(x, y - 2, z), P(x, y - 1, z), P(x, y + 1, z), P(x, y + 2, z));
-    const float fz = grad4(P(x, y, z - 2), P(x, y, z - 1), P(x, y, z + 1), P(x, y, z + 2));
-    v = sumsq3(fx, fy, fz);
+  const int64_t rows_per_box = (int64_t)nforce * nforce;
+  const int64_t nrows = rows_per_box * nbox;
+  const int sy = n, sz = n * n;
+  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < nrows; row += (int64_t)gridDim.x * wpb) {
+    const int b = (int)(row / rows_per_box);
+    const int r = (int)(row - (int64_t)b * rows_per_box);
+    const int z = r / nforce + 1, y = r - (z - 1) * nforce + 1;
+    const float* pb = phi + (size_t)b * n * n * n + (size_t)(z - m1phi) * sz + (size_t)(y - m1phi) * sy - m1phi;
+    for (int x = 1 + lane; x <= nforce; x += 32) {
+      const float* q = pb + x;
+      const float fx = grad4(q[-2], q[-1], q[1], q[2]);
+      const float fy = grad4(q[-2 * sy], q[-sy], q[sy], q[2 * sy]);
+      const float fz = grad4(q[-2 * sz], q[-sz], q[sz], q[2 * sz]);
+      v = fmaxf(v, sumsq3(fx, fy, fz));
+    }
   }
   block_max_to(v, f2out);
 }
@@ -535,38 +563,83 @@ __global__ void k_f2max_box(const float* __restrict__ phi, int n, int nforce, in
 // at each of the 27 TSC cells is differenced from phi on the fly; the values equal
 // those of a stored force grid because each uses the same four phi values.
 // =================================================================================
+// For each component the 27 TSC terms are summed in the reference order
+// (i3 outer, i2, i1 inner; kick.f90:789-795); components are independent sums, so
+// they are accumulated one after another to keep the loads to 3 x 63.
 template <class PhiFn>
 __device__ __forceinline__ void tsc_gather_force(const int i2[3], const float w[3][3], PhiFn P, float dv[3]) {
-  dv[0] = dv[1] = dv[2] = 0.f;
+  const int x0 = i2[0] - 1, y0 = i2[1] - 1, z0 = i2[2] - 1;
+  // x component: rows of 7 values along x
+  float s = 0.f;
 #pragma unroll
-  for (int a3 = 0; a3 < 3; ++a3) {
-    const int z = i2[2] - 1 + a3;
+  for (int a3 = 0; a3 < 3; ++a3)
 #pragma unroll
     for (int a2 = 0; a2 < 3; ++a2) {
-      const int y = i2[1] - 1 + a2;
+      float r[7];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) r[k] = P(x0 - 2 + k, y0 + a2, z0 + a3);
 #pragma unroll
       for (int a1 = 0; a1 < 3; ++a1) {
-        const int x = i2[0] - 1 + a1;
-        const float F0 = grad4(P(x - 2, y, z), P(x - 1, y, z), P(x + 1, y, z), P(x + 2, y, z));
-        const float F1 = grad4(P(x, y - 2, z), P(x, y - 1, z), P(x, y + 1, z), P(x, y + 2, z));
-        const float F2 = grad4(P(x, y, z - 2), P(x, y, z - 1), P(x, y, z + 1), P(x, y, z + 2));
-        const float wa = w[0][a1], wb = w[1][a2], wc = w[2][a3];
-        dv[0] = __fadd_rn(dv[0], __fmul_rn(__fmul_rn(__fmul_rn(F0, wa), wb), wc));
-        dv[1] = __fadd_rn(dv[1], __fmul_rn(__fmul_rn(__fmul_rn(F1, wa), wb), wc));
-        dv[2] = __fadd_rn(dv[2], __fmul_rn(__fmul_rn(__fmul_rn(F2, wa), wb), wc));
+        const float F = grad4(r[a1], r[a1 + 1], r[a1 + 3], r[a1 + 4]);
+        s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(F, w[0][a1]), w[1][a2]), w[2][a3]));
       }
     }
+  dv[0] = s;
+  // y component: per a3, a 7 (y) x 3 (x) block
+  s = 0.f;
+#pragma unroll
+  for (int a3 = 0; a3 < 3; ++a3) {
+    float r[7][3];
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+#pragma unroll
+      for (int a1 = 0; a1 < 3; ++a1) r[k][a1] = P(x0 + a1, y0 - 2 + k, z0 + a3);
+#pragma unroll
+    for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+      for (int a1 = 0; a1 < 3; ++a1) {
+        const float F = grad4(r[a2][a1], r[a2 + 1][a1], r[a2 + 3][a1], r[a2 + 4][a1]);
+        s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(F, w[0][a1]), w[1][a2]), w[2][a3]));
+      }
   }
+  dv[1] = s;
+  // z component: the 27 values first (columns of 7 along z), then the ordered sum
+  float F2[3][3][3];
+#pragma unroll
+  for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+    for (int a1 = 0; a1 < 3; ++a1) {
+      float r[7];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) r[k] = P(x0 + a1, y0 + a2, z0 - 2 + k);
+#pragma unroll
+      for (int a3 = 0; a3 < 3; ++a3) F2[a3][a2][a1] = grad4(r[a3], r[a3 + 1], r[a3 + 3], r[a3 + 4]);
+    }
+  s = 0.f;
+#pragma unroll
+  for (int a3 = 0; a3 < 3; ++a3)
+#pragma unroll
+    for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+      for (int a1 = 0; a1 < 3; ++a1)
+        s = __fadd_rn(s, __fmul_rn(__fmul_rn(__fmul_rn(F2[a3][a2][a1], w[0][a1]), w[1][a2]), w[2][a3]));
+  dv[2] = s;
 }
 
 __device__ __forceinline__ void apply_kick(float* vp, int64_t ip, const float dv[3], float a_mid, float dt,
-                                           float* vmax) {
+                                           float av[3]) {
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const float v = kick_add(vp[3 * ip + d], dv[d], a_mid, dt);
     vp[3 * ip + d] = v;
-    if (vmax) atomic_max_pos(vmax + d, fabsf(v));
+    av[d] = fabsf(v);
   }
+}
+
+__device__ __forceinline__ void block_vmax(const float av[3], float* vmax) {
+  block_max_to(av[0], vmax + 0);
+  block_max_to(av[1], vmax + 1);
+  block_max_to(av[2], vmax + 2);
 }
 
 __global__ void k_interp_pm1(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
@@ -583,83 +656,100 @@ __global__ void k_interp_pm1(Geo G, int64_t np, const void* __restrict__ xp, con
     i2[d] = tsc_weights(xpos, w[d]);
   }
   const int nc = G.nc;
-  // force index i (1-based, periodic) reads phi(i-2..i+2); array index (i-1) mod nc
+  // force index i (1-based, periodic) reads phi(i-2..i+2); array index (i-1) mod nc.
+  // Wrapped indices of the 7 positions i2-3..i2+3 per dimension, computed once.
+  int wx[7], wy[7], wz[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    wx[k] = wrapi(i2[0] - 4 + k, nc);
+    wy[k] = wrapi(i2[1] - 4 + k, nc) * nc;
+    wz[k] = wrapi(i2[2] - 4 + k, nc) * nc;
+  }
+  const int x0 = i2[0] - 1, y0 = i2[1] - 1, z0 = i2[2] - 1;
   auto P = [&](int a, int b, int c) {
-    return __ldg(&phi[((int64_t)wrapi(c - 1, nc) * nc + wrapi(b - 1, nc)) * nc + wrapi(a - 1, nc)]);
+    return __ldg(&phi[((size_t)wz[c - z0 + 2] + wy[b - y0 + 2]) * nc + wx[a - x0 + 2]]);
   };
-  float dv[3];
+  float dv[3], av[3];
   tsc_gather_force(i2, w, P, dv);
-  apply_kick(vp, ip, dv, a_mid, dt, nullptr);
+  apply_kick(vp, ip, dv, a_mid, dt, av);
 }
 
 __global__ void k_interp_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                              const float* __restrict__ phi, int tile0, int ntile, float* __restrict__ vp, float a_mid,
                              float dt, float* vmax, unsigned* err) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (ip >= np) return;
-  int g[3];
-  cell_coords(G, pcell[ip], g[0], g[1], g[2]);
-  const int T = ((g[2] / G.nt) * G.nnt + g[1] / G.nt) * G.nnt + g[0] / G.nt;
-  if (T < tile0 || T >= tile0 + ntile) return;
-  int i2[3];
-  float w[3][3];
-  bool oob = false;
+  float av[3] = {0.f, 0.f, 0.f};
+  if (ip < np) {
+    int g[3];
+    cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+    const int T = ((g[2] / G.nt) * G.nnt + g[1] / G.nt) * G.nnt + g[0] / G.nt;
+    if (T >= tile0 && T < tile0 + ntile) {
+      int i2[3];
+      float w[3][3];
+      bool oob = false;
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const double xpos = ((double)(g[d] % G.nt) + zfrac(load_code(xp, G.izipx, 3 * ip + d), G)) * (double)G.rcs;
-    i2[d] = tsc_weights(xpos, w[d]);
-    if (i2[d] - 1 < 0 || i2[d] + 1 > G.ngp + 1) oob = true;
+      for (int d = 0; d < 3; ++d) {
+        const double xpos = ((double)(g[d] % G.nt) + zfrac(load_code(xp, G.izipx, 3 * ip + d), G)) * (double)G.rcs;
+        i2[d] = tsc_weights(xpos, w[d]);
+        if (i2[d] - 1 < 0 || i2[d] + 1 > G.ngp + 1) oob = true;
+      }
+      if (oob) {
+        set_err(err, CUBE_DEVERR_INTERP_RANGE);
+      } else {
+        const int n = G.ngt, m1 = 1 - G.ngb;
+        const float* pb = phi + (size_t)(T - tile0) * n * n * n;
+        auto P = [&](int a, int b, int c) { return __ldg(&pb[((c - m1) * n + (b - m1)) * n + (a - m1)]); };
+        float dv[3];
+        tsc_gather_force(i2, w, P, dv);
+        apply_kick(vp, ip, dv, a_mid, dt, av);
+      }
+    }
   }
-  if (oob) {
-    set_err(err, CUBE_DEVERR_INTERP_RANGE);
-    return;
-  }
-  const int n = G.ngt, m1 = 1 - G.ngb;
-  const float* pb = phi + (int64_t)(T - tile0) * n * n * n;
-  auto P = [&](int a, int b, int c) { return __ldg(&pb[((int64_t)(c - m1) * n + (b - m1)) * n + (a - m1)]); };
-  float dv[3];
-  tsc_gather_force(i2, w, P, dv);
-  apply_kick(vp, ip, dv, a_mid, dt, vmax);
+  block_vmax(av, vmax);
 }
 
 __global__ void k_interp_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                              const float* __restrict__ phi, const int32_t* __restrict__ box_slot, int iapm,
                              float* __restrict__ vp, float a_mid, float dt, float* vmax, unsigned* err) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (ip >= np) return;
-  int g[3];
-  cell_coords(G, pcell[ip], g[0], g[1], g[2]);
-  int t[3], u[3], l[3];
+  float av[3] = {0.f, 0.f, 0.f};
+  if (ip < np) {
+    int g[3];
+    cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+    int t[3], u[3], l[3];
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    t[d] = g[d] / G.nt;
-    l[d] = g[d] - t[d] * G.nt;
-    u[d] = l[d] / G.ntt;
-  }
-  const int slot = box_slot[subtile_id(G, t, u)];
-  if (slot < 0) return;
-  const int nft = G.nft[iapm], nfp = G.nfp[iapm], nfb = G.nfb[iapm];
-  const double gs = (double)(1.f / (float)rsf_of(iapm));
-  int i2[3];
-  float w[3][3];
-  bool oob = false;
+    for (int d = 0; d < 3; ++d) {
+      t[d] = g[d] / G.nt;
+      l[d] = g[d] - t[d] * G.nt;
+      u[d] = l[d] / G.ntt;
+    }
+    const int slot = box_slot[subtile_id(G, t, u)];
+    if (slot >= 0) {
+      const int nft = G.nft[iapm], nfp = G.nfp[iapm], nfb = G.nfb[iapm];
+      const double gs = (double)(1.f / (float)rsf_of(iapm));
+      int i2[3];
+      float w[3][3];
+      bool oob = false;
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const double xpos =
-        ((double)l[d] + zfrac(load_code(xp, G.izipx, 3 * ip + d), G)) * (double)G.rcs / gs - (double)(u[d] * nfp);
-    i2[d] = tsc_weights(xpos, w[d]);
-    if (i2[d] - 1 < 0 || i2[d] + 1 > nfp + 1) oob = true;
+      for (int d = 0; d < 3; ++d) {
+        const double xpos =
+            ((double)l[d] + zfrac(load_code(xp, G.izipx, 3 * ip + d), G)) * (double)G.rcs / gs - (double)(u[d] * nfp);
+        i2[d] = tsc_weights(xpos, w[d]);
+        if (i2[d] - 1 < 0 || i2[d] + 1 > nfp + 1) oob = true;
+      }
+      if (oob) {
+        set_err(err, CUBE_DEVERR_INTERP_RANGE);
+      } else {
+        const int m1 = 1 - nfb;
+        const float* pb = phi + (size_t)slot * nft * nft * nft;
+        auto P = [&](int a, int b, int c) { return __ldg(&pb[((c - m1) * nft + (b - m1)) * nft + (a - m1)]); };
+        float dv[3];
+        tsc_gather_force(i2, w, P, dv);
+        apply_kick(vp, ip, dv, a_mid, dt, av);
+      }
+    }
   }
-  if (oob) {
-    set_err(err, CUBE_DEVERR_INTERP_RANGE);
-    return;
-  }
-  const int m1 = 1 - nfb;
-  const float* pb = phi + (int64_t)slot * nft * nft * nft;
-  auto P = [&](int a, int b, int c) { return __ldg(&pb[((int64_t)(c - m1) * nft + (b - m1)) * nft + (a - m1)]); };
-  float dv[3];
-  tsc_gather_force(i2, w, P, dv);
-  apply_kick(vp, ip, dv, a_mid, dt, vmax);
+  block_vmax(av, vmax);
 }
 
 // =================================================================================
@@ -705,8 +795,9 @@ __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32
                      const int64_t* __restrict__ cstart, const int32_t* __restrict__ ires, float* __restrict__ vp,
                      float mass_scale, float v_scale, float* f2max, float* vmax,
                      unsigned long long* npairs) {
-  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (ip >= np) return;
+  const int64_t ip0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = ip0 < np;
+  const int64_t ip = live ? ip0 : np - 1;
   int g[3];
   cell_coords(G, pcell[ip], g[0], g[1], g[2]);
   int t[3], u[3], l[3];
@@ -757,17 +848,23 @@ __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32
           }
         }
       }
-  float f1[3];
+  float f1[3], av[3] = {0.f, 0.f, 0.f};
 #pragma unroll
   for (int d = 0; d < 3; ++d) f1[d] = __fmul_rn(acc[d], mass_scale);
-  atomic_max_pos(f2max, sumsq3(f1[0], f1[1], f1[2]));
+  const float f2 = live ? sumsq3(f1[0], f1[1], f1[2]) : 0.f;
+  if (live) {
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const float v = __fadd_rn(vp[3 * ip + d], __fmul_rn(f1[d], v_scale));
-    vp[3 * ip + d] = v;
-    atomic_max_pos(vmax + d, fabsf(v));
+    for (int d = 0; d < 3; ++d) {
+      const float v = __fadd_rn(vp[3 * ip + d], __fmul_rn(f1[d], v_scale));
+      vp[3 * ip + d] = v;
+      av[d] = fabsf(v);
+    }
   }
-  if (cnt) atomicAdd(npairs, cnt);
+  block_max_to(f2, f2max);
+  block_vmax(av, vmax);
+  unsigned long long c = live ? cnt : 0ull;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(npairs, c);
 }
 
 // =================================================================================

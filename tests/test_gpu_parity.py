@@ -172,3 +172,47 @@ def test_step_sequence(oracle_lib):
     assert same > 0.999
     assert np.array_equal(rg, cur[3]) or np.abs(rg - cur[3]).sum() <= 0.002 * n
     assert abs(so.vz_max - out.vz_max) <= 1e-4 * out.vz_max
+
+
+def _all_class_state(p, seed=31):
+    """Uniform background plus three dense clumps sized to put subtiles in PM3 classes
+    3, 4 and 5 (max coarse-cell count >= 24*64, 114*64, 320*64; kick.f90:116-130)."""
+    rng = np.random.default_rng(seed)
+    parts = [rng.random((12000, 3)) * p.nc]
+    for count, centre in ((2000, (2.5, 2.5, 2.5)), (8000, (10.5, 2.5, 10.5)), (21000, (2.5, 10.5, 10.5))):
+        parts.append(np.asarray(centre) + (rng.random((count, 3)) - 0.5) * 0.9)
+    X = np.concatenate(parts)
+    V = rng.normal(size=X.shape) * 0.5
+    from tests.helpers import state_from_positions
+
+    return state_from_positions(p, X, V)
+
+
+@pytest.mark.parametrize("fixed", [False, True])
+def test_every_pm3_class(oracle_lib, fixed):
+    """Potential and velocities for subtiles of every class: exercises the fused XY FFT
+    (mesh sides 48, 96, 144) and the separate-pass FFT (192)."""
+    p = _params(fixed=fixed)
+    st = _all_class_state(p)
+    n = st[0].shape[0]
+    p.mass_p_cdm = float(p.ng) ** 3 / n
+    ires, napm = oracle_lib.classify(p, st[3])
+    assert all(napm[c] > 0 for c in (2, 3, 4, 5)), list(napm)
+    for cls in (2, 3, 4, 5):
+        box = int(np.nonzero(ires == cls)[0][0])
+        size = p.nft(cls) ** 3
+        _, ref = oracle_lib.kick(p, st[0], st[1].copy(), st[3], 0.1, 0.05, fixed=fixed, debug=(3, box, 1, size))
+        with _ctx(p, st) as ctx:
+            ctx.capture(3, box, 1)
+            ctx.kick(0.1, 0.05)
+            got = ctx.captured(size)
+        err = np.abs(got - ref).max() / np.abs(ref).max()
+        assert err < 2e-5, "class %d phi rel err %.3g" % (cls, err)
+    v_ref = st[1].copy()
+    oracle_lib.kick(p, st[0], v_ref, st[3], 0.1, 0.05, fixed=fixed)
+    with _ctx(p, st) as ctx:
+        ctx.kick(0.1, 0.05)
+        _, v_gpu, _, _ = ctx.download()
+    d = v_ref - st[1]
+    err = np.abs((v_gpu - st[1]) - d).max() / np.abs(d).max()
+    assert err < 2e-4, err
