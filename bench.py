@@ -47,6 +47,11 @@ def load_peaks():
 
 
 def workload(name: str):
+    if name == "proxy":
+        # same mesh sides as the 512^3 workload (PM2 288^3, PM3 144^3) on one tile: for ncu captures
+        p = config_512()
+        p.ng, p.nnt, p.box = 256, 1, 250.0
+        return p, "proxy: 128^3 CDM, 250 Mpc/h, ng 256, one tile (PM2 288^3, PM3 64 subtiles 144^3), int16 ZIPX"
     if name == "512":
         p = config_512()
         desc = "512^3 CDM, 1000 Mpc/h, fine mesh 1024^3 (PM1 256^3, PM2 64x288^3, PM3 4096 subtiles), int16 ZIPX"
@@ -200,7 +205,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="512", choices=["512", "128"])
+    ap.add_argument("--workload", default="512", choices=["512", "128", "proxy"])
     ap.add_argument("--deposit", default="fixed", choices=["fixed", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-json", default="")

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -16,6 +17,7 @@
 #include "../../include/cube_gpu.h"
 #include "common.cuh"
 #include "fft.cuh"
+#include "fft2.cuh"
 #include "kernels.cuh"
 
 using namespace cube;
@@ -110,6 +112,8 @@ struct cube_ctx {
   int64_t cap_n = 0;
   // timing
   cudaEvent_t ev[8];
+  // 1: use the generic Stockham passes for every size (CUBE_FFT_GENERIC=1)
+  int fft_generic = 0;
   // opt-in per-kernel timers and the launch counter
   bool prof = false;
   std::vector<cudaEvent_t> pool;
@@ -256,44 +260,91 @@ int64_t boxes_fit(cube_ctx* c, int n, bool fixed) {
   return std::max<int64_t>(1, (int64_t)(c->arena_bytes / per));
 }
 
+template <typename K>
+void smem_optin(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// Size-specialised passes (fft2.cuh) for N = R1*R2.
+template <int N, int R1, int R2>
+void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out, float2* ck,
+              const float* green, float norm, int reps, int kx, int ky, int kz, int kc) {
+  constexpr int T = f2::TPS<R1, R2>::T, NH = N / 2 + 1;
+  const float2* tw = fft_desc(c, N)->tw;
+  const int64_t nrows = nbox * (int64_t)N * N;
+  const int S = std::max(1, 256 / T);
+  const size_t smx = (size_t)(N + S * N) * sizeof(float2);
+  const unsigned gx = (unsigned)((nrows + 2 * S - 1) / (2 * S));
+  const int W = (N <= 256) ? 16 : (N <= 512 ? 8 : 4);
+  const size_t smc = (size_t)(N + W * N) * sizeof(float2);
+  dim3 gc((unsigned)(nbox * N), (unsigned)((NH + W - 1) / W));
+  if (fixed) {
+    smem_optin(f2::k_fx_r2c<N, R1, R2, long long>, smx);
+    LAUNCH(c, kx, 1, f2::k_fx_r2c<N, R1, R2, long long><<<gx, S * T, smx, c->s>>>((const long long*)real_in, ck, nrows, tw, scale));
+  } else {
+    smem_optin(f2::k_fx_r2c<N, R1, R2, float>, smx);
+    LAUNCH(c, kx, 1, f2::k_fx_r2c<N, R1, R2, float><<<gx, S * T, smx, c->s>>>((const float*)real_in, ck, nrows, tw, scale));
+  }
+  smem_optin(f2::k_fcol<N, R1, R2, 1, 0>, smc);
+  smem_optin(f2::k_fcol<N, R1, R2, 2, 2>, smc);
+  smem_optin(f2::k_fcol<N, R1, R2, 1, 1>, smc);
+  smem_optin(f2::k_fx_c2r<N, R1, R2>, smx);
+  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W));
+  LAUNCH(c, kz, 1, f2::k_fcol<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W));
+  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 1><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W));
+  LAUNCH(c, kc, 1, f2::k_fx_c2r<N, R1, R2><<<gx, S * T, smx, c->s>>>(ck, phi_out, nrows, tw, norm, reps));
+}
+
+bool fft2_dispatch(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out,
+                   float2* ck, const float* green, float norm, int reps, int kx, int ky, int kz, int kc) {
+#define CUBE_FFT2(N, R1, R2) \
+  case N: fft2_run<N, R1, R2>(c, nbox, real_in, fixed, scale, phi_out, ck, green, norm, reps, kx, ky, kz, kc); return true;
+  switch (n) {
+    CUBE_FFT2(16, 4, 4)
+    CUBE_FFT2(32, 4, 8)
+    CUBE_FFT2(48, 8, 6)
+    CUBE_FFT2(64, 8, 8)
+    CUBE_FFT2(96, 8, 12)
+    CUBE_FFT2(128, 8, 16)
+    CUBE_FFT2(144, 12, 12)
+    CUBE_FFT2(192, 16, 12)
+    CUBE_FFT2(256, 16, 16)
+    CUBE_FFT2(288, 16, 18)
+    CUBE_FFT2(432, 24, 18)
+    CUBE_FFT2(512, 16, 32)
+    CUBE_FFT2(576, 24, 24)
+    CUBE_FFT2(1024, 32, 32)
+    default: return false;
+  }
+#undef CUBE_FFT2
+}
+
 void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out,
                 float2* ck, const float* green, float norm, int reps, int level) {
   const int kx = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTX_PM2 : K_FFTX_PM3;
   const int ky = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTY_PM2 : K_FFTY_PM3;
   const int kz = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTZ_PM2 : K_FFTZ_PM3;
   const int kc = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTC_PM2 : K_FFTC_PM3;
+  if (c->fft_generic == 0 &&
+      fft2_dispatch(c, n, nbox, real_in, fixed, scale, phi_out, ck, green, norm, reps, kx, ky, kz, kc))
+    return;
   const FFTDesc& D = *fft_desc(c, n);
   const int nh = n / 2 + 1;
   const int64_t nrows = nbox * (int64_t)n * n;
   const int rpb = std::max(1, 2048 / n);
   const size_t smx = (size_t)(n + 2 * rpb * n) * sizeof(float2);
   const unsigned gx = (unsigned)((nrows + rpb - 1) / rpb);
-  const int nhh = n / 2 + 1;
-  const size_t smxy = (size_t)(n + nhh * (n + 1)) * sizeof(float2);
-  // butterflies per thread: y-FFT / unpack (nh*n/2), row packing (n*n/2 over 2*MAXB)
-  const bool fused = (n <= 160) && ((int64_t)nhh * (n / 2) <= (int64_t)XY_MAXB * 512) &&
-                     ((int64_t)(n / 2) * n <= (int64_t)2 * XY_MAXB * 512) && smxy <= 200 * 1024;
-  if (fused) {
-    const unsigned planes = (unsigned)(nbox * n);
-    if (fixed)
-      LAUNCH(c, kx, 1, k_fft_xy_r2c<long long><<<planes, 512, smxy, c->s>>>((const long long*)real_in, ck, D, scale));
-    else
-      LAUNCH(c, kx, 1, k_fft_xy_r2c<float><<<planes, 512, smxy, c->s>>>((const float*)real_in, ck, D, scale));
-  } else if (fixed)
+  if (fixed)
     LAUNCH(c, kx, 1, k_fft_x_r2c<long long><<<gx, 256, smx, c->s>>>((const long long*)real_in, ck, nrows, D, rpb, scale));
   else
     LAUNCH(c, kx, 1, k_fft_x_r2c<float><<<gx, 256, smx, c->s>>>((const float*)real_in, ck, nrows, D, rpb, scale));
   const int W = (n <= 256) ? 16 : (n <= 512 ? 8 : 4);
   const size_t smy = (size_t)(n + 2 * W * n) * sizeof(float2);
   dim3 gy((unsigned)(nbox * n), (unsigned)((nh + W - 1) / W));
-  if (!fused) LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1));
+  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1));
   LAUNCH(c, kz, 1, k_fft_z_green<<<gy, 256, smy, c->s>>>(ck, green, D, W));
-  if (fused) {
-    LAUNCH(c, kc, 1, k_fft_yx_c2r<<<(unsigned)(nbox * n), 512, smxy, c->s>>>(ck, phi_out, D, norm, reps));
-  } else {
-    LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1));
-    LAUNCH(c, kc, 1, k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, norm, reps));
-  }
+  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1));
+  LAUNCH(c, kc, 1, k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, norm, reps));
 }
 
 inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
@@ -380,6 +431,10 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
     return fail(CUBE_E_ARG, "unsupported tile geometry (nt+2ncb<=256, ntt>=2)");
   }
   c->device = device;
+  {
+    const char* e = getenv("CUBE_FFT_GENERIC");
+    c->fft_generic = (e && e[0] == '1') ? 1 : 0;
+  }
   c->ns3 = (int)((int64_t)G.nnt * G.nnt * G.nnt * G.nns * G.nns * G.nns);
   c->ntiles = G.nnt * G.nnt * G.nnt;
   c->xbytes = G.izipx;
@@ -399,9 +454,6 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
   CK(cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   CK(cudaFuncSetAttribute(k_fft_z_green, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   CK(cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  CK(cudaFuncSetAttribute(k_fft_xy_r2c<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  CK(cudaFuncSetAttribute(k_fft_xy_r2c<long long>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  CK(cudaFuncSetAttribute(k_fft_yx_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   CK(cudaFuncSetAttribute(k_drift_sort_big, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
   // cells
   const int64_t nc3 = G.ncells;

@@ -102,207 +102,6 @@ __device__ float2* fft_smem(float2* a, float2* b, int n, int nb, int sb, int se,
   return in;
 }
 
-// Single-buffer variant: each stage loads its butterflies into registers, waits for
-// the whole block, then writes the outputs into the same buffer.  MAXB bounds the
-// butterflies one thread holds per stage (checked by the host: nb*n/2 <= MAXB*blockDim).
-template <bool SFAST, int MAXB>
-__device__ void fft_smem_1buf(float2* a, int n, int nb, int sb, int se, const float2* tw, const FFTDesc& D, int dir) {
-  int Ns = 1;
-  const float s3 = 0.8660254037844386f * (float)dir;
-  for (int st = 0; st < D.nrad; ++st) {
-    const int R = D.rad[st];
-    const int m = n / R;
-    const int total = nb * m;
-    const int tws = n / (Ns * R);
-    float2 y[MAXB][4];
-#pragma unroll
-    for (int k = 0; k < MAXB; ++k) {
-      const int t = threadIdx.x + k * blockDim.x;
-      if (t < total) {
-        int s, j;
-        if (SFAST) { s = t % nb; j = t / nb; }
-        else { j = t % m; s = t / m; }
-        const int jm = j % Ns;
-        float2 v[4];
-        const float2* src = a + s * sb;
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-          if (r < R) v[r] = src[(j + r * m) * se];
-#pragma unroll
-        for (int r = 1; r < 4; ++r)
-          if (r < R) {
-            float2 w = tw[r * jm * tws];
-            if (dir > 0) w.y = -w.y;
-            v[r] = cmul(v[r], w);
-          }
-        if (R == 4) {
-          const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-          const float2 b0 = cadd(v[1], v[3]), b1 = csub(v[1], v[3]);
-          const float2 jb1 = (dir < 0) ? make_float2(b1.y, -b1.x) : make_float2(-b1.y, b1.x);
-          y[k][0] = cadd(a0, b0);
-          y[k][2] = csub(a0, b0);
-          y[k][1] = cadd(a1, jb1);
-          y[k][3] = csub(a1, jb1);
-        } else if (R == 2) {
-          y[k][0] = cadd(v[0], v[1]);
-          y[k][1] = csub(v[0], v[1]);
-        } else {
-          const float2 t1 = cadd(v[1], v[2]);
-          const float2 d = csub(v[1], v[2]);
-          const float2 m0 = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
-          const float2 id = make_float2(-d.y * s3, d.x * s3);
-          y[k][0] = cadd(v[0], t1);
-          y[k][1] = cadd(m0, id);
-          y[k][2] = csub(m0, id);
-        }
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < MAXB; ++k) {
-      const int t = threadIdx.x + k * blockDim.x;
-      if (t < total) {
-        int s, j;
-        if (SFAST) { s = t % nb; j = t / nb; }
-        else { j = t % m; s = t / m; }
-        const int jm = j % Ns;
-        const int idxD = (j / Ns) * Ns * R + jm;
-        float2* dst = a + s * sb;
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-          if (r < R) dst[(idxD + r * Ns) * se] = y[k][r];
-      }
-    }
-    __syncthreads();
-    Ns *= R;
-  }
-}
-
-// ---- Fused XY forward pass for one z-plane (n <= 160): real plane -> r2c along x
-// (two rows packed per complex FFT) -> FFT along y.  Shared layout C[kx][y] with
-// pitch n+1 (bank-conflict padding).  grid = nbox*n planes.
-constexpr int XY_MAXB = 12;
-template <typename IN>
-__global__ void __launch_bounds__(512) k_fft_xy_r2c(const IN* __restrict__ r, float2* __restrict__ c, FFTDesc D,
-                                                    float scale) {
-  extern __shared__ float2 sm[];
-  const int n = D.n, nh = n / 2 + 1, P = n + 1;
-  float2* tw = sm;
-  float2* A = sm + n;  // nh * P
-  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = D.tw[i];
-  const int64_t plane = blockIdx.x;
-  const IN* rp = r + plane * (int64_t)n * n;
-  // packed rows: Z_p[x] = R[2p][x] + i R[2p+1][x] stored as A[p*P + x]
-  for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
-    const int y = t / n, x = t - y * n;
-    const IN v = rp[t];
-    float f;
-    if (sizeof(IN) == 8) f = (float)((double)(long long)v * 9.094947017729282e-13);
-    else f = (float)v;
-    f = __fmul_rn(f, scale);
-    float* dst = reinterpret_cast<float*>(&A[(y >> 1) * P + x]);
-    dst[y & 1] = f;
-  }
-  __syncthreads();
-  fft_smem_1buf<false, XY_MAXB>(A, n, n / 2, P, 1, tw, D, -1);
-  // unpack into X[y][kx] for y=2p,2p+1 and kx=0..nh-1; held in registers then
-  // rewritten as C[kx][y] (same buffer) after a barrier
-  const int npairs = n / 2;
-  const int total = npairs * nh;
-  float2 keep[XY_MAXB][2];
-#pragma unroll
-  for (int k = 0; k < XY_MAXB; ++k) {
-    const int t = threadIdx.x + k * blockDim.x;
-    if (t < total) {
-      const int p = t / nh, kx = t - p * nh;
-      const float2 z = A[p * P + kx];
-      const float2 zc = A[p * P + ((n - kx) % n)];
-      // X0 = (Z + conj(Zc))/2, X1 = (Z - conj(Zc))/(2i)
-      keep[k][0] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
-      keep[k][1] = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < XY_MAXB; ++k) {
-    const int t = threadIdx.x + k * blockDim.x;
-    if (t < total) {
-      const int p = t / nh, kx = t - p * nh;
-      A[kx * P + 2 * p] = keep[k][0];
-      A[kx * P + 2 * p + 1] = keep[k][1];
-    }
-  }
-  __syncthreads();
-  fft_smem_1buf<false, XY_MAXB>(A, n, nh, P, 1, tw, D, -1);
-  float2* cp = c + plane * (int64_t)n * nh;
-  for (int t = threadIdx.x; t < n * nh; t += blockDim.x) {
-    const int y = t / nh, kx = t - y * nh;
-    cp[t] = A[kx * P + y];
-  }
-}
-
-// ---- Fused inverse: FFT along y, then c2r along x (two rows per complex FFT), divided
-// `reps` times by `norm`; writes the real plane.
-__global__ void __launch_bounds__(512) k_fft_yx_c2r(const float2* __restrict__ c, float* __restrict__ r, FFTDesc D,
-                                                    float norm, int reps) {
-  extern __shared__ float2 sm[];
-  const int n = D.n, nh = n / 2 + 1, P = n + 1;
-  float2* tw = sm;
-  float2* A = sm + n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = D.tw[i];
-  const int64_t plane = blockIdx.x;
-  const float2* cp = c + plane * (int64_t)n * nh;
-  for (int t = threadIdx.x; t < n * nh; t += blockDim.x) {
-    const int y = t / nh, kx = t - y * nh;
-    A[kx * P + y] = cp[t];
-  }
-  __syncthreads();
-  fft_smem_1buf<false, XY_MAXB>(A, n, nh, P, 1, tw, D, +1);
-  // pack rows y=2p (real) and 2p+1 (imag): Z[k] = X0[k] + i X1[k] over the full
-  // Hermitian extension; imaginary parts at kx=0 and n/2 are dropped (c2r convention)
-  const int npairs = n / 2;
-  const int total = npairs * n;
-  float2 keep[2 * XY_MAXB];
-#pragma unroll
-  for (int k = 0; k < 2 * XY_MAXB; ++k) {
-    const int t = threadIdx.x + k * blockDim.x;
-    if (t < total) {
-      const int p = t / n, x = t - p * n;
-      float2 a0, a1;
-      if (x < nh) {
-        a0 = A[x * P + 2 * p];
-        a1 = A[x * P + 2 * p + 1];
-        if (x == 0 || 2 * x == n) { a0.y = 0.f; a1.y = 0.f; }
-      } else {
-        a0 = A[(n - x) * P + 2 * p];
-        a1 = A[(n - x) * P + 2 * p + 1];
-        a0.y = -a0.y;
-        a1.y = -a1.y;
-      }
-      keep[k] = make_float2(a0.x - a1.y, a0.y + a1.x);
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < 2 * XY_MAXB; ++k) {
-    const int t = threadIdx.x + k * blockDim.x;
-    if (t < total) {
-      const int p = t / n, x = t - p * n;
-      A[p * P + x] = keep[k];
-    }
-  }
-  __syncthreads();
-  fft_smem_1buf<false, XY_MAXB>(A, n, n / 2, P, 1, tw, D, +1);
-  float* rp = r + plane * (int64_t)n * n;
-  for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
-    const int y = t / n, x = t - y * n;
-    const float2 z = A[(y >> 1) * P + x];
-    float v = (y & 1) ? z.y : z.x;
-    for (int q = 0; q < reps; ++q) v = __fdiv_rn(v, norm);
-    rp[t] = v;
-  }
-}
-
 // ---- X pass: real rows -> half spectrum.  IN = float (plain) or long long (fixed point).
 template <typename IN>
 __global__ void k_fft_x_r2c(const IN* __restrict__ r, float2* __restrict__ c, int64_t nrows, FFTDesc D,

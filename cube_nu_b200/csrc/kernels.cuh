@@ -663,12 +663,10 @@ __global__ void k_interp_pm1(Geo G, int64_t np, const void* __restrict__ xp, con
   for (int k = 0; k < 7; ++k) {
     wx[k] = wrapi(i2[0] - 4 + k, nc);
     wy[k] = wrapi(i2[1] - 4 + k, nc) * nc;
-    wz[k] = wrapi(i2[2] - 4 + k, nc) * nc;
+    wz[k] = wrapi(i2[2] - 4 + k, nc) * nc * nc;
   }
   const int x0 = i2[0] - 1, y0 = i2[1] - 1, z0 = i2[2] - 1;
-  auto P = [&](int a, int b, int c) {
-    return __ldg(&phi[((size_t)wz[c - z0 + 2] + wy[b - y0 + 2]) * nc + wx[a - x0 + 2]]);
-  };
+  auto P = [&](int a, int b, int c) { return __ldg(&phi[wz[c - z0 + 2] + wy[b - y0 + 2] + wx[a - x0 + 2]]); };
   float dv[3], av[3];
   tsc_gather_force(i2, w, P, dv);
   apply_kick(vp, ip, dv, a_mid, dt, av);

@@ -188,10 +188,13 @@ def _all_class_state(p, seed=31):
     return state_from_positions(p, X, V)
 
 
-@pytest.mark.parametrize("fixed", [False, True])
-def test_every_pm3_class(oracle_lib, fixed):
-    """Potential and velocities for subtiles of every class: exercises the fused XY FFT
-    (mesh sides 48, 96, 144) and the separate-pass FFT (192)."""
+@pytest.mark.parametrize("fixed,generic", [(False, False), (True, False), (False, True)])
+def test_every_pm3_class(oracle_lib, fixed, generic, monkeypatch):
+    """Potential and velocities for subtiles of every class (mesh sides 48, 96, 144, 192),
+    through the size-specialised FFT passes and, with CUBE_FFT_GENERIC=1, the generic
+    Stockham passes."""
+    if generic:
+        monkeypatch.setenv("CUBE_FFT_GENERIC", "1")
     p = _params(fixed=fixed)
     st = _all_class_state(p)
     n = st[0].shape[0]
