@@ -114,7 +114,8 @@ class Clocks:
 # algorithmic bytes per kernel launch (roofline numerators)
 # ------------------------------------------------------------------------------------
 def kernel_bytes(p, name: str, n_particles: int, napm, fixed: bool):
-    """Algorithmic HBM bytes one launch of a kernel class must move (documented in DESIGN.md)."""
+    """Algorithmic HBM bytes a kernel class must move over one whole step (all its
+    launches together; documented in DESIGN.md)."""
     bx = 3 * p.izipx
     rb = 8 if fixed else 4
 
@@ -125,14 +126,14 @@ def kernel_bytes(p, name: str, n_particles: int, napm, fixed: bool):
                 "c": nh * 8 + n3 * 4}[what]
 
     if name.startswith("fft_") and name.endswith("_pm3"):
-        # one launch per class chunk; use the dominant class (2) with all its subtiles
+        # all class-2 subtiles (the dominant class); the y pass runs forward and inverse
         n = p.nft(2)
         nb = int(napm[2]) if napm is not None else p.ns3
         what = {"fft_x_pm3": "x", "fft_y_pm3": "y", "fft_z_green_pm3": "z", "fft_c2r_pm3": "c"}[name]
-        return mesh(n, nb, what)
+        return mesh(n, nb, what) * (2 if what == "y" else 1)
     if name.startswith("fft_") and name.endswith("_pm2"):
         what = {"fft_x_pm2": "x", "fft_y_pm2": "y", "fft_z_green_pm2": "z", "fft_c2r_pm2": "c"}[name]
-        return mesh(p.ngt, p.ntiles, what)
+        return mesh(p.ngt, p.ntiles, what) * (2 if what == "y" else 1)
     if name in ("deposit_pm1", "deposit_pm2", "deposit_pm3"):
         # read position code + cell index per particle, one read-modify-write of 27 cells
         boxes = {"deposit_pm1": 1.0, "deposit_pm2": (1 + 2 * p.ncb / p.nt) ** 3, "deposit_pm3": (1 + 2 / p.ntt) ** 3}[name]
@@ -339,18 +340,20 @@ def main():
         for name, (ms, cnt) in prof.items():
             if cnt == 0:
                 continue
-            b = kernel_bytes(p, name, n, napm, fixed)
-            avg = ms / cnt
-            rows.append((ms, name, cnt, avg, b))
+            b = kernel_bytes(p, name, n, napm, fixed)  # algorithmic bytes of the whole step's work
+            per_step_ms = ms / args.steps
+            rows.append((ms, name, cnt, ms / cnt, b, per_step_ms))
         rows.sort(reverse=True)
         dom = next((r for r in rows if r[4] is not None), None)
         hbm = float(peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
         roof = None
         if dom:
-            ach = dom[4] / (dom[3] / 1e3) / 1e9
+            launches_per_step = dom[2] / args.steps
+            ach = dom[4] / (dom[5] / 1e3) / 1e9
             roof = {"kernel": dom[1], "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                     "frac": round(ach / hbm, 4), "traffic": None, "peak_kind": peak_kind,
-                    "avg_launch_ms": round(dom[3], 4), "algorithmic_bytes_per_launch": dom[4]}
+                    "avg_launch_ms": round(dom[3], 4), "launches_per_step": launches_per_step,
+                    "algorithmic_bytes_per_launch": int(dom[4] / launches_per_step)}
         cpu = None
         if base_state is not None:
             v, cores, sample, secs = cpu_baseline(p, base_state, *base_args)
@@ -379,7 +382,8 @@ def main():
         if args.profile_json:
             with open(args.profile_json, "w") as f:
                 json.dump({"kernels": [{"name": r[1], "total_ms": r[0], "launches": r[2], "avg_ms": r[3],
-                                        "alg_bytes": r[4]} for r in rows], "steps": args.steps}, f, indent=1)
+                                        "alg_bytes_per_step": r[4], "ms_per_step": r[5]} for r in rows],
+                           "steps": args.steps}, f, indent=1)
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:

@@ -275,7 +275,7 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
   const int S = std::max(1, 256 / T);
   const size_t smx = (size_t)(N + S * N) * sizeof(float2);
   const unsigned gx = (unsigned)((nrows + 2 * S - 1) / (2 * S));
-  const int W = (N <= 256) ? 16 : (N <= 512 ? 8 : 4);
+  const int W = f2::fcol_width(N, T);
   const size_t smc = (size_t)(N + W * N) * sizeof(float2);
   dim3 gc((unsigned)(nbox * N), (unsigned)((NH + W - 1) / W));
   if (fixed) {
@@ -692,7 +692,7 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, c->green2, (float)n * (float)n * (float)n, 1, 2);
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
         maybe_capture(c, 2, c->cap_box, 1, phi + (c->cap_box - t0) * n3, n3, false);
-      LAUNCH(c, K_F2_PM2, 1, k_f2max_box<<<1184, 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1));
+      LAUNCH(c, K_F2_PM2, 1, k_f2max_box<<<f2max_box_grid(G.ngp, nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1));
       LAUNCH(c, K_INT_PM2, 1, k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, a_mid, dt, vm + 0, c->err));
     }
   }
@@ -753,7 +753,7 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, g3, (float)n * (float)n * (float)n, 1, 3);
       if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 1, phi + cap_slot * n3, n3, false);
       const int nf = G.nfp[cl];
-      LAUNCH(c, K_F2_PM3, 1, k_f2max_box<<<1184, 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2));
+      LAUNCH(c, K_F2_PM3, 1, k_f2max_box<<<f2max_box_grid(nf, nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2));
       LAUNCH(c, K_INT_PM3, 1, k_interp_pm3<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp, a_mid, dt, vm + 3,
                                                 c->err));
     }

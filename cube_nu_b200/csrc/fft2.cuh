@@ -198,7 +198,8 @@ __global__ void k_fx_r2c(const IN* __restrict__ r, float2* __restrict__ c, int64
 // ---------------------------------------------------------------------------------
 template <int N, int R1, int R2, int AXIS, int MODE>
 __global__ void k_fcol(float2* __restrict__ c, const float* __restrict__ green, const float2* __restrict__ gtw, int W) {
-  constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1;
+  constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, RPT = N / T;  // rows per thread
+  static_assert(N % T == 0, "rows must split evenly over the thread group");
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* A = sm + N;
@@ -207,36 +208,49 @@ __global__ void k_fcol(float2* __restrict__ c, const float* __restrict__ green, 
   const int64_t b = line / N;
   const int o = (int)(line - b * N);
   const int kx0 = blockIdx.y * W;
-  const int wv = min(W, NH - kx0);
+  const int col = threadIdx.x % W, t = threadIdx.x / W;  // blockDim = W*T
+  const bool live = kx0 + col < NH;
   const int64_t es = (AXIS == 1) ? NH : (int64_t)N * NH;
-  float2* base = c + b * (int64_t)N * N * NH + (AXIS == 1 ? (int64_t)o * N * NH : (int64_t)o * NH) + kx0;
-  for (int i = threadIdx.x; i < N * W; i += blockDim.x) {
-    const int e = i / W, q = i - e * W;
-    A[i] = (q < wv) ? base[e * es + q] : make_float2(0.f, 0.f);
+  float2* base = c + b * (int64_t)N * N * NH + (AXIS == 1 ? (int64_t)o * N * NH : (int64_t)o * NH) + kx0 + col;
+  {
+    float2 r[RPT];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) r[k] = live ? base[(int64_t)(t + k * T) * es] : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) A[(t + k * T) * W + col] = r[k];
   }
   __syncthreads();
-  const int col = threadIdx.x % W, t = threadIdx.x / W;
   if (MODE == 1) {
     seq_transform<N, R1, R2, +1>(A + col, W, t, tw);
   } else {
     seq_transform<N, R1, R2, -1>(A + col, W, t, tw);
     if (MODE == 2) {
-      const float* gb = green + (int64_t)o * NH + kx0;  // g[kz][y][kx], kz stride N*NH
-      for (int i = threadIdx.x; i < N * W; i += blockDim.x) {
-        const int e = i / W, q = i - e * W;
-        if (q < wv) {
-          const float gv = gb[(int64_t)e * N * NH + q];
-          const float2 v = A[i];
-          A[i] = make_float2(v.x * gv, v.y * gv);
+      if (live) {
+        const float* gb = green + (int64_t)o * NH + kx0 + col;  // g[kz][y][kx], kz stride N*NH
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+          const int e = t + k * T;
+          const float gv = __ldg(gb + (int64_t)e * N * NH);
+          const float2 v = A[e * W + col];
+          A[e * W + col] = make_float2(v.x * gv, v.y * gv);
         }
       }
       __syncthreads();
       seq_transform<N, R1, R2, +1>(A + col, W, t, tw);
     }
   }
-  for (int i = threadIdx.x; i < N * W; i += blockDim.x) {
-    const int e = i / W, q = i - e * W;
-    if (q < wv) base[e * es + q] = A[i];
+  if (live) {
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) base[(int64_t)(t + k * T) * es] = A[(t + k * T) * W + col];
+  }
+}
+
+// Column-block width: the whole half row when it fits one block, else an even split.
+__host__ inline int fcol_width(int N, int T) {
+  const int NH = N / 2 + 1;
+  for (int nb = 1;; ++nb) {
+    const int W = (NH + nb - 1) / nb;
+    if (W * T <= 1024 && (size_t)W * N * 8 <= 100 * 1024) return W;
   }
 }
 

@@ -532,30 +532,48 @@ __global__ void k_f2max_periodic(const float* __restrict__ phi, int nc, float* _
   block_max_to(v, f2out);
 }
 
-// Box meshes phi[b][n^3], index i at array i-m1phi; physical cells 1..nforce.  One warp
-// per x-row of physical cells, grid-stride over (box, z, y) rows.
-__global__ void k_f2max_box(const float* __restrict__ phi, int n, int nforce, int m1phi, int nbox,
-                            float* __restrict__ f2out) {
-  const int lane = threadIdx.x & 31;
-  const int wpb = blockDim.x >> 5;
-  float v = 0.f;
-  const int64_t rows_per_box = (int64_t)nforce * nforce;
-  const int64_t nrows = rows_per_box * nbox;
-  const int sy = n, sz = n * n;
-  for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < nrows; row += (int64_t)gridDim.x * wpb) {
-    const int b = (int)(row / rows_per_box);
-    const int r = (int)(row - (int64_t)b * rows_per_box);
-    const int z = r / nforce + 1, y = r - (z - 1) * nforce + 1;
-    const float* pb = phi + (size_t)b * n * n * n + (size_t)(z - m1phi) * sz + (size_t)(y - m1phi) * sy - m1phi;
-    for (int x = 1 + lane; x <= nforce; x += 32) {
-      const float* q = pb + x;
-      const float fx = grad4(q[-2], q[-1], q[1], q[2]);
-      const float fy = grad4(q[-2 * sy], q[-sy], q[sy], q[2 * sy]);
-      const float fz = grad4(q[-2 * sz], q[-sz], q[sz], q[2 * sz]);
-      v = fmaxf(v, sumsq3(fx, fy, fz));
+// Box meshes phi[b][n^3], index i at array i-m1phi; physical cells 1..nforce.  A block
+// owns a 32x8 tile of (x,y) in one box and marches through z with a ring of five
+// planes (tile plus a 2-cell halo) in shared memory, so each phi value is read about
+// 1.7 times.  grid = nbox * tiles; blockDim = 256.
+constexpr int F2_TX = 32, F2_TY = 8, F2_PX = F2_TX + 4, F2_PY = F2_TY + 4;
+__global__ void __launch_bounds__(256) k_f2max_box(const float* __restrict__ phi, int n, int nforce, int m1phi,
+                                                   int nbox, float* __restrict__ f2out) {
+  __shared__ float ring[5][F2_PY * F2_PX];
+  const int ntx = (nforce + F2_TX - 1) / F2_TX, nty = (nforce + F2_TY - 1) / F2_TY;
+  const int tile = blockIdx.x % (ntx * nty);
+  const int b = blockIdx.x / (ntx * nty);
+  const int tx0 = (tile % ntx) * F2_TX + 1, ty0 = (tile / ntx) * F2_TY + 1;  // first physical x,y of the tile
+  const float* pb = phi + (size_t)b * n * n * n;
+  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+  auto load_plane = [&](int z, float* dst) {  // tile plane z with halo 2 in x and y
+    for (int i = threadIdx.x; i < F2_PY * F2_PX; i += blockDim.x) {
+      const int py = i / F2_PX, px = i - py * F2_PX;
+      const int x = tx0 - 2 + px, y = ty0 - 2 + py;
+      // indices stay inside the padded box: x,y in [-1, nforce+2] map to [-1-m1phi, ..] >= 0
+      const bool in = (x - m1phi) < n && (y - m1phi) < n;
+      dst[i] = in ? __ldg(pb + ((size_t)(z - m1phi) * n + (y - m1phi)) * n + (x - m1phi)) : 0.f;
     }
+  };
+  for (int k = 0; k < 4; ++k) load_plane(k - 1, ring[k]);  // planes -1, 0, 1, 2
+  float v = 0.f;
+  const bool own = (tx0 + lx <= nforce) && (ty0 + ly <= nforce);
+  for (int z = 1; z <= nforce; ++z) {
+    load_plane(z + 2, ring[(z + 3) % 5]);
+    __syncthreads();
+    const float* c = ring[(z + 1) % 5];
+    const int o = (ly + 2) * F2_PX + (lx + 2);
+    const float fx = grad4(c[o - 2], c[o - 1], c[o + 1], c[o + 2]);
+    const float fy = grad4(c[o - 2 * F2_PX], c[o - F2_PX], c[o + F2_PX], c[o + 2 * F2_PX]);
+    const float fz = grad4(ring[(z - 1) % 5][o], ring[z % 5][o], ring[(z + 2) % 5][o], ring[(z + 3) % 5][o]);
+    if (own) v = fmaxf(v, sumsq3(fx, fy, fz));
+    __syncthreads();
   }
   block_max_to(v, f2out);
+}
+
+__host__ inline unsigned f2max_box_grid(int nforce, int nbox) {
+  return (unsigned)(((nforce + F2_TX - 1) / F2_TX) * ((nforce + F2_TY - 1) / F2_TY) * nbox);
 }
 
 // =================================================================================
