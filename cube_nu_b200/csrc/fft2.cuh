@@ -155,7 +155,7 @@ __device__ __forceinline__ void seq_transform(float2* base, int se, int t, const
 // X pass, r2c.  Block: S packed sequences (2S real rows); blockDim = S*T.
 // ---------------------------------------------------------------------------------
 template <int N, int R1, int R2, typename IN>
-__global__ void k_fx_r2c(const IN* __restrict__ r, float2* __restrict__ c, int64_t nrows, const float2* __restrict__ gtw,
+__global__ void __launch_bounds__(256) k_fx_r2c(const IN* __restrict__ r, float2* __restrict__ c, int64_t nrows, const float2* __restrict__ gtw,
                          float scale) {
   constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1;
   extern __shared__ float2 sm[];
@@ -197,7 +197,7 @@ __global__ void k_fx_r2c(const IN* __restrict__ r, float2* __restrict__ c, int64
 // grid.x = b*N + (z for AXIS 1 | y for AXIS 2), grid.y = kx block of W; blockDim = W*T.
 // ---------------------------------------------------------------------------------
 template <int N, int R1, int R2, int AXIS, int MODE>
-__global__ void k_fcol(float2* __restrict__ c, const float* __restrict__ green, const float2* __restrict__ gtw, int W) {
+__global__ void __launch_bounds__(512) k_fcol(float2* __restrict__ c, const float* __restrict__ green, const float2* __restrict__ gtw, int W) {
   constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, RPT = N / T;  // rows per thread
   static_assert(N % T == 0, "rows must split evenly over the thread group");
   extern __shared__ float2 sm[];
@@ -245,12 +245,13 @@ __global__ void k_fcol(float2* __restrict__ c, const float* __restrict__ green, 
   }
 }
 
-// Column-block width: the whole half row when it fits one block, else an even split.
+// Column-block width: the whole half row when it fits one block (<= 512 threads, the
+// launch bound), else an even split.
 __host__ inline int fcol_width(int N, int T) {
   const int NH = N / 2 + 1;
   for (int nb = 1;; ++nb) {
     const int W = (NH + nb - 1) / nb;
-    if (W * T <= 1024 && (size_t)W * N * 8 <= 100 * 1024) return W;
+    if (W * T <= 512 && (size_t)W * N * 8 <= 100 * 1024) return W;
   }
 }
 
@@ -258,7 +259,7 @@ __host__ inline int fcol_width(int N, int T) {
 // X' pass, c2r, divided `reps` times by `norm`.
 // ---------------------------------------------------------------------------------
 template <int N, int R1, int R2>
-__global__ void k_fx_c2r(const float2* __restrict__ c, float* __restrict__ r, int64_t nrows, const float2* __restrict__ gtw,
+__global__ void __launch_bounds__(256) k_fx_c2r(const float2* __restrict__ c, float* __restrict__ r, int64_t nrows, const float2* __restrict__ gtw,
                          float norm, int reps) {
   constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1;
   extern __shared__ float2 sm[];

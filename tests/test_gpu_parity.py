@@ -219,3 +219,29 @@ def test_every_pm3_class(oracle_lib, fixed, generic, monkeypatch):
     d = v_ref - st[1]
     err = np.abs((v_gpu - st[1]) - d).max() / np.abs(d).max()
     assert err < 2e-4, err
+
+
+@pytest.mark.parametrize("geom", ["proxy", "ng1024"])
+def test_potential_at_bench_sizes(oracle_lib, geom):
+    """FFT sizes of the 512^3 benchmark: PM2 tiles of 288^3 and PM3 subtiles of 144^3
+    (one-tile geometry), and the PM1 mesh of 256^3 (ng=1024)."""
+    from cube_nu_b200.params import Params
+    from tests.helpers import uniform_state
+
+    if geom == "proxy":
+        p = Params(ng=256, nnt=1, nns=4, np_nc=2, izipx=2, box=250.0)
+        cases = [(1, 0, p.nc ** 3, 1), (2, 0, p.ngt ** 3, 3), (3, 5, p.nft(2) ** 3, 7)]
+    else:
+        p = Params(ng=1024, nnt=4, nns=4, np_nc=2, izipx=2, box=1000.0)
+        cases = [(1, 0, p.nc ** 3, 1)]
+    n = 40000
+    st = uniform_state(p, n, seed=41)
+    p.mass_p_cdm = float(p.ng) ** 3 / (p.nc * p.np_nc) ** 3
+    for level, box, size, only in cases:
+        _, ref = oracle_lib.kick(p, st[0], st[1].copy(), st[3], 0.1, 0.05, only=only, debug=(level, box, 1, size))
+        with _ctx(p, st) as ctx:
+            ctx.capture(level, box, 1)
+            ctx.kick(0.1, 0.05)
+            got = ctx.captured(size)
+        err = np.abs(got - ref).max() / np.abs(ref).max()
+        assert err < 2e-5, "%s level %d phi rel err %.3g" % (geom, level, err)
