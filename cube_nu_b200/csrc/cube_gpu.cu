@@ -235,22 +235,37 @@ Geo make_geo(const cube_params& p) {
   return g;
 }
 
-// Mesh bytes for nbox boxes of side n: real (4 or 8 B), half spectrum (8 B).
+// In-place mesh layout: a box of side n has n*n rows of RP bytes, RP = max(n*rb, (n/2+1)*8),
+// so a real row (rb = 4, or 8 for the int64 fixed-point deposit) and its half-spectrum
+// row share the same bytes; the potential is written back over them.
+struct Pitch {
+  int64_t rp;  // row pitch in bytes
+  int pr, pc, pf;  // real elements, complex elements and floats per row
+};
+Pitch pitch_of(int n, bool fixed) {
+  const int64_t rb = fixed ? 8 : 4;
+  Pitch p;
+  p.rp = std::max<int64_t>((int64_t)n * rb, (int64_t)(n / 2 + 1) * 8);
+  p.pr = (int)(p.rp / rb);
+  p.pc = (int)(p.rp / 8);
+  p.pf = (int)(p.rp / 4);
+  return p;
+}
+
 size_t mesh_bytes(int n, int64_t nbox, bool fixed) {
-  const size_t n3 = (size_t)n * n * n, nh = (size_t)n * n * (n / 2 + 1);
-  return (size_t)nbox * (n3 * (fixed ? 8 : 4) + nh * 8 + 256);
+  return (size_t)nbox * n * n * pitch_of(n, fixed).rp + 256;
 }
 
 struct MeshPtrs {
   void* real;
   float2* ck;
+  Pitch pt;
 };
-MeshPtrs mesh_ptrs(cube_ctx* c, int n, int64_t nbox, bool fixed) {
-  const size_t n3 = (size_t)n * n * n;
+MeshPtrs mesh_ptrs(cube_ctx* c, int n, int64_t, bool fixed) {
   MeshPtrs m;
   m.real = c->arena;
-  size_t off = ((size_t)nbox * n3 * (fixed ? 8 : 4) + 255) & ~(size_t)255;
-  m.ck = reinterpret_cast<float2*>((char*)c->arena + off);
+  m.ck = reinterpret_cast<float2*>(c->arena);
+  m.pt = pitch_of(n, fixed);
   return m;
 }
 
@@ -265,40 +280,64 @@ void smem_optin(K kernel, size_t bytes) {
   if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-// Size-specialised passes (fft2.cuh) for N = R1*R2.
+// Size-specialised passes (fft2.cuh) for N = R1*R2.  N <= 144 runs the fused plane
+// kernels (XY forward, YX inverse) around the z pass; larger N runs five passes.
 template <int N, int R1, int R2>
 void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out, float2* ck,
-              const float* green, float norm, int reps, int kx, int ky, int kz, int kc) {
+              const float* green, float norm, int reps, int kx, int ky, int kz, int kc, const Pitch& pt) {
   constexpr int T = f2::TPS<R1, R2>::T, NH = N / 2 + 1;
   const float2* tw = fft_desc(c, N)->tw;
   const int64_t nrows = nbox * (int64_t)N * N;
-  const int S = std::max(1, 256 / T);
-  const size_t smx = (size_t)(N + S * N) * sizeof(float2);
-  const unsigned gx = (unsigned)((nrows + 2 * S - 1) / (2 * S));
   const int W = f2::fcol_width(N, T);
   const size_t smc = (size_t)(N + W * N) * sizeof(float2);
   dim3 gc((unsigned)(nbox * N), (unsigned)((NH + W - 1) / W));
+  constexpr bool fused = (N <= 144) && (f2::PlaneSm<N>::BYTES <= 200 * 1024);
+  if constexpr (fused) {
+    const size_t smp = f2::PlaneSm<N>::BYTES;
+    const unsigned planes = (unsigned)(nbox * N);
+    if (fixed) {
+      smem_optin(f2::k_fxy_r2c<N, R1, R2, long long>, smp);
+      LAUNCH(c, kx, 1, f2::k_fxy_r2c<N, R1, R2, long long><<<planes, f2::PLANE_THREADS, smp, c->s>>>(
+                           (const long long*)real_in, ck, tw, scale, pt.pr, pt.pc));
+    } else {
+      smem_optin(f2::k_fxy_r2c<N, R1, R2, float>, smp);
+      LAUNCH(c, kx, 1, f2::k_fxy_r2c<N, R1, R2, float><<<planes, f2::PLANE_THREADS, smp, c->s>>>(
+                           (const float*)real_in, ck, tw, scale, pt.pr, pt.pc));
+    }
+    smem_optin(f2::k_fcol<N, R1, R2, 2, 2>, smc);
+    LAUNCH(c, kz, 1, f2::k_fcol<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc));
+    smem_optin(f2::k_fyx_c2r<N, R1, R2>, smp);
+    LAUNCH(c, kc, 1, f2::k_fyx_c2r<N, R1, R2><<<planes, f2::PLANE_THREADS, smp, c->s>>>(ck, phi_out, tw, norm, reps,
+                                                                                        pt.pc, pt.pf));
+    return;
+  } else {
+  const int S = std::max(1, 256 / T);
+  const size_t smx = (size_t)(N + S * N) * sizeof(float2);
+  const unsigned gx = (unsigned)((nrows + 2 * S - 1) / (2 * S));
   if (fixed) {
     smem_optin(f2::k_fx_r2c<N, R1, R2, long long>, smx);
-    LAUNCH(c, kx, 1, f2::k_fx_r2c<N, R1, R2, long long><<<gx, S * T, smx, c->s>>>((const long long*)real_in, ck, nrows, tw, scale));
+    LAUNCH(c, kx, 1, f2::k_fx_r2c<N, R1, R2, long long><<<gx, S * T, smx, c->s>>>((const long long*)real_in, ck, nrows,
+                                                                                 tw, scale, pt.pr, pt.pc));
   } else {
     smem_optin(f2::k_fx_r2c<N, R1, R2, float>, smx);
-    LAUNCH(c, kx, 1, f2::k_fx_r2c<N, R1, R2, float><<<gx, S * T, smx, c->s>>>((const float*)real_in, ck, nrows, tw, scale));
+    LAUNCH(c, kx, 1, f2::k_fx_r2c<N, R1, R2, float><<<gx, S * T, smx, c->s>>>((const float*)real_in, ck, nrows, tw,
+                                                                             scale, pt.pr, pt.pc));
   }
   smem_optin(f2::k_fcol<N, R1, R2, 1, 0>, smc);
   smem_optin(f2::k_fcol<N, R1, R2, 2, 2>, smc);
   smem_optin(f2::k_fcol<N, R1, R2, 1, 1>, smc);
   smem_optin(f2::k_fx_c2r<N, R1, R2>, smx);
-  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W));
-  LAUNCH(c, kz, 1, f2::k_fcol<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W));
-  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 1><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W));
-  LAUNCH(c, kc, 1, f2::k_fx_c2r<N, R1, R2><<<gx, S * T, smx, c->s>>>(ck, phi_out, nrows, tw, norm, reps));
+  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc));
+  LAUNCH(c, kz, 1, f2::k_fcol<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc));
+  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 1><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc));
+  LAUNCH(c, kc, 1, f2::k_fx_c2r<N, R1, R2><<<gx, S * T, smx, c->s>>>(ck, phi_out, nrows, tw, norm, reps, pt.pc, pt.pf));
+  }
 }
 
 bool fft2_dispatch(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out,
-                   float2* ck, const float* green, float norm, int reps, int kx, int ky, int kz, int kc) {
+                   float2* ck, const float* green, float norm, int reps, int kx, int ky, int kz, int kc, const Pitch& pt) {
 #define CUBE_FFT2(N, R1, R2) \
-  case N: fft2_run<N, R1, R2>(c, nbox, real_in, fixed, scale, phi_out, ck, green, norm, reps, kx, ky, kz, kc); return true;
+  case N: fft2_run<N, R1, R2>(c, nbox, real_in, fixed, scale, phi_out, ck, green, norm, reps, kx, ky, kz, kc, pt); return true;
   switch (n) {
     CUBE_FFT2(16, 4, 4)
     CUBE_FFT2(32, 4, 8)
@@ -325,8 +364,9 @@ void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixe
   const int ky = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTY_PM2 : K_FFTY_PM3;
   const int kz = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTZ_PM2 : K_FFTZ_PM3;
   const int kc = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTC_PM2 : K_FFTC_PM3;
+  const Pitch pt = pitch_of(n, fixed);
   if (c->fft_generic == 0 &&
-      fft2_dispatch(c, n, nbox, real_in, fixed, scale, phi_out, ck, green, norm, reps, kx, ky, kz, kc))
+      fft2_dispatch(c, n, nbox, real_in, fixed, scale, phi_out, ck, green, norm, reps, kx, ky, kz, kc, pt))
     return;
   const FFTDesc& D = *fft_desc(c, n);
   const int nh = n / 2 + 1;
@@ -335,16 +375,18 @@ void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixe
   const size_t smx = (size_t)(n + 2 * rpb * n) * sizeof(float2);
   const unsigned gx = (unsigned)((nrows + rpb - 1) / rpb);
   if (fixed)
-    LAUNCH(c, kx, 1, k_fft_x_r2c<long long><<<gx, 256, smx, c->s>>>((const long long*)real_in, ck, nrows, D, rpb, scale));
+    LAUNCH(c, kx, 1, k_fft_x_r2c<long long><<<gx, 256, smx, c->s>>>((const long long*)real_in, ck, nrows, D, rpb, scale,
+                                                                    pt.pr, pt.pc));
   else
-    LAUNCH(c, kx, 1, k_fft_x_r2c<float><<<gx, 256, smx, c->s>>>((const float*)real_in, ck, nrows, D, rpb, scale));
+    LAUNCH(c, kx, 1, k_fft_x_r2c<float><<<gx, 256, smx, c->s>>>((const float*)real_in, ck, nrows, D, rpb, scale, pt.pr,
+                                                                pt.pc));
   const int W = (n <= 256) ? 16 : (n <= 512 ? 8 : 4);
   const size_t smy = (size_t)(n + 2 * W * n) * sizeof(float2);
   dim3 gy((unsigned)(nbox * n), (unsigned)((nh + W - 1) / W));
-  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1));
-  LAUNCH(c, kz, 1, k_fft_z_green<<<gy, 256, smy, c->s>>>(ck, green, D, W));
-  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1));
-  LAUNCH(c, kc, 1, k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, norm, reps));
+  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1, pt.pc));
+  LAUNCH(c, kz, 1, k_fft_z_green<<<gy, 256, smy, c->s>>>(ck, green, D, W, pt.pc));
+  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1, pt.pc));
+  LAUNCH(c, kc, 1, k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, norm, reps, pt.pc, pt.pf));
 }
 
 inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
@@ -365,15 +407,18 @@ float* green3(cube_ctx* c, int iapm) {
   return c->green3[iapm];
 }
 
-// Copy a box field into the capture buffer when it is the one requested.
-void maybe_capture(cube_ctx* c, int level, int64_t box, int what, const void* src, int64_t n, bool fixed_int) {
+// Copy a box field (n^3 values in rows of `row_bytes` at `pitch` bytes) into a dense
+// capture buffer when it is the one requested.
+void maybe_capture(cube_ctx* c, int level, int64_t box, int what, const void* src, int n, bool fixed_int,
+                   int64_t pitch) {
   if (c->cap_level != level || c->cap_box != box || c->cap_what != what) return;
   cudaFree(c->cap_buf);
   c->cap_buf = nullptr;
-  c->cap_n = n;
-  if (cudaMalloc(&c->cap_buf, n * (fixed_int ? 8 : 4)) != cudaSuccess) return;
-  cudaMemcpyAsync(c->cap_buf, src, n * (fixed_int ? 8 : 4), cudaMemcpyDeviceToDevice, c->s);
-  if (fixed_int) c->cap_n = -n;  // marks int64 content
+  const int64_t cnt = (int64_t)n * n * n;
+  const size_t eb = fixed_int ? 8 : 4;
+  if (cudaMalloc(&c->cap_buf, cnt * eb) != cudaSuccess) return;
+  cudaMemcpy2DAsync(c->cap_buf, n * eb, src, pitch, n * eb, (size_t)n * n, cudaMemcpyDeviceToDevice, c->s);
+  c->cap_n = fixed_int ? -cnt : cnt;  // negative marks int64 content
 }
 
 }  // namespace
@@ -524,7 +569,8 @@ static int alloc_particles(cube_ctx* c, int64_t np) {
   const Geo& G = c->G;
   const bool fixed = c->P.deposit_mode == CUBE_DEPOSIT_FIXED;
   size_t need = std::max(mesh_bytes(G.nc, 1, fixed), mesh_bytes(G.ngt, c->ntiles, fixed));
-  for (int i = 2; i <= 5; ++i) need = std::max(need, mesh_bytes(G.nft[i], c->ns3, fixed) / 4);
+  need = std::max(need, mesh_bytes(G.nft[2], c->ns3, fixed));  // every subtile in the lightest class
+  for (int i = 3; i <= 5; ++i) need = std::max(need, mesh_bytes(G.nft[i], std::max<int64_t>(1, c->ns3 / 16), fixed));
   size_t fre = 0, tot = 0;
   CK(cudaMemGetInfo(&fre, &tot));
   size_t budget = (size_t)(0.7 * (double)fre);
@@ -663,37 +709,36 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
   {
     const int n = G.nc;
     MeshPtrs m = mesh_ptrs(c, n, 1, fixed);
-    const int64_t n3 = (int64_t)n * n * n;
-    CK(cudaMemsetAsync(m.real, 0, n3 * (fixed ? 8 : 4), c->s));
-    if (fixed) LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real));
-    else LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real));
-    maybe_capture(c, 1, 0, 0, m.real, n3, fixed);
+    CK(cudaMemsetAsync(m.real, 0, mesh_bytes(n, 1, fixed), c->s));
+    if (fixed) LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr));
+    else LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr));
+    maybe_capture(c, 1, 0, 0, m.real, n, fixed, m.pt.rp);
     float* phi = reinterpret_cast<float*>(m.real);
     launch_fft(c, n, 1, m.real, fixed, G.mass_p, phi, m.ck, c->green1, (float)n, 3, 1);
-    maybe_capture(c, 1, 0, 1, phi, n3, false);
-    LAUNCH(c, K_F2_PM1, 1, k_f2max_periodic<<<(unsigned)std::min<int64_t>(1184, (int64_t)n * n / 8 + 1), 256, 0, c->s>>>(phi, n, f2 + 0));
-    LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, a_mid, dt));
+    maybe_capture(c, 1, 0, 1, phi, n, false, m.pt.rp);
+    LAUNCH(c, K_F2_PM1, 1, k_f2max_periodic<<<(unsigned)std::min<int64_t>(1184, (int64_t)n * n / 8 + 1), 256, 0, c->s>>>(phi, n, f2 + 0, m.pt.pf));
+    LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, a_mid, dt, m.pt.pf));
   }
   CK(cudaEventRecord(c->ev[1], c->s));
   // ---------------- PM2 (kick.f90:47-77) ----------------
   {
     const int n = G.ngt;
-    const int64_t n3 = (int64_t)n * n * n;
     const int64_t per = std::min<int64_t>(c->ntiles, boxes_fit(c, n, fixed));
     for (int t0 = 0; t0 < c->ntiles; t0 += (int)per) {
       const int nb = (int)std::min<int64_t>(per, c->ntiles - t0);
       MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
-      CK(cudaMemsetAsync(m.real, 0, nb * n3 * (fixed ? 8 : 4), c->s));
-      if (fixed) LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb));
-      else LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb));
+      const int64_t boxb = (int64_t)n * n * m.pt.rp;
+      CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
+      if (fixed) LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb, m.pt.pr));
+      else LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb, m.pt.pr));
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
-        maybe_capture(c, 2, c->cap_box, 0, (char*)m.real + (c->cap_box - t0) * n3 * (fixed ? 8 : 4), n3, fixed);
+        maybe_capture(c, 2, c->cap_box, 0, (char*)m.real + (c->cap_box - t0) * boxb, n, fixed, m.pt.rp);
       float* phi = reinterpret_cast<float*>(m.real);
       launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, c->green2, (float)n * (float)n * (float)n, 1, 2);
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
-        maybe_capture(c, 2, c->cap_box, 1, phi + (c->cap_box - t0) * n3, n3, false);
-      LAUNCH(c, K_F2_PM2, 1, k_f2max_box<<<f2max_box_grid(G.ngp, nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1));
-      LAUNCH(c, K_INT_PM2, 1, k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, a_mid, dt, vm + 0, c->err));
+        maybe_capture(c, 2, c->cap_box, 1, (char*)m.real + (c->cap_box - t0) * boxb, n, false, m.pt.rp);
+      LAUNCH(c, K_F2_PM2, 1, k_f2max_box<<<f2max_box_grid(G.ngp, nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1, m.pt.pf));
+      LAUNCH(c, K_INT_PM2, 1, k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, a_mid, dt, vm + 0, c->err, m.pt.pf));
     }
   }
   CK(cudaEventRecord(c->ev[2], c->s));
@@ -737,25 +782,25 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     for (int64_t k = 0; k < nch; ++k) {
       const int cl = chunks[k].iapm, nb = chunks[k].nb;
       const int n = G.nft[cl];
-      const int64_t n3 = (int64_t)n * n * n;
       const float* g3 = green3(c, cl);
       if (!g3) return CUBE_E_CUDA;
       const int32_t* slots = c->box_slot + k * c->ns3;
       MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
-      CK(cudaMemsetAsync(m.real, 0, nb * n3 * (fixed ? 8 : 4), c->s));
-      if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err));
-      else LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err));
+      const int64_t boxb = (int64_t)n * n * m.pt.rp;
+      CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
+      if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr));
+      else LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr));
       int cap_slot = -1;
       if (c->cap_level == 3 && c->cap_box >= 0 && c->cap_box < c->ns3 && ires[c->cap_box] == cl)
         cap_slot = c->h_slots[k * c->ns3 + c->cap_box];
-      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 0, (char*)m.real + cap_slot * n3 * (fixed ? 8 : 4), n3, fixed);
+      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 0, (char*)m.real + cap_slot * boxb, n, fixed, m.pt.rp);
       float* phi = reinterpret_cast<float*>(m.real);
       launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, g3, (float)n * (float)n * (float)n, 1, 3);
-      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 1, phi + cap_slot * n3, n3, false);
+      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 1, (char*)m.real + cap_slot * boxb, n, false, m.pt.rp);
       const int nf = G.nfp[cl];
-      LAUNCH(c, K_F2_PM3, 1, k_f2max_box<<<f2max_box_grid(nf, nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2));
+      LAUNCH(c, K_F2_PM3, 1, k_f2max_box<<<f2max_box_grid(nf, nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2, m.pt.pf));
       LAUNCH(c, K_INT_PM3, 1, k_interp_pm3<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp, a_mid, dt, vm + 3,
-                                                c->err));
+                                                c->err, m.pt.pf));
     }
   }
   CK(cudaEventRecord(c->ev[3], c->s));

@@ -104,8 +104,7 @@ __device__ float2* fft_smem(float2* a, float2* b, int n, int nb, int sb, int se,
 
 // ---- X pass: real rows -> half spectrum.  IN = float (plain) or long long (fixed point).
 template <typename IN>
-__global__ void k_fft_x_r2c(const IN* __restrict__ r, float2* __restrict__ c, int64_t nrows, FFTDesc D,
-                            int rpb, float scale) {
+__global__ void k_fft_x_r2c(const IN* r, float2* c, int64_t nrows, FFTDesc D, int rpb, float scale, int pr, int pc) {
   extern __shared__ float2 sm[];
   const int n = D.n, nh = n / 2 + 1;
   float2* tw = sm;
@@ -115,7 +114,8 @@ __global__ void k_fft_x_r2c(const IN* __restrict__ r, float2* __restrict__ c, in
   const int64_t row0 = (int64_t)blockIdx.x * rpb;
   const int nr = (int)min((int64_t)rpb, nrows - row0);
   for (int t = threadIdx.x; t < nr * n; t += blockDim.x) {
-    const IN v = r[row0 * n + t];
+    const int rr = t / n, x = t - rr * n;
+    const IN v = r[(row0 + rr) * pr + x];
     float f;
     if (sizeof(IN) == 8) f = (float)((double)(long long)v * 9.094947017729282e-13);  // 2^-40
     else f = (float)v;
@@ -125,12 +125,12 @@ __global__ void k_fft_x_r2c(const IN* __restrict__ r, float2* __restrict__ c, in
   float2* res = fft_smem<false>(a, b, n, nr, n, 1, tw, D, -1);
   for (int t = threadIdx.x; t < nr * nh; t += blockDim.x) {
     const int rr = t / nh, x = t - rr * nh;
-    c[(row0 + rr) * nh + x] = res[rr * n + x];
+    c[(row0 + rr) * pc + x] = res[rr * n + x];
   }
 }
 
 // ---- Y pass (forward or inverse) on c[b][z][y][kx]; grid = (b*n+z, kx block).
-__global__ void k_fft_y(float2* __restrict__ c, FFTDesc D, int W, int dir) {
+__global__ void k_fft_y(float2* __restrict__ c, FFTDesc D, int W, int dir, int pc) {
   extern __shared__ float2 sm[];
   const int n = D.n, nh = n / 2 + 1;
   float2* tw = sm;
@@ -140,22 +140,22 @@ __global__ void k_fft_y(float2* __restrict__ c, FFTDesc D, int W, int dir) {
   const int64_t bz = blockIdx.x;  // b*n + z
   const int kx0 = blockIdx.y * W;
   const int wv = min(W, nh - kx0);
-  float2* base = c + bz * (int64_t)n * nh + kx0;
+  float2* base = c + bz * (int64_t)n * pc + kx0;
   for (int t = threadIdx.x; t < n * W; t += blockDim.x) {
     const int y = t / W, q = t - y * W;
-    a[y * W + q] = (q < wv) ? base[(int64_t)y * nh + q] : make_float2(0.f, 0.f);
+    a[y * W + q] = (q < wv) ? base[(int64_t)y * pc + q] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   float2* res = fft_smem<true>(a, b, n, W, 1, W, tw, D, dir);
   for (int t = threadIdx.x; t < n * W; t += blockDim.x) {
     const int y = t / W, q = t - y * W;
-    if (q < wv) base[(int64_t)y * nh + q] = res[y * W + q];
+    if (q < wv) base[(int64_t)y * pc + q] = res[y * W + q];
   }
 }
 
 // ---- Z pass: forward FFT along z, multiply by the Green table g[kz][ky][kx], inverse.
 // grid = (b*n+y, kx block).
-__global__ void k_fft_z_green(float2* __restrict__ c, const float* __restrict__ g, FFTDesc D, int W) {
+__global__ void k_fft_z_green(float2* __restrict__ c, const float* __restrict__ g, FFTDesc D, int W, int pc) {
   extern __shared__ float2 sm[];
   const int n = D.n, nh = n / 2 + 1;
   float2* tw = sm;
@@ -167,19 +167,19 @@ __global__ void k_fft_z_green(float2* __restrict__ c, const float* __restrict__ 
   const int y = (int)(by - bb * n);
   const int kx0 = blockIdx.y * W;
   const int wv = min(W, nh - kx0);
-  const int64_t zstride = (int64_t)n * nh;
-  float2* base = c + bb * (int64_t)n * zstride + (int64_t)y * nh + kx0;
+  const int64_t zstride = (int64_t)n * pc;
+  float2* base = c + bb * (int64_t)n * zstride + (int64_t)y * pc + kx0;
   for (int t = threadIdx.x; t < n * W; t += blockDim.x) {
     const int z = t / W, q = t - z * W;
     a[z * W + q] = (q < wv) ? base[(int64_t)z * zstride + q] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   float2* res = fft_smem<true>(a, b, n, W, 1, W, tw, D, -1);
-  const float* gb = g + (int64_t)y * nh + kx0;
+  const float* gb = g + (int64_t)y * nh + kx0;  // dense table, pitch nh
   for (int t = threadIdx.x; t < n * W; t += blockDim.x) {
     const int z = t / W, q = t - z * W;
     if (q < wv) {
-      const float gv = gb[(int64_t)z * zstride + q];
+      const float gv = gb[(int64_t)z * n * nh + q];
       float2 v = res[z * W + q];
       res[z * W + q] = make_float2(v.x * gv, v.y * gv);
     }
@@ -195,8 +195,8 @@ __global__ void k_fft_z_green(float2* __restrict__ c, const float* __restrict__ 
 
 // ---- X' pass: half spectrum rows -> real rows, divided `reps` times by `norm`
 // (PM1: three times by nw, pencil_fft.f90:77; PM2/PM3: once by nwork^3, kick.f90:846).
-__global__ void k_fft_x_c2r(const float2* __restrict__ c, float* __restrict__ r, int64_t nrows, FFTDesc D, int rpb,
-                            float norm, int reps) {
+__global__ void k_fft_x_c2r(const float2* c, float* r, int64_t nrows, FFTDesc D, int rpb, float norm, int reps,
+                            int pc, int pf) {
   extern __shared__ float2 sm[];
   const int n = D.n, nh = n / 2 + 1;
   float2* tw = sm;
@@ -209,10 +209,10 @@ __global__ void k_fft_x_c2r(const float2* __restrict__ c, float* __restrict__ r,
     const int rr = t / n, x = t - rr * n;
     float2 v;
     if (x < nh) {
-      v = c[(row0 + rr) * nh + x];
+      v = c[(row0 + rr) * pc + x];
       if (x == 0 || 2 * x == n) v.y = 0.f;
     } else {
-      v = c[(row0 + rr) * nh + (n - x)];
+      v = c[(row0 + rr) * pc + (n - x)];
       v.y = -v.y;
     }
     a[t] = v;
@@ -222,7 +222,8 @@ __global__ void k_fft_x_c2r(const float2* __restrict__ c, float* __restrict__ r,
   for (int t = threadIdx.x; t < nr * n; t += blockDim.x) {
     float v = res[t].x;
     for (int q = 0; q < reps; ++q) v = __fdiv_rn(v, norm);
-    r[row0 * n + t] = v;
+    const int rr = t / n, x = t - rr * n;
+    r[(row0 + rr) * pf + x] = v;
   }
 }
 

@@ -151,12 +151,31 @@ __device__ __forceinline__ void seq_transform(float2* base, int se, int t, const
   __syncthreads();
 }
 
+// Same as seq_transform, for thread groups where some threads have no sequence this
+// round (they still take part in the barriers).
+template <int N, int R1, int R2, int DIR>
+__device__ __forceinline__ void seq_transform_g(float2* base, int se, int t, const float2* tw, bool active) {
+  using S = Seq<N, R1, R2, DIR>;
+  if (active && t < R2) S::step1(base, se, t, tw);
+  __syncthreads();
+  float2 w[R2];
+  if (active && t < R1) S::step2_load(base, se, t, w, tw);
+  __syncthreads();
+  if (active && t < R1) S::step2_store(base, se, t, w);
+  __syncthreads();
+}
+
+// Mesh layout (in place): box of side N, row pitch RP bytes = max(N*rb, (N/2+1)*8) so a
+// real row and its half-spectrum row share the same bytes (FFTW's in-place r2c layout).
+// pr = RP/rb real elements, pc = RP/8 complex elements, pf = RP/4 floats per row.
+
 // ---------------------------------------------------------------------------------
-// X pass, r2c.  Block: S packed sequences (2S real rows); blockDim = S*T.
+// X pass, r2c.  Block: S packed sequences (2S real rows); blockDim = S*T.  In place:
+// the block loads all its rows before writing their spectra.
 // ---------------------------------------------------------------------------------
 template <int N, int R1, int R2, typename IN>
-__global__ void __launch_bounds__(256) k_fx_r2c(const IN* __restrict__ r, float2* __restrict__ c, int64_t nrows, const float2* __restrict__ gtw,
-                         float scale) {
+__global__ void __launch_bounds__(256) k_fx_r2c(const IN* r, float2* c, int64_t nrows, const float2* __restrict__ gtw,
+                                                float scale, int pr, int pc) {
   constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1;
   extern __shared__ float2 sm[];
   float2* tw = sm;
@@ -165,12 +184,11 @@ __global__ void __launch_bounds__(256) k_fx_r2c(const IN* __restrict__ r, float2
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
   const int64_t row0 = (int64_t)blockIdx.x * 2 * S;
   const int nr = (int)min((int64_t)2 * S, nrows - row0);
-  const IN* rp = r + row0 * N;
   for (int i = threadIdx.x; i < 2 * S * N; i += blockDim.x) {
     const int row = i / N, x = i - row * N;
     float f = 0.f;
     if (row < nr) {
-      const IN v = rp[i];
+      const IN v = r[(row0 + row) * pr + x];
       if (sizeof(IN) == 8) f = (float)((double)(long long)v * 9.094947017729282e-13);  // 2^-40
       else f = (float)v;
       f = __fmul_rn(f, scale);
@@ -180,24 +198,25 @@ __global__ void __launch_bounds__(256) k_fx_r2c(const IN* __restrict__ r, float2
   __syncthreads();
   const int s = threadIdx.x / T, t = threadIdx.x - s * T;
   seq_transform<N, R1, R2, -1>(Z + s * N, 1, t, tw);
-  float2* cp = c + row0 * NH;
   for (int i = threadIdx.x; i < S * NH; i += blockDim.x) {
     const int q = i / NH, k = i - q * NH;
     if (2 * q >= nr) continue;
     const float2 z = Z[q * N + k];
     const float2 zc = Z[q * N + ((N - k) % N)];
-    cp[(2 * q) * NH + k] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
-    if (2 * q + 1 < nr) cp[(2 * q + 1) * NH + k] = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+    c[(row0 + 2 * q) * pc + k] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+    if (2 * q + 1 < nr) c[(row0 + 2 * q + 1) * pc + k] = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
   }
 }
 
 // ---------------------------------------------------------------------------------
-// Column pass on the half spectrum c[b][z][y][kx].  MODE 0: forward, 1: inverse,
-// 2: forward, times green[kz][ky][kx], inverse (z pass).  AXIS 1: y, 2: z.
-// grid.x = b*N + (z for AXIS 1 | y for AXIS 2), grid.y = kx block of W; blockDim = W*T.
+// Column pass on the half spectrum c[b][z][y][kx] (row pitch pc).  MODE 0: forward,
+// 1: inverse, 2: forward, times green[kz][ky][kx] (dense, pitch N/2+1), inverse (z pass).
+// AXIS 1: y, 2: z.  grid.x = b*N + (z for AXIS 1 | y for AXIS 2), grid.y = kx block of W;
+// blockDim = W*T.
 // ---------------------------------------------------------------------------------
 template <int N, int R1, int R2, int AXIS, int MODE>
-__global__ void __launch_bounds__(512) k_fcol(float2* __restrict__ c, const float* __restrict__ green, const float2* __restrict__ gtw, int W) {
+__global__ void __launch_bounds__(512) k_fcol(float2* __restrict__ c, const float* __restrict__ green,
+                                              const float2* __restrict__ gtw, int W, int pc) {
   constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, RPT = N / T;  // rows per thread
   static_assert(N % T == 0, "rows must split evenly over the thread group");
   extern __shared__ float2 sm[];
@@ -210,8 +229,8 @@ __global__ void __launch_bounds__(512) k_fcol(float2* __restrict__ c, const floa
   const int kx0 = blockIdx.y * W;
   const int col = threadIdx.x % W, t = threadIdx.x / W;  // blockDim = W*T
   const bool live = kx0 + col < NH;
-  const int64_t es = (AXIS == 1) ? NH : (int64_t)N * NH;
-  float2* base = c + b * (int64_t)N * N * NH + (AXIS == 1 ? (int64_t)o * N * NH : (int64_t)o * NH) + kx0 + col;
+  const int64_t es = (AXIS == 1) ? pc : (int64_t)N * pc;
+  float2* base = c + b * (int64_t)N * N * pc + (AXIS == 1 ? (int64_t)o * N * pc : (int64_t)o * pc) + kx0 + col;
   {
     float2 r[RPT];
 #pragma unroll
@@ -256,11 +275,11 @@ __host__ inline int fcol_width(int N, int T) {
 }
 
 // ---------------------------------------------------------------------------------
-// X' pass, c2r, divided `reps` times by `norm`.
+// X' pass, c2r, divided `reps` times by `norm`.  In place (complex rows pc -> real rows pf).
 // ---------------------------------------------------------------------------------
 template <int N, int R1, int R2>
-__global__ void __launch_bounds__(256) k_fx_c2r(const float2* __restrict__ c, float* __restrict__ r, int64_t nrows, const float2* __restrict__ gtw,
-                         float norm, int reps) {
+__global__ void __launch_bounds__(256) k_fx_c2r(const float2* c, float* r, int64_t nrows, const float2* __restrict__ gtw,
+                                                float norm, int reps, int pc, int pf) {
   constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1;
   extern __shared__ float2 sm[];
   float2* tw = sm;
@@ -269,13 +288,12 @@ __global__ void __launch_bounds__(256) k_fx_c2r(const float2* __restrict__ c, fl
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
   const int64_t row0 = (int64_t)blockIdx.x * 2 * S;
   const int nr = (int)min((int64_t)2 * S, nrows - row0);
-  const float2* cp = c + row0 * NH;
   for (int i = threadIdx.x; i < S * N; i += blockDim.x) {
     const int q = i / N, x = i - q * N;
     float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f);
     const int k = (x < NH) ? x : N - x;
-    if (2 * q < nr) a0 = cp[(2 * q) * NH + k];
-    if (2 * q + 1 < nr) a1 = cp[(2 * q + 1) * NH + k];
+    if (2 * q < nr) a0 = c[(row0 + 2 * q) * pc + k];
+    if (2 * q + 1 < nr) a1 = c[(row0 + 2 * q + 1) * pc + k];
     if (k == 0 || 2 * k == N) { a0.y = 0.f; a1.y = 0.f; }
     if (x >= NH) { a0.y = -a0.y; a1.y = -a1.y; }
     Z[q * N + x] = make_float2(a0.x - a1.y, a0.y + a1.x);
@@ -283,14 +301,161 @@ __global__ void __launch_bounds__(256) k_fx_c2r(const float2* __restrict__ c, fl
   __syncthreads();
   const int s = threadIdx.x / T, t = threadIdx.x - s * T;
   seq_transform<N, R1, R2, +1>(Z + s * N, 1, t, tw);
-  float* rp = r + row0 * N;
   for (int i = threadIdx.x; i < 2 * S * N; i += blockDim.x) {
     const int row = i / N, x = i - row * N;
     if (row >= nr) continue;
     const float2 z = Z[(row >> 1) * N + x];
     float v = (row & 1) ? z.y : z.x;
     for (int q = 0; q < reps; ++q) v = __fdiv_rn(v, norm);
-    rp[i] = v;
+    r[(row0 + row) * pf + x] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Fused plane passes (one block per z plane; N small enough that a half-spectrum plane
+// fits in shared memory).  Forward: load the real plane, r2c along x (rows packed in
+// pairs), FFT along y, store the complex plane in place.  Inverse: the reverse.  This
+// removes one read and one write of the whole mesh per direction.
+// ---------------------------------------------------------------------------------
+template <int N>
+struct PlaneSm {
+  static constexpr int NH = N / 2 + 1, SP = N + 1;  // packed-row pitch (bank padding)
+  static constexpr int ELEMS = ((N / 2) * SP > N * NH) ? (N / 2) * SP : N * NH;
+  static constexpr size_t BYTES = (size_t)(N + ELEMS) * 8;
+};
+
+constexpr int PLANE_THREADS = 512;
+
+template <int N, int R1, int R2, typename IN>
+__global__ void __launch_bounds__(PLANE_THREADS) k_fxy_r2c(const IN* r, float2* c, const float2* __restrict__ gtw,
+                                                          float scale, int pr, int pc) {
+  constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, SP = PlaneSm<N>::SP;
+  constexpr int NPAIR = N / 2;
+  constexpr int KU = (NPAIR * NH + PLANE_THREADS - 1) / PLANE_THREADS;  // unpack items per thread
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* Z = sm + N;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
+  const int64_t row0 = (int64_t)blockIdx.x * N;  // first row of this plane (all boxes stacked)
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
+    const int y = i / N, x = i - y * N;
+    const IN v = r[(row0 + y) * pr + x];
+    float f;
+    if (sizeof(IN) == 8) f = (float)((double)(long long)v * 9.094947017729282e-13);
+    else f = (float)v;
+    reinterpret_cast<float*>(Z + (y >> 1) * SP + x)[y & 1] = __fmul_rn(f, scale);
+  }
+  __syncthreads();
+  {  // x transforms of the packed rows, G at a time
+    constexpr int G = PLANE_THREADS / T;
+    const int s = threadIdx.x / T, t = threadIdx.x - s * T;
+    for (int p0 = 0; p0 < NPAIR; p0 += G) {
+      const int p = p0 + s;
+      seq_transform_g<N, R1, R2, -1>(Z + p * SP, 1, t, tw, s < G && p < NPAIR);
+    }
+  }
+  {  // unpack to the half-spectrum plane X[y][kx] (pitch NH), through registers
+    float2 k0[KU], k1[KU];
+#pragma unroll
+    for (int u = 0; u < KU; ++u) {
+      const int i = threadIdx.x + u * PLANE_THREADS;
+      if (i < NPAIR * NH) {
+        const int p = i / NH, k = i - p * NH;
+        const float2 z = Z[p * SP + k];
+        const float2 zc = Z[p * SP + ((N - k) % N)];
+        k0[u] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+        k1[u] = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < KU; ++u) {
+      const int i = threadIdx.x + u * PLANE_THREADS;
+      if (i < NPAIR * NH) {
+        const int p = i / NH, k = i - p * NH;
+        Z[(2 * p) * NH + k] = k0[u];
+        Z[(2 * p + 1) * NH + k] = k1[u];
+      }
+    }
+    __syncthreads();
+  }
+  {  // y transforms of the columns kx (element stride NH), G columns per round
+    constexpr int G = PLANE_THREADS / T;
+    const int col = threadIdx.x % G, t = threadIdx.x / G;
+    for (int k0 = 0; k0 < NH; k0 += G) {
+      const int kx = k0 + col;
+      seq_transform_g<N, R1, R2, -1>(Z + kx, NH, t, tw, t < T && kx < NH);
+    }
+  }
+  for (int i = threadIdx.x; i < N * NH; i += blockDim.x) {
+    const int y = i / NH, k = i - y * NH;
+    c[(row0 + y) * pc + k] = Z[i];
+  }
+}
+
+template <int N, int R1, int R2>
+__global__ void __launch_bounds__(PLANE_THREADS) k_fyx_c2r(const float2* c, float* r, const float2* __restrict__ gtw,
+                                                          float norm, int reps, int pc, int pf) {
+  constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, SP = PlaneSm<N>::SP;
+  constexpr int NPAIR = N / 2;
+  constexpr int KP = (NPAIR * N + PLANE_THREADS - 1) / PLANE_THREADS;  // pack items per thread
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* Z = sm + N;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
+  const int64_t row0 = (int64_t)blockIdx.x * N;
+  for (int i = threadIdx.x; i < N * NH; i += blockDim.x) {
+    const int y = i / NH, k = i - y * NH;
+    Z[i] = c[(row0 + y) * pc + k];
+  }
+  __syncthreads();
+  {  // inverse y transforms of the columns
+    constexpr int G = PLANE_THREADS / T;
+    const int col = threadIdx.x % G, t = threadIdx.x / G;
+    for (int k0 = 0; k0 < NH; k0 += G) {
+      const int kx = k0 + col;
+      seq_transform_g<N, R1, R2, +1>(Z + kx, NH, t, tw, t < T && kx < NH);
+    }
+  }
+  {  // pack rows (2p, 2p+1) as X0 + i X1 over the Hermitian extension (c2r convention)
+    float2 kp[KP];
+#pragma unroll
+    for (int u = 0; u < KP; ++u) {
+      const int i = threadIdx.x + u * PLANE_THREADS;
+      if (i < NPAIR * N) {
+        const int p = i / N, x = i - p * N;
+        const int k = (x < NH) ? x : N - x;
+        float2 a0 = Z[(2 * p) * NH + k], a1 = Z[(2 * p + 1) * NH + k];
+        if (k == 0 || 2 * k == N) { a0.y = 0.f; a1.y = 0.f; }
+        if (x >= NH) { a0.y = -a0.y; a1.y = -a1.y; }
+        kp[u] = make_float2(a0.x - a1.y, a0.y + a1.x);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < KP; ++u) {
+      const int i = threadIdx.x + u * PLANE_THREADS;
+      if (i < NPAIR * N) {
+        const int p = i / N, x = i - p * N;
+        Z[p * SP + x] = kp[u];
+      }
+    }
+    __syncthreads();
+  }
+  {  // inverse x transforms of the packed rows
+    constexpr int G = PLANE_THREADS / T;
+    const int s = threadIdx.x / T, t = threadIdx.x - s * T;
+    for (int p0 = 0; p0 < NPAIR; p0 += G) {
+      const int p = p0 + s;
+      seq_transform_g<N, R1, R2, +1>(Z + p * SP, 1, t, tw, s < G && p < NPAIR);
+    }
+  }
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
+    const int y = i / N, x = i - y * N;
+    const float2 z = Z[(y >> 1) * SP + x];
+    float v = (y & 1) ? z.y : z.x;
+    for (int q = 0; q < reps; ++q) v = __fdiv_rn(v, norm);
+    r[(row0 + y) * pf + x] = v;
   }
 }
 
