@@ -114,6 +114,8 @@ struct cube_ctx {
   cudaEvent_t ev[8];
   // 1: use the generic Stockham passes for every size (CUBE_FFT_GENERIC=1)
   int fft_generic = 0;
+  // 1: fused plane FFT kernels for sides <= 144 (CUBE_FFT_FUSED, default 1)
+  int fft_fused = 1;
   // opt-in per-kernel timers and the launch counter
   bool prof = false;
   std::vector<cudaEvent_t> pool;
@@ -235,25 +237,44 @@ Geo make_geo(const cube_params& p) {
   return g;
 }
 
-// In-place mesh layout: a box of side n has n*n rows of RP bytes, RP = max(n*rb, (n/2+1)*8),
-// so a real row (rb = 4, or 8 for the int64 fixed-point deposit) and its half-spectrum
-// row share the same bytes; the potential is written back over them.
+// In-place mesh layouts (fft2.cuh): boxes of side n are n planes of `psb` bytes.
+//  row-pitched: rows of RP = max(n*rb, (n/2+1)*8) bytes, psb = n*RP;
+//  plane-compact (sizes that run the fused plane FFT): rows of n reals / n/2+1 complex /
+//    n floats from the start of the plane, psb = max(n*n*rb, n*(n/2+1)*8).
+// rb = 4, or 8 for the int64 fixed-point deposit.
 struct Pitch {
-  int64_t rp;  // row pitch in bytes
-  int pr, pc, pf;  // real elements, complex elements and floats per row
+  int64_t rp;    // bytes per real row (capture copies)
+  int64_t psb;   // bytes per plane
+  int pr, pc, pf;        // row pitch: real elements, complex elements, floats
+  int64_t plr, plc, plf;  // plane pitch in the same units
 };
-Pitch pitch_of(int n, bool fixed) {
-  const int64_t rb = fixed ? 8 : 4;
+
+bool fused_layout(const cube_ctx* c, int n);
+
+Pitch pitch_of(const cube_ctx* c, int n, bool fixed) {
+  const int64_t rb = fixed ? 8 : 4, nh = n / 2 + 1;
   Pitch p;
-  p.rp = std::max<int64_t>((int64_t)n * rb, (int64_t)(n / 2 + 1) * 8);
-  p.pr = (int)(p.rp / rb);
-  p.pc = (int)(p.rp / 8);
-  p.pf = (int)(p.rp / 4);
+  if (fused_layout(c, n)) {
+    p.psb = std::max<int64_t>((int64_t)n * n * rb, (int64_t)n * nh * 8);
+    p.pr = n;
+    p.pc = (int)nh;
+    p.pf = n;
+    p.rp = n * rb;
+  } else {
+    p.rp = std::max<int64_t>((int64_t)n * rb, nh * 8);
+    p.psb = n * p.rp;
+    p.pr = (int)(p.rp / rb);
+    p.pc = (int)(p.rp / 8);
+    p.pf = (int)(p.rp / 4);
+  }
+  p.plr = p.psb / rb;
+  p.plc = p.psb / 8;
+  p.plf = p.psb / 4;
   return p;
 }
 
-size_t mesh_bytes(int n, int64_t nbox, bool fixed) {
-  return (size_t)nbox * n * n * pitch_of(n, fixed).rp + 256;
+size_t mesh_bytes(const cube_ctx* c, int n, int64_t nbox, bool fixed) {
+  return (size_t)nbox * n * pitch_of(c, n, fixed).psb + 256;
 }
 
 struct MeshPtrs {
@@ -265,13 +286,13 @@ MeshPtrs mesh_ptrs(cube_ctx* c, int n, int64_t, bool fixed) {
   MeshPtrs m;
   m.real = c->arena;
   m.ck = reinterpret_cast<float2*>(c->arena);
-  m.pt = pitch_of(n, fixed);
+  m.pt = pitch_of(c, n, fixed);
   return m;
 }
 
 // How many boxes of side n fit in the arena.
 int64_t boxes_fit(cube_ctx* c, int n, bool fixed) {
-  const size_t per = mesh_bytes(n, 1, fixed);
+  const size_t per = mesh_bytes(c, n, 1, fixed);
   return std::max<int64_t>(1, (int64_t)(c->arena_bytes / per));
 }
 
@@ -291,26 +312,27 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
   const int W = f2::fcol_width(N, T);
   const size_t smc = (size_t)(N + W * N) * sizeof(float2);
   dim3 gc((unsigned)(nbox * N), (unsigned)((NH + W - 1) / W));
-  constexpr bool fused = (N <= 144) && (f2::PlaneSm<N>::BYTES <= 200 * 1024);
-  if constexpr (fused) {
-    const size_t smp = f2::PlaneSm<N>::BYTES;
-    const unsigned planes = (unsigned)(nbox * N);
-    if (fixed) {
-      smem_optin(f2::k_fxy_r2c<N, R1, R2, long long>, smp);
-      LAUNCH(c, kx, 1, f2::k_fxy_r2c<N, R1, R2, long long><<<planes, f2::PLANE_THREADS, smp, c->s>>>(
-                           (const long long*)real_in, ck, tw, scale, pt.pr, pt.pc));
-    } else {
-      smem_optin(f2::k_fxy_r2c<N, R1, R2, float>, smp);
-      LAUNCH(c, kx, 1, f2::k_fxy_r2c<N, R1, R2, float><<<planes, f2::PLANE_THREADS, smp, c->s>>>(
-                           (const float*)real_in, ck, tw, scale, pt.pr, pt.pc));
+  if constexpr (N <= 144) {
+    if (fused_layout(c, N)) {
+      const size_t smp = f2::PlaneSm<N>::BYTES;
+      const unsigned planes = (unsigned)(nbox * N);
+      if (fixed) {
+        smem_optin(f2::k_fxy_r2c<N, R1, R2, long long>, smp);
+        LAUNCH(c, kx, 1, f2::k_fxy_r2c<N, R1, R2, long long><<<planes, f2::PLANE_THREADS, smp, c->s>>>(
+                             (const long long*)real_in, ck, tw, scale, pt.pr, pt.pc, pt.plr, pt.plc));
+      } else {
+        smem_optin(f2::k_fxy_r2c<N, R1, R2, float>, smp);
+        LAUNCH(c, kx, 1, f2::k_fxy_r2c<N, R1, R2, float><<<planes, f2::PLANE_THREADS, smp, c->s>>>(
+                             (const float*)real_in, ck, tw, scale, pt.pr, pt.pc, pt.plr, pt.plc));
+      }
+      smem_optin(f2::k_fcol<N, R1, R2, 2, 2>, smc);
+      LAUNCH(c, kz, 1, f2::k_fcol<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
+      smem_optin(f2::k_fyx_c2r<N, R1, R2>, smp);
+      LAUNCH(c, kc, 1, f2::k_fyx_c2r<N, R1, R2><<<planes, f2::PLANE_THREADS, smp, c->s>>>(
+                           ck, phi_out, tw, norm, reps, pt.pc, pt.pf, pt.plc, pt.plf));
+      return;
     }
-    smem_optin(f2::k_fcol<N, R1, R2, 2, 2>, smc);
-    LAUNCH(c, kz, 1, f2::k_fcol<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc));
-    smem_optin(f2::k_fyx_c2r<N, R1, R2>, smp);
-    LAUNCH(c, kc, 1, f2::k_fyx_c2r<N, R1, R2><<<planes, f2::PLANE_THREADS, smp, c->s>>>(ck, phi_out, tw, norm, reps,
-                                                                                        pt.pc, pt.pf));
-    return;
-  } else {
+  }
   const int S = std::max(1, 256 / T);
   const size_t smx = (size_t)(N + S * N) * sizeof(float2);
   const unsigned gx = (unsigned)((nrows + 2 * S - 1) / (2 * S));
@@ -327,12 +349,23 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
   smem_optin(f2::k_fcol<N, R1, R2, 2, 2>, smc);
   smem_optin(f2::k_fcol<N, R1, R2, 1, 1>, smc);
   smem_optin(f2::k_fx_c2r<N, R1, R2>, smx);
-  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc));
-  LAUNCH(c, kz, 1, f2::k_fcol<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc));
-  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 1><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc));
+  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
+  LAUNCH(c, kz, 1, f2::k_fcol<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
+  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 1><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
   LAUNCH(c, kc, 1, f2::k_fx_c2r<N, R1, R2><<<gx, S * T, smx, c->s>>>(ck, phi_out, nrows, tw, norm, reps, pt.pc, pt.pf));
+}
+
+bool fft2_size(int n) {
+  switch (n) {
+    case 16: case 32: case 48: case 64: case 96: case 128: case 144: case 192: case 256: case 288: case 432:
+    case 512: case 576: case 1024:
+      return true;
+    default:
+      return false;
   }
 }
+
+bool fused_layout(const cube_ctx* c, int n) { return !c->fft_generic && c->fft_fused && n <= 144 && fft2_size(n); }
 
 bool fft2_dispatch(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out,
                    float2* ck, const float* green, float norm, int reps, int kx, int ky, int kz, int kc, const Pitch& pt) {
@@ -364,7 +397,7 @@ void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixe
   const int ky = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTY_PM2 : K_FFTY_PM3;
   const int kz = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTZ_PM2 : K_FFTZ_PM3;
   const int kc = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTC_PM2 : K_FFTC_PM3;
-  const Pitch pt = pitch_of(n, fixed);
+  const Pitch pt = pitch_of(c, n, fixed);
   if (c->fft_generic == 0 &&
       fft2_dispatch(c, n, nbox, real_in, fixed, scale, phi_out, ck, green, norm, reps, kx, ky, kz, kc, pt))
     return;
@@ -383,9 +416,9 @@ void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixe
   const int W = (n <= 256) ? 16 : (n <= 512 ? 8 : 4);
   const size_t smy = (size_t)(n + 2 * W * n) * sizeof(float2);
   dim3 gy((unsigned)(nbox * n), (unsigned)((nh + W - 1) / W));
-  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1, pt.pc));
-  LAUNCH(c, kz, 1, k_fft_z_green<<<gy, 256, smy, c->s>>>(ck, green, D, W, pt.pc));
-  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1, pt.pc));
+  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1, pt.pc, pt.plc));
+  LAUNCH(c, kz, 1, k_fft_z_green<<<gy, 256, smy, c->s>>>(ck, green, D, W, pt.pc, pt.plc));
+  LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1, pt.pc, pt.plc));
   LAUNCH(c, kc, 1, k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, norm, reps, pt.pc, pt.pf));
 }
 
@@ -407,17 +440,19 @@ float* green3(cube_ctx* c, int iapm) {
   return c->green3[iapm];
 }
 
-// Copy a box field (n^3 values in rows of `row_bytes` at `pitch` bytes) into a dense
-// capture buffer when it is the one requested.
+// Copy a box field (n planes of n rows of n values, row pitch `rp` and plane pitch `psb`
+// bytes) into a dense capture buffer when it is the one requested.
 void maybe_capture(cube_ctx* c, int level, int64_t box, int what, const void* src, int n, bool fixed_int,
-                   int64_t pitch) {
+                   int64_t rp, int64_t psb) {
   if (c->cap_level != level || c->cap_box != box || c->cap_what != what) return;
   cudaFree(c->cap_buf);
   c->cap_buf = nullptr;
   const int64_t cnt = (int64_t)n * n * n;
   const size_t eb = fixed_int ? 8 : 4;
   if (cudaMalloc(&c->cap_buf, cnt * eb) != cudaSuccess) return;
-  cudaMemcpy2DAsync(c->cap_buf, n * eb, src, pitch, n * eb, (size_t)n * n, cudaMemcpyDeviceToDevice, c->s);
+  for (int z = 0; z < n; ++z)
+    cudaMemcpy2DAsync((char*)c->cap_buf + (size_t)z * n * n * eb, n * eb, (const char*)src + (size_t)z * psb, rp,
+                      n * eb, (size_t)n, cudaMemcpyDeviceToDevice, c->s);
   c->cap_n = fixed_int ? -cnt : cnt;  // negative marks int64 content
 }
 
@@ -479,6 +514,8 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
   {
     const char* e = getenv("CUBE_FFT_GENERIC");
     c->fft_generic = (e && e[0] == '1') ? 1 : 0;
+    const char* f = getenv("CUBE_FFT_FUSED");
+    c->fft_fused = (f && f[0] == '0') ? 0 : 1;
   }
   c->ns3 = (int)((int64_t)G.nnt * G.nnt * G.nnt * G.nns * G.nns * G.nns);
   c->ntiles = G.nnt * G.nnt * G.nnt;
@@ -568,14 +605,15 @@ static int alloc_particles(cube_ctx* c, int64_t np) {
   // mesh arena: everything that fits of what the largest level needs, within 70% of free memory
   const Geo& G = c->G;
   const bool fixed = c->P.deposit_mode == CUBE_DEPOSIT_FIXED;
-  size_t need = std::max(mesh_bytes(G.nc, 1, fixed), mesh_bytes(G.ngt, c->ntiles, fixed));
-  need = std::max(need, mesh_bytes(G.nft[2], c->ns3, fixed));  // every subtile in the lightest class
-  for (int i = 3; i <= 5; ++i) need = std::max(need, mesh_bytes(G.nft[i], std::max<int64_t>(1, c->ns3 / 16), fixed));
+  size_t need = std::max(mesh_bytes(c, G.nc, 1, fixed), mesh_bytes(c, G.ngt, c->ntiles, fixed));
+  need = std::max(need, mesh_bytes(c, G.nft[2], c->ns3, fixed));  // every subtile in the lightest class
+  for (int i = 3; i <= 5; ++i)
+    need = std::max(need, mesh_bytes(c, G.nft[i], std::max<int64_t>(1, c->ns3 / 16), fixed));
   size_t fre = 0, tot = 0;
   CK(cudaMemGetInfo(&fre, &tot));
   size_t budget = (size_t)(0.7 * (double)fre);
   size_t want = std::min(need, budget);
-  want = std::max(want, std::max(mesh_bytes(G.nc, 1, fixed), mesh_bytes(G.nft[5], 1, fixed)));
+  want = std::max(want, std::max(mesh_bytes(c, G.nc, 1, fixed), mesh_bytes(c, G.nft[5], 1, fixed)));
   if (c->arena) cudaFree(c->arena);
   c->arena = nullptr;
   CK(cudaMalloc(&c->arena, want));
@@ -709,15 +747,15 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
   {
     const int n = G.nc;
     MeshPtrs m = mesh_ptrs(c, n, 1, fixed);
-    CK(cudaMemsetAsync(m.real, 0, mesh_bytes(n, 1, fixed), c->s));
-    if (fixed) LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr));
-    else LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr));
-    maybe_capture(c, 1, 0, 0, m.real, n, fixed, m.pt.rp);
+    CK(cudaMemsetAsync(m.real, 0, mesh_bytes(c, n, 1, fixed), c->s));
+    if (fixed) LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr, m.pt.plr));
+    else LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr, m.pt.plr));
+    maybe_capture(c, 1, 0, 0, m.real, n, fixed, m.pt.rp, m.pt.psb);
     float* phi = reinterpret_cast<float*>(m.real);
     launch_fft(c, n, 1, m.real, fixed, G.mass_p, phi, m.ck, c->green1, (float)n, 3, 1);
-    maybe_capture(c, 1, 0, 1, phi, n, false, m.pt.rp);
-    LAUNCH(c, K_F2_PM1, 1, k_f2max_periodic<<<(unsigned)std::min<int64_t>(1184, (int64_t)n * n / 8 + 1), 256, 0, c->s>>>(phi, n, f2 + 0, m.pt.pf));
-    LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, a_mid, dt, m.pt.pf));
+    maybe_capture(c, 1, 0, 1, phi, n, false, (int64_t)m.pt.pf * 4, m.pt.psb);
+    LAUNCH(c, K_F2_PM1, 1, k_f2max_periodic<<<(unsigned)std::min<int64_t>(1184, (int64_t)n * n / 8 + 1), 256, 0, c->s>>>(phi, n, f2 + 0, m.pt.pf, m.pt.plf));
+    LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, a_mid, dt, m.pt.pf, m.pt.plf));
   }
   CK(cudaEventRecord(c->ev[1], c->s));
   // ---------------- PM2 (kick.f90:47-77) ----------------
@@ -727,18 +765,19 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     for (int t0 = 0; t0 < c->ntiles; t0 += (int)per) {
       const int nb = (int)std::min<int64_t>(per, c->ntiles - t0);
       MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
-      const int64_t boxb = (int64_t)n * n * m.pt.rp;
+      const int64_t boxb = (int64_t)n * m.pt.psb;
       CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
-      if (fixed) LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb, m.pt.pr));
-      else LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb, m.pt.pr));
+      if (fixed) LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb, m.pt.pr, m.pt.plr));
+      else LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb, m.pt.pr, m.pt.plr));
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
-        maybe_capture(c, 2, c->cap_box, 0, (char*)m.real + (c->cap_box - t0) * boxb, n, fixed, m.pt.rp);
+        maybe_capture(c, 2, c->cap_box, 0, (char*)m.real + (c->cap_box - t0) * boxb, n, fixed, m.pt.rp, m.pt.psb);
       float* phi = reinterpret_cast<float*>(m.real);
       launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, c->green2, (float)n * (float)n * (float)n, 1, 2);
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
-        maybe_capture(c, 2, c->cap_box, 1, (char*)m.real + (c->cap_box - t0) * boxb, n, false, m.pt.rp);
-      LAUNCH(c, K_F2_PM2, 1, k_f2max_box<<<f2max_box_grid(G.ngp, nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1, m.pt.pf));
-      LAUNCH(c, K_INT_PM2, 1, k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, a_mid, dt, vm + 0, c->err, m.pt.pf));
+        maybe_capture(c, 2, c->cap_box, 1, (char*)m.real + (c->cap_box - t0) * boxb, n, false, (int64_t)m.pt.pf * 4,
+                      m.pt.psb);
+      LAUNCH(c, K_F2_PM2, 1, k_f2max_box<<<f2max_box_grid(G.ngp, nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1, m.pt.pf, m.pt.plf));
+      LAUNCH(c, K_INT_PM2, 1, k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, a_mid, dt, vm + 0, c->err, m.pt.pf, m.pt.plf));
     }
   }
   CK(cudaEventRecord(c->ev[2], c->s));
@@ -786,21 +825,22 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       if (!g3) return CUBE_E_CUDA;
       const int32_t* slots = c->box_slot + k * c->ns3;
       MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
-      const int64_t boxb = (int64_t)n * n * m.pt.rp;
+      const int64_t boxb = (int64_t)n * m.pt.psb;
       CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
-      if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr));
-      else LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr));
+      if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));
+      else LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));
       int cap_slot = -1;
       if (c->cap_level == 3 && c->cap_box >= 0 && c->cap_box < c->ns3 && ires[c->cap_box] == cl)
         cap_slot = c->h_slots[k * c->ns3 + c->cap_box];
-      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 0, (char*)m.real + cap_slot * boxb, n, fixed, m.pt.rp);
+      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 0, (char*)m.real + cap_slot * boxb, n, fixed, m.pt.rp, m.pt.psb);
       float* phi = reinterpret_cast<float*>(m.real);
       launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, g3, (float)n * (float)n * (float)n, 1, 3);
-      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 1, (char*)m.real + cap_slot * boxb, n, false, m.pt.rp);
+      if (cap_slot >= 0)
+        maybe_capture(c, 3, c->cap_box, 1, (char*)m.real + cap_slot * boxb, n, false, (int64_t)m.pt.pf * 4, m.pt.psb);
       const int nf = G.nfp[cl];
-      LAUNCH(c, K_F2_PM3, 1, k_f2max_box<<<f2max_box_grid(nf, nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2, m.pt.pf));
+      LAUNCH(c, K_F2_PM3, 1, k_f2max_box<<<f2max_box_grid(nf, nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2, m.pt.pf, m.pt.plf));
       LAUNCH(c, K_INT_PM3, 1, k_interp_pm3<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp, a_mid, dt, vm + 3,
-                                                c->err, m.pt.pf));
+                                                c->err, m.pt.pf, m.pt.plf));
     }
   }
   CK(cudaEventRecord(c->ev[3], c->s));

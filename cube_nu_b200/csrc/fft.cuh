@@ -130,7 +130,7 @@ __global__ void k_fft_x_r2c(const IN* r, float2* c, int64_t nrows, FFTDesc D, in
 }
 
 // ---- Y pass (forward or inverse) on c[b][z][y][kx]; grid = (b*n+z, kx block).
-__global__ void k_fft_y(float2* __restrict__ c, FFTDesc D, int W, int dir, int pc) {
+__global__ void k_fft_y(float2* __restrict__ c, FFTDesc D, int W, int dir, int pc, int64_t plc) {
   extern __shared__ float2 sm[];
   const int n = D.n, nh = n / 2 + 1;
   float2* tw = sm;
@@ -140,7 +140,7 @@ __global__ void k_fft_y(float2* __restrict__ c, FFTDesc D, int W, int dir, int p
   const int64_t bz = blockIdx.x;  // b*n + z
   const int kx0 = blockIdx.y * W;
   const int wv = min(W, nh - kx0);
-  float2* base = c + bz * (int64_t)n * pc + kx0;
+  float2* base = c + bz * plc + kx0;
   for (int t = threadIdx.x; t < n * W; t += blockDim.x) {
     const int y = t / W, q = t - y * W;
     a[y * W + q] = (q < wv) ? base[(int64_t)y * pc + q] : make_float2(0.f, 0.f);
@@ -155,7 +155,8 @@ __global__ void k_fft_y(float2* __restrict__ c, FFTDesc D, int W, int dir, int p
 
 // ---- Z pass: forward FFT along z, multiply by the Green table g[kz][ky][kx], inverse.
 // grid = (b*n+y, kx block).
-__global__ void k_fft_z_green(float2* __restrict__ c, const float* __restrict__ g, FFTDesc D, int W, int pc) {
+__global__ void k_fft_z_green(float2* __restrict__ c, const float* __restrict__ g, FFTDesc D, int W, int pc,
+                              int64_t plc) {
   extern __shared__ float2 sm[];
   const int n = D.n, nh = n / 2 + 1;
   float2* tw = sm;
@@ -167,7 +168,7 @@ __global__ void k_fft_z_green(float2* __restrict__ c, const float* __restrict__ 
   const int y = (int)(by - bb * n);
   const int kx0 = blockIdx.y * W;
   const int wv = min(W, nh - kx0);
-  const int64_t zstride = (int64_t)n * pc;
+  const int64_t zstride = plc;
   float2* base = c + bb * (int64_t)n * zstride + (int64_t)y * pc + kx0;
   for (int t = threadIdx.x; t < n * W; t += blockDim.x) {
     const int z = t / W, q = t - z * W;

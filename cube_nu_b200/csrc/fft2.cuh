@@ -165,9 +165,13 @@ __device__ __forceinline__ void seq_transform_g(float2* base, int se, int t, con
   __syncthreads();
 }
 
-// Mesh layout (in place): box of side N, row pitch RP bytes = max(N*rb, (N/2+1)*8) so a
-// real row and its half-spectrum row share the same bytes (FFTW's in-place r2c layout).
-// pr = RP/rb real elements, pc = RP/8 complex elements, pf = RP/4 floats per row.
+// Mesh layouts (both in place, potential written over the input):
+//  row-pitched (five-pass sizes): row pitch RP bytes = max(N*rb, (N/2+1)*8), so a real
+//    row and its half-spectrum row share bytes (FFTW's in-place r2c layout); plane = N rows;
+//  plane-compact (fused sizes): real rows of N, half-spectrum rows of N/2+1 and phi rows of
+//    N packed from the start of each plane; plane pitch max(N*N*rb, N*(N/2+1)*8) bytes.
+// Kernels take the row pitch (pr real elements, pc complex, pf floats) and the plane pitch
+// in the same units (plr, plc, plf).
 
 // ---------------------------------------------------------------------------------
 // X pass, r2c.  Block: S packed sequences (2S real rows); blockDim = S*T.  In place:
@@ -215,8 +219,8 @@ __global__ void __launch_bounds__(256) k_fx_r2c(const IN* r, float2* c, int64_t 
 // blockDim = W*T.
 // ---------------------------------------------------------------------------------
 template <int N, int R1, int R2, int AXIS, int MODE>
-__global__ void __launch_bounds__(512) k_fcol(float2* __restrict__ c, const float* __restrict__ green,
-                                              const float2* __restrict__ gtw, int W, int pc) {
+__global__ void __launch_bounds__(512, 2) k_fcol(float2* __restrict__ c, const float* __restrict__ green,
+                                                 const float2* __restrict__ gtw, int W, int pc, int64_t plc) {
   constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, RPT = N / T;  // rows per thread
   static_assert(N % T == 0, "rows must split evenly over the thread group");
   extern __shared__ float2 sm[];
@@ -229,8 +233,8 @@ __global__ void __launch_bounds__(512) k_fcol(float2* __restrict__ c, const floa
   const int kx0 = blockIdx.y * W;
   const int col = threadIdx.x % W, t = threadIdx.x / W;  // blockDim = W*T
   const bool live = kx0 + col < NH;
-  const int64_t es = (AXIS == 1) ? pc : (int64_t)N * pc;
-  float2* base = c + b * (int64_t)N * N * pc + (AXIS == 1 ? (int64_t)o * N * pc : (int64_t)o * pc) + kx0 + col;
+  const int64_t es = (AXIS == 1) ? pc : plc;
+  float2* base = c + b * (int64_t)N * plc + (AXIS == 1 ? (int64_t)o * plc : (int64_t)o * pc) + kx0 + col;
   {
     float2 r[RPT];
 #pragma unroll
@@ -327,8 +331,8 @@ struct PlaneSm {
 constexpr int PLANE_THREADS = 512;
 
 template <int N, int R1, int R2, typename IN>
-__global__ void __launch_bounds__(PLANE_THREADS) k_fxy_r2c(const IN* r, float2* c, const float2* __restrict__ gtw,
-                                                          float scale, int pr, int pc) {
+__global__ void __launch_bounds__(PLANE_THREADS, 2) k_fxy_r2c(const IN* r, float2* c, const float2* __restrict__ gtw,
+                                                             float scale, int pr, int pc, int64_t plr, int64_t plc) {
   constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, SP = PlaneSm<N>::SP;
   constexpr int NPAIR = N / 2;
   constexpr int KU = (NPAIR * NH + PLANE_THREADS - 1) / PLANE_THREADS;  // unpack items per thread
@@ -336,10 +340,12 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_fxy_r2c(const IN* r, float2* 
   float2* tw = sm;
   float2* Z = sm + N;
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
-  const int64_t row0 = (int64_t)blockIdx.x * N;  // first row of this plane (all boxes stacked)
+  const int64_t plane = blockIdx.x;  // b*N + z
+  const IN* rp = r + plane * plr;
+  float2* cp = c + plane * plc;
   for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
     const int y = i / N, x = i - y * N;
-    const IN v = r[(row0 + y) * pr + x];
+    const IN v = rp[y * pr + x];
     float f;
     if (sizeof(IN) == 8) f = (float)((double)(long long)v * 9.094947017729282e-13);
     else f = (float)v;
@@ -389,13 +395,14 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_fxy_r2c(const IN* r, float2* 
   }
   for (int i = threadIdx.x; i < N * NH; i += blockDim.x) {
     const int y = i / NH, k = i - y * NH;
-    c[(row0 + y) * pc + k] = Z[i];
+    cp[y * pc + k] = Z[i];
   }
 }
 
 template <int N, int R1, int R2>
-__global__ void __launch_bounds__(PLANE_THREADS) k_fyx_c2r(const float2* c, float* r, const float2* __restrict__ gtw,
-                                                          float norm, int reps, int pc, int pf) {
+__global__ void __launch_bounds__(PLANE_THREADS, 2) k_fyx_c2r(const float2* c, float* r, const float2* __restrict__ gtw,
+                                                             float norm, int reps, int pc, int pf, int64_t plc,
+                                                             int64_t plf) {
   constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, SP = PlaneSm<N>::SP;
   constexpr int NPAIR = N / 2;
   constexpr int KP = (NPAIR * N + PLANE_THREADS - 1) / PLANE_THREADS;  // pack items per thread
@@ -403,10 +410,12 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_fyx_c2r(const float2* c, floa
   float2* tw = sm;
   float2* Z = sm + N;
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
-  const int64_t row0 = (int64_t)blockIdx.x * N;
+  const int64_t plane = blockIdx.x;
+  const float2* cp = c + plane * plc;
+  float* rp = r + plane * plf;
   for (int i = threadIdx.x; i < N * NH; i += blockDim.x) {
     const int y = i / NH, k = i - y * NH;
-    Z[i] = c[(row0 + y) * pc + k];
+    Z[i] = cp[y * pc + k];
   }
   __syncthreads();
   {  // inverse y transforms of the columns
@@ -455,7 +464,7 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_fyx_c2r(const float2* c, floa
     const float2 z = Z[(y >> 1) * SP + x];
     float v = (y & 1) ? z.y : z.x;
     for (int q = 0; q < reps; ++q) v = __fdiv_rn(v, norm);
-    r[(row0 + y) * pf + x] = v;
+    rp[y * pf + x] = v;
   }
 }
 

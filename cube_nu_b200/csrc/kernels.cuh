@@ -290,7 +290,7 @@ __device__ __forceinline__ void dep_add(void* rho, int64_t i, float w) {
 
 template <bool FIXED>
 __global__ void k_deposit_pm1(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
-                              void* __restrict__ rho, int pr) {
+                              void* __restrict__ rho, int pr, int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= np) return;
   int g[3];
@@ -313,7 +313,7 @@ __global__ void k_deposit_pm1(Geo G, int64_t np, const void* __restrict__ xp, co
       for (int a1 = 0; a1 < 3; ++a1) {
         const int x = wrapi(i2[0] - 2 + a1, nc);
         const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
-        dep_add<FIXED>(rho, ((int64_t)z * nc + y) * pr + x, ww);
+        dep_add<FIXED>(rho, (int64_t)z * pl + (int64_t)y * pr + x, ww);
       }
     }
   }
@@ -334,7 +334,7 @@ __device__ __forceinline__ int tile_cands(const Geo& G, int g, int* t, int* li) 
 // PM2 tile meshes [tile - tile0][ngt^3]; fine index i maps to array i-(1-ngb).
 template <bool FIXED>
 __global__ void k_deposit_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
-                              void* __restrict__ rho, int tile0, int ntile, int pr) {
+                              void* __restrict__ rho, int tile0, int ntile, int pr, int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= np) return;
   int g[3];
@@ -347,7 +347,7 @@ __global__ void k_deposit_pm2(Geo G, int64_t np, const void* __restrict__ xp, co
     f[d] = zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
   }
   const int ngt = G.ngt;
-  const int64_t box = (int64_t)ngt * ngt * pr;  // elements per box
+  const int64_t box = (int64_t)ngt * pl;  // elements per box
   for (int cz = 0; cz < nca[2]; ++cz)
     for (int cy = 0; cy < nca[1]; ++cy)
       for (int cx = 0; cx < nca[0]; ++cx) {
@@ -375,7 +375,7 @@ __global__ void k_deposit_pm2(Geo G, int64_t np, const void* __restrict__ xp, co
               const int x = i2[0] - 1 + a1 - (1 - G.ngb);
               if (x < 0 || x >= ngt) continue;
               const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
-              dep_add<FIXED>(base, ((int64_t)z * ngt + y) * pr + x, ww);
+              dep_add<FIXED>(base, (int64_t)z * pl + (int64_t)y * pr + x, ww);
             }
           }
         }
@@ -414,7 +414,7 @@ __device__ __forceinline__ int subtile_id(const Geo& G, const int t[3], const in
 template <bool FIXED>
 __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                               const int32_t* __restrict__ box_slot, int iapm, void* __restrict__ rho,
-                              unsigned* err, int pr) {
+                              unsigned* err, int pr, int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= np) return;
   int g[3];
@@ -427,7 +427,7 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
     f[d] = zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
   }
   const int nft = G.nft[iapm], nfp = G.nfp[iapm], nfb = G.nfb[iapm];
-  const int64_t box = (int64_t)nft * nft * pr;  // elements per box
+  const int64_t box = (int64_t)nft * pl;  // elements per box
   const double gs = (double)(1.f / (float)rsf_of(iapm));  // pm%gridsize, real4
   for (int cz = 0; cz < nca[2]; ++cz)
     for (int cy = 0; cy < nca[1]; ++cy)
@@ -464,7 +464,7 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
               const int x = i2[0] - 1 + a1 - (1 - nfb);
               if (x < 0 || x >= nft) continue;
               const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
-              dep_add<FIXED>(base, ((int64_t)z * nft + y) * pr + x, ww);
+              dep_add<FIXED>(base, (int64_t)z * pl + (int64_t)y * pr + x, ww);
             }
           }
         }
@@ -510,7 +510,7 @@ __device__ __forceinline__ void block_max_to(float v, float* out) {
 }
 
 // PM1: periodic nc^3 phi[z][y][x].  One warp per x-row, grid-stride over rows.
-__global__ void k_f2max_periodic(const float* __restrict__ phi, int nc, float* __restrict__ f2out, int pf) {
+__global__ void k_f2max_periodic(const float* __restrict__ phi, int nc, float* __restrict__ f2out, int pf, int64_t pl) {
   const int lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   float v = 0.f;
@@ -519,7 +519,7 @@ __global__ void k_f2max_periodic(const float* __restrict__ phi, int nc, float* _
     const int z = row / nc, y = row - z * nc;
     const int zm2 = wrapi(z - 2, nc), zm1 = wrapi(z - 1, nc), zp1 = wrapi(z + 1, nc), zp2 = wrapi(z + 2, nc);
     const int ym2 = wrapi(y - 2, nc), ym1 = wrapi(y - 1, nc), yp1 = wrapi(y + 1, nc), yp2 = wrapi(y + 2, nc);
-    auto R = [&](int zz, int yy) { return phi + ((size_t)zz * nc + yy) * pf; };
+    auto R = [&](int zz, int yy) { return phi + (size_t)zz * pl + (size_t)yy * pf; };
     const float* r0 = R(z, y);
     for (int x = lane; x < nc; x += 32) {
       const int xm2 = wrapi(x - 2, nc), xm1 = wrapi(x - 1, nc), xp1 = wrapi(x + 1, nc), xp2 = wrapi(x + 2, nc);
@@ -538,13 +538,13 @@ __global__ void k_f2max_periodic(const float* __restrict__ phi, int nc, float* _
 // 1.7 times.  grid = nbox * tiles; blockDim = 256.
 constexpr int F2_TX = 32, F2_TY = 8, F2_PX = F2_TX + 4, F2_PY = F2_TY + 4;
 __global__ void __launch_bounds__(256) k_f2max_box(const float* __restrict__ phi, int n, int nforce, int m1phi,
-                                                   int nbox, float* __restrict__ f2out, int pf) {
+                                                   int nbox, float* __restrict__ f2out, int pf, int64_t pl) {
   __shared__ float ring[5][F2_PY * F2_PX];
   const int ntx = (nforce + F2_TX - 1) / F2_TX, nty = (nforce + F2_TY - 1) / F2_TY;
   const int tile = blockIdx.x % (ntx * nty);
   const int b = blockIdx.x / (ntx * nty);
   const int tx0 = (tile % ntx) * F2_TX + 1, ty0 = (tile / ntx) * F2_TY + 1;  // first physical x,y of the tile
-  const float* pb = phi + (size_t)b * n * n * pf;
+  const float* pb = phi + (size_t)b * n * pl;
   const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
   auto load_plane = [&](int z, float* dst) {  // tile plane z with halo 2 in x and y
     for (int i = threadIdx.x; i < F2_PY * F2_PX; i += blockDim.x) {
@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(256) k_f2max_box(const float* __restrict__ phi
       const int x = tx0 - 2 + px, y = ty0 - 2 + py;
       // indices stay inside the padded box: x,y in [-1, nforce+2] map to [-1-m1phi, ..] >= 0
       const bool in = (x - m1phi) < n && (y - m1phi) < n;
-      dst[i] = in ? __ldg(pb + ((size_t)(z - m1phi) * n + (y - m1phi)) * pf + (x - m1phi)) : 0.f;
+      dst[i] = in ? __ldg(pb + (size_t)(z - m1phi) * pl + (size_t)(y - m1phi) * pf + (x - m1phi)) : 0.f;
     }
   };
   for (int k = 0; k < 4; ++k) load_plane(k - 1, ring[k]);  // planes -1, 0, 1, 2
@@ -661,7 +661,8 @@ __device__ __forceinline__ void block_vmax(const float av[3], float* vmax) {
 }
 
 __global__ void k_interp_pm1(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
-                             const float* __restrict__ phi, float* __restrict__ vp, float a_mid, float dt, int pf) {
+                             const float* __restrict__ phi, float* __restrict__ vp, float a_mid, float dt, int pf,
+                             int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= np) return;
   int g[3];
@@ -681,7 +682,7 @@ __global__ void k_interp_pm1(Geo G, int64_t np, const void* __restrict__ xp, con
   for (int k = 0; k < 7; ++k) {
     wx[k] = wrapi(i2[0] - 4 + k, nc);
     wy[k] = wrapi(i2[1] - 4 + k, nc) * pf;
-    wz[k] = wrapi(i2[2] - 4 + k, nc) * nc * pf;
+    wz[k] = wrapi(i2[2] - 4 + k, nc) * (int)pl;
   }
   const int x0 = i2[0] - 1, y0 = i2[1] - 1, z0 = i2[2] - 1;
   auto P = [&](int a, int b, int c) { return __ldg(&phi[wz[c - z0 + 2] + wy[b - y0 + 2] + wx[a - x0 + 2]]); };
@@ -692,7 +693,7 @@ __global__ void k_interp_pm1(Geo G, int64_t np, const void* __restrict__ xp, con
 
 __global__ void k_interp_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                              const float* __restrict__ phi, int tile0, int ntile, float* __restrict__ vp, float a_mid,
-                             float dt, float* vmax, unsigned* err, int pf) {
+                             float dt, float* vmax, unsigned* err, int pf, int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   float av[3] = {0.f, 0.f, 0.f};
   if (ip < np) {
@@ -713,8 +714,9 @@ __global__ void k_interp_pm2(Geo G, int64_t np, const void* __restrict__ xp, con
         set_err(err, CUBE_DEVERR_INTERP_RANGE);
       } else {
         const int n = G.ngt, m1 = 1 - G.ngb;
-        const float* pb = phi + (size_t)(T - tile0) * n * n * pf;
-        auto P = [&](int a, int b, int c) { return __ldg(&pb[((c - m1) * n + (b - m1)) * pf + (a - m1)]); };
+        const float* pb = phi + (size_t)(T - tile0) * n * pl;
+        const int ipl = (int)pl;
+        auto P = [&](int a, int b, int c) { return __ldg(&pb[(c - m1) * ipl + (b - m1) * pf + (a - m1)]); };
         float dv[3];
         tsc_gather_force(i2, w, P, dv);
         apply_kick(vp, ip, dv, a_mid, dt, av);
@@ -726,7 +728,8 @@ __global__ void k_interp_pm2(Geo G, int64_t np, const void* __restrict__ xp, con
 
 __global__ void k_interp_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                              const float* __restrict__ phi, const int32_t* __restrict__ box_slot, int iapm,
-                             float* __restrict__ vp, float a_mid, float dt, float* vmax, unsigned* err, int pf) {
+                             float* __restrict__ vp, float a_mid, float dt, float* vmax, unsigned* err, int pf,
+                             int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   float av[3] = {0.f, 0.f, 0.f};
   if (ip < np) {
@@ -757,8 +760,9 @@ __global__ void k_interp_pm3(Geo G, int64_t np, const void* __restrict__ xp, con
         set_err(err, CUBE_DEVERR_INTERP_RANGE);
       } else {
         const int m1 = 1 - nfb;
-        const float* pb = phi + (size_t)slot * nft * nft * pf;
-        auto P = [&](int a, int b, int c) { return __ldg(&pb[((c - m1) * nft + (b - m1)) * pf + (a - m1)]); };
+        const float* pb = phi + (size_t)slot * nft * pl;
+        const int ipl = (int)pl;
+        auto P = [&](int a, int b, int c) { return __ldg(&pb[(c - m1) * ipl + (b - m1) * pf + (a - m1)]); };
         float dv[3];
         tsc_gather_force(i2, w, P, dv);
         apply_kick(vp, ip, dv, a_mid, dt, av);
