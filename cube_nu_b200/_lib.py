@@ -20,6 +20,7 @@ EXPORTS = (
     "cube_gpu_drift", "cube_gpu_kick", "cube_gpu_step", "cube_gpu_capture", "cube_gpu_captured",
     "cube_gpu_green_table", "cube_gpu_subtile_class", "cube_gpu_last_error", "cube_gpu_version",
     "cube_gpu_profile", "cube_gpu_profile_read", "cube_gpu_profile_name", "cube_gpu_kernel_launches",
+    "cube_gpu_zipv_encode", "cube_gpu_zipv_decode", "cube_gpu_download_zipv",
 )
 
 
@@ -72,6 +73,9 @@ def load():
     L.cube_gpu_profile_name.restype = ctypes.c_char_p
     L.cube_gpu_kernel_launches.argtypes = [vp]
     L.cube_gpu_kernel_launches.restype = ctypes.c_int64
+    L.cube_gpu_zipv_encode.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_float]
+    L.cube_gpu_zipv_decode.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_float]
+    L.cube_gpu_download_zipv.argtypes = [vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_float]
     _LIB = L
     return L
 
@@ -185,6 +189,30 @@ class Context:
 
     def launches(self) -> int:
         return int(self._lib.cube_gpu_kernel_launches(self._h))
+
+    def zipv_encode(self, v, sigma_vi: float) -> np.ndarray:
+        v = np.ascontiguousarray(v, dtype=np.float32)
+        out = np.empty(v.shape, dtype=np.int16)
+        _check(self._lib.cube_gpu_zipv_encode(self._h, _ptr(v), _ptr(out), v.size, sigma_vi), "cube_gpu_zipv_encode")
+        return out
+
+    def zipv_decode(self, code, sigma_vi: float) -> np.ndarray:
+        code = np.ascontiguousarray(code, dtype=np.int16)
+        out = np.empty(code.shape, dtype=np.float32)
+        _check(self._lib.cube_gpu_zipv_decode(self._h, _ptr(code), _ptr(out), code.size, sigma_vi),
+               "cube_gpu_zipv_decode")
+        return out
+
+    def download_zipv(self, sigma_vi: float):
+        p = self.params
+        xp = np.empty((self.np, 3), dtype=p.xdtype)
+        code = np.empty((self.np, 3), dtype=np.int16)
+        pid = np.empty(self.np, dtype=np.int64)
+        rhoc = np.empty(p.ncells, dtype=np.int32)
+        n = ctypes.c_int64()
+        _check(self._lib.cube_gpu_download_zipv(self._h, _ptr(xp), _ptr(code), _ptr(pid), _ptr(rhoc), ctypes.byref(n),
+                                                sigma_vi), "cube_gpu_download_zipv")
+        return xp, code, pid, rhoc
 
     def subtile_class(self) -> np.ndarray:
         out = np.empty(self.params.ns3, dtype=np.int32)

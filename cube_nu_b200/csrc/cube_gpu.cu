@@ -968,6 +968,50 @@ int cube_gpu_captured(cube_ctx* c, float* out, int64_t n) {
   return (int)m;
 }
 
+// ZIPV codec on host arrays, computed on the context's device.
+static int zipv_run(cube_ctx* c, const void* in, void* out, int64_t n, float sigma_vi, bool encode) {
+  if (!c || !in || !out || n < 0) return fail(CUBE_E_ARG, "bad zipv arguments");
+  if (!(sigma_vi > 0.f)) return fail(CUBE_E_ARG, "sigma_vi must be positive");
+  if (n == 0) return 0;
+  CK(cudaSetDevice(c->device));
+  void *din = nullptr, *dout = nullptr;
+  const size_t bin = encode ? 4 : 2, bout = encode ? 2 : 4;
+  CK(cudaMalloc(&din, n * bin));
+  CK(cudaMalloc(&dout, n * bout));
+  CK(cudaMemcpyAsync(din, in, n * bin, cudaMemcpyHostToDevice, c->s));
+  if (encode)
+    LAUNCH(c, K_FILL, 1, k_zipv_encode<<<nblk(n), 256, 0, c->s>>>((const float*)din, (int16_t*)dout, n, sigma_vi));
+  else
+    LAUNCH(c, K_FILL, 1, k_zipv_decode<<<nblk(n), 256, 0, c->s>>>((const int16_t*)din, (float*)dout, n, sigma_vi));
+  CK(cudaMemcpyAsync(out, dout, n * bout, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  cudaFree(din);
+  cudaFree(dout);
+  return 0;
+}
+
+int cube_gpu_zipv_encode(cube_ctx* c, const float* v, int16_t* code, int64_t n, float sigma_vi) {
+  return zipv_run(c, v, code, n, sigma_vi, true);
+}
+
+int cube_gpu_zipv_decode(cube_ctx* c, const int16_t* code, float* v, int64_t n, float sigma_vi) {
+  return zipv_run(c, code, v, n, sigma_vi, false);
+}
+
+int cube_gpu_download_zipv(cube_ctx* c, void* xp, int16_t* vp_code, int64_t* pid, int32_t* rhoc, int64_t* nplocal,
+                           float sigma_vi) {
+  if (!c || !c->loaded) return fail(CUBE_E_STATE, "no particles on device");
+  if (!(sigma_vi > 0.f)) return fail(CUBE_E_ARG, "sigma_vi must be positive");
+  CK(cudaSetDevice(c->device));
+  int16_t* dcode = nullptr;
+  CK(cudaMalloc(&dcode, (size_t)c->np * 3 * 2));
+  LAUNCH(c, K_FILL, 1, k_zipv_encode<<<nblk(c->np * 3), 256, 0, c->s>>>(c->vp, dcode, c->np * 3, sigma_vi));
+  if (vp_code) CK(cudaMemcpyAsync(vp_code, dcode, (size_t)c->np * 6, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  cudaFree(dcode);
+  return cube_gpu_download(c, xp, nullptr, pid, rhoc, nplocal);
+}
+
 int cube_gpu_green_table(cube_ctx* c, int level, int iapm, float* out, int64_t n) {
   if (!c || !out) return fail(CUBE_E_ARG, "null argument");
   CK(cudaSetDevice(c->device));

@@ -139,13 +139,17 @@ __global__ void k_drift_dest(Geo G, int64_t np, const void* __restrict__ xp, con
     if (!(ig >= (double)(1 - 2 * G.ncb) && ig <= (double)(G.nt + 2 * G.ncb))) bad = true;
     dn[d] = bad ? 0 : (int)ig - (li + 1);
   }
+  // Source coordinate (i-1) in the destination tile's frame: the ghost copy that lands
+  // in the destination's physical cell is the one at (destination - displacement).  When a
+  // tile's ghost region wraps onto itself (nc < nt+2ncb) a cell has two copies there and
+  // only this one reaches a physical cell.
   int dst[3], rel[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     dst[d] = wrapi(g[d] + dn[d], G.nc);
-    const int torg = (dst[d] / G.nt) * G.nt;
-    rel[d] = wrapi(g[d] - torg + G.ncb, G.nc) - G.ncb;  // source coordinate (i-1) in the dest tile
-    if (rel[d] >= G.nt + G.ncb) bad = true;             // outside the dest tile's ghost region
+    const int dloc = dst[d] % G.nt;
+    rel[d] = dloc - dn[d];
+    if (rel[d] < -G.ncb || rel[d] >= G.nt + G.ncb) bad = true;  // source outside the dest tile's ghost region
   }
   if (bad || l >= (1 << 24)) {
     set_err(err, CUBE_DEVERR_DRIFT_RANGE);
@@ -885,6 +889,30 @@ __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32
   unsigned long long c = live ? cnt : 0ull;
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(npairs, c);
+}
+
+// =================================================================================
+// ZIPV int16 velocity codec (utilities/pp_subtile.f90:61 decode, :125 encode), izipv=2:
+//   v = tan(pi*vp/(nvbin-1)) / (sqrt(pi/2)/(sigma_vi*vrel_boost))
+//   vp = nint((nvbin-1)*atan(sqrt(pi/2)/(sigma_vi*vrel_boost)*v)/pi)
+// with nvbin = 2^16 and vrel_boost = 2.5 (parameters.f90:90,135); FP64 as the reference.
+// =================================================================================
+__device__ __forceinline__ double zipv_scale(float sigma_vi) {
+  return sqrt(3.141592653589793 / 2.0) / ((double)sigma_vi * 2.5);
+}
+
+__global__ void k_zipv_decode(const int16_t* __restrict__ code, float* __restrict__ v, int64_t n, float sigma_vi) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double arg = 3.141592653589793 * (double)(float)code[i] / (double)65535.f;
+  v[i] = (float)(tan(arg) / zipv_scale(sigma_vi));
+}
+
+__global__ void k_zipv_encode(const float* __restrict__ v, int16_t* __restrict__ code, int64_t n, float sigma_vi) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x = (double)65535.f * atan(zipv_scale(sigma_vi) * (double)v[i]) / 3.141592653589793;
+  code[i] = (int16_t)llround(x);
 }
 
 // =================================================================================

@@ -139,8 +139,12 @@ def zeldovich(p: Params, z_i: float = 49.0, seed: int = 1, use_torch: bool = Fal
     npt = nt * npnc
     npb = npnc
     tile = cellw // nt
-    lat_loc = lat_idx - tile * npt  # local lattice index (0-based), wrap into [-npb, npt+npb)
-    lat_loc = (lat_loc + npb) % (nlat) - npb
+    # local lattice index (0-based) of the copy whose particle lands in the tile: when a
+    # tile's buffer wraps onto itself (one tile) the lattice point has two copies, and the
+    # one within a lattice span of the particle's local position is the landing one
+    lat_loc = lat_idx - tile * npt
+    xloc = np.mod(X, p.nc) - tile * nt
+    lat_loc = lat_loc + nlat * np.round((xloc - (lat_loc + 0.5) / npnc) / p.nc).astype(np.int64)
     nlayer = 2 * int(math.ceil(float(np.float32(grad_max[2])) * npnc / (8 * nic * math.pi * rcs))) + 3
     kk = lat_loc[:, 2] + npb  # 0-based from 1-npb
     ilayer = kk % nlayer
@@ -245,7 +249,9 @@ def zeldovich_torch(p: Params, z_i: float = 49.0, seed: int = 1, device: str = "
         npt = nt * npnc
         npb = npnc
         tile = cellw // nt
-        lat_loc = (lat_idx - tile * npt + npb) % nlat - npb
+        Xw = torch.remainder(X, float(p.nc))
+        lat_loc = lat_idx - tile * npt
+        lat_loc = lat_loc + nlat * torch.round((Xw - tile * nt - (lat_loc + 0.5) / npnc) / p.nc).long()
         nlayer = 2 * int(math.ceil(float(grad_max[2]) * npnc / (8 * nic * math.pi * rcs))) + 3
         kk = lat_loc[:, 2] + npb
         span = npt + 2 * npb

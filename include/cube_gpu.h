@@ -119,6 +119,15 @@ int cube_gpu_upload(cube_ctx* ctx, const void* xp, const float* vp, const int64_
 int cube_gpu_download(cube_ctx* ctx, void* xp, float* vp, int64_t* pid, int32_t* rhoc,
                       int64_t* nplocal);
 
+/* ZIPV int16 velocity codec (utilities/pp_subtile.f90:61 decode, :125 encode; izipv=2,
+ * vrel_boost=2.5): code = nint(65535*atan(sqrt(pi/2)/(sigma_vi*2.5)*v)/pi) and back.
+ * Host arrays of n values, converted on the context's device. */
+int cube_gpu_zipv_encode(cube_ctx* ctx, const float* v, int16_t* code, int64_t n, float sigma_vi);
+int cube_gpu_zipv_decode(cube_ctx* ctx, const int16_t* code, float* v, int64_t n, float sigma_vi);
+/* cube_gpu_download with the velocities written in the ZIPV int16 format (vp_code(3,np)). */
+int cube_gpu_download_zipv(cube_ctx* ctx, void* xp, int16_t* vp_code, int64_t* pid, int32_t* rhoc,
+                           int64_t* nplocal, float sigma_vi);
+
 /* drift.f90:1-233 with dt_mid=(dt_old+dt)/2; bit-exact arrival order and ZIPX update. */
 int cube_gpu_drift(cube_ctx* ctx, const cube_step_in* in);
 /* kick.f90:1-353: PM1 + PM2 + PM3 + PP velocity updates and dt criteria. */

@@ -1014,6 +1014,18 @@ int oracle_kick64(const cube_params* p, const void* xp, double* vp, const int32_
                                     dbg_box, dbg_what, dbg_out, dbg_n);
 }
 
+// ZIPV codec (utilities/pp_subtile.f90:61,125), FP64 as the reference, nvbin=2^16.
+int oracle_zipv_encode(const float* v, int16_t* code, int64_t n, float sigma_vi) {
+  const double sc = std::sqrt(M_PI / 2) / ((double)sigma_vi * 2.5);
+  for (int64_t i = 0; i < n; ++i) code[i] = (int16_t)std::llround((double)65535.f * std::atan(sc * (double)v[i]) / M_PI);
+  return 0;
+}
+int oracle_zipv_decode(const int16_t* code, float* v, int64_t n, float sigma_vi) {
+  const double sc = std::sqrt(M_PI / 2) / ((double)sigma_vi * 2.5);
+  for (int64_t i = 0; i < n; ++i) v[i] = (float)(std::tan(M_PI * (double)(float)code[i] / (double)65535.f) / sc);
+  return 0;
+}
+
 // Subtile classes (kick.f90:108-133).
 int oracle_classify(const cube_params* p, const int32_t* rhoc, int32_t* ires_out, int32_t* napm) {
   Geo G = make_geo(p);

@@ -64,6 +64,8 @@ def lib():
                                     ctypes.POINTER(KickOut), ctypes.c_int, ctypes.c_int64, ctypes.c_int, vp,
                                     ctypes.c_int64]
         L.oracle_classify.argtypes = [P, vp, vp, vp]
+        L.oracle_zipv_encode.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_float]
+        L.oracle_zipv_decode.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_float]
         _LIB = L
     return _LIB
 
@@ -167,3 +169,17 @@ def classify(p: Params, rhoc):
     cp = p.to_c()
     lib().oracle_classify(ctypes.byref(cp), _ptr(np.ascontiguousarray(rhoc)), _ptr(ires), _ptr(napm))
     return ires, napm
+
+
+def zipv_encode(v, sigma_vi: float):
+    v = np.ascontiguousarray(v, dtype=np.float32)
+    out = np.empty(v.shape, dtype=np.int16)
+    lib().oracle_zipv_encode(_ptr(v), _ptr(out), v.size, sigma_vi)
+    return out
+
+
+def zipv_decode(code, sigma_vi: float):
+    code = np.ascontiguousarray(code, dtype=np.int16)
+    out = np.empty(code.shape, dtype=np.float32)
+    lib().oracle_zipv_decode(_ptr(code), _ptr(out), code.size, sigma_vi)
+    return out

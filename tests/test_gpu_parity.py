@@ -245,3 +245,24 @@ def test_potential_at_bench_sizes(oracle_lib, geom):
             got = ctx.captured(size)
         err = np.abs(got - ref).max() / np.abs(ref).max()
         assert err < 2e-5, "%s level %d phi rel err %.3g" % (geom, level, err)
+
+
+def test_zipv_codec_matches_oracle(oracle_lib):
+    p = _params()
+    st = lattice_state(p, seed=3)
+    rng = np.random.default_rng(9)
+    v = (rng.normal(size=300000) * 3.0).astype(np.float32)
+    sigma = 0.41
+    with _ctx(p, st) as ctx:
+        code = ctx.zipv_encode(v, sigma)
+        back = ctx.zipv_decode(code, sigma)
+        xp, code_ck, pid, rhoc = ctx.download_zipv(sigma)
+    ref_code = oracle_lib.zipv_encode(v, sigma)
+    # FP64 atan/tan differ from the host's libm by at most an ulp: codes agree except
+    # where the unrounded value sits on a half-integer
+    assert np.mean(code == ref_code) > 0.9999 and np.abs(code.astype(int) - ref_code).max() <= 1
+    ref_back = oracle_lib.zipv_decode(code, sigma)
+    assert np.abs(back - ref_back).max() <= 1e-6 * np.abs(ref_back).max()
+    assert np.array_equal(pid, st[2]) and np.array_equal(rhoc, st[3])
+    ck_ref = oracle_lib.zipv_encode(st[1], sigma)
+    assert np.abs(code_ck.astype(int) - ck_ref).max() <= 1

@@ -92,3 +92,21 @@ def test_classify(oracle_lib):
     assert napm.sum() == p.ns3
     assert set(np.unique(ires)).issubset({2, 3, 4, 5})
     assert ires.max() >= 3  # a tight blob pushes a subtile into a heavier class
+
+
+def test_zipv_codec_round_trip(oracle_lib):
+    """ZIPV int16 velocity codec (utilities/pp_subtile.f90:61,125): codes cover
+    [-32767, 32767], decode(encode(v)) is within half a code step, and encode is
+    idempotent on decoded values."""
+    rng = np.random.default_rng(7)
+    sigma = 0.37
+    v = np.concatenate([rng.normal(size=20000).astype(np.float32) * 2.0, np.array([0, 1e-6, -1e-6, 50, -50], np.float32)])
+    code = oracle_lib.zipv_encode(v, sigma)
+    assert code.dtype == np.int16 and abs(int(code.astype(np.int64).max())) <= 32767
+    back = oracle_lib.zipv_decode(code, sigma)
+    assert np.array_equal(oracle_lib.zipv_encode(back, sigma), code)
+    # step of the code at v: dv/dcode = pi/65535 * (1 + (s v)^2)/s, s = sqrt(pi/2)/(2.5 sigma)
+    s = np.sqrt(np.pi / 2) / (sigma * 2.5)
+    step = np.pi / 65535 * (1 + (s * v.astype(np.float64)) ** 2) / s
+    assert np.all(np.abs(back - v) <= 0.51 * step + 1e-6 * np.abs(v))
+    assert code[np.argmin(np.abs(v))] == 0
