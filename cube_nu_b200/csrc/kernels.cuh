@@ -536,41 +536,70 @@ __global__ void k_f2max_periodic(const float* __restrict__ phi, int nc, float* _
   block_max_to(v, f2out);
 }
 
-// Box meshes phi[b][n^3], index i at array i-m1phi; physical cells 1..nforce.  A block
-// owns a 32x8 tile of (x,y) in one box and marches through z with a ring of five
-// planes (tile plus a 2-cell halo) in shared memory, so each phi value is read about
-// 1.7 times.  grid = nbox * tiles; blockDim = 256.
-constexpr int F2_TX = 32, F2_TY = 8, F2_PX = F2_TX + 4, F2_PY = F2_TY + 4;
+// Box meshes phi[b] (row pitch pf, plane pitch pl floats), index i at array i-m1phi;
+// physical cells 1..nforce.  A block owns a 32x16 tile of (x,y) in one box and marches
+// through z with a ring of five planes (tile plus a 2-cell halo) in shared memory; the
+// plane needed next is prefetched into registers while the current plane is
+// differenced, so each phi value is read about 1.4 times and the load latency overlaps
+// the arithmetic.  grid = nbox * tiles; blockDim = 256.
+constexpr int F2_TX = 32, F2_TY = 16, F2_PX = F2_TX + 4, F2_PY = F2_TY + 4, F2_HALO = F2_PX * F2_PY;
+constexpr int F2_LOADS = (F2_HALO + 255) / 256;
 __global__ void __launch_bounds__(256) k_f2max_box(const float* __restrict__ phi, int n, int nforce, int m1phi,
                                                    int nbox, float* __restrict__ f2out, int pf, int64_t pl) {
-  __shared__ float ring[5][F2_PY * F2_PX];
+  __shared__ float ring[5][F2_HALO];
   const int ntx = (nforce + F2_TX - 1) / F2_TX, nty = (nforce + F2_TY - 1) / F2_TY;
   const int tile = blockIdx.x % (ntx * nty);
   const int b = blockIdx.x / (ntx * nty);
   const int tx0 = (tile % ntx) * F2_TX + 1, ty0 = (tile / ntx) * F2_TY + 1;  // first physical x,y of the tile
   const float* pb = phi + (size_t)b * n * pl;
-  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
-  auto load_plane = [&](int z, float* dst) {  // tile plane z with halo 2 in x and y
-    for (int i = threadIdx.x; i < F2_PY * F2_PX; i += blockDim.x) {
+  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;  // rows ly and ly+8
+  // halo element k of this thread: offset within the plane (or -1 when outside the box)
+  int off[F2_LOADS];
+#pragma unroll
+  for (int k = 0; k < F2_LOADS; ++k) {
+    const int i = threadIdx.x + k * 256;
+    off[k] = -1;
+    if (i < F2_HALO) {
       const int py = i / F2_PX, px = i - py * F2_PX;
-      const int x = tx0 - 2 + px, y = ty0 - 2 + py;
-      // indices stay inside the padded box: x,y in [-1, nforce+2] map to [-1-m1phi, ..] >= 0
-      const bool in = (x - m1phi) < n && (y - m1phi) < n;
-      dst[i] = in ? __ldg(pb + (size_t)(z - m1phi) * pl + (size_t)(y - m1phi) * pf + (x - m1phi)) : 0.f;
+      const int x = tx0 - 2 + px - m1phi, y = ty0 - 2 + py - m1phi;  // array coordinates, >= 0 (m1phi <= -1)
+      if (x < n && y < n) off[k] = y * pf + x;
+    }
+  }
+  auto fetch = [&](int z, float* r) {
+    const float* pz = pb + (size_t)(z - m1phi) * pl;
+#pragma unroll
+    for (int k = 0; k < F2_LOADS; ++k) r[k] = (off[k] >= 0) ? __ldg(pz + off[k]) : 0.f;
+  };
+  auto put = [&](const float* r, float* dst) {
+#pragma unroll
+    for (int k = 0; k < F2_LOADS; ++k) {
+      const int i = threadIdx.x + k * 256;
+      if (i < F2_HALO) dst[i] = r[k];
     }
   };
-  for (int k = 0; k < 4; ++k) load_plane(k - 1, ring[k]);  // planes -1, 0, 1, 2
+  float pre[F2_LOADS];
+  for (int p = -1; p <= 3; ++p) {  // planes -1..3 into slots (p+1)%5
+    fetch(p, pre);
+    put(pre, ring[(p + 1) % 5]);
+  }
+  __syncthreads();
   float v = 0.f;
-  const bool own = (tx0 + lx <= nforce) && (ty0 + ly <= nforce);
+  const bool own0 = (tx0 + lx <= nforce) && (ty0 + ly <= nforce);
+  const bool own1 = (tx0 + lx <= nforce) && (ty0 + ly + 8 <= nforce);
   for (int z = 1; z <= nforce; ++z) {
-    load_plane(z + 2, ring[(z + 3) % 5]);
-    __syncthreads();
+    const bool more = z + 3 <= nforce + 2;
+    if (more) fetch(z + 3, pre);
     const float* c = ring[(z + 1) % 5];
-    const int o = (ly + 2) * F2_PX + (lx + 2);
-    const float fx = grad4(c[o - 2], c[o - 1], c[o + 1], c[o + 2]);
-    const float fy = grad4(c[o - 2 * F2_PX], c[o - F2_PX], c[o + F2_PX], c[o + 2 * F2_PX]);
-    const float fz = grad4(ring[(z - 1) % 5][o], ring[z % 5][o], ring[(z + 2) % 5][o], ring[(z + 3) % 5][o]);
-    if (own) v = fmaxf(v, sumsq3(fx, fy, fz));
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int o = (ly + 8 * h + 2) * F2_PX + (lx + 2);
+      const float fx = grad4(c[o - 2], c[o - 1], c[o + 1], c[o + 2]);
+      const float fy = grad4(c[o - 2 * F2_PX], c[o - F2_PX], c[o + F2_PX], c[o + 2 * F2_PX]);
+      const float fz = grad4(ring[(z - 1) % 5][o], ring[z % 5][o], ring[(z + 2) % 5][o], ring[(z + 3) % 5][o]);
+      if (h == 0 ? own0 : own1) v = fmaxf(v, sumsq3(fx, fy, fz));
+    }
+    __syncthreads();
+    if (more) put(pre, ring[(z + 4) % 5]);  // plane z+3 takes the slot of plane z-2
     __syncthreads();
   }
   block_max_to(v, f2out);
