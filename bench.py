@@ -180,14 +180,23 @@ def cpu_baseline(p, st, dt, dt_old, a_mid, vz, frac_tiles=1 / 64):
 
 
 def make_ic(p, seed, device):
+    """Host-side IC (numpy) for the CPU reference arm."""
     from cube_nu_b200 import ic
 
-    if p.ng >= 256:
-        d = ic.zeldovich_torch(p, z_i=49.0, seed=seed, device=device)
-    else:
-        d = ic.zeldovich(p, z_i=49.0, seed=seed)
+    d = ic.zeldovich(p, z_i=49.0, seed=seed)
     p.mass_p_cdm = d["mass_p_cdm"]
     return d
+
+
+def device_ic(p, seed, device):
+    """ICs generated on the GPU (cube_gpu_ic); returns the context and header values."""
+    from cube_nu_b200 import ic
+    from cube_nu_b200._lib import Context
+
+    p.mass_p_cdm = float(p.ng) ** 3 / float(p.npglobal)
+    ctx = Context(p, device=device)
+    d = ic.zeldovich_device(ctx, p, z_i=49.0, seed=seed)
+    return ctx, d
 
 
 def pinned_like(a):
@@ -238,13 +247,9 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    d = make_ic(p, seed=1 + rank, device="cuda:%d" % local)
-    n = d["xp"].shape[0]
-    st = (d["xp"], d["vp"], d["pid"], d["rhoc"])
-    from cube_nu_b200._lib import Context
-
-    ctx = Context(p, device=local)
-    ctx.upload(*st)
+    ctx, d = device_ic(p, seed=1 + rank, device=local)
+    n = d["nplocal"]
+    st = ctx.download()
     tab = cosmology.expansion_table(p.h0, p.omega_m, p.omega_r)
     bg = cosmology.Background.from_table(tab)
     S = cosmology.StepState(a=d["a"], dt_vmax=d["dt_vmax"], vz_max=d["vz_max"])
@@ -395,15 +400,14 @@ def run_reference(args, p, desc):
     """--impl reference: the CPU restatement timed on the host cores."""
     import torch
 
-    dev = "cuda:0" if torch.cuda.is_available() else None
-    if dev:
-        d = make_ic(p, seed=1, device=dev)
+    if torch.cuda.is_available():
+        # the same ICs as the GPU arm, generated on the device and copied to the host
+        ctx, d = device_ic(p, seed=1, device=0)
+        st = ctx.download()
+        ctx.close()
     else:
-        from cube_nu_b200 import ic
-
-        d = ic.zeldovich(p, z_i=49.0, seed=1)
-        p.mass_p_cdm = d["mass_p_cdm"]
-    st = (d["xp"], d["vp"], d["pid"], d["rhoc"])
+        d = make_ic(p, seed=1, device=None)
+        st = (d["xp"], d["vp"], d["pid"], d["rhoc"])
     n = st[0].shape[0]
     tab = cosmology.expansion_table(p.h0, p.omega_m, p.omega_r)
     bg = cosmology.Background.from_table(tab)

@@ -20,13 +20,25 @@ EXPORTS = (
     "cube_gpu_drift", "cube_gpu_kick", "cube_gpu_step", "cube_gpu_capture", "cube_gpu_captured",
     "cube_gpu_green_table", "cube_gpu_subtile_class", "cube_gpu_last_error", "cube_gpu_version",
     "cube_gpu_profile", "cube_gpu_profile_read", "cube_gpu_profile_name", "cube_gpu_kernel_launches",
-    "cube_gpu_zipv_encode", "cube_gpu_zipv_decode", "cube_gpu_download_zipv",
+    "cube_gpu_zipv_encode", "cube_gpu_zipv_decode", "cube_gpu_download_zipv", "cube_gpu_ic",
 )
 
 
 class StepIn(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_float), ("dt_old", ctypes.c_float), ("a_mid", ctypes.c_float),
                 ("vz_max", ctypes.c_float)]
+
+
+class ICIn(ctypes.Structure):
+    _fields_ = [("nic", ctypes.c_int32), ("npk", ctypes.c_int32), ("seed", ctypes.c_uint64),
+                ("vfactor", ctypes.c_float), ("reserved", ctypes.c_float),
+                ("pk_k", ctypes.POINTER(ctypes.c_double)), ("pk_p", ctypes.POINTER(ctypes.c_double))]
+
+
+class ICOut(ctypes.Structure):
+    _fields_ = [("nplocal", ctypes.c_int64), ("grad_max", ctypes.c_float * 3), ("vmax", ctypes.c_float * 3),
+                ("vz_max", ctypes.c_float), ("dt_vmax", ctypes.c_float), ("nlayer", ctypes.c_int32),
+                ("mass_p_cdm", ctypes.c_float)]
 
 
 class StepOut(ctypes.Structure):
@@ -73,6 +85,7 @@ def load():
     L.cube_gpu_profile_name.restype = ctypes.c_char_p
     L.cube_gpu_kernel_launches.argtypes = [vp]
     L.cube_gpu_kernel_launches.restype = ctypes.c_int64
+    L.cube_gpu_ic.argtypes = [vp, ctypes.POINTER(ICIn), ctypes.POINTER(ICOut)]
     L.cube_gpu_zipv_encode.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_float]
     L.cube_gpu_zipv_decode.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_float]
     L.cube_gpu_download_zipv.argtypes = [vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_float]

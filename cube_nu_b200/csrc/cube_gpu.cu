@@ -19,6 +19,7 @@
 #include "fft.cuh"
 #include "fft2.cuh"
 #include "kernels.cuh"
+#include "ic.cuh"
 
 using namespace cube;
 
@@ -966,6 +967,115 @@ int cube_gpu_captured(cube_ctx* c, float* out, int64_t n) {
     for (int64_t i = 0; i < m; ++i) out[i] = (c->cap_what == 0) ? h[i] * sc : h[i];
   }
   return (int)m;
+}
+
+int cube_gpu_ic(cube_ctx* c, const cube_ic_in* in, cube_ic_out* out) {
+  if (!c || !in || !in->pk_k || !in->pk_p || in->npk < 2 || in->nic < 1) return fail(CUBE_E_ARG, "bad IC arguments");
+  CK(cudaSetDevice(c->device));
+  const Geo& G = c->G;
+  const int nw = in->nic * G.ng;
+  const int nlat = G.nc * (int)c->P.np_nc;
+  if ((G.rcs * in->nic) % (int)c->P.np_nc) return fail(CUBE_E_ARG, "ratio_cs*nic must be a multiple of np_nc");
+  const int64_t np = (int64_t)nlat * nlat * nlat;
+  int rc = alloc_particles(c, np);
+  if (!rc) rc = add_fft(c, nw);
+  if (rc) return rc;
+  // mesh: the arena when it is large enough, else a temporary buffer
+  const Pitch pt = pitch_of(c, nw, false);
+  const size_t mbytes = mesh_bytes(c, nw, 1, false);
+  void* mesh = c->arena;
+  void* tmp_mesh = nullptr;
+  if (mbytes > c->arena_bytes) {
+    CK(cudaMalloc(&tmp_mesh, mbytes));
+    mesh = tmp_mesh;
+  }
+  float* gtab = nullptr;
+  double *lk = nullptr, *lp = nullptr;
+  const int64_t gcount = (int64_t)nw * nw * (nw / 2 + 1);
+  CK(cudaMalloc(&gtab, gcount * sizeof(float)));
+  std::vector<double> hk(in->npk), hp(in->npk);
+  for (int i = 0; i < in->npk; ++i) {
+    if (!(in->pk_k[i] > 0) || !(in->pk_p[i] > 0)) return fail(CUBE_E_ARG, "P(k) table must be positive");
+    hk[i] = std::log(in->pk_k[i]);
+    hp[i] = std::log(in->pk_p[i]);
+  }
+  CK(cudaMalloc(&lk, in->npk * sizeof(double)));
+  CK(cudaMalloc(&lp, in->npk * sizeof(double)));
+  CK(cudaMemcpyAsync(lk, hk.data(), in->npk * sizeof(double), cudaMemcpyHostToDevice, c->s));
+  CK(cudaMemcpyAsync(lp, hp.data(), in->npk * sizeof(double), cudaMemcpyHostToDevice, c->s));
+  CK(cudaMemsetAsync(mesh, 0, mbytes, c->s));
+  const uint2 key = make_uint2((uint32_t)in->seed, (uint32_t)(in->seed >> 32));
+  const int64_t npair = (int64_t)nw * nw * nw / 2;
+  LAUNCH(c, K_FILL, 1, k_ic_noise<<<nblk(npair), 256, 0, c->s>>>((float*)mesh, nw, pt.pr, pt.plr, key));
+  LAUNCH(c, K_GREEN, 1, k_ic_multiplier<<<nblk(gcount), 256, 0, c->s>>>(gtab, nw, c->P.box, lk, lp, in->npk));
+  float* phi = (float*)mesh;
+  launch_fft(c, nw, 1, mesh, false, 1.f, phi, (float2*)mesh, gtab, (float)nw, 3, 1);
+  ICArgs A;
+  A.nw = nw;
+  A.nlat = nlat;
+  A.step = G.rcs * in->nic / (int)c->P.np_nc;
+  A.np_nc = (int)c->P.np_nc;
+  A.nic = in->nic;
+  A.vf = in->vfactor;
+  A.lat_off = (0.5 / in->nic) / G.rcs;
+  CK(cudaMemsetAsync(c->red, 0, 64 * sizeof(float), c->s));
+  LAUNCH(c, K_FILL, 1, k_ic_gradmax<<<nblk(np), 256, 0, c->s>>>(phi, pt.pf, pt.plf, A, c->red));
+  float gm[3];
+  CK(cudaMemcpyAsync(gm, c->red, sizeof(gm), cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  // reference grad_max is |phi(i)-phi(i+2)| on the IC grid; the corner gradient is half of it
+  const double PI = 3.141592653589793;
+  for (int d = 0; d < 3; ++d) gm[d] *= 2.f;
+  A.nlayer = 2 * (int)std::ceil(gm[2] * A.np_nc / (8.0 * A.nic * PI * G.rcs)) + 3;  // ic.f90:587
+  CK(cudaMemsetAsync(c->rhoc2, 0, G.ncells * 4, c->s));
+  CK(cudaMemsetAsync(c->fill, 0, G.ncells * 4, c->s));
+  CK(cudaMemsetAsync(c->nbig, 0, 4, c->s));
+  LAUNCH(c, K_FILL, 1, k_ic_particles<<<nblk(np), 256, 0, c->s>>>(G, phi, pt.pf, pt.plf, A, c->xp, c->vp, c->pid, c->dest,
+                                                                  c->key, c->rhoc2, c->err));
+  LAUNCH(c, K_SCAN, 3, exclusive_scan(c->rhoc2, c->cstart2, G.ncells, c->scan_tmp, c->s));
+  LAUNCH(c, K_DRIFT_SCATTER, 1, k_drift_scatter<<<nblk(np), 256, 0, c->s>>>(np, c->dest, c->key, c->cstart2, c->fill, c->skey, c->ssrc));
+  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_small<<<nblk(G.ncells * 32), 256, 0, c->s>>>(G.ncells, c->rhoc2, c->cstart2, c->skey,
+                                                                                     c->ssrc, c->biglist, c->nbig));
+  int nb_host = 0;
+  CK(cudaMemcpyAsync(&nb_host, c->nbig, 4, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  const int max_seg = c->P.max_segment > 0 ? std::min(c->P.max_segment, 16384) : 16384;
+  if (nb_host > 0)
+    LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nb_host, 512, (size_t)max_seg * 12, c->s>>>(
+                                   c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey, c->ssrc, max_seg, c->err));
+  c->np = np;
+  LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp, c->pid, 0.f,
+                                                                         c->xp2, c->vp2, c->pid2, c->pcell2));
+  CK(cudaGetLastError());
+  rc = check_err(c);
+  cudaFree(gtab);
+  cudaFree(lk);
+  cudaFree(lp);
+  if (tmp_mesh) cudaFree(tmp_mesh);
+  if (rc) return rc;
+  std::swap(c->xp, c->xp2);
+  std::swap(c->vp, c->vp2);
+  std::swap(c->pid, c->pid2);
+  std::swap(c->pcell, c->pcell2);
+  std::swap(c->rhoc, c->rhoc2);
+  std::swap(c->cstart, c->cstart2);
+  c->loaded = true;
+  prof_collect(c);
+  if (out) {
+    memset(out, 0, sizeof(*out));
+    out->nplocal = np;
+    float vm = 0.f;
+    for (int d = 0; d < 3; ++d) {
+      out->grad_max[d] = gm[d];
+      out->vmax[d] = (float)(gm[d] / (8.0 * A.nic * PI) * in->vfactor);
+      vm = std::max(vm, std::fabs(out->vmax[d]));
+    }
+    out->vz_max = out->vmax[2];
+    out->dt_vmax = 0.9f * 16.f / vm;
+    out->nlayer = A.nlayer;
+    out->mass_p_cdm = (float)((double)G.ng * G.ng * G.ng / (double)np);
+  }
+  return 0;
 }
 
 // ZIPV codec on host arrays, computed on the context's device.

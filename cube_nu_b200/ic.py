@@ -22,11 +22,45 @@ from . import cosmology
 from .params import Params
 
 
+def philox4x32_10(ctr: np.ndarray, key: tuple[int, int]):
+    """Philox4x32-10 (Salmon et al. 2011) on uint64 arrays holding 32-bit lanes; ctr is
+    (4, n).  The device generator (csrc/ic.cuh) computes the same function."""
+    M0, M1, W0, W1 = 0xD2511F53, 0xCD9E8D57, 0x9E3779B9, 0xBB67AE85
+    mask = np.uint64(0xFFFFFFFF)
+    c0, c1, c2, c3 = (ctr[i].astype(np.uint64) for i in range(4))
+    k0, k1 = np.uint64(key[0] & 0xFFFFFFFF), np.uint64(key[1] & 0xFFFFFFFF)
+    for _ in range(10):
+        p0 = np.uint64(M0) * c0
+        p1 = np.uint64(M1) * c2
+        hi0, lo0 = p0 >> np.uint64(32), p0 & mask
+        hi1, lo1 = p1 >> np.uint64(32), p1 & mask
+        c0, c1, c2, c3 = (hi1 ^ c1 ^ k0) & mask, lo1, (hi0 ^ c3 ^ k1) & mask, lo0
+        k0 = (k0 + np.uint64(W0)) & mask
+        k1 = (k1 + np.uint64(W1)) & mask
+    return c0, c1, c2, c3
+
+
 def noise_field(n: int, seed: int) -> np.ndarray:
-    """Uniform [0,1) float32 noise, Fortran order (x fastest) as noise_<img>.bin stores it.
-    Returned as array[z, y, x]."""
-    rng = np.random.Generator(np.random.Philox(key=seed))
-    return rng.random((n, n, n), dtype=np.float32)
+    """Uniform [0,1) float32 noise on an n^3 grid, array[z, y, x] (x fastest, as
+    noise_<img>.bin stores it).  Counter = Box-Muller pair index m (cells 2m, 2m+1),
+    key = seed; u(2m) and u(2m+1) are the top 24 bits of the first two Philox outputs,
+    the same stream the device IC (cube_gpu_ic) draws."""
+    m = np.arange(n * n * n // 2, dtype=np.uint64)
+    ctr = np.stack([m & np.uint64(0xFFFFFFFF), m >> np.uint64(32), np.zeros_like(m), np.zeros_like(m)])
+    r0, r1, _, _ = philox4x32_10(ctr, (seed & 0xFFFFFFFF, seed >> 32))
+    u = np.empty(n * n * n, dtype=np.float32)
+    u[0::2] = (r0 >> np.uint64(8)).astype(np.float32) * np.float32(2.0 ** -24)
+    u[1::2] = (r1 >> np.uint64(8)).astype(np.float32) * np.float32(2.0 ** -24)
+    return u.reshape(n, n, n)
+
+
+def pk_table(p: Params, a: float, nw: int, npts: int = 4096):
+    """Linear P(k) at scale factor a on a log grid covering the IC grid's modes (the
+    table format of Pcb_ic.txt: k in h/Mpc, P in (Mpc/h)^3)."""
+    kmin = 2 * math.pi / p.box * 0.5
+    kmax = 2 * math.pi / p.box * nw * math.sqrt(3.0)
+    k = np.logspace(math.log10(kmin), math.log10(kmax), npts)
+    return k, cosmology.linear_power(k, a, p)
 
 
 def box_muller(u: np.ndarray) -> np.ndarray:
@@ -54,7 +88,10 @@ def potential_field(p: Params, a: float, seed: int, use_torch: bool = False) -> 
     ky = k1[None, :, None]
     kxx = kx[None, None, :]
     kr = 2 * math.pi * np.sqrt(kxx ** 2 + ky ** 2 + kz ** 2) / p.box
-    tf = np.sqrt(cosmology.linear_power(kr, a, p) * (nw / p.box) ** 3)
+    tk, tp = pk_table(p, a, nw)
+    with np.errstate(divide="ignore"):
+        lp = np.interp(np.log(np.where(kr > 0, kr, tk[0])), np.log(tk), np.log(tp))  # ic.f90 interp_tf, log-log
+    tf = np.sqrt(np.exp(lp) * (nw / p.box) ** 3)
     s = np.sin(np.pi * np.arange(nw) / nw)
     kdisc = (2 * s[None, None, : nw // 2 + 1]) ** 2 + (2 * np.sin(np.pi * k1 / nw))[None, :, None] ** 2 \
         + (2 * np.sin(np.pi * k1 / nw))[:, None, None] ** 2
@@ -280,3 +317,25 @@ def zeldovich_torch(p: Params, z_i: float = 49.0, seed: int = 1, device: str = "
     del X, vel, cell, cellw, lat_idx, iq, pid, tile, lat_loc, kk, key, loc, order_cell, perm, code, rhoc
     torch.cuda.empty_cache()
     return out
+
+
+def zeldovich_device(ctx, p: Params, z_i: float = 49.0, seed: int = 1) -> dict:
+    """Generate the ICs on the GPU (cube_gpu_ic) as the context's particle state; returns
+    the header values the reference's IC writes (ic.f90:575-590, 839)."""
+    import ctypes
+
+    from . import _lib
+
+    a = 1.0 / (1.0 + z_i)
+    nw = p.nic * p.ng
+    k, pk = pk_table(p, a, nw)
+    k = np.ascontiguousarray(k, dtype=np.float64)
+    pk = np.ascontiguousarray(pk, dtype=np.float64)
+    cin = _lib.ICIn(nic=p.nic, npk=k.size, seed=seed, vfactor=cosmology.vfactor(a, p.omega_m, p.omega_l),
+                    reserved=0.0, pk_k=k.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                    pk_p=pk.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    out = _lib.ICOut()
+    _lib._check(ctx._lib.cube_gpu_ic(ctx._h, ctypes.byref(cin), ctypes.byref(out)), "cube_gpu_ic")
+    ctx.np = int(out.nplocal)
+    return {"a": a, "mass_p_cdm": float(out.mass_p_cdm), "vz_max": float(out.vz_max), "dt_vmax": float(out.dt_vmax),
+            "nplocal": int(out.nplocal), "grad_max": list(out.grad_max), "nlayer": int(out.nlayer)}

@@ -119,6 +119,31 @@ int cube_gpu_upload(cube_ctx* ctx, const void* xp, const float* vp, const int64_
 int cube_gpu_download(cube_ctx* ctx, void* xp, float* vp, int64_t* pid, int32_t* rhoc,
                       int64_t* nplocal);
 
+/* Zel'dovich initial conditions generated on the device (utilities/ic.f90), left as the
+ * context's particle state (replaces reading the IC checkpoint).  The noise comes from
+ * Philox4x32-10 keyed by `seed` (counter = Box-Muller pair index on the nic*ng grid);
+ * pk_k/pk_p tabulate the linear P(k) at the IC redshift (k in h/Mpc, P in (Mpc/h)^3),
+ * interpolated in log-log as ic.f90's interp_tf. */
+typedef struct cube_ic_in {
+  int32_t nic;       /* IC grid refinement (parameters.f90:33)            */
+  int32_t npk;       /* table length                                       */
+  uint64_t seed;
+  float vfactor;     /* a^2 H(a) in code units (ic.f90:937-945)           */
+  float reserved;
+  const double* pk_k;
+  const double* pk_p;
+} cube_ic_in;
+typedef struct cube_ic_out {
+  int64_t nplocal;
+  float grad_max[3]; /* max |gradphi| per axis on the lattice             */
+  float vmax[3];     /* grad_max/(8 nic pi)*vfactor (ic.f90:584)           */
+  float vz_max;
+  float dt_vmax;     /* 0.9*16/max(vmax) (ic.f90:585)                     */
+  int32_t nlayer;
+  float mass_p_cdm;
+} cube_ic_out;
+int cube_gpu_ic(cube_ctx* ctx, const cube_ic_in* in, cube_ic_out* out);
+
 /* ZIPV int16 velocity codec (utilities/pp_subtile.f90:61 decode, :125 encode; izipv=2,
  * vrel_boost=2.5): code = nint(65535*atan(sqrt(pi/2)/(sigma_vi*2.5)*v)/pi) and back.
  * Host arrays of n values, converted on the context's device. */

@@ -266,3 +266,33 @@ def test_zipv_codec_matches_oracle(oracle_lib):
     assert np.array_equal(pid, st[2]) and np.array_equal(rhoc, st[3])
     ck_ref = oracle_lib.zipv_encode(st[1], sigma)
     assert np.abs(code_ck.astype(int) - ck_ref).max() <= 1
+
+
+@pytest.mark.parametrize("izipx", [1, 2])
+def test_device_ic_matches_host_ic(izipx):
+    """cube_gpu_ic against the numpy IC (same Philox noise and P(k) table; FP32 vs FP64
+    FFT): same particles (PIDs), codes within one step, velocities to 1e-4."""
+    from cube_nu_b200 import ic
+    from cube_nu_b200._lib import Context
+    from cube_nu_b200.params import Params
+
+    p = Params(ng=64, nnt=2, nns=2, np_nc=2, izipx=izipx, box=100.0, nic=2)
+    host = ic.zeldovich(p, z_i=49.0, seed=11)
+    p.mass_p_cdm = host["mass_p_cdm"]
+    with Context(p) as ctx:
+        dev = ic.zeldovich_device(ctx, p, z_i=49.0, seed=11)
+        xp, vp, pid, rhoc = ctx.download()
+    assert dev["nplocal"] == host["xp"].shape[0]
+    assert abs(dev["mass_p_cdm"] - host["mass_p_cdm"]) < 1e-6
+    assert np.array_equal(np.sort(pid), np.sort(host["pid"]))
+    oh, od = np.argsort(host["pid"]), np.argsort(pid)
+    dx = np.abs(xp[od].astype(np.int64) - host["xp"][oh].astype(np.int64))
+    mod = 1 << (8 * izipx)
+    dx = np.minimum(dx, mod - dx)
+    assert dx.max() <= (1 if izipx == 1 else 8)
+    assert np.mean(dx == 0) > (0.999 if izipx == 1 else 0.5)
+    dv = np.abs(vp[od] - host["vp"][oh]).max() / np.abs(host["vp"]).max()
+    assert dv < 1e-4, dv
+    # same cell occupancy except particles on a cell face
+    assert np.abs(rhoc - host["rhoc"]).sum() <= 0.001 * pid.size
+    assert abs(dev["vz_max"] - host["vz_max"]) <= 1e-3 * host["vz_max"]

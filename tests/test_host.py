@@ -1,0 +1,73 @@
+"""Host-side pieces: Philox known answers, expansion table and timestep, checkpoint
+round trip, P(k) table."""
+import os
+
+import numpy as np
+
+from cube_nu_b200 import checkpoint, cosmology, ic
+from cube_nu_b200.params import Params
+
+
+def test_philox_known_answers():
+    """Random123's published Philox4x32-10 test vectors."""
+    kat = [((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+           ((0xFFFFFFFF,) * 4, (0xFFFFFFFF, 0xFFFFFFFF), (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+           ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+            (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1))]
+    for ctr, key, want in kat:
+        c = np.array(ctr, dtype=np.uint64).reshape(4, 1)
+        got = tuple(int(x[0]) for x in ic.philox4x32_10(c, key))
+        assert got == want
+
+
+def test_noise_is_uniform():
+    u = ic.noise_field(32, seed=5)
+    assert u.dtype == np.float32 and u.min() >= 0 and u.max() < 1
+    assert abs(u.mean() - 0.5) < 0.01 and abs(u.var() - 1 / 12) < 0.005
+
+
+def test_timestep_reaches_checkpoint():
+    tab = cosmology.expansion_table(0.6817, 0.3013, 5.0467e-5)
+    bg = cosmology.Background.from_table(tab)
+    st = cosmology.StepState(a=1 / 50.0)
+    bg.init_cursor(st.a)
+    n = 0
+    while not st.final_step and n < 200:
+        cosmology.timestep(bg, st, [49.0, 10.0])
+        n += 1
+        assert st.dt > 0
+        assert st.a_mid > 0
+    assert st.final_step and abs(1 / st.a - 1 - 10.0) < 1e-3
+    # expansion-limited: da/a <= ra_max per step (timestep.f90:21-33)
+    assert n >= 10
+
+
+def test_checkpoint_round_trip(tmp_path):
+    p = Params(ng=32, nnt=1, nns=2, np_nc=2, izipx=2)
+    from tests.helpers import uniform_state
+
+    xp, vp, pid, rhoc = uniform_state(p, 500, seed=1)
+    h = checkpoint.new_header(nplocal=500, npglobal=500, izipx=2, izipv=2, a=0.02, mass_p_cdm=8.0)
+    ck = checkpoint.Checkpoint(h, xp, vp, rhoc, pid)
+    checkpoint.write(str(tmp_path), 1, 49.0, ck)
+    assert os.path.getsize(checkpoint.output_name(str(tmp_path), 1, 49.0, "info")) == 224
+    back = checkpoint.read(str(tmp_path), 1, 49.0, 2)
+    assert np.array_equal(back.xp, xp) and np.array_equal(back.vp, vp)
+    assert np.array_equal(back.pid, pid) and np.array_equal(back.rhoc, rhoc)
+    try:
+        checkpoint.read(str(tmp_path), 1, 49.0, 1)
+        assert False, "izipx mismatch must be rejected (particle_initialization.f90:38-42)"
+    except ValueError:
+        pass
+
+
+def test_linear_power_shape():
+    p = Params()
+    k = np.logspace(-3, 1, 200)
+    P = cosmology.linear_power(k, 1.0, p)
+    assert np.all(P > 0)
+    kpk = k[np.argmax(P)]
+    assert 0.01 < kpk < 0.03  # turnover near k_eq
+    # growth scales as D^2
+    assert np.allclose(cosmology.linear_power(k, 0.5, p) / P, (cosmology.growth_cpt(0.5, p.omega_m, p.omega_l)
+                                                               / cosmology.growth_cpt(1.0, p.omega_m, p.omega_l)) ** 2)
