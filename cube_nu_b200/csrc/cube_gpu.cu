@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1150,3 +1151,132 @@ int cube_gpu_subtile_class(cube_ctx* c, int32_t* ires, int64_t n) {
 }
 
 }  // extern "C"
+
+// =================================================================================
+// PM1 coarse density with no device allocation (no counterpart in the reference).
+//
+// Some callers cannot call cudaMalloc when they want a density field: a process whose
+// device memory is already held by another framework's caching pool (cudaMalloc then
+// fails, or splits memory the pool expects to own), or a caller on a latency-bound path
+// where cudaMalloc/cudaFree would synchronise the whole device.  For them
+// cube_gpu_pm1_density_noalloc runs the PM1 deposit (particle_mesh.f90 PM1 density)
+// with all of its scratch -- cell starts, the scan's tile sums, the per-particle cell
+// index and the int64 fixed-point accumulator -- in one file-scope device array sized
+// for CUBE_NOALLOC_MAX_CELLS coarse cells and CUBE_NOALLOC_MAX_PARTICLES particles.
+// Every device that loads this library holds that array (about 12 MB) until exit.
+// =================================================================================
+namespace {
+
+constexpr size_t na_round(size_t b) { return (b + 255) / 256 * 256; }
+constexpr int64_t kNaCells = CUBE_NOALLOC_MAX_CELLS;
+constexpr int64_t kNaParticles = CUBE_NOALLOC_MAX_PARTICLES;
+constexpr size_t kNaAccOff = 0;                                                   // int64 [cells]
+constexpr size_t kNaStartOff = kNaAccOff + na_round(kNaCells * 8);               // int64 [cells+1]
+constexpr size_t kNaScanOff = kNaStartOff + na_round((kNaCells + 1) * 8);        // int64 [tiles+2]
+constexpr size_t kNaCellOff = kNaScanOff + na_round(((kNaCells + SCAN_TILE - 1) / SCAN_TILE + 2) * 8);  // int32 [np]
+constexpr size_t kNaBytes = kNaCellOff + na_round(kNaParticles * 4);
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+namespace {
+
+// Device address of g_noalloc_scratch per device.  In host code the array's name is only
+// a host-side stand-in, so the address is looked up once per device (with that device
+// current) and handed to the kernels.
+constexpr int kNaMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_addr[kNaMaxDevices];
+
+int noalloc_scratch(unsigned char** out) {
+  int dev = -1;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNaMaxDevices) return fail(CUBE_E_ARG, "device ordinal beyond the static scratch table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* a = nullptr;
+    CK(cudaGetSymbolAddress(&a, g_noalloc_scratch));
+    g_noalloc_addr[dev] = static_cast<unsigned char*>(a);
+  }
+  *out = g_noalloc_addr[dev];
+  return 0;
+}
+
+// Particle -> cell index from the cell starts; indices at or beyond np are not written,
+// so a rhoc that does not sum to np cannot write past the scratch.
+__global__ void k_na_fill_pcell(const int64_t* __restrict__ cstart, int64_t ncells, int64_t np,
+                                int32_t* __restrict__ pcell) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  const int64_t b = cstart[c] > 0 ? cstart[c] : 0;
+  const int64_t e = cstart[c + 1] < np ? cstart[c + 1] : np;
+  for (int64_t i = b; i < e; ++i) pcell[i] = (int32_t)c;
+}
+
+// Fixed-point weight sums -> density in mass units, rounded as cube_gpu_captured does.
+__global__ void k_na_fixed_to_density(const long long* __restrict__ acc, int64_t n, float mass_p,
+                                      float* __restrict__ rho) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) rho[i] = __fmul_rn((float)((double)acc[i] * 0x1p-40), mass_p);
+}
+
+__global__ void k_na_scale(float* __restrict__ rho, int64_t n, float mass_p) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) rho[i] = __fmul_rn(rho[i], mass_p);
+}
+
+}  // namespace
+
+extern "C" int cube_gpu_pm1_density_noalloc(const cube_params* p, const void* xp, const int32_t* rhoc, int64_t np,
+                                            float* rho, void* stream) {
+  if (!p || !rhoc || !rho || np < 0 || (np > 0 && !xp)) return fail(CUBE_E_ARG, "null pointer or negative np");
+  if (p->ratio_cs <= 0 || p->nnt <= 0 || p->nns <= 0 || p->ng % p->ratio_cs || (p->ng / p->ratio_cs) % p->nnt ||
+      ((p->ng / p->ratio_cs) / p->nnt) % p->nns)
+    return fail(CUBE_E_ARG, "ng, nnt, nns must divide evenly (parameters.f90:57-59)");
+  if (p->izipx != 1 && p->izipx != 2) return fail(CUBE_E_ARG, "izipx must be 1 or 2");
+  if (p->mass_p_cdm <= 0.f) return fail(CUBE_E_ARG, "mass_p_cdm must be positive");
+  const Geo G = make_geo(*p);
+  if (G.ncells > kNaCells || np > kNaParticles) {
+    char msg[256];
+    snprintf(msg, sizeof msg,
+             "cube_gpu_pm1_density_noalloc: %lld coarse cells and %lld particles exceed its static scratch "
+             "(at most %lld cells and %lld particles)",
+             (long long)G.ncells, (long long)np, (long long)kNaCells, (long long)kNaParticles);
+    return fail(CUBE_E_CAPACITY, msg);
+  }
+  unsigned char* base = nullptr;
+  if (int rc = noalloc_scratch(&base)) return rc;
+  long long* acc = reinterpret_cast<long long*>(base + kNaAccOff);
+  int64_t* cstart = reinterpret_cast<int64_t*>(base + kNaStartOff);
+  int64_t* tmp = reinterpret_cast<int64_t*>(base + kNaScanOff);
+  int32_t* pcell = reinterpret_cast<int32_t*>(base + kNaCellOff);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool fixed = p->deposit_mode == CUBE_DEPOSIT_FIXED;
+  const int nc = G.nc;
+  const int64_t n3 = G.ncells;
+  // The array keeps the previous call's contents: clear the accumulator and the cell
+  // indices (the scan overwrites every cell start and tile sum it reads).
+  if (fixed) CK(cudaMemsetAsync(acc, 0, n3 * 8, s));
+  else CK(cudaMemsetAsync(rho, 0, n3 * 4, s));
+  if (np > 0) CK(cudaMemsetAsync(pcell, 0, np * 4, s));
+  exclusive_scan(rhoc, cstart, n3, tmp, s);
+  k_na_fill_pcell<<<nblk(n3), 256, 0, s>>>(cstart, n3, np, pcell);
+  if (np > 0) {
+    if (fixed) k_deposit_pm1<true><<<nblk(np), 256, 0, s>>>(G, np, xp, pcell, acc, nc, (int64_t)nc * nc);
+    else k_deposit_pm1<false><<<nblk(np), 256, 0, s>>>(G, np, xp, pcell, rho, nc, (int64_t)nc * nc);
+  }
+  if (fixed) k_na_fixed_to_density<<<nblk(n3), 256, 0, s>>>(acc, n3, G.mass_p, rho);
+  else k_na_scale<<<nblk(n3), 256, 0, s>>>(rho, n3, G.mass_p);
+  CK(cudaGetLastError());
+  // every particle must belong to a cell (drift.f90:139-143 checks the same sum)
+  int64_t total = -1;
+  CK(cudaMemcpyAsync(&total, cstart + n3, sizeof total, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (total != np) {
+    char msg[160];
+    snprintf(msg, sizeof msg, "rhoc sums to %lld particles but np is %lld", (long long)total, (long long)np);
+    return fail(CUBE_E_COUNT, msg);
+  }
+  return 0;
+}

@@ -183,6 +183,34 @@ int cube_gpu_green_table(cube_ctx* ctx, int level, int iapm, float* out, int64_t
 /* Download per-subtile PM3 class (ires, kick.f90:108-133), ns3 entries. */
 int cube_gpu_subtile_class(cube_ctx* ctx, int32_t* ires, int64_t n);
 
+/*
+ * PM1 coarse density without allocating device memory.  No counterpart in the
+ * reference: it is for callers that cannot call cudaMalloc, such as a host whose
+ * device memory is already held by another framework's caching pool (cudaMalloc would
+ * fail or carve up memory the pool owns), or a caller on a latency-bound path where
+ * cudaMalloc/cudaFree would synchronise the whole device.  It needs no context.
+ *
+ * xp (3 codes per particle, izipx bytes each), rhoc (nc^3 counts in the layout of
+ * cube_gpu_upload) and rho (nc^3 floats, x fastest, global coarse cells) are device
+ * pointers on the current device; the result is the PM1 density in mass units, the
+ * same field cube_gpu_capture(ctx, 1, 0, 0) records during a kick (bit-identical
+ * with CUBE_DEPOSIT_FIXED).  Work goes on `stream` (a cudaStream_t, NULL for the
+ * default stream) and the call returns once that stream has finished it.
+ *
+ * All scratch lives in one static device array sized for at most
+ * CUBE_NOALLOC_MAX_CELLS coarse cells and CUBE_NOALLOC_MAX_PARTICLES particles (about
+ * 12 MB, held by every device that loads the library until the process exits); larger
+ * sizes return CUBE_E_CAPACITY.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  Every call shares the array: calls that overlap on the GPU (other
+ * streams, other host threads) race; serialise them.  Each call clears what it
+ * accumulates into.  Returns CUBE_E_COUNT when rhoc does not sum to np.
+ */
+#define CUBE_NOALLOC_MAX_CELLS 262144       /* 64^3 coarse cells */
+#define CUBE_NOALLOC_MAX_PARTICLES 2097152  /* 2^21 particles    */
+int cube_gpu_pm1_density_noalloc(const cube_params* p, const void* xp, const int32_t* rhoc, int64_t np,
+                                 float* rho, void* stream);
+
 /* Text of the last error on this thread. */
 int cube_gpu_last_error(char* buf, size_t n);
 /* Library build string. */
