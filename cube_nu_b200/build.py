@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libcube_gpu.so")
 SOURCES = ["cube_gpu.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh"]
+HEADERS = ["common.cuh", "fft.cuh", "fft2.cuh", "ic.cuh", "kernels.cuh"]
 
 
 def nvcc() -> str:
