@@ -219,6 +219,8 @@ def main():
     ap.add_argument("--deposit", default="fixed", choices=["fixed", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-json", default="")
+    ap.add_argument("--pk", type=int, default=0,
+                    help="after the timed steps, also time cube_gpu_power on an NW^3 mesh (outside the metric)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -337,6 +339,15 @@ def main():
     io_bytes = n * (3 * p.izipx + 12 + 8) + p.ncells * 4
     e2e_value = total_particles * e2e_steps / t_e2e
 
+    analysis = None
+    if args.pk:
+        # power spectrum of the evolved particles (cicpower + auto_power): first call
+        # builds the FFT tables, the second is timed on the device
+        ctx.power(args.pk, n_corr=1)
+        xi, _, po = ctx.power(args.pk)
+        analysis = {"pk_nw": args.pk, "pk_ms": round(po.ms, 3), "pk_alpha": float(po.alpha),
+                    "pk_corrections": po.n_corr_done, "pk_nbin": int(po.nbin)}
+
     if rank == 0:
         peaks, peak_kind = load_peaks()
         napm = list(sos[-1].napm)
@@ -384,6 +395,8 @@ def main():
             "stage_ms_per_step": {k: round(float(v) / args.steps, 3) for k, v in
                                   zip(("drift", "pm1", "pm2", "pm3", "pp", "kick", "step"), stage)},
         }
+        if analysis:
+            line["analysis"] = analysis
         if args.profile_json:
             with open(args.profile_json, "w") as f:
                 json.dump({"kernels": [{"name": r[1], "total_ms": r[0], "launches": r[2], "avg_ms": r[3],

@@ -20,7 +20,7 @@ EXPORTS = (
     "cube_gpu_drift", "cube_gpu_kick", "cube_gpu_step", "cube_gpu_capture", "cube_gpu_captured",
     "cube_gpu_green_table", "cube_gpu_subtile_class", "cube_gpu_last_error", "cube_gpu_version",
     "cube_gpu_profile", "cube_gpu_profile_read", "cube_gpu_profile_name", "cube_gpu_kernel_launches",
-    "cube_gpu_zipv_encode", "cube_gpu_zipv_decode", "cube_gpu_download_zipv", "cube_gpu_ic",
+    "cube_gpu_zipv_encode", "cube_gpu_zipv_decode", "cube_gpu_download_zipv", "cube_gpu_ic", "cube_gpu_power",
 )
 
 
@@ -39,6 +39,17 @@ class ICOut(ctypes.Structure):
     _fields_ = [("nplocal", ctypes.c_int64), ("grad_max", ctypes.c_float * 3), ("vmax", ctypes.c_float * 3),
                 ("vz_max", ctypes.c_float), ("dt_vmax", ctypes.c_float), ("nlayer", ctypes.c_int32),
                 ("mass_p_cdm", ctypes.c_float)]
+
+
+class PowerIn(ctypes.Structure):
+    _fields_ = [("nw", ctypes.c_int32), ("n_interp", ctypes.c_int32), ("n_int", ctypes.c_int32),
+                ("n_corr", ctypes.c_int32)]
+
+
+class PowerOut(ctypes.Structure):
+    _fields_ = [("nbin", ctypes.c_int64), ("mean", ctypes.c_double), ("alpha", ctypes.c_float),
+                ("n_corr_done", ctypes.c_int32), ("delta_min", ctypes.c_float), ("delta_max", ctypes.c_float),
+                ("ms", ctypes.c_float)]
 
 
 class StepOut(ctypes.Structure):
@@ -89,6 +100,7 @@ def load():
     L.cube_gpu_zipv_encode.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_float]
     L.cube_gpu_zipv_decode.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_float]
     L.cube_gpu_download_zipv.argtypes = [vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_float]
+    L.cube_gpu_power.argtypes = [vp, ctypes.POINTER(PowerIn), vp, ctypes.c_int64, vp, ctypes.POINTER(PowerOut)]
     _LIB = L
     return L
 
@@ -226,6 +238,21 @@ class Context:
         _check(self._lib.cube_gpu_download_zipv(self._h, _ptr(xp), _ptr(code), _ptr(pid), _ptr(rhoc), ctypes.byref(n),
                                                 sigma_vi), "cube_gpu_download_zipv")
         return xp, code, pid, rhoc
+
+    def power(self, nw: int, n_interp: int = 2, n_int: int = 3, n_corr: int = 4, want_delta: bool = False):
+        """Power spectrum of the resident particles (cicpower.f90 + powerspectrum.f90).
+
+        Returns (xi, delta, out): xi has shape (nbin+1, 10), rows as xi(10,0:nbin) in the
+        reference; delta is the (nw,nw,nw) density contrast or None; out a PowerOut."""
+        nbin = int(round(float(np.float32(nw // 2) * np.sqrt(np.float32(3)))))
+        xi = np.zeros((nbin + 2, 10), dtype=np.float32)
+        delta = np.empty((nw, nw, nw), dtype=np.float32) if want_delta else None
+        pin = PowerIn(nw, n_interp, n_int, n_corr)
+        out = PowerOut()
+        _check(self._lib.cube_gpu_power(self._h, ctypes.byref(pin), _ptr(xi), xi.size,
+                                        _ptr(delta) if delta is not None else None, ctypes.byref(out)),
+               "cube_gpu_power")
+        return xi[:out.nbin + 1].copy(), delta, out
 
     def subtile_class(self) -> np.ndarray:
         out = np.empty(self.params.ns3, dtype=np.int32)

@@ -21,6 +21,7 @@
 #include "fft2.cuh"
 #include "kernels.cuh"
 #include "ic.cuh"
+#include "power.cuh"
 
 using namespace cube;
 
@@ -57,13 +58,14 @@ struct FFTTable {
 enum KClass {
   K_DRIFT_DEST, K_DRIFT_SCATTER, K_DRIFT_SORT, K_DRIFT_GATHER, K_SCAN, K_DEP_PM1, K_FFT_PM1, K_F2_PM1, K_INT_PM1,
   K_DEP_PM2, K_FFTX_PM2, K_FFTY_PM2, K_FFTZ_PM2, K_FFTC_PM2, K_F2_PM2, K_INT_PM2, K_DEP_PM3, K_FFTX_PM3, K_FFTY_PM3,
-  K_FFTZ_PM3, K_FFTC_PM3, K_F2_PM3, K_INT_PM3, K_PP, K_CLASSIFY, K_GREEN, K_FILL, K_NCLASS
+  K_FFTZ_PM3, K_FFTC_PM3, K_F2_PM3, K_INT_PM3, K_PP, K_CLASSIFY, K_GREEN, K_FILL, K_PK_DEP, K_PK_FFT, K_PK_BIN,
+  K_PK_ALIAS, K_NCLASS
 };
 const char* const KNAMES[K_NCLASS] = {
     "drift_dest", "drift_scatter", "drift_sort", "drift_gather", "scan", "deposit_pm1", "fft_pm1", "f2max_pm1",
     "interp_pm1", "deposit_pm2", "fft_x_pm2", "fft_y_pm2", "fft_z_green_pm2", "fft_c2r_pm2", "f2max_pm2",
     "interp_pm2", "deposit_pm3", "fft_x_pm3", "fft_y_pm3", "fft_z_green_pm3", "fft_c2r_pm3", "f2max_pm3",
-    "interp_pm3", "pp", "classify", "green", "fill_pcell"};
+    "interp_pm3", "pp", "classify", "green", "fill_pcell", "pk_deposit", "pk_fft", "pk_bin", "pk_alias"};
 
 struct ProfRec {
   int cls;
@@ -316,21 +318,21 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
   dim3 gc((unsigned)(nbox * N), (unsigned)((NH + W - 1) / W));
   if constexpr (N <= 144) {
     if (fused_layout(c, N)) {
-      const size_t smp = f2::PlaneSm<N>::BYTES;
+      const size_t smf = f2::Plane3Sm<N>::FWD, smi = f2::Plane3Sm<N>::INV;
       const unsigned planes = (unsigned)(nbox * N);
       if (fixed) {
-        smem_optin(f2::k_fxy_r2c<N, R1, R2, long long>, smp);
-        LAUNCH(c, kx, 1, f2::k_fxy_r2c<N, R1, R2, long long><<<planes, f2::PLANE_THREADS, smp, c->s>>>(
+        smem_optin(f2::k_fxy3_r2c<N, R1, R2, long long>, smf);
+        LAUNCH(c, kx, 1, f2::k_fxy3_r2c<N, R1, R2, long long><<<planes, f2::PLANE3_THREADS, smf, c->s>>>(
                              (const long long*)real_in, ck, tw, scale, pt.pr, pt.pc, pt.plr, pt.plc));
       } else {
-        smem_optin(f2::k_fxy_r2c<N, R1, R2, float>, smp);
-        LAUNCH(c, kx, 1, f2::k_fxy_r2c<N, R1, R2, float><<<planes, f2::PLANE_THREADS, smp, c->s>>>(
+        smem_optin(f2::k_fxy3_r2c<N, R1, R2, float>, smf);
+        LAUNCH(c, kx, 1, f2::k_fxy3_r2c<N, R1, R2, float><<<planes, f2::PLANE3_THREADS, smf, c->s>>>(
                              (const float*)real_in, ck, tw, scale, pt.pr, pt.pc, pt.plr, pt.plc));
       }
-      smem_optin(f2::k_fcol<N, R1, R2, 2, 2>, smc);
-      LAUNCH(c, kz, 1, f2::k_fcol<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
-      smem_optin(f2::k_fyx_c2r<N, R1, R2>, smp);
-      LAUNCH(c, kc, 1, f2::k_fyx_c2r<N, R1, R2><<<planes, f2::PLANE_THREADS, smp, c->s>>>(
+      smem_optin(f2::k_fcol3<N, R1, R2, 2, 2>, smc);
+      LAUNCH(c, kz, 1, f2::k_fcol3<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
+      smem_optin(f2::k_fyx3_c2r<N, R1, R2>, smi);
+      LAUNCH(c, kc, 1, f2::k_fyx3_c2r<N, R1, R2><<<planes, f2::PLANE3_THREADS, smi, c->s>>>(
                            ck, phi_out, tw, norm, reps, pt.pc, pt.pf, pt.plc, pt.plf));
       return;
     }
@@ -347,13 +349,13 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
     LAUNCH(c, kx, 1, f2::k_fx_r2c<N, R1, R2, float><<<gx, S * T, smx, c->s>>>((const float*)real_in, ck, nrows, tw,
                                                                              scale, pt.pr, pt.pc));
   }
-  smem_optin(f2::k_fcol<N, R1, R2, 1, 0>, smc);
-  smem_optin(f2::k_fcol<N, R1, R2, 2, 2>, smc);
-  smem_optin(f2::k_fcol<N, R1, R2, 1, 1>, smc);
+  smem_optin(f2::k_fcol3<N, R1, R2, 1, 0>, smc);
+  smem_optin(f2::k_fcol3<N, R1, R2, 2, 2>, smc);
+  smem_optin(f2::k_fcol3<N, R1, R2, 1, 1>, smc);
   smem_optin(f2::k_fx_c2r<N, R1, R2>, smx);
-  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
-  LAUNCH(c, kz, 1, f2::k_fcol<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
-  LAUNCH(c, ky, 1, f2::k_fcol<N, R1, R2, 1, 1><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
+  LAUNCH(c, ky, 1, f2::k_fcol3<N, R1, R2, 1, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
+  LAUNCH(c, kz, 1, f2::k_fcol3<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
+  LAUNCH(c, ky, 1, f2::k_fcol3<N, R1, R2, 1, 1><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
   LAUNCH(c, kc, 1, f2::k_fx_c2r<N, R1, R2><<<gx, S * T, smx, c->s>>>(ck, phi_out, nrows, tw, norm, reps, pt.pc, pt.pf));
 }
 
@@ -391,6 +393,61 @@ bool fft2_dispatch(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool f
     default: return false;
   }
 #undef CUBE_FFT2
+}
+
+// Forward-only r2c transform of one real mesh (float, layout of pitch_of(c, N, false))
+// into its half spectrum, in place: the x (or fused xy) pass, then y and z forward.
+template <int N, int R1, int R2>
+void fft2_forward(cube_ctx* c, float* real, const Pitch& pt, int cls) {
+  constexpr int T = f2::TPS<R1, R2>::T, NH = N / 2 + 1;
+  const float2* tw = fft_desc(c, N)->tw;
+  float2* ck = reinterpret_cast<float2*>(real);
+  const int64_t nrows = (int64_t)N * N;
+  const int W = f2::fcol_width(N, T);
+  const size_t smc = (size_t)(N + W * N) * sizeof(float2);
+  dim3 gc((unsigned)N, (unsigned)((NH + W - 1) / W));
+  smem_optin(f2::k_fcol3<N, R1, R2, 2, 0>, smc);
+  if constexpr (N <= 144) {
+    if (fused_layout(c, N)) {
+      const size_t smf = f2::Plane3Sm<N>::FWD;
+      smem_optin(f2::k_fxy3_r2c<N, R1, R2, float>, smf);
+      LAUNCH(c, cls, 1, f2::k_fxy3_r2c<N, R1, R2, float><<<(unsigned)N, f2::PLANE3_THREADS, smf, c->s>>>(
+                            real, ck, tw, 1.f, pt.pr, pt.pc, pt.plr, pt.plc));
+      LAUNCH(c, cls, 1, f2::k_fcol3<N, R1, R2, 2, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
+      return;
+    }
+  }
+  const int S = std::max(1, 256 / T);
+  const size_t smx = (size_t)(N + S * N) * sizeof(float2);
+  const unsigned gx = (unsigned)((nrows + 2 * S - 1) / (2 * S));
+  smem_optin(f2::k_fx_r2c<N, R1, R2, float>, smx);
+  smem_optin(f2::k_fcol3<N, R1, R2, 1, 0>, smc);
+  LAUNCH(c, cls, 1, f2::k_fx_r2c<N, R1, R2, float><<<gx, S * T, smx, c->s>>>(real, ck, nrows, tw, 1.f, pt.pr, pt.pc));
+  LAUNCH(c, cls, 1, f2::k_fcol3<N, R1, R2, 1, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
+  LAUNCH(c, cls, 1, f2::k_fcol3<N, R1, R2, 2, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
+}
+
+bool fft2_forward_dispatch(cube_ctx* c, int n, float* real, const Pitch& pt, int cls) {
+#define CUBE_FFT2F(N, R1, R2) \
+  case N: fft2_forward<N, R1, R2>(c, real, pt, cls); return true;
+  switch (n) {
+    CUBE_FFT2F(16, 4, 4)
+    CUBE_FFT2F(32, 4, 8)
+    CUBE_FFT2F(48, 8, 6)
+    CUBE_FFT2F(64, 8, 8)
+    CUBE_FFT2F(96, 8, 12)
+    CUBE_FFT2F(128, 8, 16)
+    CUBE_FFT2F(144, 12, 12)
+    CUBE_FFT2F(192, 16, 12)
+    CUBE_FFT2F(256, 16, 16)
+    CUBE_FFT2F(288, 16, 18)
+    CUBE_FFT2F(432, 24, 18)
+    CUBE_FFT2F(512, 16, 32)
+    CUBE_FFT2F(576, 24, 24)
+    CUBE_FFT2F(1024, 32, 32)
+    default: return false;
+  }
+#undef CUBE_FFT2F
 }
 
 void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out,
@@ -1278,5 +1335,207 @@ extern "C" int cube_gpu_pm1_density_noalloc(const cube_params* p, const void* xp
     snprintf(msg, sizeof msg, "rhoc sums to %lld particles but np is %lld", (long long)total, (long long)np);
     return fail(CUBE_E_COUNT, msg);
   }
+  return 0;
+}
+
+// =================================================================================
+// Power spectrum of the device-resident particles (utilities/cicpower.f90,
+// utilities/powerspectrum.f90 auto_power and pk_correction).
+// =================================================================================
+namespace {
+
+// interp1 (powerspectrum.f90:261-275) as auto_power calls it: the sections xi(2,:) and
+// xi(5,:) of xi(10,0:nbin) reach dummies of size nbin, so xdata(i) is bin i-1.
+float pk_interp1(const float* xi, int64_t nbin, int rx, int ry, float xq) {
+  auto X = [&](int64_t i) { return xi[(i - 1) * 10 + rx]; };
+  auto Y = [&](int64_t i) { return xi[(i - 1) * 10 + ry]; };
+  int64_t i1 = 1, i2 = nbin;
+  while (i2 - i1 > 1) {
+    const int64_t im = (i1 + i2) / 2;
+    if (xq > X(im)) i1 = im;
+    else i2 = im;
+  }
+  return Y(i1) + (xq - X(i1)) / (X(i2) - X(i1)) * (Y(i2) - Y(i1));
+}
+
+// real**integer as gfortran evaluates it (square and multiply).
+float pk_powi(float x, int n) {
+  float y = (n & 1) ? x : 1.f;
+  while (n >>= 1) {
+    x = x * x;
+    if (n & 1) y = y * x;
+  }
+  return y;
+}
+
+float pk_key_to_float(int k) {
+  const int i = k >= 0 ? k : k ^ 0x7fffffff;
+  float f;
+  memcpy(&f, &i, sizeof f);
+  return f;
+}
+
+}  // namespace
+
+extern "C" int cube_gpu_power(cube_ctx* c, const cube_power_in* in, float* xi, int64_t nxi, float* delta,
+                              cube_power_out* out) {
+  if (!c || !in || !xi) return fail(CUBE_E_ARG, "null argument");
+  if (!c->loaded) return fail(CUBE_E_STATE, "power spectrum before upload");
+  const int nw = in->nw;
+  if (c->fft_generic || !fft2_size(nw))
+    return fail(CUBE_E_ARG, "nw must be one of 16 32 48 64 96 128 144 192 256 288 432 512 576 1024");
+  if (in->n_interp < 1 || in->n_interp > 3) return fail(CUBE_E_ARG, "n_interp must be 1 (NGP), 2 (CIC) or 3 (TSC)");
+  if (in->n_int < 0 || in->n_int > PK_MAX_NINT) return fail(CUBE_E_ARG, "n_int must be in 0..4");
+  const int nyq = nw / 2;
+  const int64_t nbin = std::lround((float)nyq * std::sqrt(3.f));  // powerspectrum.f90:15
+  if (nxi < 10 * (nbin + 1)) return fail(CUBE_E_ARG, "xi needs 10*(nbin+1) floats, nbin = nint(nw/2*sqrt(3))");
+  CK(cudaSetDevice(c->device));
+  int rc = add_fft(c, nw);
+  if (rc) return rc;
+  const Geo& G = c->G;
+  const bool fixed = c->P.deposit_mode == CUBE_DEPOSIT_FIXED;
+  const Pitch pt = pitch_of(c, nw, false);
+  const int64_t n3 = (int64_t)nw * nw * nw;
+  const size_t mbytes = (mesh_bytes(c, nw, 1, false) + 255) / 256 * 256;
+  const size_t abytes = fixed ? (size_t)n3 * 8 : 0;
+  // the mesh (and the fixed-point sums) in the arena when they fit, else temporaries
+  void* big = nullptr;
+  char* base = static_cast<char*>(c->arena);
+  if (mbytes + abytes > c->arena_bytes) {
+    CK(cudaMalloc(&big, mbytes + abytes));
+    base = static_cast<char*>(big);
+  }
+  float* mesh = reinterpret_cast<float*>(base);
+  long long* acc = reinterpret_cast<long long*>(base + mbytes);
+  const int nred = 4 * 148;
+  const size_t nbins4 = 4 * (size_t)(nbin + 1), nbins3 = 3 * (size_t)(nbin + 1);
+  void* small = nullptr;
+  const size_t sbytes = (nred + 1 + nbins4 + nbins3) * sizeof(double) + 2 * sizeof(int);
+  if (cudaMalloc(&small, sbytes) != cudaSuccess) {
+    if (big) cudaFree(big);
+    return fail(CUBE_E_CUDA, "cudaMalloc of the power-spectrum sums failed");
+  }
+  double* partial = static_cast<double*>(small);
+  double* total = partial + nred;
+  double* bins = total + 1;
+  double* cb = bins + nbins4;
+  int* mm = reinterpret_cast<int*>(cb + nbins3);
+  auto cleanup = [&]() {
+    cudaFree(small);
+    if (big) cudaFree(big);
+  };
+#define PK_CK(call)                                                                     \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) {                                                            \
+      cleanup();                                                                        \
+      return fail(CUBE_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    }                                                                                   \
+  } while (0)
+  PK_CK(cudaEventRecord(c->ev[0], c->s));
+  const int64_t np = c->np;
+  // cicpower.f90:76-98
+  if (fixed) {
+    PK_CK(cudaMemsetAsync(acc, 0, abytes, c->s));
+    LAUNCH(c, K_PK_DEP, 1, k_cic_deposit<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, acc, nw, nw, (int64_t)nw * nw));
+    LAUNCH(c, K_PK_DEP, 1, k_pk_density<true><<<nred, 256, 0, c->s>>>(acc, mesh, nw, pt.pr, pt.plr, partial));
+  } else {
+    PK_CK(cudaMemsetAsync(mesh, 0, mbytes, c->s));
+    LAUNCH(c, K_PK_DEP, 1, k_cic_deposit<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, mesh, nw, pt.pr, pt.plr));
+    LAUNCH(c, K_PK_DEP, 1, k_pk_density<false><<<nred, 256, 0, c->s>>>(nullptr, mesh, nw, pt.pr, pt.plr, partial));
+  }
+  k_pk_sum_partials<<<1, 256, 0, c->s>>>(partial, nred, total);
+  double rho8 = 0.0;
+  PK_CK(cudaMemcpyAsync(&rho8, total, sizeof(double), cudaMemcpyDeviceToHost, c->s));
+  PK_CK(cudaStreamSynchronize(c->s));
+  // cicpower.f90:171-180: mean = rho8/nw/nw/nw, delta = rho/mean - 1
+  const double mean = rho8 / (double)nw / (double)nw / (double)nw;
+  const int mm0[2] = {0x7fffffff, (int)0x80000000};
+  PK_CK(cudaMemcpyAsync(mm, mm0, sizeof(mm0), cudaMemcpyHostToDevice, c->s));
+  LAUNCH(c, K_PK_DEP, 1, k_pk_delta<<<nred, 256, 0, c->s>>>(mesh, nw, pt.pr, pt.plr, mean, mm));
+  if (delta) {
+    if (pt.pr == nw)  // plane-compact: each plane's rows are contiguous
+      PK_CK(cudaMemcpy2DAsync(delta, (size_t)nw * nw * 4, mesh, pt.psb, (size_t)nw * nw * 4, nw, cudaMemcpyDeviceToHost, c->s));
+    else
+      PK_CK(cudaMemcpy2DAsync(delta, (size_t)nw * 4, mesh, pt.rp, (size_t)nw * 4, (size_t)nw * nw, cudaMemcpyDeviceToHost, c->s));
+  }
+  // powerspectrum.f90:148-187
+  fft2_forward_dispatch(c, nw, mesh, pt, K_PK_FFT);
+  PK_CK(cudaMemsetAsync(bins, 0, nbins4 * sizeof(double), c->s));
+  smem_optin(k_pk_bin, nbins4 * sizeof(double));
+  LAUNCH(c, K_PK_BIN, 1, k_pk_bin<<<nred, 256, nbins4 * sizeof(double), c->s>>>(
+                             reinterpret_cast<const float2*>(mesh), nw, pt.pc, pt.plc, (int)nbin, (float)np, in->n_interp, bins));
+  std::vector<double> hb(nbins4), hc(nbins3);
+  int hmm[2];
+  PK_CK(cudaMemcpyAsync(hb.data(), bins, nbins4 * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+  PK_CK(cudaMemcpyAsync(hmm, mm, sizeof(hmm), cudaMemcpyDeviceToHost, c->s));
+  PK_CK(cudaStreamSynchronize(c->s));
+  for (int64_t b = 0; b <= nbin; ++b) {
+    float* x = xi + 10 * b;
+    for (int r = 0; r < 10; ++r) x[r] = 0.f;
+    x[0] = (float)hb[4 * b];
+    x[1] = (float)hb[4 * b + 1] / x[0];
+    x[2] = (float)hb[4 * b + 2] / x[0];
+    x[3] = (float)hb[4 * b + 3] / x[0];
+    x[4] = x[3];
+  }
+  // powerspectrum.f90:194-201: up to n_corr pk_correction passes while alpha is a number
+  float alpha = 0.f;
+  int done = 0;
+  const int64_t npairs = (int64_t)(nyq + 1) * (nyq + 2) / 2;
+  const size_t smc3 = nbins3 * sizeof(double);
+  smem_optin(k_pk_alias<0>, smc3);
+  smem_optin(k_pk_alias<1>, smc3);
+  smem_optin(k_pk_alias<2>, smc3);
+  smem_optin(k_pk_alias<3>, smc3);
+  smem_optin(k_pk_alias<4>, smc3);
+  for (int it = 0; it < in->n_corr; ++it) {
+    if (it > 0 && std::isnan(alpha)) break;
+    alpha = (std::log(pk_interp1(xi, nbin, 1, 4, (float)nyq)) - std::log(pk_interp1(xi, nbin, 1, 4, (float)nyq / 2))) /
+            std::log(2.f);
+    if (std::isnan(alpha)) continue;
+    PK_CK(cudaMemsetAsync(cb, 0, nbins3 * sizeof(double), c->s));
+    const int p2 = 2 * in->n_interp;
+    switch (in->n_int) {
+      case 0: LAUNCH(c, K_PK_ALIAS, 1, k_pk_alias<0><<<(unsigned)npairs, 128, smc3, c->s>>>(nw, (int)nbin, alpha, p2, cb)); break;
+      case 1: LAUNCH(c, K_PK_ALIAS, 1, k_pk_alias<1><<<(unsigned)npairs, 128, smc3, c->s>>>(nw, (int)nbin, alpha, p2, cb)); break;
+      case 2: LAUNCH(c, K_PK_ALIAS, 1, k_pk_alias<2><<<(unsigned)npairs, 128, smc3, c->s>>>(nw, (int)nbin, alpha, p2, cb)); break;
+      case 3: LAUNCH(c, K_PK_ALIAS, 1, k_pk_alias<3><<<(unsigned)npairs, 128, smc3, c->s>>>(nw, (int)nbin, alpha, p2, cb)); break;
+      default: LAUNCH(c, K_PK_ALIAS, 1, k_pk_alias<4><<<(unsigned)npairs, 128, smc3, c->s>>>(nw, (int)nbin, alpha, p2, cb)); break;
+    }
+    PK_CK(cudaMemcpyAsync(hc.data(), cb, nbins3 * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    PK_CK(cudaStreamSynchronize(c->s));
+    for (int64_t b = 1; b <= nbin; ++b) {
+      const float ratio = (float)hc[3 * b + 2] / (float)hc[3 * b];
+      xi[10 * b + 4] = xi[10 * b + 3] / ratio;
+    }
+    ++done;
+  }
+  // powerspectrum.f90:203-206: k in h/Mpc, power in (Mpc/h)^3
+  const double PI = 3.141592653589793;
+  const float box = c->P.box, box3 = pk_powi(box, 3);
+  for (int64_t b = 0; b <= nbin; ++b) {
+    float* x = xi + 10 * b;
+    x[1] = (float)((double)x[1] * (2 * PI) / (double)box);
+    x[2] = x[2] * box3;
+    x[3] = x[3] * box3;
+    x[4] = x[4] * box3;
+  }
+  PK_CK(cudaEventRecord(c->ev[1], c->s));
+  PK_CK(cudaGetLastError());
+  PK_CK(cudaEventSynchronize(c->ev[1]));
+  prof_collect(c);
+  if (out) {
+    memset(out, 0, sizeof(*out));
+    out->nbin = nbin;
+    out->mean = mean;
+    out->alpha = alpha;
+    out->n_corr_done = done;
+    out->delta_min = pk_key_to_float(hmm[0]);
+    out->delta_max = pk_key_to_float(hmm[1]);
+    cudaEventElapsedTime(&out->ms, c->ev[0], c->ev[1]);
+  }
+  cleanup();
+#undef PK_CK
   return 0;
 }

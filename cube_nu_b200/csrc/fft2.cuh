@@ -10,13 +10,15 @@
 // parameter every index is strength-reduced; no runtime integer division remains in
 // the butterflies.
 //
-// Passes (the same five as the generic kernels in fft.cuh):
-//   k_fx_r2c : rows of reals, two rows packed as one complex sequence, unpacked into
-//              two half spectra (r2c)
-//   k_fcol   : columns (y or z) of the half spectrum, forward / inverse, or forward ->
-//              Green multiply -> inverse (z pass)
-//   k_fx_c2r : two half-spectrum rows packed as one Hermitian-extended sequence,
-//              inverse, real and imaginary parts are the two real rows (c2r)
+// Passes:
+//   k_fx_r2c   : rows of reals, two rows packed as one complex sequence, unpacked into
+//                two half spectra (r2c)
+//   k_fcol3    : columns (y or z) of the half spectrum, forward / inverse, or forward ->
+//                Green multiply -> inverse (z pass); sequences stay in registers
+//   k_fx_c2r   : two half-spectrum rows packed as one Hermitian-extended sequence,
+//                inverse, real and imaginary parts are the two real rows (c2r)
+//   k_fxy3_r2c : for N <= 144 the x and y forward passes of one plane in one block
+//   k_fyx3_c2r : its inverse (y then x)
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -213,58 +215,116 @@ __global__ void __launch_bounds__(256) k_fx_r2c(const IN* r, float2* c, int64_t 
 }
 
 // ---------------------------------------------------------------------------------
-// Column pass on the half spectrum c[b][z][y][kx] (row pitch pc).  MODE 0: forward,
-// 1: inverse, 2: forward, times green[kz][ky][kx] (dense, pitch N/2+1), inverse (z pass).
-// AXIS 1: y, 2: z.  grid.x = b*N + (z for AXIS 1 | y for AXIS 2), grid.y = kx block of W;
-// blockDim = W*T.
+// Column pass with the sequences kept in registers.  Thread (t, col), blockDim = W*T,
+// col fastest (coalesced rows of the half spectrum).  Forward (N = R1*R2, n = R2*n1+n2):
+// thread t = n2 loads x[R2*n1 + t] straight from global memory, R1-point DFT, twiddle,
+// one shared-memory exchange, then thread t = k1 runs the R2-point DFT and holds
+// X[t + R1*k2].  The inverse uses the swapped factorisation (n = R1*n1 + n2), whose
+// first step needs in thread t exactly the X[t + R1*k2] it already holds, so
+// forward -> Green multiply -> inverse costs two exchanges in all.
+//   MODE 0: forward, 1: inverse, 2: forward -> multiply by green[kz][y][kx] -> inverse.
 // ---------------------------------------------------------------------------------
+// Launch bounds of the column pass: two blocks per SM where the sequences fit in 64
+// registers (or 73 with the 444-thread blocks of N = 144), one block above N = 192.
+template <int N>
+struct FcolBounds {
+  static constexpr int MAXT = (N == 144) ? 448 : 512, MINB = (N <= 192) ? 2 : 1;
+};
+
 template <int N, int R1, int R2, int AXIS, int MODE>
-__global__ void __launch_bounds__(512, 2) k_fcol(float2* __restrict__ c, const float* __restrict__ green,
-                                                 const float2* __restrict__ gtw, int W, int pc, int64_t plc) {
-  constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, RPT = N / T;  // rows per thread
-  static_assert(N % T == 0, "rows must split evenly over the thread group");
+__global__ void __launch_bounds__(FcolBounds<N>::MAXT, FcolBounds<N>::MINB) k_fcol3(float2* __restrict__ c, const float* __restrict__ green,
+                                                  const float2* __restrict__ gtw, int W, int pc, int64_t plc) {
+  constexpr int NH = N / 2 + 1;
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* A = sm + N;
+  float2* A = sm + N;  // exchange slots, [N][W]
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
   const int64_t line = blockIdx.x;
   const int64_t b = line / N;
   const int o = (int)(line - b * N);
   const int kx0 = blockIdx.y * W;
-  const int col = threadIdx.x % W, t = threadIdx.x / W;  // blockDim = W*T
+  const int col = threadIdx.x % W, t = threadIdx.x / W;
   const bool live = kx0 + col < NH;
   const int64_t es = (AXIS == 1) ? pc : plc;
   float2* base = c + b * (int64_t)N * plc + (AXIS == 1 ? (int64_t)o * plc : (int64_t)o * pc) + kx0 + col;
-  {
-    float2 r[RPT];
-#pragma unroll
-    for (int k = 0; k < RPT; ++k) r[k] = live ? base[(int64_t)(t + k * T) * es] : make_float2(0.f, 0.f);
-#pragma unroll
-    for (int k = 0; k < RPT; ++k) A[(t + k * T) * W + col] = r[k];
-  }
+  float2* Ac = A + col;
   __syncthreads();
-  if (MODE == 1) {
-    seq_transform<N, R1, R2, +1>(A + col, W, t, tw);
-  } else {
-    seq_transform<N, R1, R2, -1>(A + col, W, t, tw);
-    if (MODE == 2) {
-      if (live) {
-        const float* gb = green + (int64_t)o * NH + kx0 + col;  // g[kz][y][kx], kz stride N*NH
+  if (MODE != 1) {
+    // ---- forward: n = R2*n1 + n2 ----
+    if (t < R2) {
+      float2 v[R1];
 #pragma unroll
-        for (int k = 0; k < RPT; ++k) {
-          const int e = t + k * T;
-          const float gv = __ldg(gb + (int64_t)e * N * NH);
-          const float2 v = A[e * W + col];
-          A[e * W + col] = make_float2(v.x * gv, v.y * gv);
-        }
-      }
-      __syncthreads();
-      seq_transform<N, R1, R2, +1>(A + col, W, t, tw);
+      for (int n1 = 0; n1 < R1; ++n1) v[n1] = live ? base[(int64_t)(R2 * n1 + t) * es] : make_float2(0.f, 0.f);
+      DFT<R1, N, -1>::run(v, tw);
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) Ac[(k1 * R2 + t) * W] = (k1 == 0) ? v[0] : cmul(v[k1], twid<-1>(tw, t * k1));
     }
-  }
-  if (live) {
+    __syncthreads();
+    float2 w[R2];
+    if (t < R1) {
 #pragma unroll
-    for (int k = 0; k < RPT; ++k) base[(int64_t)(t + k * T) * es] = A[(t + k * T) * W + col];
+      for (int n2 = 0; n2 < R2; ++n2) w[n2] = Ac[(t * R2 + n2) * W];
+      DFT<R2, N, -1>::run(w, tw);
+    }
+    if (MODE == 0) {
+      if (t < R1 && live) {
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) base[(int64_t)(t + R1 * k2) * es] = w[k2];
+      }
+      return;
+    }
+    // ---- Green multiply at kz = t + R1*k2 ----
+    if (t < R1 && live) {
+      const float* gb = green + (int64_t)o * NH + kx0 + col;  // g[kz][y][kx]
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) {
+        const float gv = __ldg(gb + (int64_t)(t + R1 * k2) * N * NH);
+        w[k2] = make_float2(w[k2].x * gv, w[k2].y * gv);
+      }
+    }
+    // ---- inverse, n = R1*n1 + n2 with n2 = t, n1 = k2: first step in registers ----
+    if (t < R1) {
+      DFT<R2, N, +1>::run(w, tw);
+#pragma unroll
+      for (int k1 = 1; k1 < R2; ++k1) w[k1] = cmul(w[k1], twid<+1>(tw, t * k1));
+    }
+    __syncthreads();  // every forward read of the slots is done
+    if (t < R1) {
+#pragma unroll
+      for (int k1 = 0; k1 < R2; ++k1) Ac[(k1 * R1 + t) * W] = w[k1];
+    }
+    __syncthreads();
+    if (t < R2) {
+      float2 u[R1];
+#pragma unroll
+      for (int n2 = 0; n2 < R1; ++n2) u[n2] = Ac[(t * R1 + n2) * W];
+      DFT<R1, N, +1>::run(u, tw);
+      if (live) {
+#pragma unroll
+        for (int k2 = 0; k2 < R1; ++k2) base[(int64_t)(t + R2 * k2) * es] = u[k2];
+      }
+    }
+  } else {
+    // ---- inverse only, n = R1*n1 + n2: thread t = n2 < R1 loads x[R1*n1 + t] ----
+    if (t < R1) {
+      float2 w[R2];
+#pragma unroll
+      for (int n1 = 0; n1 < R2; ++n1) w[n1] = live ? base[(int64_t)(R1 * n1 + t) * es] : make_float2(0.f, 0.f);
+      DFT<R2, N, +1>::run(w, tw);
+#pragma unroll
+      for (int k1 = 0; k1 < R2; ++k1) Ac[(k1 * R1 + t) * W] = (k1 == 0) ? w[0] : cmul(w[k1], twid<+1>(tw, t * k1));
+    }
+    __syncthreads();
+    if (t < R2) {
+      float2 u[R1];
+#pragma unroll
+      for (int n2 = 0; n2 < R1; ++n2) u[n2] = Ac[(t * R1 + n2) * W];
+      DFT<R1, N, +1>::run(u, tw);
+      if (live) {
+#pragma unroll
+        for (int k2 = 0; k2 < R1; ++k2) base[(int64_t)(t + R2 * k2) * es] = u[k2];
+      }
+    }
   }
 }
 
@@ -272,9 +332,10 @@ __global__ void __launch_bounds__(512, 2) k_fcol(float2* __restrict__ c, const f
 // launch bound), else an even split.
 __host__ inline int fcol_width(int N, int T) {
   const int NH = N / 2 + 1;
+  const int maxt = (N == 144) ? 448 : 512;  // FcolBounds<N>::MAXT
   for (int nb = 1;; ++nb) {
     const int W = (NH + nb - 1) / nb;
-    if (W * T <= 512 && (size_t)W * N * 8 <= 100 * 1024) return W;
+    if (W * T <= maxt && (size_t)W * N * 8 <= 100 * 1024) return W;
   }
 }
 
@@ -316,155 +377,231 @@ __global__ void __launch_bounds__(256) k_fx_c2r(const float2* c, float* r, int64
 }
 
 // ---------------------------------------------------------------------------------
-// Fused plane passes (one block per z plane; N small enough that a half-spectrum plane
-// fits in shared memory).  Forward: load the real plane, r2c along x (rows packed in
-// pairs), FFT along y, store the complex plane in place.  Inverse: the reverse.  This
-// removes one read and one write of the whole mesh per direction.
+// Plane kernels with register-resident sequences (N <= 144, T = max(R1,R2) <= 16).
+// Rows run warp-synchronously: each warp holds two sequences (lanes 0..T-1 and
+// 16..16+T-1), loads them straight from global memory and exchanges through a skewed
+// slot layout (slot(k1, n2) = k1*R2 + (n2 + k1) mod R2) that is free of bank conflicts
+// in both directions.  Columns run as in k_fcol3, W columns by T threads per round.
+// The r2c unpack and the c2r Hermitian pack happen on the fly inside the other phase,
+// and column results go straight to global memory.
 // ---------------------------------------------------------------------------------
+constexpr int PLANE3_THREADS = 448;
+
 template <int N>
-struct PlaneSm {
-  static constexpr int NH = N / 2 + 1, SP = N + 1;  // packed-row pitch (bank padding)
-  static constexpr int ELEMS = ((N / 2) * SP > N * NH) ? (N / 2) * SP : N * NH;
-  static constexpr size_t BYTES = (size_t)(N + ELEMS) * 8;
+struct Plane3Sm {
+  static constexpr int NH = N / 2 + 1;
+  // forward: packed rows Z[N/2][N] + scratch for the self-conjugate columns 0, N/2
+  static constexpr size_t FWD = (size_t)(N + (N / 2) * N + 2 * N) * 8;
+  // inverse: half spectrum H[N][NH]
+  static constexpr size_t INV = (size_t)(N + N * NH) * 8;
 };
 
-constexpr int PLANE_THREADS = 512;
+template <int R2>
+__device__ __forceinline__ int skew(int k1, int n2) {
+  int j = n2 + k1;
+  j = j % R2;
+  return k1 * R2 + j;
+}
 
 template <int N, int R1, int R2, typename IN>
-__global__ void __launch_bounds__(PLANE_THREADS, 2) k_fxy_r2c(const IN* r, float2* c, const float2* __restrict__ gtw,
-                                                             float scale, int pr, int pc, int64_t plr, int64_t plc) {
-  constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, SP = PlaneSm<N>::SP;
-  constexpr int NPAIR = N / 2;
-  constexpr int KU = (NPAIR * NH + PLANE_THREADS - 1) / PLANE_THREADS;  // unpack items per thread
+__global__ void __launch_bounds__(PLANE3_THREADS, 2) k_fxy3_r2c(const IN* __restrict__ r, float2* __restrict__ c,
+                                                               const float2* __restrict__ gtw, float scale, int pr,
+                                                               int pc, int64_t plr, int64_t plc) {
+  constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, NP = N / 2;
+  static_assert(T <= 16, "two sequences per warp");
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* Z = sm + N;
+  float2* Z = sm + N;             // packed rows, pitch N
+  float2* S = Z + (size_t)NP * N;  // exchange slots of columns 0 and N/2
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
-  const int64_t plane = blockIdx.x;  // b*N + z
+  const int64_t plane = blockIdx.x;
   const IN* rp = r + plane * plr;
   float2* cp = c + plane * plc;
-  for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
-    const int y = i / N, x = i - y * N;
-    const IN v = rp[y * pr + x];
-    float f;
-    if (sizeof(IN) == 8) f = (float)((double)(long long)v * 9.094947017729282e-13);
-    else f = (float)v;
-    reinterpret_cast<float*>(Z + (y >> 1) * SP + x)[y & 1] = __fmul_rn(f, scale);
+  __syncthreads();
+  {  // ---- rows: packed pairs (2p, 2p+1) as re/im ----
+    const int lane = threadIdx.x & 31, t = lane & 15;
+    const int g = (threadIdx.x >> 5) * 2 + (lane >> 4);
+    const int ngr = (blockDim.x >> 5) * 2;
+    for (int p0 = 0; p0 < NP; p0 += ngr) {
+      const int p = p0 + g;
+      const bool act = p < NP;
+      float2* Zr = Z + (size_t)(act ? p : 0) * N;
+      if (act && t < R2) {
+        float2 v[R1];
+#pragma unroll
+        for (int n1 = 0; n1 < R1; ++n1) {
+          const int x = R2 * n1 + t;
+          const IN a = rp[(2 * p) * pr + x], b = rp[(2 * p + 1) * pr + x];
+          float fa, fb;
+          if (sizeof(IN) == 8) {
+            fa = (float)((double)(long long)a * 9.094947017729282e-13);
+            fb = (float)((double)(long long)b * 9.094947017729282e-13);
+          } else {
+            fa = (float)a;
+            fb = (float)b;
+          }
+          v[n1] = make_float2(__fmul_rn(fa, scale), __fmul_rn(fb, scale));
+        }
+        DFT<R1, N, -1>::run(v, tw);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) Zr[skew<R2>(k1, t)] = (k1 == 0) ? v[0] : cmul(v[k1], twid<-1>(tw, t * k1));
+      }
+      __syncwarp();
+      float2 w[R2];
+      if (act && t < R1) {
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) w[n2] = Zr[skew<R2>(t, n2)];
+        DFT<R2, N, -1>::run(w, tw);
+      }
+      __syncwarp();
+      if (act && t < R1) {
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) Zr[t + R1 * k2] = w[k2];
+      }
+      __syncwarp();
+    }
   }
   __syncthreads();
-  {  // x transforms of the packed rows, G at a time
-    constexpr int G = PLANE_THREADS / T;
-    const int s = threadIdx.x / T, t = threadIdx.x - s * T;
-    for (int p0 = 0; p0 < NPAIR; p0 += G) {
-      const int p = p0 + s;
-      seq_transform_g<N, R1, R2, -1>(Z + p * SP, 1, t, tw, s < G && p < NPAIR);
-    }
-  }
-  {  // unpack to the half-spectrum plane X[y][kx] (pitch NH), through registers
-    float2 k0[KU], k1[KU];
+  {  // ---- columns kx of the half spectrum, unpacked on the fly ----
+    const int W = (NH < (int)blockDim.x / T) ? NH : (int)blockDim.x / T;
+    const int col = threadIdx.x % W, t = threadIdx.x / W;
+    for (int kx0 = 0; kx0 < NH; kx0 += W) {
+      const int kx = kx0 + col;
+      const bool act = t < T && kx < NH && col < W;
+      const int kc = (N - kx) % N;
+      // exchange slot s of column kx: columns kx and N-kx of Z are read only by column kx
+      auto slot = [&](int s) -> float2* {
+        if (kx == 0) return S + s;
+        if (2 * kx == N) return S + N + s;
+        return (s < NP) ? Z + (size_t)s * N + kx : Z + (size_t)(s - NP) * N + kc;
+      };
+      float2 v[R1];
+      if (act && t < R2) {
 #pragma unroll
-    for (int u = 0; u < KU; ++u) {
-      const int i = threadIdx.x + u * PLANE_THREADS;
-      if (i < NPAIR * NH) {
-        const int p = i / NH, k = i - p * NH;
-        const float2 z = Z[p * SP + k];
-        const float2 zc = Z[p * SP + ((N - k) % N)];
-        k0[u] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
-        k1[u] = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+        for (int n1 = 0; n1 < R1; ++n1) {
+          const int y = R2 * n1 + t;
+          const float2* zr = Z + (size_t)(y >> 1) * N;
+          const float2 z = zr[kx], zc = zr[kc];
+          v[n1] = (y & 1) ? make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x))
+                          : make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+        }
+        DFT<R1, N, -1>::run(v, tw);
+      }
+      __syncthreads();  // all unpack reads of this round are done
+      if (act && t < R2) {
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) *slot(k1 * R2 + t) = (k1 == 0) ? v[0] : cmul(v[k1], twid<-1>(tw, t * k1));
+      }
+      __syncthreads();
+      if (act && t < R1) {
+        float2 w[R2];
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) w[n2] = *slot(t * R2 + n2);
+        DFT<R2, N, -1>::run(w, tw);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) cp[(int64_t)(t + R1 * k2) * pc + kx] = w[k2];
       }
     }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < KU; ++u) {
-      const int i = threadIdx.x + u * PLANE_THREADS;
-      if (i < NPAIR * NH) {
-        const int p = i / NH, k = i - p * NH;
-        Z[(2 * p) * NH + k] = k0[u];
-        Z[(2 * p + 1) * NH + k] = k1[u];
-      }
-    }
-    __syncthreads();
-  }
-  {  // y transforms of the columns kx (element stride NH), G columns per round
-    constexpr int G = PLANE_THREADS / T;
-    const int col = threadIdx.x % G, t = threadIdx.x / G;
-    for (int k0 = 0; k0 < NH; k0 += G) {
-      const int kx = k0 + col;
-      seq_transform_g<N, R1, R2, -1>(Z + kx, NH, t, tw, t < T && kx < NH);
-    }
-  }
-  for (int i = threadIdx.x; i < N * NH; i += blockDim.x) {
-    const int y = i / NH, k = i - y * NH;
-    cp[y * pc + k] = Z[i];
   }
 }
 
 template <int N, int R1, int R2>
-__global__ void __launch_bounds__(PLANE_THREADS, 2) k_fyx_c2r(const float2* c, float* r, const float2* __restrict__ gtw,
-                                                             float norm, int reps, int pc, int pf, int64_t plc,
-                                                             int64_t plf) {
-  constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, SP = PlaneSm<N>::SP;
-  constexpr int NPAIR = N / 2;
-  constexpr int KP = (NPAIR * N + PLANE_THREADS - 1) / PLANE_THREADS;  // pack items per thread
+__global__ void __launch_bounds__(PLANE3_THREADS, 2) k_fyx3_c2r(const float2* __restrict__ c, float* __restrict__ r,
+                                                               const float2* __restrict__ gtw, float norm, int reps,
+                                                               int pc, int pf, int64_t plc, int64_t plf) {
+  constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, NP = N / 2;
+  static_assert(T <= 16, "two sequences per warp");
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* Z = sm + N;
+  float2* H = sm + N;  // half spectrum after the inverse y transforms, [N][NH]
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
   const int64_t plane = blockIdx.x;
   const float2* cp = c + plane * plc;
   float* rp = r + plane * plf;
-  for (int i = threadIdx.x; i < N * NH; i += blockDim.x) {
-    const int y = i / NH, k = i - y * NH;
-    Z[i] = cp[y * pc + k];
+  __syncthreads();
+  {  // ---- inverse y transforms of the columns kx, n = R2*n1 + n2 ----
+    const int W = (NH < (int)blockDim.x / T) ? NH : (int)blockDim.x / T;
+    const int col = threadIdx.x % W, t = threadIdx.x / W;
+    for (int kx0 = 0; kx0 < NH; kx0 += W) {
+      const int kx = kx0 + col;
+      const bool act = t < T && kx < NH && col < W;
+      float2* Hc = H + kx;  // column kx: N slots, read and written only by column kx
+      if (act && t < R2) {
+        float2 v[R1];
+#pragma unroll
+        for (int n1 = 0; n1 < R1; ++n1) v[n1] = cp[(int64_t)(R2 * n1 + t) * pc + kx];
+        DFT<R1, N, +1>::run(v, tw);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) Hc[(k1 * R2 + t) * NH] = (k1 == 0) ? v[0] : cmul(v[k1], twid<+1>(tw, t * k1));
+      }
+      __syncthreads();
+      float2 w[R2];
+      if (act && t < R1) {
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) w[n2] = Hc[(t * R2 + n2) * NH];
+        DFT<R2, N, +1>::run(w, tw);
+      }
+      __syncthreads();  // every read of the column's slots is done
+      if (act && t < R1) {
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) Hc[(t + R1 * k2) * NH] = w[k2];
+      }
+    }
   }
   __syncthreads();
-  {  // inverse y transforms of the columns
-    constexpr int G = PLANE_THREADS / T;
-    const int col = threadIdx.x % G, t = threadIdx.x / G;
-    for (int k0 = 0; k0 < NH; k0 += G) {
-      const int kx = k0 + col;
-      seq_transform_g<N, R1, R2, +1>(Z + kx, NH, t, tw, t < T && kx < NH);
-    }
-  }
-  {  // pack rows (2p, 2p+1) as X0 + i X1 over the Hermitian extension (c2r convention)
-    float2 kp[KP];
+  {  // ---- rows: pack (2p, 2p+1) over the Hermitian extension, inverse x transform ----
+    const int lane = threadIdx.x & 31, t = lane & 15;
+    const int g = (threadIdx.x >> 5) * 2 + (lane >> 4);
+    const int ngr = (blockDim.x >> 5) * 2;
+    for (int p0 = 0; p0 < NP; p0 += ngr) {
+      const int p = p0 + g;
+      const bool act = p < NP;
+      float2* H0 = H + (size_t)(act ? 2 * p : 0) * NH;  // rows 2p, 2p+1: 2*NH >= N contiguous slots
+      const float2* H1 = H0 + NH;
+      float2 v[R1];
+      if (act && t < R2) {
 #pragma unroll
-    for (int u = 0; u < KP; ++u) {
-      const int i = threadIdx.x + u * PLANE_THREADS;
-      if (i < NPAIR * N) {
-        const int p = i / N, x = i - p * N;
-        const int k = (x < NH) ? x : N - x;
-        float2 a0 = Z[(2 * p) * NH + k], a1 = Z[(2 * p + 1) * NH + k];
-        if (k == 0 || 2 * k == N) { a0.y = 0.f; a1.y = 0.f; }
-        if (x >= NH) { a0.y = -a0.y; a1.y = -a1.y; }
-        kp[u] = make_float2(a0.x - a1.y, a0.y + a1.x);
+        for (int n1 = 0; n1 < R1; ++n1) {
+          const int x = R2 * n1 + t;
+          const int k = (x < NH) ? x : N - x;
+          float2 a0 = H0[k], a1 = H1[k];
+          if (k == 0 || 2 * k == N) {
+            a0.y = 0.f;
+            a1.y = 0.f;
+          }
+          if (x >= NH) {
+            a0.y = -a0.y;
+            a1.y = -a1.y;
+          }
+          v[n1] = make_float2(a0.x - a1.y, a0.y + a1.x);
+        }
+        DFT<R1, N, +1>::run(v, tw);
       }
-    }
-    __syncthreads();
+      __syncwarp();  // the pack reads of rows 2p, 2p+1 are done
+      if (act && t < R2) {
 #pragma unroll
-    for (int u = 0; u < KP; ++u) {
-      const int i = threadIdx.x + u * PLANE_THREADS;
-      if (i < NPAIR * N) {
-        const int p = i / N, x = i - p * N;
-        Z[p * SP + x] = kp[u];
+        for (int k1 = 0; k1 < R1; ++k1) H0[skew<R2>(k1, t)] = (k1 == 0) ? v[0] : cmul(v[k1], twid<+1>(tw, t * k1));
       }
+      __syncwarp();
+      if (act && t < R1) {
+        float2 w[R2];
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) w[n2] = H0[skew<R2>(t, n2)];
+        DFT<R2, N, +1>::run(w, tw);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) {
+          const int x = t + R1 * k2;
+          float a = w[k2].x, b = w[k2].y;
+          for (int q = 0; q < reps; ++q) {
+            a = __fdiv_rn(a, norm);
+            b = __fdiv_rn(b, norm);
+          }
+          rp[(2 * p) * pf + x] = a;
+          rp[(2 * p + 1) * pf + x] = b;
+        }
+      }
+      __syncwarp();
     }
-    __syncthreads();
-  }
-  {  // inverse x transforms of the packed rows
-    constexpr int G = PLANE_THREADS / T;
-    const int s = threadIdx.x / T, t = threadIdx.x - s * T;
-    for (int p0 = 0; p0 < NPAIR; p0 += G) {
-      const int p = p0 + s;
-      seq_transform_g<N, R1, R2, +1>(Z + p * SP, 1, t, tw, s < G && p < NPAIR);
-    }
-  }
-  for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
-    const int y = i / N, x = i - y * N;
-    const float2 z = Z[(y >> 1) * SP + x];
-    float v = (y & 1) ? z.y : z.x;
-    for (int q = 0; q < reps; ++q) v = __fdiv_rn(v, norm);
-    rp[y * pf + x] = v;
   }
 }
 

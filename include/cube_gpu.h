@@ -153,6 +153,37 @@ int cube_gpu_zipv_decode(cube_ctx* ctx, const int16_t* code, float* v, int64_t n
 int cube_gpu_download_zipv(cube_ctx* ctx, void* xp, int16_t* vp_code, int64_t* pid, int32_t* rhoc,
                            int64_t* nplocal, float sigma_vi);
 
+/*
+ * Power spectrum of the device-resident particles, replacing the cicpower utility
+ * (utilities/cicpower.f90:76-219) run on a checkpoint: CIC density on an nw^3 mesh,
+ * delta = rho/mean - 1, then auto_power (utilities/powerspectrum.f90:140-210) with
+ * up to n_corr pk_correction passes (powerspectrum.f90:212-259).  xi receives
+ * xi(10,0:nbin) in the reference's layout (10 values per bin, bin 0 first):
+ * 1 mode count, 2 mean k [h/Mpc], 3 raw power, 4 power minus shot noise, 5 aliasing-
+ * corrected power [(Mpc/h)^3], 6-10 zero.  delta (NULL to skip) receives delta_c
+ * (nw^3 floats, x fastest) as cicpower writes it.  With CUBE_DEPOSIT_FIXED the density
+ * is summed in int64 fixed point (order independent).
+ */
+typedef struct cube_power_in {
+  int32_t nw;       /* mesh side, ng*nic in cicpower (parameters.f90:73 with FFTFINE);
+                       one of 16 32 48 64 96 128 144 192 256 288 432 512 576 1024      */
+  int32_t n_interp; /* shot-noise window: 1 NGP, 2 CIC (as cicpower.f90:220 calls it), 3 TSC */
+  int32_t n_int;    /* alias images per side in pk_correction, 3 in the reference (0..4) */
+  int32_t n_corr;   /* pk_correction passes, 4 in the reference (powerspectrum.f90:198-201) */
+} cube_power_in;
+
+typedef struct cube_power_out {
+  int64_t nbin;        /* nint(nyquist*sqrt(3)) (powerspectrum.f90:15)          */
+  double mean;         /* particles per mesh cell, rho8/nw^3 (cicpower.f90:171) */
+  float alpha;         /* slope of the last pk_correction pass (NaN: none ran)  */
+  int32_t n_corr_done; /* pk_correction passes applied                          */
+  float delta_min, delta_max;
+  float ms;            /* device time of the call                               */
+} cube_power_out;
+
+int cube_gpu_power(cube_ctx* ctx, const cube_power_in* in, float* xi, int64_t nxi, float* delta,
+                   cube_power_out* out);
+
 /* drift.f90:1-233 with dt_mid=(dt_old+dt)/2; bit-exact arrival order and ZIPX update. */
 int cube_gpu_drift(cube_ctx* ctx, const cube_step_in* in);
 /* kick.f90:1-353: PM1 + PM2 + PM3 + PP velocity updates and dt criteria. */

@@ -66,6 +66,10 @@ def lib():
         L.oracle_classify.argtypes = [P, vp, vp, vp]
         L.oracle_zipv_encode.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_float]
         L.oracle_zipv_decode.argtypes = [vp, vp, ctypes.c_int64, ctypes.c_float]
+        L.oracle_power.restype = ctypes.c_int64
+        L.oracle_power.argtypes = [P, vp, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, vp, vp, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)]
         _LIB = L
     return _LIB
 
@@ -183,3 +187,29 @@ def zipv_decode(code, sigma_vi: float):
     out = np.empty(code.shape, dtype=np.float32)
     lib().oracle_zipv_decode(_ptr(code), _ptr(out), code.size, sigma_vi)
     return out
+
+
+class PowerOut:
+    """xi is xi(10,0:nbin) as rows per bin (shape (nbin+1, 10)); see oracle/power.cpp."""
+
+    def __init__(self, xi, delta, mean, alpha, n_done):
+        self.xi, self.delta, self.mean, self.alpha, self.n_done = xi, delta, mean, alpha, n_done
+
+
+def power(p: Params, xp, rhoc, nw: int, n_interp: int = 2, n_int: int = 3, n_corr: int = 4, fixed: bool = False,
+          want_delta: bool = False) -> PowerOut:
+    """CIC power spectrum of the particles (cicpower.f90 + powerspectrum.f90 auto_power)."""
+    xp = np.ascontiguousarray(xp)
+    rhoc = np.ascontiguousarray(rhoc, dtype=np.int32)
+    nbin = int(round(float(np.float32(nw // 2) * np.sqrt(np.float32(3)))))
+    xi = np.zeros((nbin + 2, 10), dtype=np.float32)
+    delta = np.empty(nw ** 3, dtype=np.float32) if want_delta else None
+    mean, alpha, done = ctypes.c_double(), ctypes.c_float(), ctypes.c_int()
+    cp = p.to_c()
+    nb = lib().oracle_power(ctypes.byref(cp), _ptr(xp), _ptr(rhoc), int(xp.shape[0]), nw, n_interp, n_int, n_corr,
+                            int(fixed), _ptr(xi), _ptr(delta) if delta is not None else None, ctypes.byref(mean),
+                            ctypes.byref(alpha), ctypes.byref(done))
+    if nb < 0:
+        raise ValueError("bad power-spectrum arguments")
+    return PowerOut(xi[:nb + 1].copy(), delta.reshape(nw, nw, nw) if delta is not None else None, mean.value,
+                    alpha.value, done.value)

@@ -110,3 +110,25 @@ def test_zipv_codec_round_trip(oracle_lib):
     step = np.pi / 65535 * (1 + (s * v.astype(np.float64)) ** 2) / s
     assert np.all(np.abs(back - v) <= 0.51 * step + 1e-6 * np.abs(v))
     assert code[np.argmin(np.abs(v))] == 0
+
+
+@pytest.mark.parametrize("nw", [16, 32])
+def test_power_spectrum_invariants(oracle_lib, nw):
+    """cicpower + auto_power restatement: every independent mode lands in one bin
+    ((nw^3-8)/2 + 7 of them for even nw), delta has zero mean, fixed-point and FP32
+    deposits agree, and a sub-Poisson lattice leaves pk_correction off (alpha NaN)."""
+    p = _p(izipx=2)
+    st = clustered_state(p, 40000, seed=8, nblob=20, sigma=0.4, frac=0.8)
+    n = st[0].shape[0]
+    a = oracle_lib.power(p, st[0], st[3], nw, fixed=True, want_delta=True)
+    b = oracle_lib.power(p, st[0], st[3], nw, fixed=False)
+    assert a.xi[:, 0].sum() == (nw ** 3 - 8) // 2 + 7
+    assert abs(a.mean - n / nw ** 3) < 1e-9 * n / nw ** 3
+    assert abs(float(a.delta.astype(np.float64).mean())) < 1e-6
+    assert a.n_done == 4 and np.isfinite(a.alpha)
+    scale = np.abs(b.xi[1:, 2]).max()  # raw-power scale: bins near k_max hold far less power
+    np.testing.assert_allclose(a.xi[1:, :5], b.xi[1:, :5], rtol=2e-4, atol=1e-5 * scale)
+    lat = lattice_state(p, seed=9, disp=0.05)
+    c = oracle_lib.power(p, lat[0], lat[3], nw)
+    assert np.isnan(c.alpha) and c.n_done == 0
+    assert np.array_equal(c.xi[1:, 4], c.xi[1:, 3])
