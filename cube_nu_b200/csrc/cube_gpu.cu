@@ -315,6 +315,7 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
   const int64_t nrows = nbox * (int64_t)N * N;
   const int W = f2::fcol_width(N, T);
   const size_t smc = (size_t)(N + W * N) * sizeof(float2);
+  const size_t smg = smc + (size_t)W * N * sizeof(float);  // z pass: + prefetched Green values
   dim3 gc((unsigned)(nbox * N), (unsigned)((NH + W - 1) / W));
   if constexpr (N <= 144) {
     if (fused_layout(c, N)) {
@@ -329,8 +330,8 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
         LAUNCH(c, kx, 1, f2::k_fxy3_r2c<N, R1, R2, float><<<planes, f2::PLANE3_THREADS, smf, c->s>>>(
                              (const float*)real_in, ck, tw, scale, pt.pr, pt.pc, pt.plr, pt.plc));
       }
-      smem_optin(f2::k_fcol3<N, R1, R2, 2, 2>, smc);
-      LAUNCH(c, kz, 1, f2::k_fcol3<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
+      smem_optin(f2::k_fcol3<N, R1, R2, 2, 2>, smg);
+      LAUNCH(c, kz, 1, f2::k_fcol3<N, R1, R2, 2, 2><<<gc, W * T, smg, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
       smem_optin(f2::k_fyx3_c2r<N, R1, R2>, smi);
       LAUNCH(c, kc, 1, f2::k_fyx3_c2r<N, R1, R2><<<planes, f2::PLANE3_THREADS, smi, c->s>>>(
                            ck, phi_out, tw, norm, reps, pt.pc, pt.pf, pt.plc, pt.plf));
@@ -350,11 +351,11 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
                                                                              scale, pt.pr, pt.pc));
   }
   smem_optin(f2::k_fcol3<N, R1, R2, 1, 0>, smc);
-  smem_optin(f2::k_fcol3<N, R1, R2, 2, 2>, smc);
+  smem_optin(f2::k_fcol3<N, R1, R2, 2, 2>, smg);
   smem_optin(f2::k_fcol3<N, R1, R2, 1, 1>, smc);
   smem_optin(f2::k_fx_c2r<N, R1, R2>, smx);
   LAUNCH(c, ky, 1, f2::k_fcol3<N, R1, R2, 1, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
-  LAUNCH(c, kz, 1, f2::k_fcol3<N, R1, R2, 2, 2><<<gc, W * T, smc, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
+  LAUNCH(c, kz, 1, f2::k_fcol3<N, R1, R2, 2, 2><<<gc, W * T, smg, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
   LAUNCH(c, ky, 1, f2::k_fcol3<N, R1, R2, 1, 1><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
   LAUNCH(c, kc, 1, f2::k_fx_c2r<N, R1, R2><<<gx, S * T, smx, c->s>>>(ck, phi_out, nrows, tw, norm, reps, pt.pc, pt.pf));
 }
@@ -835,7 +836,7 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
         maybe_capture(c, 2, c->cap_box, 1, (char*)m.real + (c->cap_box - t0) * boxb, n, false, (int64_t)m.pt.pf * 4,
                       m.pt.psb);
-      LAUNCH(c, K_F2_PM2, 1, k_f2max_box<<<f2max_box_grid(G.ngp, nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1, m.pt.pf, m.pt.plf));
+      LAUNCH(c, K_F2_PM2, 1, k_f2max_box2<<<f2max_box2_grid(G.ngp, nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1, m.pt.pf, m.pt.plf));
       LAUNCH(c, K_INT_PM2, 1, k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, a_mid, dt, vm + 0, c->err, m.pt.pf, m.pt.plf));
     }
   }
@@ -897,7 +898,7 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       if (cap_slot >= 0)
         maybe_capture(c, 3, c->cap_box, 1, (char*)m.real + cap_slot * boxb, n, false, (int64_t)m.pt.pf * 4, m.pt.psb);
       const int nf = G.nfp[cl];
-      LAUNCH(c, K_F2_PM3, 1, k_f2max_box<<<f2max_box_grid(nf, nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2, m.pt.pf, m.pt.plf));
+      LAUNCH(c, K_F2_PM3, 1, k_f2max_box2<<<f2max_box2_grid(nf, nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2, m.pt.pf, m.pt.plf));
       LAUNCH(c, K_INT_PM3, 1, k_interp_pm3<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp, a_mid, dt, vm + 3,
                                                 c->err, m.pt.pf, m.pt.plf));
     }

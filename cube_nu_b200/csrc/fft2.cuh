@@ -28,6 +28,15 @@
 namespace cube {
 namespace f2 {
 
+// 4-byte asynchronous global -> shared copies (sm_80+ cp.async), used to prefetch the
+// Green table while the column data are in flight.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 template <int DIR>
 __device__ __forceinline__ float2 twid(const float2* tw, int j) {
   float2 w = tw[j];
@@ -223,6 +232,8 @@ __global__ void __launch_bounds__(256) k_fx_r2c(const IN* r, float2* c, int64_t 
 // first step needs in thread t exactly the X[t + R1*k2] it already holds, so
 // forward -> Green multiply -> inverse costs two exchanges in all.
 //   MODE 0: forward, 1: inverse, 2: forward -> multiply by green[kz][y][kx] -> inverse.
+// Shared memory: tw[N], exchange slots [N][W] float2, and for MODE 2 the column's Green
+// values [N][W] float, prefetched with cp.async at the start.
 // ---------------------------------------------------------------------------------
 // Launch bounds of the column pass: two blocks per SM where the sequences fit in 64
 // registers (or 73 with the 444-thread blocks of N = 144), one block above N = 192.
@@ -248,6 +259,15 @@ __global__ void __launch_bounds__(FcolBounds<N>::MAXT, FcolBounds<N>::MINB) k_fc
   const int64_t es = (AXIS == 1) ? pc : plc;
   float2* base = c + b * (int64_t)N * plc + (AXIS == 1 ? (int64_t)o * plc : (int64_t)o * pc) + kx0 + col;
   float2* Ac = A + col;
+  float* Gc = reinterpret_cast<float*>(A + (size_t)N * W) + col;  // MODE 2: green[kz] of this column, [N][W]
+  if (MODE == 2) {
+    if (t < R1 && live) {
+      const float* gb = green + (int64_t)o * NH + kx0 + col;  // g[kz][y][kx]
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) cp_async4(Gc + (t + R1 * k2) * W, gb + (int64_t)(t + R1 * k2) * N * NH);
+    }
+    cp_async_commit();
+  }
   __syncthreads();
   if (MODE != 1) {
     // ---- forward: n = R2*n1 + n2 ----
@@ -273,12 +293,12 @@ __global__ void __launch_bounds__(FcolBounds<N>::MAXT, FcolBounds<N>::MINB) k_fc
       }
       return;
     }
-    // ---- Green multiply at kz = t + R1*k2 ----
+    // ---- Green multiply at kz = t + R1*k2 (values this thread prefetched) ----
+    cp_async_wait_all();
     if (t < R1 && live) {
-      const float* gb = green + (int64_t)o * NH + kx0 + col;  // g[kz][y][kx]
 #pragma unroll
       for (int k2 = 0; k2 < R2; ++k2) {
-        const float gv = __ldg(gb + (int64_t)(t + R1 * k2) * N * NH);
+        const float gv = Gc[(t + R1 * k2) * W];
         w[k2] = make_float2(w[k2].x * gv, w[k2].y * gv);
       }
     }

@@ -536,77 +536,104 @@ __global__ void k_f2max_periodic(const float* __restrict__ phi, int nc, float* _
   block_max_to(v, f2out);
 }
 
-// Box meshes phi[b] (row pitch pf, plane pitch pl floats), index i at array i-m1phi;
-// physical cells 1..nforce.  A block owns a 32x16 tile of (x,y) in one box and marches
-// through z with a ring of five planes (tile plus a 2-cell halo) in shared memory; the
-// plane needed next is prefetched into registers while the current plane is
-// differenced, so each phi value is read about 1.4 times and the load latency overlaps
-// the arithmetic.  grid = nbox * tiles; blockDim = 256.
-constexpr int F2_TX = 32, F2_TY = 16, F2_PX = F2_TX + 4, F2_PY = F2_TY + 4, F2_HALO = F2_PX * F2_PY;
-constexpr int F2_LOADS = (F2_HALO + 255) / 256;
-__global__ void __launch_bounds__(256) k_f2max_box(const float* __restrict__ phi, int n, int nforce, int m1phi,
-                                                   int nbox, float* __restrict__ f2out, int pf, int64_t pl) {
-  __shared__ float ring[5][F2_HALO];
-  const int ntx = (nforce + F2_TX - 1) / F2_TX, nty = (nforce + F2_TY - 1) / F2_TY;
-  const int tile = blockIdx.x % (ntx * nty);
-  const int b = blockIdx.x / (ntx * nty);
-  const int tx0 = (tile % ntx) * F2_TX + 1, ty0 = (tile / ntx) * F2_TY + 1;  // first physical x,y of the tile
+// f2max over box meshes phi[b] (row pitch pf, plane pitch pl floats; coordinate i is
+// array index i - m1phi; physical cells 1..nforce), z stencil in registers.  Block: a 32x32 (x,y) tile of one
+// box, 256 threads; thread (lx, ly) owns cells y = 4*ly .. 4*ly+3 at x = lx.  Halo
+// planes (36x36) of phi stream through a 4-stage shared-memory ring filled with cp.async,
+// three planes ahead of the one being reduced.  From a plane a thread takes one column
+// of 8 values (own phi and the y stencils of its 4 cells) and 4 x stencils, 6 loads per
+// cell.  Own phi values of the last 5 planes and fx, fy of the last 3 stay in registers,
+// so the force at plane zc-2 completes when plane zc arrives.
+constexpr int F3_T = 32, F3_P = F3_T + 4, F3_HALO = F3_P * F3_P, F3_LOADS = (F3_HALO + 255) / 256, F3_STAGES = 4;
+__device__ __forceinline__ void f3_cp_async4(float* smem, const float* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__global__ void __launch_bounds__(256, 3) k_f2max_box2(const float* __restrict__ phi, int n, int nforce, int m1phi,
+                                                       int nbox, float* __restrict__ f2out, int pf, int64_t pl) {
+  __shared__ float pln[F3_STAGES][F3_HALO];
+  const int nt = (nforce + F3_T - 1) / F3_T;
+  const int tile = blockIdx.x % (nt * nt);
+  const int b = blockIdx.x / (nt * nt);
+  const int tx0 = (tile % nt) * F3_T + 1, ty0 = (tile / nt) * F3_T + 1;  // first physical x, y
   const float* pb = phi + (size_t)b * n * pl;
-  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;  // rows ly and ly+8
-  // halo element k of this thread: offset within the plane (or -1 when outside the box)
-  int off[F2_LOADS];
+  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+  int off[F3_LOADS];
 #pragma unroll
-  for (int k = 0; k < F2_LOADS; ++k) {
+  for (int k = 0; k < F3_LOADS; ++k) {
     const int i = threadIdx.x + k * 256;
-    off[k] = -1;
-    if (i < F2_HALO) {
-      const int py = i / F2_PX, px = i - py * F2_PX;
-      const int x = tx0 - 2 + px - m1phi, y = ty0 - 2 + py - m1phi;  // array coordinates, >= 0 (m1phi <= -1)
-      if (x < n && y < n) off[k] = y * pf + x;
+    off[k] = -2;  // not a halo element of this thread
+    if (i < F3_HALO) {
+      const int py = i / F3_P, px = i - py * F3_P;
+      const int x = tx0 - 2 + px - m1phi, y = ty0 - 2 + py - m1phi;  // array coordinates, >= 0
+      off[k] = (x < n && y < n) ? y * pf + x : -1;
+      if (off[k] < 0)
+#pragma unroll
+        for (int st = 0; st < F3_STAGES; ++st) pln[st][i] = 0.f;  // outside the box: zero, never copied
     }
   }
-  auto fetch = [&](int z, float* r) {
-    const float* pz = pb + (size_t)(z - m1phi) * pl;
+  const int zlast = nforce + 2;
+  auto issue = [&](int zc) {  // copy plane zc into its stage; always commits a group
+    if (zc <= zlast) {
+      const float* pz = pb + (size_t)(zc - m1phi) * pl;
+      float* dst = pln[(zc + 1) & (F3_STAGES - 1)];
 #pragma unroll
-    for (int k = 0; k < F2_LOADS; ++k) r[k] = (off[k] >= 0) ? __ldg(pz + off[k]) : 0.f;
-  };
-  auto put = [&](const float* r, float* dst) {
-#pragma unroll
-    for (int k = 0; k < F2_LOADS; ++k) {
-      const int i = threadIdx.x + k * 256;
-      if (i < F2_HALO) dst[i] = r[k];
+      for (int k = 0; k < F3_LOADS; ++k)
+        if (off[k] >= 0) f3_cp_async4(dst + threadIdx.x + k * 256, pz + off[k]);
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
-  float pre[F2_LOADS];
-  for (int p = -1; p <= 3; ++p) {  // planes -1..3 into slots (p+1)%5
-    fetch(p, pre);
-    put(pre, ring[(p + 1) % 5]);
+  const bool xin = tx0 + lx <= nforce;
+  bool own[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) own[j] = xin && (ty0 + 4 * ly + j <= nforce);
+  float P[4][5], FX[4][3], FY[4][3];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) P[j][q] = 0.f;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) FX[j][q] = FY[j][q] = 0.f;
   }
-  __syncthreads();
   float v = 0.f;
-  const bool own0 = (tx0 + lx <= nforce) && (ty0 + ly <= nforce);
-  const bool own1 = (tx0 + lx <= nforce) && (ty0 + ly + 8 <= nforce);
-  for (int z = 1; z <= nforce; ++z) {
-    const bool more = z + 3 <= nforce + 2;
-    if (more) fetch(z + 3, pre);
-    const float* c = ring[(z + 1) % 5];
+  issue(-1);
+  issue(0);
+  issue(1);
+  for (int zc = -1; zc <= zlast; ++zc) {
+    asm volatile("cp.async.wait_group 2;\n" ::: "memory");  // this thread's copies of plane zc landed
+    __syncthreads();  // everyone's copies landed; the stage of plane zc-1 is free again
+    issue(zc + 3);
+    const float* c = pln[(zc + 1) & (F3_STAGES - 1)];
+    // own column: rows 4*ly .. 4*ly+7 of the halo plane at x = lx + 2
+    float col[8];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int o = (ly + 8 * h + 2) * F2_PX + (lx + 2);
-      const float fx = grad4(c[o - 2], c[o - 1], c[o + 1], c[o + 2]);
-      const float fy = grad4(c[o - 2 * F2_PX], c[o - F2_PX], c[o + F2_PX], c[o + 2 * F2_PX]);
-      const float fz = grad4(ring[(z - 1) % 5][o], ring[z % 5][o], ring[(z + 2) % 5][o], ring[(z + 3) % 5][o]);
-      if (h == 0 ? own0 : own1) v = fmaxf(v, sumsq3(fx, fy, fz));
+    for (int r = 0; r < 8; ++r) col[r] = c[(4 * ly + r) * F3_P + lx + 2];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) P[j][q] = P[j][q + 1];
+      P[j][4] = col[j + 2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        FX[j][q] = FX[j][q + 1];
+        FY[j][q] = FY[j][q + 1];
+      }
+      const float* row = c + (4 * ly + j + 2) * F3_P + lx + 2;
+      FX[j][2] = grad4(row[-2], row[-1], row[1], row[2]);
+      FY[j][2] = grad4(col[j], col[j + 1], col[j + 3], col[j + 4]);
+      if (zc >= 3 && own[j]) {  // plane zc-2 is complete: phi(zc-4..zc) in P, fx, fy in slot 0
+        const float fz = grad4(P[j][0], P[j][1], P[j][3], P[j][4]);
+        v = fmaxf(v, sumsq3(FX[j][0], FY[j][0], fz));
+      }
     }
-    __syncthreads();
-    if (more) put(pre, ring[(z + 4) % 5]);  // plane z+3 takes the slot of plane z-2
-    __syncthreads();
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   block_max_to(v, f2out);
 }
 
-__host__ inline unsigned f2max_box_grid(int nforce, int nbox) {
-  return (unsigned)(((nforce + F2_TX - 1) / F2_TX) * ((nforce + F2_TY - 1) / F2_TY) * nbox);
+__host__ inline unsigned f2max_box2_grid(int nforce, int nbox) {
+  const int nt = (nforce + F3_T - 1) / F3_T;
+  return (unsigned)(nt * nt * nbox);
 }
 
 // =================================================================================
@@ -724,7 +751,7 @@ __global__ void k_interp_pm1(Geo G, int64_t np, const void* __restrict__ xp, con
   apply_kick(vp, ip, dv, a_mid, dt, av);
 }
 
-__global__ void k_interp_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+__global__ void __launch_bounds__(256, 3) k_interp_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                              const float* __restrict__ phi, int tile0, int ntile, float* __restrict__ vp, float a_mid,
                              float dt, float* vmax, unsigned* err, int pf, int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -759,7 +786,7 @@ __global__ void k_interp_pm2(Geo G, int64_t np, const void* __restrict__ xp, con
   block_vmax(av, vmax);
 }
 
-__global__ void k_interp_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+__global__ void __launch_bounds__(256, 3) k_interp_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                              const float* __restrict__ phi, const int32_t* __restrict__ box_slot, int iapm,
                              float* __restrict__ vp, float a_mid, float dt, float* vmax, unsigned* err, int pf,
                              int64_t pl) {
