@@ -293,7 +293,7 @@ __device__ __forceinline__ void dep_add(void* rho, int64_t i, float w) {
 }
 
 template <bool FIXED>
-__global__ void k_deposit_pm1(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+__global__ void __launch_bounds__(256, 6) k_deposit_pm1(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                               void* __restrict__ rho, int pr, int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= np) return;
@@ -337,7 +337,7 @@ __device__ __forceinline__ int tile_cands(const Geo& G, int g, int* t, int* li) 
 
 // PM2 tile meshes [tile - tile0][ngt^3]; fine index i maps to array i-(1-ngb).
 template <bool FIXED>
-__global__ void k_deposit_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+__global__ void __launch_bounds__(256, 5) k_deposit_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                               void* __restrict__ rho, int tile0, int ntile, int pr, int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= np) return;
@@ -423,7 +423,7 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
   if (ip >= np) return;
   int g[3];
   cell_coords(G, pcell[ip], g[0], g[1], g[2]);
-  int tc[3][3], uc[3][3], lc[3][3], nca[3];
+  int tc[3][2], uc[3][2], lc[3][2], nca[3];  // at most two candidate subtiles per dimension (ntt >= 2)
   double f[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
