@@ -35,6 +35,15 @@ from cube_nu_b200.params import DEPOSIT_FIXED, DEPOSIT_FP32, config_512, config_
 
 METRIC = "particle-steps/s P3M KDK @512^3"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+# DRAM bytes (read + write) per class-2 PM3 box of 144^3, measured with ncu on the proxy
+# workload (one launch over 64 boxes; profiles/pm3_kernels_proxy.md).  Traffic grows with
+# the number of boxes, so a launch over B such boxes moves B times these.
+PM3_TRAFFIC_PER_BOX = {
+    "deposit_pm3": 1.892842e9 / 64,
+    "fft_x_pm3": 2.271174e9 / 64,
+    "fft_z_green_pm3": 1.910046e9 / 64,
+    "fft_c2r_pm3": 1.485638e9 / 64,
+}
 
 
 def load_peaks():
@@ -366,8 +375,13 @@ def main():
         if dom:
             launches_per_step = dom[2] / args.steps
             ach = dom[4] / (dom[5] / 1e3) / 1e9
+            traffic = None
+            if dom[1] in PM3_TRAFFIC_PER_BOX and p.nft(2) == 144 and sum(napm[3:6]) == 0:
+                traffic = int(PM3_TRAFFIC_PER_BOX[dom[1]] * napm[2] / launches_per_step)
             roof = {"kernel": dom[1], "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                    "frac": round(ach / hbm, 4), "traffic": None, "peak_kind": peak_kind,
+                    "frac": round(ach / hbm, 4), "traffic": traffic,
+                    "traffic_source": ("ncu DRAM bytes of one 64-box launch (proxy workload), scaled by boxes"
+                                       if traffic else None), "peak_kind": peak_kind,
                     "avg_launch_ms": round(dom[3], 4), "launches_per_step": launches_per_step,
                     "algorithmic_bytes_per_launch": int(dom[4] / launches_per_step)}
         cpu = None

@@ -21,6 +21,7 @@ EXPORTS = (
     "cube_gpu_green_table", "cube_gpu_subtile_class", "cube_gpu_last_error", "cube_gpu_version",
     "cube_gpu_profile", "cube_gpu_profile_read", "cube_gpu_profile_name", "cube_gpu_kernel_launches",
     "cube_gpu_zipv_encode", "cube_gpu_zipv_decode", "cube_gpu_download_zipv", "cube_gpu_ic", "cube_gpu_power",
+    "cube_gpu_int2real",
 )
 
 
@@ -101,6 +102,7 @@ def load():
     L.cube_gpu_zipv_decode.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_float]
     L.cube_gpu_download_zipv.argtypes = [vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_float]
     L.cube_gpu_power.argtypes = [vp, ctypes.POINTER(PowerIn), vp, ctypes.c_int64, vp, ctypes.POINTER(PowerOut)]
+    L.cube_gpu_int2real.argtypes = [vp, vp, ctypes.c_int64]
     _LIB = L
     return L
 
@@ -253,6 +255,12 @@ class Context:
                                         _ptr(delta) if delta is not None else None, ctypes.byref(out)),
                "cube_gpu_power")
         return xi[:out.nbin + 1].copy(), delta, out
+
+    def int2real(self) -> np.ndarray:
+        """Real positions (np, 3) float32 in coarse-cell units (int2real.f90:68-86)."""
+        out = np.empty((self.np, 3), dtype=np.float32)
+        _check(self._lib.cube_gpu_int2real(self._h, _ptr(out), out.size), "cube_gpu_int2real")
+        return out
 
     def subtile_class(self) -> np.ndarray:
         out = np.empty(self.params.ns3, dtype=np.int32)

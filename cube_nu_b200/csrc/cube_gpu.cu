@@ -1181,6 +1181,22 @@ int cube_gpu_download_zipv(cube_ctx* c, void* xp, int16_t* vp_code, int64_t* pid
   return cube_gpu_download(c, xp, nullptr, pid, rhoc, nplocal);
 }
 
+int cube_gpu_int2real(cube_ctx* c, float* xv, int64_t n) {
+  if (!c || !xv) return fail(CUBE_E_ARG, "null argument");
+  if (!c->loaded) return fail(CUBE_E_STATE, "int2real before upload");
+  if (n < 3 * c->np) return fail(CUBE_E_ARG, "xv needs 3*nplocal floats");
+  CK(cudaSetDevice(c->device));
+  float* d = nullptr;
+  CK(cudaMalloc(&d, (size_t)c->np * 3 * sizeof(float)));
+  LAUNCH(c, K_FILL, 1, k_int2real<<<nblk(c->np), 256, 0, c->s>>>(c->G, c->np, c->xp, c->pcell, d));
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(xv, d, (size_t)c->np * 3 * sizeof(float), cudaMemcpyDeviceToHost, c->s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->s);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(CUBE_E_CUDA, std::string("int2real: ") + cudaGetErrorString(e));
+  return 0;
+}
+
 int cube_gpu_green_table(cube_ctx* c, int level, int iapm, float* out, int64_t n) {
   if (!c || !out) return fail(CUBE_E_ARG, "null argument");
   CK(cudaSetDevice(c->device));

@@ -972,6 +972,21 @@ __global__ void k_zipv_encode(const float* __restrict__ v, int16_t* __restrict__
 }
 
 // =================================================================================
+// int2real (utilities/int2real.f90:68-86): xv(3,np) real(4) = ZIPX offset + cell index in
+// coarse-cell units; the real(8) sum is exact, so one rounding to float.
+// =================================================================================
+__global__ void k_int2real(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+                           float* __restrict__ xv) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= np) return;
+  int g[3];
+  cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    xv[3 * ip + d] = __double2float_rn(zfrac(load_code(xp, G.izipx, 3 * ip + d), G) + (double)g[d]);
+}
+
+// =================================================================================
 // Green's function (Green/Green.f90:1-80) in FP64, stored real32.
 // =================================================================================
 __global__ void k_green(float* __restrict__ Gk, int n, float apm_soft, float apm_range, float gridsize) {

@@ -209,6 +209,10 @@ const char* cube_gpu_profile_name(int i);
 /* Number of kernels this context has launched since creation. */
 int64_t cube_gpu_kernel_launches(cube_ctx* ctx);
 
+/* Real positions of the resident particles, replacing the int2real utility
+ * (utilities/int2real.f90:68-86): xv(3,np) real(4) in coarse-cell units (0..nc),
+ * the ZIPX offset plus the cell index, in the resident particle order. */
+int cube_gpu_int2real(cube_ctx* ctx, float* xv, int64_t n);
 /* Download the Green table of a level (1, 2, or 3 with class iapm 2..5). */
 int cube_gpu_green_table(cube_ctx* ctx, int level, int iapm, float* out, int64_t n);
 /* Download per-subtile PM3 class (ires, kick.f90:108-133), ns3 entries. */

@@ -213,3 +213,20 @@ def power(p: Params, xp, rhoc, nw: int, n_interp: int = 2, n_int: int = 3, n_cor
         raise ValueError("bad power-spectrum arguments")
     return PowerOut(xi[:nb + 1].copy(), delta.reshape(nw, nw, nw) if delta is not None else None, mean.value,
                     alpha.value, done.value)
+
+
+def int2real(p: Params, xp, rhoc) -> np.ndarray:
+    """utilities/int2real.f90:68-86: xv = real(4)((int(xp+ishift)+rshift)*x_resolution + cell),
+    coarse-cell units, particles in storage order (tile z,y,x, then cell z,y,x)."""
+    xp = np.asarray(xp)
+    u = xp.astype(np.int64) & (0xFF if p.izipx == 1 else 0xFFFF)
+    frac = (u.astype(np.float64) + 0.5) * 2.0 ** (-8 * p.izipx)
+    nt, nnt = p.nt, p.nnt
+    s = np.arange(p.nc ** 3, dtype=np.int64)
+    i, j, k = s % nt, (s // nt) % nt, (s // nt ** 2) % nt
+    t = s // nt ** 3
+    tx, ty, tz = t % nnt, (t // nnt) % nnt, t // nnt ** 2
+    cell = np.stack([tx * nt + i, ty * nt + j, tz * nt + k], axis=-1)
+    counts = np.asarray(rhoc, dtype=np.int64).ravel()
+    g = np.repeat(cell, counts, axis=0)
+    return (frac + g).astype(np.float32)

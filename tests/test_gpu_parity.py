@@ -296,3 +296,19 @@ def test_device_ic_matches_host_ic(izipx):
     # same cell occupancy except particles on a cell face
     assert np.abs(rhoc - host["rhoc"]).sum() <= 0.001 * pid.size
     assert abs(dev["vz_max"] - host["vz_max"]) <= 1e-3 * host["vz_max"]
+
+
+@pytest.mark.parametrize("izipx", [1, 2])
+def test_int2real_matches_oracle(oracle_lib, izipx):
+    """utilities/int2real.f90:68-86 on the resident particles, after a drift reorders
+    them: bit-identical to the restatement on the downloaded state."""
+    p = _params(izipx=izipx)
+    st = clustered_state(p, 20000, seed=61)
+    with _ctx(p, st) as ctx:
+        ctx.drift(0.3, 0.5, float(np.abs(st[1][:, 2]).max()))
+        xv = ctx.int2real()
+        xp, _, _, rhoc = ctx.download()
+    ref = oracle_lib.int2real(p, xp, rhoc)
+    assert xv.shape == ref.shape and xv.dtype == np.float32
+    assert np.array_equal(xv, ref)
+    assert xv.min() >= 0.0 and xv.max() < p.nc
