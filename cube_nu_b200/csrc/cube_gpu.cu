@@ -678,6 +678,10 @@ static int alloc_particles(cube_ctx* c, int64_t np) {
   c->arena = nullptr;
   CK(cudaMalloc(&c->arena, want));
   c->arena_bytes = want;
+  const char* verbose = getenv("CUBE_VERBOSE");
+  if (verbose && verbose[0] == '1')
+    fprintf(stderr, "cube_gpu: free %.2f GB, mesh budget %.2f GB, arena %.2f GB (largest level wants %.2f GB)\n",
+            fre / 1e9, budget / 1e9, want / 1e9, need / 1e9);
   return 0;
 }
 
