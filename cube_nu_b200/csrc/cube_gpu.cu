@@ -914,8 +914,15 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
                                  ? (float)((double)G.mass_p * ((1.0 - (double)G.f_nu) * (1.0 - (double)G.f_nu)))
                                  : G.mass_p;
     const float v_scale = (float)((double)(a_mid * dt / 6.f) / M_PI);
-    LAUNCH(c, K_PP, 1, k_pp<<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->xp, c->pcell, c->cstart, c->ires, c->vp, mass_scale, v_scale,
-                                          f2 + 3, vm + 6, c->pairs));
+    // FP32 candidate positions are exact when lq + offset fits 24 bits: int8 codes, or
+    // int16 codes with tile-local coordinates |lq| <= nt < 128
+    const bool pp_fast = G.izipx == 1 || G.nt < 127;
+    if (pp_fast)
+      LAUNCH(c, K_PP, 1, k_pp<true><<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->xp, c->pcell, c->cstart, c->ires, c->vp,
+                                                                    mass_scale, v_scale, f2 + 3, vm + 6, c->pairs));
+    else
+      LAUNCH(c, K_PP, 1, k_pp<false><<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->xp, c->pcell, c->cstart, c->ires, c->vp,
+                                                                     mass_scale, v_scale, f2 + 3, vm + 6, c->pairs));
   }
   CK(cudaEventRecord(c->ev[4], c->s));
   CK(cudaGetLastError());

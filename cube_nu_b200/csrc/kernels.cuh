@@ -871,6 +871,20 @@ __device__ __forceinline__ float F_ra(float r, float apm) {
   return 0.f;
 }
 
+// Candidate coordinate (xq in kick.f90:424): ((lq + (u+0.5)*x_res) * ratio_cs) rounded to
+// float.  FAST: lq + (u+0.5)*x_res has at most 8*izipx+1+log2|lq| significant bits; when
+// that is <= 24 (int8 codes, or int16 codes with |lq| < 128) the sum is exact in FP32 and
+// the result equals the FP64 form bit for bit.
+template <bool FAST>
+__device__ __forceinline__ float pp_xq(const Geo& G, int lq, int code, float xres_f) {
+  if (FAST) {
+    const float f = __fmul_rn(__fadd_rn((float)((uint32_t)code & G.zmask), 0.5f), xres_f);
+    return __fmul_rn(__fadd_rn((float)lq, f), (float)G.rcs);
+  }
+  return __fmul_rn((float)((double)lq + zfrac(code, G)), (float)G.rcs);
+}
+
+template <bool FAST>
 __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                      const int64_t* __restrict__ cstart, const int32_t* __restrict__ ires, float* __restrict__ vp,
                      float mass_scale, float v_scale, float* f2max, float* vmax,
@@ -888,6 +902,7 @@ __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32
     u[d] = l[d] / G.ntt;
   }
   const int iapm = ires[subtile_id(G, t, u)];
+  const float xres_f = (float)G.x_res;  // a power of two
   const float range = __fdiv_rn(3.5f, (float)rsf_of(iapm));  // apm3(iapm)
   const float range2 = __fmul_rn(range, range);
   float xf[3], fin[3];
@@ -914,10 +929,7 @@ __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32
         for (int64_t q = s; q < e; ++q) {
           float rv[3];
 #pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            const float xq = __fmul_rn((float)((double)lq[d] + zfrac(load_code(xp, G.izipx, 3 * q + d), G)), (float)G.rcs);
-            rv[d] = __fsub_rn(xq, xf[d]);
-          }
+          for (int d = 0; d < 3; ++d) rv[d] = __fsub_rn(pp_xq<FAST>(G, lq[d], load_code(xp, G.izipx, 3 * q + d), xres_f), xf[d]);
           const float r2 = sumsq3(rv[0], rv[1], rv[2]);
           if (r2 > 0.f && r2 < range2) {
             const float rm = __fsqrt_rn(r2);
