@@ -428,6 +428,26 @@ void fft2_forward(cube_ctx* c, float* real, const Pitch& pt, int cls) {
   LAUNCH(c, cls, 1, f2::k_fcol3<N, R1, R2, 2, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
 }
 
+// Forward-only r2c with the generic Stockham passes (any 2^a 3^b size, row-pitched layout):
+// x r2c, then the column kernel along y and, with the two pitches swapped, along z (the
+// plane pitch of the row-pitched layout is n row pitches, so plane z of line y sits at
+// y*pc + z*plc either way).
+void fft_forward_generic(cube_ctx* c, int n, float* real, const Pitch& pt, int cls) {
+  const FFTDesc& D = *fft_desc(c, n);
+  float2* ck = reinterpret_cast<float2*>(real);
+  const int nh = n / 2 + 1;
+  const int64_t nrows = (int64_t)n * n;
+  const int rpb = std::max(1, 2048 / n);
+  const size_t smx = (size_t)(n + 2 * rpb * n) * sizeof(float2);
+  const unsigned gx = (unsigned)((nrows + rpb - 1) / rpb);
+  LAUNCH(c, cls, 1, k_fft_x_r2c<float><<<gx, 256, smx, c->s>>>(real, ck, nrows, D, rpb, 1.f, pt.pr, pt.pc));
+  const int W = (n <= 256) ? 16 : (n <= 512 ? 8 : 4);
+  const size_t smy = (size_t)(n + 2 * W * n) * sizeof(float2);
+  dim3 gy((unsigned)n, (unsigned)((nh + W - 1) / W));
+  LAUNCH(c, cls, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1, pt.pc, pt.plc));
+  LAUNCH(c, cls, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1, (int)pt.plc, (int64_t)pt.pc));
+}
+
 bool fft2_forward_dispatch(cube_ctx* c, int n, float* real, const Pitch& pt, int cls) {
 #define CUBE_FFT2F(N, R1, R2) \
   case N: fft2_forward<N, R1, R2>(c, real, pt, cls); return true;
@@ -1410,8 +1430,9 @@ extern "C" int cube_gpu_power(cube_ctx* c, const cube_power_in* in, float* xi, i
   if (!c || !in || !xi) return fail(CUBE_E_ARG, "null argument");
   if (!c->loaded) return fail(CUBE_E_STATE, "power spectrum before upload");
   const int nw = in->nw;
-  if (c->fft_generic || !fft2_size(nw))
-    return fail(CUBE_E_ARG, "nw must be one of 16 32 48 64 96 128 144 192 256 288 432 512 576 1024");
+  if (nw < 16 || nw > 4096 || !smooth23(nw) || nw % 2)
+    return fail(CUBE_E_ARG, "nw must be an even 2^a 3^b size in 16..4096");
+  const bool special = !c->fft_generic && fft2_size(nw);  // size-specialised passes, else generic
   if (in->n_interp < 1 || in->n_interp > 3) return fail(CUBE_E_ARG, "n_interp must be 1 (NGP), 2 (CIC) or 3 (TSC)");
   if (in->n_int < 0 || in->n_int > PK_MAX_NINT) return fail(CUBE_E_ARG, "n_int must be in 0..4");
   const int nyq = nw / 2;
@@ -1488,7 +1509,8 @@ extern "C" int cube_gpu_power(cube_ctx* c, const cube_power_in* in, float* xi, i
       PK_CK(cudaMemcpy2DAsync(delta, (size_t)nw * 4, mesh, pt.rp, (size_t)nw * 4, (size_t)nw * nw, cudaMemcpyDeviceToHost, c->s));
   }
   // powerspectrum.f90:148-187
-  fft2_forward_dispatch(c, nw, mesh, pt, K_PK_FFT);
+  if (special) fft2_forward_dispatch(c, nw, mesh, pt, K_PK_FFT);
+  else fft_forward_generic(c, nw, mesh, pt, K_PK_FFT);
   PK_CK(cudaMemsetAsync(bins, 0, nbins4 * sizeof(double), c->s));
   smem_optin(k_pk_bin, nbins4 * sizeof(double));
   LAUNCH(c, K_PK_BIN, 1, k_pk_bin<<<nred, 256, nbins4 * sizeof(double), c->s>>>(

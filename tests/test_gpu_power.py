@@ -59,8 +59,10 @@ def _compare(xi, ref):
 
 
 @pytest.mark.parametrize("izipx,fixed,nw", [(2, True, 32), (1, True, 64), (2, False, 48), (2, True, 128),
-                                            (1, False, 192)])
+                                            (1, False, 192), (2, True, 72), (1, False, 108)])
 def test_power_matches_oracle(oracle_lib, izipx, fixed, nw):
+    """72 and 108 take the generic forward FFT (no size-specialised passes), the rest the
+    size-specialised plane or row passes."""
     p = _params(izipx, fixed)
     st = clustered_state(p, 50000, seed=40 + nw, nblob=24, sigma=0.4, frac=0.8)
     xi, delta, out = _run(p, st, nw)
