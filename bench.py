@@ -46,6 +46,23 @@ PM3_TRAFFIC_PER_BOX = {
 }
 
 
+def over_ranks(values, op: str, dist=None, device: str = "cuda"):
+    """Elementwise max or sum of per-rank floats across the process group (identity
+    without one).  Every rank must call it, with the same number of values."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return [float(x) for x in t.tolist()]
+
+
+def job_rate(total_particles: float, steps: int, seconds: float) -> float:
+    """Whole-job particle-steps/s: every rank's particles over the slowest rank's time."""
+    return total_particles * steps / seconds
+
+
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -307,13 +324,9 @@ def main():
     prof = ctx.profile_read()
     ctx.profile(False)
     # max over ranks of the device time
-    dev_s = dev_ms / 1e3
-    if dist:
-        tt = torch.tensor([dev_s, t_wall], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dev_s, t_wall = float(tt[0]), float(tt[1])
-    total_particles = n * world
-    value = total_particles * args.steps / dev_s
+    dev_s, t_wall = over_ranks([dev_ms / 1e3, t_wall], "max", dist)
+    total_particles = over_ranks([n], "sum", dist)[0]
+    value = job_rate(total_particles, args.steps, dev_s)
 
     # ---------------- end to end through the C ABI with pinned host buffers ----------------
     xh, xt = pinned_like(st[0])
@@ -341,12 +354,9 @@ def main():
         _check(lib.cube_gpu_download(ctx._h, _ptr(xh), _ptr(vh), _ptr(ph), _ptr(rh), ctypes.byref(nplocal)), "download")
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t_e2e
-    if dist:
-        tt = torch.tensor([t_e2e], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt[0])
+    t_e2e = over_ranks([t_e2e], "max", dist)[0]
     io_bytes = n * (3 * p.izipx + 12 + 8) + p.ncells * 4
-    e2e_value = total_particles * e2e_steps / t_e2e
+    e2e_value = job_rate(total_particles, e2e_steps, t_e2e)
 
     analysis = None
     if args.pk:
