@@ -416,10 +416,11 @@ struct Plane3Sm {
   static constexpr size_t INV = (size_t)(N + N * NH) * 8;
 };
 
-template <int R2>
+template <int R1, int R2>
 __device__ __forceinline__ int skew(int k1, int n2) {
-  int j = n2 + k1;
-  j = j % R2;
+  int j = n2 + k1;  // < R1 + R2
+  if (R1 <= R2) j = (j >= R2) ? j - R2 : j;
+  else j = j % R2;
   return k1 * R2 + j;
 }
 
@@ -464,13 +465,13 @@ __global__ void __launch_bounds__(PLANE3_THREADS, 2) k_fxy3_r2c(const IN* __rest
         }
         DFT<R1, N, -1>::run(v, tw);
 #pragma unroll
-        for (int k1 = 0; k1 < R1; ++k1) Zr[skew<R2>(k1, t)] = (k1 == 0) ? v[0] : cmul(v[k1], twid<-1>(tw, t * k1));
+        for (int k1 = 0; k1 < R1; ++k1) Zr[skew<R1, R2>(k1, t)] = (k1 == 0) ? v[0] : cmul(v[k1], twid<-1>(tw, t * k1));
       }
       __syncwarp();
       float2 w[R2];
       if (act && t < R1) {
 #pragma unroll
-        for (int n2 = 0; n2 < R2; ++n2) w[n2] = Zr[skew<R2>(t, n2)];
+        for (int n2 = 0; n2 < R2; ++n2) w[n2] = Zr[skew<R1, R2>(t, n2)];
         DFT<R2, N, -1>::run(w, tw);
       }
       __syncwarp();
@@ -489,12 +490,14 @@ __global__ void __launch_bounds__(PLANE3_THREADS, 2) k_fxy3_r2c(const IN* __rest
       const int kx = kx0 + col;
       const bool act = t < T && kx < NH && col < W;
       const int kc = (N - kx) % N;
-      // exchange slot s of column kx: columns kx and N-kx of Z are read only by column kx
-      auto slot = [&](int s) -> float2* {
-        if (kx == 0) return S + s;
-        if (2 * kx == N) return S + N + s;
-        return (s < NP) ? Z + (size_t)s * N + kx : Z + (size_t)(s - NP) * N + kc;
-      };
+      // exchange slot s of column kx (columns kx and N-kx of Z are read only by column
+      // kx): slot s < NP at lo + s*st, else at hi + s*st; the self-conjugate columns 0
+      // and N/2 use the contiguous scratch S.
+      const bool selfc = (kx == 0) || (2 * kx == N);
+      const int st = selfc ? 1 : N;
+      // offsets from Z (S follows Z): slot s at Z[lo + s*st] for s < NP, else Z[hi + s*st]
+      const int64_t lo = selfc ? (int64_t)NP * N + (kx ? N : 0) : (int64_t)kx;
+      const int64_t hi = selfc ? lo : (int64_t)kc - (int64_t)NP * N;
       float2 v[R1];
       if (act && t < R2) {
 #pragma unroll
@@ -509,14 +512,25 @@ __global__ void __launch_bounds__(PLANE3_THREADS, 2) k_fxy3_r2c(const IN* __rest
       }
       __syncthreads();  // all unpack reads of this round are done
       if (act && t < R2) {
+        // s = k1*R2 + t < NP exactly when k1 < R1/2 (R1 even) -- resolved per unrolled k1
 #pragma unroll
-        for (int k1 = 0; k1 < R1; ++k1) *slot(k1 * R2 + t) = (k1 == 0) ? v[0] : cmul(v[k1], twid<-1>(tw, t * k1));
+        for (int k1 = 0; k1 < R1; ++k1) {
+          const int sl = k1 * R2 + t;
+          const int64_t b = (k1 * R2 + R2 - 1 < NP) ? lo : ((k1 * R2 >= NP) ? hi : (sl < NP ? lo : hi));
+          Z[b + (int64_t)sl * st] = (k1 == 0) ? v[0] : cmul(v[k1], twid<-1>(tw, t * k1));
+        }
       }
       __syncthreads();
       if (act && t < R1) {
         float2 w[R2];
+        const int s0 = t * R2;
+        const bool whole = (s0 + R2 - 1 < NP) || (s0 >= NP);  // R1 even: always
+        const int64_t b = (s0 < NP) ? lo : hi;
 #pragma unroll
-        for (int n2 = 0; n2 < R2; ++n2) w[n2] = *slot(t * R2 + n2);
+        for (int n2 = 0; n2 < R2; ++n2) {
+          const int sl = s0 + n2;
+          w[n2] = Z[(whole ? b : (sl < NP ? lo : hi)) + (int64_t)sl * st];
+        }
         DFT<R2, N, -1>::run(w, tw);
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) cp[(int64_t)(t + R1 * k2) * pc + kx] = w[k2];
@@ -600,13 +614,13 @@ __global__ void __launch_bounds__(PLANE3_THREADS, 2) k_fyx3_c2r(const float2* __
       __syncwarp();  // the pack reads of rows 2p, 2p+1 are done
       if (act && t < R2) {
 #pragma unroll
-        for (int k1 = 0; k1 < R1; ++k1) H0[skew<R2>(k1, t)] = (k1 == 0) ? v[0] : cmul(v[k1], twid<+1>(tw, t * k1));
+        for (int k1 = 0; k1 < R1; ++k1) H0[skew<R1, R2>(k1, t)] = (k1 == 0) ? v[0] : cmul(v[k1], twid<+1>(tw, t * k1));
       }
       __syncwarp();
       if (act && t < R1) {
         float2 w[R2];
 #pragma unroll
-        for (int n2 = 0; n2 < R2; ++n2) w[n2] = H0[skew<R2>(t, n2)];
+        for (int n2 = 0; n2 < R2; ++n2) w[n2] = H0[skew<R1, R2>(t, n2)];
         DFT<R2, N, +1>::run(w, tw);
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) {
