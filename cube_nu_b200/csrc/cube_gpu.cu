@@ -79,6 +79,7 @@ struct cube_ctx {
   Geo G;
   int device = 0;
   cudaStream_t s = nullptr;
+  int nsm = 148;  // multiprocessors of the device
   bool loaded = false;
   int64_t np = 0, cap = 0;
   int xbytes = 1;
@@ -307,6 +308,20 @@ void smem_optin(K kernel, size_t bytes) {
 
 // Size-specialised passes (fft2.cuh) for N = R1*R2.  N <= 144 runs the fused plane
 // kernels (XY forward, YX inverse) around the z pass; larger N runs five passes.
+// z pass with Green multiply for the row-pitched sizes (N >= 192): the persistent
+// streamed kernel, which keeps the next line's loads in flight.
+template <int N, int R1, int R2>
+void fz_green(cube_ctx* c, int64_t nbox, float2* ck, const float* green, const float2* tw, const Pitch& pt, int kz) {
+  constexpr int T = f2::TPS<R1, R2>::T;
+  int W = 0, ncg = 0;
+  f2::fz_stream_shape(N, T, W, ncg);
+  const size_t sm = f2::fz_stream_smem(N, W);
+  const int64_t nitems = nbox * (int64_t)N * ncg;
+  const unsigned grid = (unsigned)std::min<int64_t>(nitems, 2 * (int64_t)c->nsm);
+  smem_optin(f2::k_fz_stream<N, R1, R2>, sm);
+  LAUNCH(c, kz, 1, f2::k_fz_stream<N, R1, R2><<<grid, W * T, sm, c->s>>>(ck, green, tw, W, ncg, pt.pc, pt.plc, nitems));
+}
+
 template <int N, int R1, int R2>
 void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out, float2* ck,
               const float* green, float norm, int reps, int kx, int ky, int kz, int kc, const Pitch& pt) {
@@ -315,7 +330,6 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
   const int64_t nrows = nbox * (int64_t)N * N;
   const int W = f2::fcol_width(N, T);
   const size_t smc = (size_t)(N + W * N) * sizeof(float2);
-  const size_t smg = smc + (size_t)W * N * sizeof(float);  // z pass: + prefetched Green values
   dim3 gc((unsigned)(nbox * N), (unsigned)((NH + W - 1) / W));
   if constexpr (N <= 144) {
     if (fused_layout(c, N)) {
@@ -330,6 +344,8 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
         LAUNCH(c, kx, 1, f2::k_fxy3_r2c<N, R1, R2, float><<<planes, f2::PLANE3_THREADS, smf, c->s>>>(
                              (const float*)real_in, ck, tw, scale, pt.pr, pt.pc, pt.plr, pt.plc));
       }
+      // plane sizes: the block-per-line column pass hides latency with more warps
+      const size_t smg = smc + (size_t)W * N * sizeof(float);  // + prefetched Green values
       smem_optin(f2::k_fcol3<N, R1, R2, 2, 2>, smg);
       LAUNCH(c, kz, 1, f2::k_fcol3<N, R1, R2, 2, 2><<<gc, W * T, smg, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
       smem_optin(f2::k_fyx3_c2r<N, R1, R2>, smi);
@@ -351,11 +367,10 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
                                                                              scale, pt.pr, pt.pc));
   }
   smem_optin(f2::k_fcol3<N, R1, R2, 1, 0>, smc);
-  smem_optin(f2::k_fcol3<N, R1, R2, 2, 2>, smg);
   smem_optin(f2::k_fcol3<N, R1, R2, 1, 1>, smc);
   smem_optin(f2::k_fx_c2r<N, R1, R2>, smx);
   LAUNCH(c, ky, 1, f2::k_fcol3<N, R1, R2, 1, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
-  LAUNCH(c, kz, 1, f2::k_fcol3<N, R1, R2, 2, 2><<<gc, W * T, smg, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
+  fz_green<N, R1, R2>(c, nbox, ck, green, tw, pt, kz);
   LAUNCH(c, ky, 1, f2::k_fcol3<N, R1, R2, 1, 1><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
   LAUNCH(c, kc, 1, f2::k_fx_c2r<N, R1, R2><<<gx, S * T, smx, c->s>>>(ck, phi_out, nrows, tw, norm, reps, pt.pc, pt.pf));
 }
@@ -602,6 +617,7 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
   c->xbytes = G.izipx;
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking));
+  CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
   for (int i = 0; i < 8; ++i) CK(cudaEventCreate(&c->ev[i]));
   int rc = add_fft(c, G.nc);
   if (!rc) rc = add_fft(c, G.ngt);

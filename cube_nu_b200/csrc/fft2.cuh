@@ -23,6 +23,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "fft.cuh"
 
 namespace cube {
@@ -347,6 +349,128 @@ __global__ void __launch_bounds__(FcolBounds<N>::MAXT, FcolBounds<N>::MINB) k_fc
     }
   }
 }
+
+// ---------------------------------------------------------------------------------
+// Persistent z pass with Green multiply: the work of k_fcol3<...,2,2> (forward z DFT,
+// Green multiply, inverse), one item = W columns of one line (box b, row y), looped over
+// by a grid of a few blocks per SM.  The column data and Green values of the next item
+// are copied into the other of two shared-memory stages with cp.async while the current
+// one is transformed, so the loads stay in flight; the current stage doubles as the
+// exchange slots.  Items: it = (b*N + y)*ncg + column group.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+__host__ __device__ constexpr int fzs_maxt(int N) { return N <= 192 ? 320 : 512; }
+
+template <int N, int R1, int R2>
+__global__ void __launch_bounds__(fzs_maxt(N), (N <= 192 ? 2 : 1)) k_fz_stream(float2* __restrict__ c, const float* __restrict__ green,
+                                                            const float2* __restrict__ gtw, int W, int ncg, int pc,
+                                                            int64_t plc, int64_t nitems) {
+  constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1;
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* stg = sm + N;                                          // [2][N][W] float2
+  float* gst = reinterpret_cast<float*>(stg + (size_t)2 * N * W);  // [2][N][W] float
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
+  const int col = threadIdx.x % W, t = threadIdx.x / W;
+  const bool thr = t < T;
+  auto issue = [&](int64_t it, int st) {  // copy item `it` into stage `st`; always commits a group
+    if (it < nitems && thr) {
+      const int64_t line = it / ncg;
+      const int kx = (int)(it - line * ncg) * W + col;
+      if (kx < NH) {
+        const int64_t b = line / N;
+        const int y = (int)(line - b * N);
+        const float2* base = c + b * (int64_t)N * plc + (int64_t)y * pc + kx;
+        const float* gb = green + (int64_t)y * NH + kx;
+        float2* ds = stg + (size_t)st * N * W + col;
+        float* dg = gst + (size_t)st * N * W + col;
+#pragma unroll 4
+        for (int z = t; z < N; z += T) {
+          cp_async8(ds + (size_t)z * W, base + (int64_t)z * plc);
+          cp_async4(dg + (size_t)z * W, gb + (int64_t)z * N * NH);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  int64_t it = blockIdx.x;
+  issue(it, 0);
+  for (int s = 0; it < nitems; it += gridDim.x, s ^= 1) {
+    issue(it + gridDim.x, s ^ 1);
+    cp_async_wait_one();  // this thread's copies of item `it` have landed
+    __syncthreads();      // and everyone's
+    const int64_t line = it / ncg;
+    const int kx = (int)(it - line * ncg) * W + col;
+    const bool live = thr && kx < NH;
+    const int64_t b = line / N;
+    const int y = (int)(line - b * N);
+    float2* out = c + b * (int64_t)N * plc + (int64_t)y * pc + kx;
+    float2* Ac = stg + (size_t)s * N * W + col;
+    const float* Gc = gst + (size_t)s * N * W + col;
+    // forward, n = R2*n1 + n2: thread t = n2
+    float2 v[R1];
+    if (thr && t < R2) {
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) v[n1] = live ? Ac[(R2 * n1 + t) * W] : make_float2(0.f, 0.f);
+      DFT<R1, N, -1>::run(v, tw);
+    }
+    __syncthreads();  // the stage's data are in registers; its slots become the exchange
+    if (thr && t < R2) {
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) Ac[(k1 * R2 + t) * W] = (k1 == 0) ? v[0] : cmul(v[k1], twid<-1>(tw, t * k1));
+    }
+    __syncthreads();
+    float2 w[R2];
+    if (thr && t < R1) {
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) w[n2] = Ac[(t * R2 + n2) * W];
+      DFT<R2, N, -1>::run(w, tw);
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) {  // Green at kz = t + R1*k2
+        const float gv = Gc[(t + R1 * k2) * W];
+        w[k2] = make_float2(w[k2].x * gv, w[k2].y * gv);
+      }
+      // inverse, n = R1*n1 + n2 with n2 = t, n1 = k2
+      DFT<R2, N, +1>::run(w, tw);
+#pragma unroll
+      for (int k1 = 1; k1 < R2; ++k1) w[k1] = cmul(w[k1], twid<+1>(tw, t * k1));
+    }
+    __syncthreads();
+    if (thr && t < R1) {
+#pragma unroll
+      for (int k1 = 0; k1 < R2; ++k1) Ac[(k1 * R1 + t) * W] = w[k1];
+    }
+    __syncthreads();
+    if (thr && t < R2) {
+      float2 u[R1];
+#pragma unroll
+      for (int n2 = 0; n2 < R1; ++n2) u[n2] = Ac[(t * R1 + n2) * W];
+      DFT<R1, N, +1>::run(u, tw);
+      if (live) {
+#pragma unroll
+        for (int k2 = 0; k2 < R1; ++k2) out[(int64_t)(t + R2 * k2) * plc] = u[k2];
+      }
+    }
+    __syncthreads();  // this stage is free for the copy issued next iteration
+  }
+  cp_async_wait_all();
+}
+
+// Width and count of the column groups of k_fz_stream: two blocks per SM within
+// ~100 KB of shared memory each, at most fzs_maxt(N) threads.
+__host__ inline void fz_stream_shape(int N, int T, int& W, int& ncg) {
+  const int NH = N / 2 + 1;
+  int wmax = (int)((100 * 1024 - 8 * N) / (2 * 12 * N));
+  wmax = std::min(wmax, fzs_maxt(N) / T);
+  ncg = (NH + wmax - 1) / wmax;
+  W = (NH + ncg - 1) / ncg;
+}
+__host__ inline size_t fz_stream_smem(int N, int W) { return (size_t)N * 8 + (size_t)2 * N * W * 12; }
 
 // Column-block width: the whole half row when it fits one block (<= 512 threads, the
 // launch bound), else an even split.
