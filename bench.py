@@ -141,7 +141,9 @@ class Clocks:
 # ------------------------------------------------------------------------------------
 def kernel_bytes(p, name: str, n_particles: int, napm, fixed: bool):
     """Algorithmic HBM bytes a kernel class must move over one whole step (all its
-    launches together; documented in DESIGN.md)."""
+    launches together): mesh passes read and write each cell once at the element size
+    of the pass, particle kernels read each particle's code and velocity once, the
+    deposit adds 27 read-modify-writes per particle and box it lands in."""
     bx = 3 * p.izipx
     rb = 8 if fixed else 4
 

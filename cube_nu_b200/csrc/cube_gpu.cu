@@ -1095,16 +1095,19 @@ int cube_gpu_ic(cube_ctx* c, const cube_ic_in* in, cube_ic_out* out) {
     CK(cudaMalloc(&tmp_mesh, mbytes));
     mesh = tmp_mesh;
   }
+  std::vector<double> hk(in->npk), hp(in->npk);
+  for (int i = 0; i < in->npk; ++i) {
+    if (!(in->pk_k[i] > 0) || !(in->pk_p[i] > 0)) {
+      if (tmp_mesh) cudaFree(tmp_mesh);
+      return fail(CUBE_E_ARG, "P(k) table must be positive");
+    }
+    hk[i] = std::log(in->pk_k[i]);
+    hp[i] = std::log(in->pk_p[i]);
+  }
   float* gtab = nullptr;
   double *lk = nullptr, *lp = nullptr;
   const int64_t gcount = (int64_t)nw * nw * (nw / 2 + 1);
   CK(cudaMalloc(&gtab, gcount * sizeof(float)));
-  std::vector<double> hk(in->npk), hp(in->npk);
-  for (int i = 0; i < in->npk; ++i) {
-    if (!(in->pk_k[i] > 0) || !(in->pk_p[i] > 0)) return fail(CUBE_E_ARG, "P(k) table must be positive");
-    hk[i] = std::log(in->pk_k[i]);
-    hp[i] = std::log(in->pk_p[i]);
-  }
   CK(cudaMalloc(&lk, in->npk * sizeof(double)));
   CK(cudaMalloc(&lp, in->npk * sizeof(double)));
   CK(cudaMemcpyAsync(lk, hk.data(), in->npk * sizeof(double), cudaMemcpyHostToDevice, c->s));
