@@ -556,8 +556,7 @@ __global__ void __launch_bounds__(PLANE3_THREADS, 2) k_fxy3_r2c(const IN* __rest
   static_assert(T <= 16, "two sequences per warp");
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  float2* Z = sm + N;             // packed rows, pitch N
-  float2* S = Z + (size_t)NP * N;  // exchange slots of columns 0 and N/2
+  float2* Z = sm + N;  // packed rows, pitch N; then 2N exchange slots for columns 0 and N/2
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = gtw[i];
   const int64_t plane = blockIdx.x;
   const IN* rp = r + plane * plr;
