@@ -789,7 +789,7 @@ static int drift_enqueue(cube_ctx* c, const cube_step_in* in) {
                                            c->rhoc2, c->err));
   LAUNCH(c, K_SCAN, 3, exclusive_scan(c->rhoc2, c->cstart2, G.ncells, c->scan_tmp, c->s));
   LAUNCH(c, K_DRIFT_SCATTER, 1, k_drift_scatter<<<nblk(np), 256, 0, c->s>>>(np, c->dest, c->key, c->cstart2, c->fill, c->skey, c->ssrc));
-  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_small<<<nblk(G.ncells * 32), 256, 0, c->s>>>(G.ncells, c->rhoc2, c->cstart2, c->skey, c->ssrc,
+  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_small<<<nblk((G.ncells + 1) / 2 * 32), 256, 0, c->s>>>(G.ncells, c->rhoc2, c->cstart2, c->skey, c->ssrc,
                                                             c->biglist, c->nbig));
   const int max_seg = c->P.max_segment > 0 ? std::min(c->P.max_segment, 16384) : 16384;
   // One block per listed long segment; the grid is bounded by the cell count.
@@ -1143,7 +1143,7 @@ int cube_gpu_ic(cube_ctx* c, const cube_ic_in* in, cube_ic_out* out) {
                                                                   c->key, c->rhoc2, c->err));
   LAUNCH(c, K_SCAN, 3, exclusive_scan(c->rhoc2, c->cstart2, G.ncells, c->scan_tmp, c->s));
   LAUNCH(c, K_DRIFT_SCATTER, 1, k_drift_scatter<<<nblk(np), 256, 0, c->s>>>(np, c->dest, c->key, c->cstart2, c->fill, c->skey, c->ssrc));
-  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_small<<<nblk(G.ncells * 32), 256, 0, c->s>>>(G.ncells, c->rhoc2, c->cstart2, c->skey,
+  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_small<<<nblk((G.ncells + 1) / 2 * 32), 256, 0, c->s>>>(G.ncells, c->rhoc2, c->cstart2, c->skey,
                                                                                      c->ssrc, c->biglist, c->nbig));
   int nb_host = 0;
   CK(cudaMemcpyAsync(&nb_host, c->nbig, 4, cudaMemcpyDeviceToHost, c->s));

@@ -177,36 +177,67 @@ __global__ void k_drift_scatter(int64_t np, const int32_t* __restrict__ dest, co
   ssrc[pos] = (uint32_t)ip;
 }
 
-// Warp per destination cell: segments of <=32 sorted in registers (bitonic over
-// the warp); longer ones are listed for the block sorter.
+// Ascending bitonic sort of (key, value) pairs across groups of W lanes (W = 16 or 32);
+// lanes pass their index within the group.  Keys are unique; padding lanes hold ~0.
+template <int W>
+__device__ __forceinline__ void group_bitonic(uint64_t& k, uint32_t& v, int gl) {
+#pragma unroll
+  for (int size = 2; size <= W; size <<= 1)
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, stride);
+      const uint32_t ov = __shfl_xor_sync(0xffffffffu, v, stride);
+      const bool up = ((gl & size) == 0);
+      const bool lower = ((gl & stride) == 0);
+      const bool take = lower ? (up ? (ok < k) : (ok > k)) : (up ? (ok > k) : (ok < k));
+      if (take) {
+        k = ok;
+        v = ov;
+      }
+    }
+}
+
+// Two destination cells per warp, one per 16-lane half: segments of <=16 (nearly all at
+// 8 particles per cell) are sorted in registers by the half; segments of 17..32 are then
+// sorted by the whole warp, one at a time; longer ones are listed for the block sorter.
+// Launch (ncells + 1) / 2 warps.
 __global__ void k_drift_sort_small(int64_t ncells, const int32_t* __restrict__ count_new,
                                    const int64_t* __restrict__ cstart_new, uint64_t* __restrict__ skey,
                                    uint32_t* __restrict__ ssrc, int32_t* __restrict__ biglist,
                                    int32_t* __restrict__ nbig) {
-  const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (2 * w >= ncells) return;  // warp-uniform
   const int lane = threadIdx.x & 31;
-  if (c >= ncells) return;
-  const int n = count_new[c];
-  if (n <= 1) return;
-  if (n > 32) {
-    if (lane == 0) biglist[atomicAdd(nbig, 1)] = (int32_t)c;
-    return;
-  }
-  const int64_t base = cstart_new[c];
-  uint64_t k = (lane < n) ? skey[base + lane] : ~0ull;
-  uint32_t v = (lane < n) ? ssrc[base + lane] : 0u;
-  for (int size = 2; size <= 32; size <<= 1)
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, stride);
-      const uint32_t ov = __shfl_xor_sync(0xffffffffu, v, stride);
-      const bool up = ((lane & size) == 0);
-      const bool lower = ((lane & stride) == 0);
-      const bool take = lower ? (up ? (ok < k) : (ok > k)) : (up ? (ok > k) : (ok < k));
-      if (take) { k = ok; v = ov; }
+  const int hl = lane & 15;
+  const int64_t c = 2 * w + (lane >> 4);
+  const int n = (c < ncells) ? count_new[c] : 0;
+  if (n > 32 && hl == 0) biglist[atomicAdd(nbig, 1)] = (int32_t)c;
+  const bool small = n > 1 && n <= 16;
+  if (__any_sync(0xffffffffu, small)) {
+    const int64_t base = small ? cstart_new[c] : 0;
+    const bool live = small && hl < n;
+    uint64_t k = live ? skey[base + hl] : ~0ull;
+    uint32_t v = live ? ssrc[base + hl] : 0u;
+    group_bitonic<16>(k, v, hl);
+    if (live) {
+      skey[base + hl] = k;
+      ssrc[base + hl] = v;
     }
-  if (lane < n) {
-    skey[base + lane] = k;
-    ssrc[base + lane] = v;
+  }
+  unsigned mid = __ballot_sync(0xffffffffu, n > 16 && n <= 32 && hl == 0);
+  while (mid) {
+    const int h = __ffs(mid) - 1;
+    mid &= mid - 1;
+    const int64_t cm = 2 * w + (h >> 4);
+    const int nm = count_new[cm];
+    const int64_t base = cstart_new[cm];
+    uint64_t k = (lane < nm) ? skey[base + lane] : ~0ull;
+    uint32_t v = (lane < nm) ? ssrc[base + lane] : 0u;
+    group_bitonic<32>(k, v, lane);
+    if (lane < nm) {
+      skey[base + lane] = k;
+      ssrc[base + lane] = v;
+    }
   }
 }
 

@@ -66,7 +66,8 @@ def test_drift_bitexact(oracle_lib, izipx, kind):
 
 
 def test_drift_long_segments(oracle_lib):
-    """Destination cells with more than 32 arrivals go through the block sorter."""
+    """Destination cells of every sorter class: 2..16 arrivals (half-warp sort), 17..32
+    (whole-warp sort) and more than 32 (block sorter)."""
     p = _params()
     n = 30000
     st = clustered_state(p, n, seed=5, nblob=2, sigma=0.3, frac=0.8, vscale=1.0)
@@ -74,6 +75,9 @@ def test_drift_long_segments(oracle_lib):
     p.mass_p_cdm = float(p.ng) ** 3 / n
     vz = float(np.abs(st[1][:, 2]).max())
     ref = oracle_lib.drift(p, *st, 0.5, 0.5, vz)
+    cnt = ref[3]
+    for lo, hi in ((2, 16), (17, 32), (33, 1 << 30)):
+        assert np.any((cnt >= lo) & (cnt <= hi)), (lo, hi)
     with _ctx(p, st) as ctx:
         ctx.drift(0.5, 0.5, vz)
         got = ctx.download()
