@@ -359,11 +359,13 @@ __global__ void __launch_bounds__(256, 6) k_deposit_pm1(Geo G, int64_t np, const
 // Writes (tile, local coordinate i-1 in that tile) pairs; returns the count (1 or 2).
 __device__ __forceinline__ int tile_cands(const Geo& G, int g, int* t, int* li) {
   const int tt = g / G.nt, l = g - tt * G.nt;
-  int n = 0;
-  t[n] = tt; li[n] = l; ++n;
-  if (l < G.ncb) { t[n] = wrapi(tt - 1, G.nnt); li[n] = l + G.nt; ++n; }
-  else if (l >= G.nt - G.ncb) { t[n] = wrapi(tt + 1, G.nnt); li[n] = l - G.nt; ++n; }
-  return n;
+  t[0] = tt;
+  li[0] = l;
+  // constant slot indices keep the caller's arrays in registers
+  const bool lo = l < G.ncb, hi = !lo && l >= G.nt - G.ncb;
+  t[1] = wrapi(lo ? tt - 1 : tt + 1, G.nnt);
+  li[1] = lo ? l + G.nt : l - G.nt;
+  return (lo || hi) ? 2 : 1;
 }
 
 // PM2 tile meshes [tile - tile0][ngt^3]; fine index i maps to array i-(1-ngb).
@@ -383,9 +385,15 @@ __global__ void __launch_bounds__(256, 5) k_deposit_pm2(Geo G, int64_t np, const
   }
   const int ngt = G.ngt;
   const int64_t box = (int64_t)ngt * pl;  // elements per box
-  for (int cz = 0; cz < nca[2]; ++cz)
-    for (int cy = 0; cy < nca[1]; ++cy)
-      for (int cx = 0; cx < nca[0]; ++cx) {
+  // Candidate loops fully unrolled (at most two per dimension) so the candidate arrays
+  // stay in registers.
+#pragma unroll
+  for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+    for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+      for (int cx = 0; cx < 2; ++cx) {
+        if (cz >= nca[2] || cy >= nca[1] || cx >= nca[0]) continue;
         const int T = (tc[2][cz] * G.nnt + tc[1][cy]) * G.nnt + tc[0][cx];
         if (T < tile0 || T >= tile0 + ntile) continue;
         const int l[3] = {lc[0][cx], lc[1][cy], lc[2][cz]};
@@ -424,19 +432,24 @@ __global__ void __launch_bounds__(256, 5) k_deposit_pm2(Geo G, int64_t np, const
 __device__ __forceinline__ int sub_cands(const Geo& G, int g, int* t, int* u, int* li) {
   const int tt = g / G.nt, l = g - tt * G.nt;
   const int uu = l / G.ntt, r = l - uu * G.ntt;
-  int n = 0;
-  t[n] = tt; u[n] = uu; li[n] = l; ++n;
-  if (r == 0) {
-    if (uu > 0) { t[n] = tt; u[n] = uu - 1; li[n] = l; }
-    else { t[n] = wrapi(tt - 1, G.nnt); u[n] = G.nns - 1; li[n] = l + G.nt; }
-    ++n;
+  t[0] = tt;
+  u[0] = uu;
+  li[0] = l;
+  // With ntt >= 2 at most one of the two faces is adjacent; constant slot indices keep
+  // the caller's arrays in registers.
+  const bool lo = r == 0, hi = r == G.ntt - 1;
+  if (lo) {
+    const bool wrap = uu == 0;
+    t[1] = wrap ? wrapi(tt - 1, G.nnt) : tt;
+    u[1] = wrap ? G.nns - 1 : uu - 1;
+    li[1] = wrap ? l + G.nt : l;
+  } else {
+    const bool wrap = uu == G.nns - 1;
+    t[1] = wrap ? wrapi(tt + 1, G.nnt) : tt;
+    u[1] = wrap ? 0 : uu + 1;
+    li[1] = wrap ? l - G.nt : l;
   }
-  if (r == G.ntt - 1) {
-    if (uu < G.nns - 1) { t[n] = tt; u[n] = uu + 1; li[n] = l; }
-    else { t[n] = wrapi(tt + 1, G.nnt); u[n] = 0; li[n] = l - G.nt; }
-    ++n;
-  }
-  return n;
+  return (lo || hi) ? 2 : 1;
 }
 
 __device__ __forceinline__ int subtile_id(const Geo& G, const int t[3], const int u[3]) {
@@ -464,9 +477,15 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
   const int nft = G.nft[iapm], nfp = G.nfp[iapm], nfb = G.nfb[iapm];
   const int64_t box = (int64_t)nft * pl;  // elements per box
   const double gs = (double)(1.f / (float)rsf_of(iapm));  // pm%gridsize, real4
-  for (int cz = 0; cz < nca[2]; ++cz)
-    for (int cy = 0; cy < nca[1]; ++cy)
-      for (int cx = 0; cx < nca[0]; ++cx) {
+  // Candidate loops fully unrolled (at most two per dimension) so the candidate arrays
+  // stay in registers.
+#pragma unroll
+  for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+    for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+      for (int cx = 0; cx < 2; ++cx) {
+        if (cz >= nca[2] || cy >= nca[1] || cx >= nca[0]) continue;
         const int t[3] = {tc[0][cx], tc[1][cy], tc[2][cz]};
         const int u[3] = {uc[0][cx], uc[1][cy], uc[2][cz]};
         const int slot = box_slot[subtile_id(G, t, u)];
