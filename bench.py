@@ -36,10 +36,11 @@ from cube_nu_b200.params import DEPOSIT_FIXED, DEPOSIT_FP32, config_512, config_
 METRIC = "particle-steps/s P3M KDK @512^3"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # DRAM bytes (read + write) per class-2 PM3 box of 144^3, measured with ncu on the proxy
-# workload (one launch over 64 boxes; profiles/pm3_kernels_proxy.md).  Traffic grows with
-# the number of boxes, so a launch over B such boxes moves B times these.
+# workload (one launch over 64 boxes; profiles/pm3_kernels_proxy.md, and for the
+# owner-computes deposit profiles/deposit_pm3_owner_proxy.md).  Traffic grows with the
+# number of boxes, so a launch over B such boxes moves B times these.
 PM3_TRAFFIC_PER_BOX = {
-    "deposit_pm3": 1.892842e9 / 64,
+    "deposit_pm3": 1.4917e9 / 64,
     "fft_x_pm3": 2.271174e9 / 64,
     "fft_z_green_pm3": 1.910046e9 / 64,
     "fft_c2r_pm3": 1.485638e9 / 64,
@@ -162,6 +163,11 @@ def kernel_bytes(p, name: str, n_particles: int, napm, fixed: bool):
     if name.startswith("fft_") and name.endswith("_pm2"):
         what = {"fft_x_pm2": "x", "fft_y_pm2": "y", "fft_z_green_pm2": "z", "fft_c2r_pm2": "c"}[name]
         return mesh(p.ngt, p.ntiles, what) * (2 if what == "y" else 1)
+    if name == "deposit_pm3" and fixed:
+        # owner-computes form: every cell of every box written once (no memset, no
+        # read-back), each particle's position code read once
+        nbs = napm if napm is not None else [0, 0, p.ns3, 0, 0, 0]
+        return int(sum(int(nbs[c]) * p.nft(c) ** 3 * 8 for c in range(2, 6)) + n_particles * bx)
     if name in ("deposit_pm1", "deposit_pm2", "deposit_pm3"):
         # read position code + cell index per particle, one read-modify-write of 27 cells
         boxes = {"deposit_pm1": 1.0, "deposit_pm2": (1 + 2 * p.ncb / p.nt) ** 3, "deposit_pm3": (1 + 2 / p.ntt) ** 3}[name]

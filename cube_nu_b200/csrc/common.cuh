@@ -9,8 +9,9 @@ namespace cube {
 
 // ratio_sf, parameters.f90:26 (1-based; class iapm uses RSF[iapm]).
 __host__ __device__ inline int rsf_of(int iapm) {
-  const int t[8] = {0, 1, 2, 4, 6, 8, 12, 16};
-  return t[iapm & 7];
+  // {0, 1, 2, 4, 6, 8, 12, 16}[iapm & 7], without a local-memory table
+  const int i = iapm & 7;
+  return i <= 2 ? i : i == 3 ? 4 : i == 4 ? 6 : i == 5 ? 8 : i == 6 ? 12 : 16;
 }
 
 // Geometry derived from cube_params (parameters.f90:57-82).  Plain struct passed to

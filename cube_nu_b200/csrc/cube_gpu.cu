@@ -295,6 +295,20 @@ MeshPtrs mesh_ptrs(cube_ctx* c, int n, int64_t, bool fixed) {
   return m;
 }
 
+// The owner-computes PM3 deposit covers a class when every region of DEP3_R^3 cells of
+// its boxes draws on at most DEP3_MAXC coarse cells (same range as dep3_krange).
+bool dep3_own_fits(const Geo& G, int iapm) {
+  const int nft = G.nft[iapm], nfb = G.nfb[iapm];
+  auto fdiv = [](int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); };
+  int mk = 0;
+  for (int o = 0; o < nft; o += DEP3_R) {
+    const int e = std::min(DEP3_R, nft - o);
+    const int klo = std::max(-1, fdiv(o - nfb - 2, nfb)), khi = std::min(G.ntt, fdiv(o + e - nfb + 1, nfb));
+    mk = std::max(mk, khi - klo + 1);
+  }
+  return nfb > 0 && (int64_t)mk * mk * mk <= DEP3_MAXC;
+}
+
 // How many boxes of side n fit in the arena.
 int64_t boxes_fit(cube_ctx* c, int n, bool fixed) {
   const size_t per = mesh_bytes(c, n, 1, fixed);
@@ -903,21 +917,30 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
         chunks.push_back({cl, f, (int)std::min<int64_t>(per, (int64_t)lists[cl].size() - f)});
     }
     const int64_t nch = (int64_t)chunks.size();
+    // [nch][ns3] subtile -> slot maps, then the chunks' slot -> subtile lists (ns3 in all)
     if (nch > c->slot_chunks) {
       if (c->box_slot) cudaFree(c->box_slot);
       if (c->h_slots) cudaFreeHost(c->h_slots);
       c->box_slot = nullptr;
       c->h_slots = nullptr;
-      CK(cudaMalloc(&c->box_slot, nch * c->ns3 * 4));
-      CK(cudaMallocHost(&c->h_slots, nch * c->ns3 * 4));
+      CK(cudaMalloc(&c->box_slot, (nch + 1) * c->ns3 * 4));
+      CK(cudaMallocHost(&c->h_slots, (nch + 1) * c->ns3 * 4));
       c->slot_chunks = nch;
     }
+    std::vector<int64_t> list_off(nch);
+    int64_t off = nch * c->ns3;
     for (int64_t k = 0; k < nch; ++k) {
       int32_t* hs = c->h_slots + k * c->ns3;
       std::fill(hs, hs + c->ns3, -1);
-      for (int j = 0; j < chunks[k].nb; ++j) hs[lists[chunks[k].iapm][chunks[k].first + j]] = j;
+      list_off[k] = off;
+      for (int j = 0; j < chunks[k].nb; ++j) {
+        const int sub = lists[chunks[k].iapm][chunks[k].first + j];
+        hs[sub] = j;
+        c->h_slots[off + j] = sub;
+      }
+      off += chunks[k].nb;
     }
-    if (nch) CK(cudaMemcpyAsync(c->box_slot, c->h_slots, nch * c->ns3 * 4, cudaMemcpyHostToDevice, c->s));
+    if (nch) CK(cudaMemcpyAsync(c->box_slot, c->h_slots, off * 4, cudaMemcpyHostToDevice, c->s));
     for (int64_t k = 0; k < nch; ++k) {
       const int cl = chunks[k].iapm, nb = chunks[k].nb;
       const int n = G.nft[cl];
@@ -926,9 +949,19 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       const int32_t* slots = c->box_slot + k * c->ns3;
       MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
       const int64_t boxb = (int64_t)n * m.pt.psb;
-      CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
-      if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));
-      else LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));
+      if (fixed && dep3_own_fits(G, cl)) {
+        // owner-computes deposit: writes every cell, no memset
+        const int nr = (n + DEP3_R - 1) / DEP3_R;
+        const size_t sm = (size_t)DEP3_R * DEP3_R * DEP3_R * 8;
+        smem_optin(k_deposit_pm3_own, sm);
+        LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3_own<<<(unsigned)((int64_t)nb * nr * nr * nr), DEP3_THREADS, sm, c->s>>>(
+                                    G, c->xp, c->cstart, c->box_slot + list_off[k], cl,
+                                    reinterpret_cast<unsigned long long*>(m.real), c->err, m.pt.pr, m.pt.plr, nr, nr, nr));
+      } else {
+        CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
+        if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));
+        else LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));
+      }
       int cap_slot = -1;
       if (c->cap_level == 3 && c->cap_box >= 0 && c->cap_box < c->ns3 && ires[c->cap_box] == cl)
         cap_slot = c->h_slots[k * c->ns3 + c->cap_box];

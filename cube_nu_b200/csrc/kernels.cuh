@@ -459,6 +459,14 @@ __device__ __forceinline__ int subtile_id(const Geo& G, const int t[3], const in
 
 // PM3 meshes of one class: slot = box_slot[subtile] (or -1), mesh [slot][nft^3];
 // refined index i maps to array i-(1-nfb).
+// xpos of kick.f90:628-629, ((l + f) * ratio_cs) / gridsize - u * nfp in real(8), with
+// gridsize = real(1/rsf, 4).  For rsf a power of two gridsize is exact and the division
+// equals the multiplication by rsf (exact scaling by a power of two).
+__device__ __forceinline__ double pm3_xpos(double lf, const Geo& G, double gs, int rsf, int unfp) {
+  const double a = lf * (double)G.rcs;
+  return (((rsf & (rsf - 1)) == 0) ? a * (double)rsf : a / gs) - (double)unfp;
+}
+
 template <bool FIXED>
 __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                               const int32_t* __restrict__ box_slot, int iapm, void* __restrict__ rho,
@@ -496,7 +504,7 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
         bool oob = false;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          const double xpos = ((double)l[d] + f[d]) * (double)G.rcs / gs - (double)(u[d] * nfp);  // kick.f90:628-629
+          const double xpos = pm3_xpos((double)l[d] + f[d], G, gs, rsf_of(iapm), u[d] * nfp);  // kick.f90:628-629
           i2[d] = tsc_weights(xpos, w[d]);
           if (i2[d] - 1 < -nfb || i2[d] + 1 > nfp + nfb + 1) oob = true;
         }
@@ -523,6 +531,158 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
           }
         }
       }
+}
+
+// Owner-computes form of the fixed-point PM3 deposit: one block per region of
+// DEP3_R^3 cells of one box.  The block sums, in shared memory, the contributions of the
+// particles of every coarse cell whose TSC footprint can reach the region, then writes
+// every cell of the region (zeros included) with plain stores, so the mesh needs no
+// memset and no cell is read back from DRAM.  Particle arithmetic is that of
+// k_deposit_pm3 (a box's candidate particles are those of coarse cells k = -1..ntt
+// around its subtile, with tile-local coordinate l = u*ntt + k), so the int64 sums are
+// identical.  Requires the int64 layouts (no padding between real rows) and at most
+// DEP3_MAXC candidate coarse cells per region (checked on the host).
+constexpr int DEP3_R = 24;
+constexpr int DEP3_MAXC = 125;
+constexpr int DEP3_THREADS = 512;
+
+__device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+// Candidate coarse-cell range (box-relative k) along one dimension for region cells
+// [o, o+e): TSC footprints fl+nfb-1..fl+nfb+1, one cell of margin for the FP64 rounding
+// of xpos.
+__device__ __forceinline__ void dep3_krange(int o, int e, int nfb, int ntt, int& klo, int& nk) {
+  klo = max(-1, floor_div(o - nfb - 2, nfb));
+  const int khi = min(ntt, floor_div(o + e - nfb + 1, nfb));
+  nk = khi - klo + 1;
+}
+
+__global__ void __launch_bounds__(DEP3_THREADS, 2) k_deposit_pm3_own(Geo G, const void* __restrict__ xp,
+                                                                     const int64_t* __restrict__ cstart,
+                                                                     const int32_t* __restrict__ box_sub, int iapm,
+                                                                     unsigned long long* __restrict__ rho, unsigned* err,
+                                                                     int pr, int64_t pl, int nrx, int nry, int nrz) {
+  constexpr int R = DEP3_R;
+  static_assert(R % 2 == 0 && R / 2 <= 16, "a half warp writes one region row");
+  extern __shared__ __align__(16) unsigned long long acc[];  // [R][R][R]
+  __shared__ int64_t cst[DEP3_MAXC];
+  __shared__ int ccnt[DEP3_MAXC], ckk[DEP3_MAXC], cpre[DEP3_MAXC + 1];
+  const int tid = threadIdx.x;
+  const int nft = G.nft[iapm], nfp = G.nfp[iapm], nfb = G.nfb[iapm];
+  const int nreg = nrx * nry * nrz;
+  const int64_t j = blockIdx.x / nreg;
+  const int r = (int)(blockIdx.x - j * nreg);
+  const int o[3] = {(r % nrx) * R, ((r / nrx) % nry) * R, (r / (nrx * nry)) * R};
+  const int e[3] = {min(R, nft - o[0]), min(R, nft - o[1]), min(R, nft - o[2])};
+  // subtile of this box
+  const int s = box_sub[j];
+  const int nns3 = G.nns * G.nns * G.nns;
+  const int T = s / nns3, f = s - T * nns3;
+  const int t[3] = {T % G.nnt, (T / G.nnt) % G.nnt, T / (G.nnt * G.nnt)};
+  const int u[3] = {f % G.nns, (f / G.nns) % G.nns, f / (G.nns * G.nns)};
+  int klo[3], nk[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) dep3_krange(o[d], e[d], nfb, G.ntt, klo[d], nk[d]);
+  const int ncand = nk[0] * nk[1] * nk[2];
+  if (ncand > DEP3_MAXC) {  // block-uniform; the host sizes regions so this does not happen
+    if (tid == 0) set_err(err, CUBE_DEVERR_DEPOSIT_RANGE);
+    return;
+  }
+  // one thread per candidate coarse cell: its particle range and box-relative k
+  if (tid < ncand) {
+    const int kx = klo[0] + tid % nk[0], ky = klo[1] + (tid / nk[0]) % nk[1], kz = klo[2] + tid / (nk[0] * nk[1]);
+    const int64_t cell = cell_index(G, t[0] * G.nt + u[0] * G.ntt + kx, t[1] * G.nt + u[1] * G.ntt + ky,
+                                    t[2] * G.nt + u[2] * G.ntt + kz);
+    const int64_t a = cstart[cell];
+    cst[tid] = a;
+    ccnt[tid] = (int)(cstart[cell + 1] - a);
+    ckk[tid] = (kx + 1) | ((ky + 1) << 10) | ((kz + 1) << 20);
+  }
+  {
+    ulonglong2* a2 = reinterpret_cast<ulonglong2*>(acc);
+    for (int i = tid; i < R * R * R / 2; i += blockDim.x) a2[i] = make_ulonglong2(0ull, 0ull);
+  }
+  __syncthreads();
+  if (tid < 32) {  // prefix of the counts
+    int carry = 0;
+    for (int b0 = 0; b0 < ncand; b0 += 32) {
+      const int i = b0 + tid;
+      int incl = (i < ncand) ? ccnt[i] : 0;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (tid >= off) incl += v;
+      }
+      if (i < ncand) cpre[i + 1] = carry + incl;
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (tid == 0) cpre[0] = 0;
+  }
+  __syncthreads();
+  const int total = cpre[ncand];
+  const double gs = (double)(1.f / (float)rsf_of(iapm));  // pm%gridsize, real4
+  for (int v = tid; v < total; v += blockDim.x) {
+    int lo = 0, hi = ncand;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (cpre[mid] <= v) lo = mid;
+      else hi = mid;
+    }
+    const int64_t ip = cst[lo] + (v - cpre[lo]);
+    const int kk = ckk[lo];
+    const int k[3] = {(kk & 1023) - 1, ((kk >> 10) & 1023) - 1, (kk >> 20) - 1};
+    int i2[3], c0[3];
+    float w[3][3];
+    bool oob = false, miss = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int l = u[d] * G.ntt + k[d];
+      const double fr = zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
+      const double xpos = pm3_xpos((double)l + fr, G, gs, rsf_of(iapm), u[d] * nfp);
+      i2[d] = tsc_weights(xpos, w[d]);
+      if (i2[d] - 1 < -nfb || i2[d] + 1 > nfp + nfb + 1) oob = true;
+      c0[d] = i2[d] + nfb - 2 - o[d];  // region-local cell of the footprint's first weight
+      if (c0[d] + 2 < 0 || c0[d] >= e[d]) miss = true;
+    }
+    if (oob) {
+      set_err(err, CUBE_DEVERR_DEPOSIT_RANGE);
+      continue;
+    }
+    if (miss) continue;
+#pragma unroll
+    for (int a3 = 0; a3 < 3; ++a3) {
+      const int z = c0[2] + a3;
+      if (z < 0 || z >= e[2]) continue;
+#pragma unroll
+      for (int a2 = 0; a2 < 3; ++a2) {
+        const int y = c0[1] + a2;
+        if (y < 0 || y >= e[1]) continue;
+#pragma unroll
+        for (int a1 = 0; a1 < 3; ++a1) {
+          const int x = c0[0] + a1;
+          if (x < 0 || x >= e[0]) continue;
+          const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
+          const long long q = __float2ll_rn(__fmul_rn(ww, FIXED_SCALE));
+          atomicAdd(&acc[(z * R + y) * R + x], (unsigned long long)q);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // every cell of the region: a half warp per row, two cells per 16-byte store (e[0] and
+  // the pitches are even).  z = row / e[1] through a float reciprocal: (row + 0.5) / e[1]
+  // is at least 0.5/e[1] from an integer, far above the rounding error for row < R*R.
+  unsigned long long* base = rho + j * (int64_t)nft * pl + (int64_t)o[2] * pl + (int64_t)o[1] * pr + o[0];
+  const int hx = e[0] >> 1, nrow = e[1] * e[2], hl = tid & 15;
+  const float inv_e1 = 1.f / (float)e[1];
+  for (int row = tid >> 4; row < nrow; row += blockDim.x >> 4) {
+    const int z = (int)(((float)row + 0.5f) * inv_e1);
+    const int y = row - z * e[1];
+    if (hl < hx) {
+      const ulonglong2 val = *reinterpret_cast<const ulonglong2*>(&acc[(z * R + y) * R + 2 * hl]);
+      __stcs(reinterpret_cast<ulonglong2*>(base + (int64_t)z * pl + (int64_t)y * pr) + hl, val);
+    }
+  }
 }
 
 // =================================================================================
@@ -861,8 +1021,7 @@ __global__ void __launch_bounds__(256, 3) k_interp_pm3(Geo G, int64_t np, const 
       bool oob = false;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const double xpos =
-            ((double)l[d] + zfrac(load_code(xp, G.izipx, 3 * ip + d), G)) * (double)G.rcs / gs - (double)(u[d] * nfp);
+        const double xpos = pm3_xpos((double)l[d] + zfrac(load_code(xp, G.izipx, 3 * ip + d), G), G, gs, rsf_of(iapm), u[d] * nfp);
         i2[d] = tsc_weights(xpos, w[d]);
         if (i2[d] - 1 < 0 || i2[d] + 1 > nfp + 1) oob = true;
       }
