@@ -5,6 +5,7 @@
 // periodic copies when nn=1, so every kernel reads neighbour cells through periodic
 // cell indexing instead of materialised ghost copies.
 #pragma once
+#include <type_traits>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -545,6 +546,7 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
 constexpr int DEP3_R = 24;
 constexpr int DEP3_MAXC = 125;
 constexpr int DEP3_THREADS = 512;
+constexpr int DEP3_SPLIT_MAX = 4095;
 
 __device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
@@ -620,54 +622,74 @@ __global__ void __launch_bounds__(DEP3_THREADS, 2) k_deposit_pm3_own(Geo G, cons
   }
   __syncthreads();
   const int total = cpre[ncand];
-  const double gs = (double)(1.f / (float)rsf_of(iapm));  // pm%gridsize, real4
-  for (int v = tid; v < total; v += blockDim.x) {
-    int lo = 0, hi = ncand;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (cpre[mid] <= v) lo = mid;
-      else hi = mid;
-    }
-    const int64_t ip = cst[lo] + (v - cpre[lo]);
-    const int kk = ckk[lo];
-    const int k[3] = {(kk & 1023) - 1, ((kk >> 10) & 1023) - 1, (kk >> 20) - 1};
-    int i2[3], c0[3];
-    float w[3][3];
-    bool oob = false, miss = false;
+  const int rsf = rsf_of(iapm);
+  const double gs = (double)(1.f / (float)rsf);  // pm%gridsize, real4
+  // Each q = round(w * 2^40) <= 2^40.  With at most DEP3_SPLIT_MAX candidate particles no
+  // cell takes more than that many contributions, so the low 20 bits and the rest of q
+  // can be summed in the two 32-bit halves of the cell without overflow:
+  // sum q = (sum hi << 20) + sum lo.  Denser regions use 64-bit atomics.
+  const bool split = total <= DEP3_SPLIT_MAX;
+  // the visit loop, instantiated for each summation form (block-uniform choice)
+  auto visits = [&](auto split_tag) {
+    constexpr bool SPLIT = decltype(split_tag)::value;
+    for (int v = tid; v < total; v += blockDim.x) {
+      int lo = 0, hi = ncand;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (cpre[mid] <= v) lo = mid;
+        else hi = mid;
+      }
+      const int64_t ip = cst[lo] + (v - cpre[lo]);
+      const int kk = ckk[lo];
+      const int k[3] = {(kk & 1023) - 1, ((kk >> 10) & 1023) - 1, (kk >> 20) - 1};
+      int code[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const int l = u[d] * G.ntt + k[d];
-      const double fr = zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
-      const double xpos = pm3_xpos((double)l + fr, G, gs, rsf_of(iapm), u[d] * nfp);
-      i2[d] = tsc_weights(xpos, w[d]);
-      if (i2[d] - 1 < -nfb || i2[d] + 1 > nfp + nfb + 1) oob = true;
-      c0[d] = i2[d] + nfb - 2 - o[d];  // region-local cell of the footprint's first weight
-      if (c0[d] + 2 < 0 || c0[d] >= e[d]) miss = true;
-    }
-    if (oob) {
-      set_err(err, CUBE_DEVERR_DEPOSIT_RANGE);
-      continue;
-    }
-    if (miss) continue;
+      for (int d = 0; d < 3; ++d) code[d] = load_code(xp, G.izipx, 3 * ip + d);
+      int i2[3], c0[3];
+      float w[3][3];
+      bool oob = false, miss = false;
 #pragma unroll
-    for (int a3 = 0; a3 < 3; ++a3) {
-      const int z = c0[2] + a3;
-      if (z < 0 || z >= e[2]) continue;
+      for (int d = 0; d < 3; ++d) {
+        const double xpos = pm3_xpos((double)(u[d] * G.ntt + k[d]) + zfrac(code[d], G), G, gs, rsf, u[d] * nfp);
+        i2[d] = tsc_weights(xpos, w[d]);  // kick.f90:628-629
+        if (i2[d] - 1 < -nfb || i2[d] + 1 > nfp + nfb + 1) oob = true;
+        c0[d] = i2[d] + nfb - 2 - o[d];  // region-local cell of the footprint's first weight
+        if (c0[d] + 2 < 0 || c0[d] >= e[d]) miss = true;
+      }
+      if (oob) {
+        set_err(err, CUBE_DEVERR_DEPOSIT_RANGE);
+        continue;
+      }
+      if (miss) continue;
 #pragma unroll
-      for (int a2 = 0; a2 < 3; ++a2) {
-        const int y = c0[1] + a2;
-        if (y < 0 || y >= e[1]) continue;
+      for (int a3 = 0; a3 < 3; ++a3) {
+        const int z = c0[2] + a3;
+        if (z < 0 || z >= e[2]) continue;
 #pragma unroll
-        for (int a1 = 0; a1 < 3; ++a1) {
-          const int x = c0[0] + a1;
-          if (x < 0 || x >= e[0]) continue;
-          const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
-          const long long q = __float2ll_rn(__fmul_rn(ww, FIXED_SCALE));
-          atomicAdd(&acc[(z * R + y) * R + x], (unsigned long long)q);
+        for (int a2 = 0; a2 < 3; ++a2) {
+          const int y = c0[1] + a2;
+          if (y < 0 || y >= e[1]) continue;
+#pragma unroll
+          for (int a1 = 0; a1 < 3; ++a1) {
+            const int x = c0[0] + a1;
+            if (x < 0 || x >= e[0]) continue;
+            const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
+            const unsigned long long q = (unsigned long long)__float2ll_rn(__fmul_rn(ww, FIXED_SCALE));
+            unsigned long long* cell = &acc[(z * R + y) * R + x];
+            if (SPLIT) {
+              unsigned* h = reinterpret_cast<unsigned*>(cell);
+              atomicAdd(h, (unsigned)(q & 0xfffffull));
+              atomicAdd(h + 1, (unsigned)(q >> 20));
+            } else {
+              atomicAdd(cell, q);
+            }
+          }
         }
       }
     }
-  }
+  };
+  if (split) visits(std::true_type{});
+  else visits(std::false_type{});
   __syncthreads();
   // every cell of the region: a half warp per row, two cells per 16-byte store (e[0] and
   // the pitches are even).  z = row / e[1] through a float reciprocal: (row + 0.5) / e[1]
@@ -679,7 +701,11 @@ __global__ void __launch_bounds__(DEP3_THREADS, 2) k_deposit_pm3_own(Geo G, cons
     const int z = (int)(((float)row + 0.5f) * inv_e1);
     const int y = row - z * e[1];
     if (hl < hx) {
-      const ulonglong2 val = *reinterpret_cast<const ulonglong2*>(&acc[(z * R + y) * R + 2 * hl]);
+      ulonglong2 val = *reinterpret_cast<const ulonglong2*>(&acc[(z * R + y) * R + 2 * hl]);
+      if (split) {
+        val.x = ((val.x >> 32) << 20) + (val.x & 0xffffffffull);
+        val.y = ((val.y >> 32) << 20) + (val.y & 0xffffffffull);
+      }
       __stcs(reinterpret_cast<ulonglong2*>(base + (int64_t)z * pl + (int64_t)y * pr) + hl, val);
     }
   }

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from cube_nu_b200.params import DEPOSIT_FIXED, DEPOSIT_FP32, config_small
-from tests.helpers import clustered_state, lattice_state, uniform_state
+from tests.helpers import clustered_state, lattice_state, state_from_positions, uniform_state
 
 pytestmark = pytest.mark.gpu
 
@@ -116,6 +116,39 @@ def test_density_and_potential(oracle_lib, fixed):
             else:
                 err = np.abs(got - ref).max() / np.abs(ref).max()
                 assert err < 2e-5, "phi rel err %.3g (level %d box %d)" % (err, level, box)
+
+
+def test_pm3_density_dense_blob(oracle_lib):
+    """A blob of 20000 particles (sigma 0.3 coarse cells) puts one subtile in a heavy class
+    (rsf 6, where gridsize is inexact and the deposit takes the FP64 path for every test)
+    and gives its regions more candidate particles than the 32-bit split sums allow (the
+    64-bit shared-memory sums); the fixed-point density of that box and of a neighbour that
+    holds the blob's ghost particles is bit-exact."""
+    p = _params(fixed=True)
+    rng = np.random.default_rng(21)
+    c = np.array([5.4, 9.6, 2.5])  # inside subtile (1, 0, 0) of tile (0, 1, 0)
+    X = np.concatenate([c + rng.normal(size=(20000, 3)) * 0.3, rng.random((6000, 3)) * p.nc])
+    st = state_from_positions(p, X, rng.normal(size=X.shape))
+    p.mass_p_cdm = float(p.ng) ** 3 / X.shape[0]
+    ires, _ = oracle_lib.classify(p, st[3])
+
+    def sub_of(g):
+        t, l = g // p.nt, g % p.nt
+        u = l // (p.nt // p.nns)
+        T = (t[2] * p.nnt + t[1]) * p.nnt + t[0]
+        return int(((T * p.nns + u[2]) * p.nns + u[1]) * p.nns + u[0])
+
+    box = sub_of(np.floor(c).astype(int))
+    nb = sub_of(np.floor(c).astype(int) + np.array([-2, 0, 0]))
+    assert ires[box] >= 4, ires[box]
+    for b in (box, nb):
+        size = p.nft(int(ires[b])) ** 3
+        _, ref = oracle_lib.kick(p, st[0], st[1].copy(), st[3], 0.1, 0.05, fixed=True, debug=(3, b, 0, size))
+        with _ctx(p, st) as ctx:
+            ctx.capture(3, b, 0)
+            ctx.kick(0.1, 0.05)
+            got = ctx.captured(size)
+        assert np.array_equal(got, ref), "fixed-point density differs (box %d class %d)" % (b, int(ires[b]))
 
 
 @pytest.mark.parametrize("izipx,fixed,kind", [(1, False, "lattice"), (2, True, "lattice"), (1, False, "clustered"),
