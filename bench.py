@@ -40,7 +40,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # owner-computes deposit profiles/deposit_pm3_owner_proxy.md).  Traffic grows with the
 # number of boxes, so a launch over B such boxes moves B times these.
 PM3_TRAFFIC_PER_BOX = {
-    "deposit_pm3": 1.4917e9 / 64,
+    "deposit_pm3": (14870016 + 1470362368) / 64,
     "fft_x_pm3": 2.271174e9 / 64,
     "fft_z_green_pm3": 1.910046e9 / 64,
     "fft_c2r_pm3": 1.485638e9 / 64,
