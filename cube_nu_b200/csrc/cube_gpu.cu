@@ -295,18 +295,22 @@ MeshPtrs mesh_ptrs(cube_ctx* c, int n, int64_t, bool fixed) {
   return m;
 }
 
-// The owner-computes PM3 deposit covers a class when every region of DEP3_R^3 cells of
-// its boxes draws on at most DEP3_MAXC coarse cells (same range as dep3_krange).
+// The owner-computes PM3 deposit covers a class when every region of DEP3_R x DEP3_R x
+// DEP3_RZ cells of its boxes draws on at most DEP3_MAXC coarse cells (same range as
+// dep3_krange).
 bool dep3_own_fits(const Geo& G, int iapm) {
   const int nft = G.nft[iapm], nfb = G.nfb[iapm];
   auto fdiv = [](int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); };
-  int mk = 0;
-  for (int o = 0; o < nft; o += DEP3_R) {
-    const int e = std::min(DEP3_R, nft - o);
-    const int klo = std::max(-1, fdiv(o - nfb - 2, nfb)), khi = std::min(G.ntt, fdiv(o + e - nfb + 1, nfb));
-    mk = std::max(mk, khi - klo + 1);
-  }
-  return nfb > 0 && (int64_t)mk * mk * mk <= DEP3_MAXC;
+  auto most = [&](int R) {
+    int mk = 0;
+    for (int o = 0; o < nft; o += R) {
+      const int e = std::min(R, nft - o);
+      const int klo = std::max(-1, fdiv(o - nfb - 2, nfb)), khi = std::min(G.ntt, fdiv(o + e - nfb + 1, nfb));
+      mk = std::max(mk, khi - klo + 1);
+    }
+    return (int64_t)mk;
+  };
+  return nfb > 0 && most(DEP3_R) * most(DEP3_R) * most(DEP3_RZ) <= DEP3_MAXC;
 }
 
 // How many boxes of side n fit in the arena.
@@ -951,12 +955,12 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       const int64_t boxb = (int64_t)n * m.pt.psb;
       if (fixed && dep3_own_fits(G, cl)) {
         // owner-computes deposit: writes every cell, no memset
-        const int nr = (n + DEP3_R - 1) / DEP3_R;
-        const size_t sm = (size_t)DEP3_R * DEP3_R * DEP3_R * 8;
+        const int nr = (n + DEP3_R - 1) / DEP3_R, nrz = (n + DEP3_RZ - 1) / DEP3_RZ;
+        const size_t sm = (size_t)DEP3_R * DEP3_R * DEP3_RZ * 8;
         smem_optin(k_deposit_pm3_own, sm);
-        LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3_own<<<(unsigned)((int64_t)nb * nr * nr * nr), DEP3_THREADS, sm, c->s>>>(
+        LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3_own<<<(unsigned)((int64_t)nb * nr * nr * nrz), DEP3_THREADS, sm, c->s>>>(
                                     G, c->xp, c->cstart, c->box_slot + list_off[k], cl,
-                                    reinterpret_cast<unsigned long long*>(m.real), c->err, m.pt.pr, m.pt.plr, nr, nr, nr));
+                                    reinterpret_cast<unsigned long long*>(m.real), c->err, m.pt.pr, m.pt.plr, nr, nr, nrz));
       } else {
         CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
         if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));

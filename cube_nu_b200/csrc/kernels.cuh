@@ -535,7 +535,7 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
 }
 
 // Owner-computes form of the fixed-point PM3 deposit: one block per region of
-// DEP3_R^3 cells of one box.  The block sums, in shared memory, the contributions of the
+// DEP3_R x DEP3_R x DEP3_RZ cells of one box.  The block sums, in shared memory, the contributions of the
 // particles of every coarse cell whose TSC footprint can reach the region, then writes
 // every cell of the region (zeros included) with plain stores, so the mesh needs no
 // memset and no cell is read back from DRAM.  Particle arithmetic is that of
@@ -543,9 +543,11 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
 // around its subtile, with tile-local coordinate l = u*ntt + k), so the int64 sums are
 // identical.  Requires the int64 layouts (no padding between real rows) and at most
 // DEP3_MAXC candidate coarse cells per region (checked on the host).
-constexpr int DEP3_R = 24;
+constexpr int DEP3_R = 24;   // region extent in x and y (cells)
+constexpr int DEP3_RZ = 24;  // region extent in z
 constexpr int DEP3_MAXC = 125;
 constexpr int DEP3_THREADS = 512;
+constexpr int DEP3_MINB = 2;  // blocks per SM
 constexpr int DEP3_SPLIT_MAX = 4095;
 
 __device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
@@ -559,14 +561,14 @@ __device__ __forceinline__ void dep3_krange(int o, int e, int nfb, int ntt, int&
   nk = khi - klo + 1;
 }
 
-__global__ void __launch_bounds__(DEP3_THREADS, 2) k_deposit_pm3_own(Geo G, const void* __restrict__ xp,
+__global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo G, const void* __restrict__ xp,
                                                                      const int64_t* __restrict__ cstart,
                                                                      const int32_t* __restrict__ box_sub, int iapm,
                                                                      unsigned long long* __restrict__ rho, unsigned* err,
                                                                      int pr, int64_t pl, int nrx, int nry, int nrz) {
-  constexpr int R = DEP3_R;
+  constexpr int R = DEP3_R, RZ = DEP3_RZ;
   static_assert(R % 2 == 0 && R / 2 <= 16, "a half warp writes one region row");
-  extern __shared__ __align__(16) unsigned long long acc[];  // [R][R][R]
+  extern __shared__ __align__(16) unsigned long long acc[];  // [RZ][R][R]
   __shared__ int64_t cst[DEP3_MAXC];
   __shared__ int ccnt[DEP3_MAXC], ckk[DEP3_MAXC], cpre[DEP3_MAXC + 1];
   const int tid = threadIdx.x;
@@ -574,8 +576,8 @@ __global__ void __launch_bounds__(DEP3_THREADS, 2) k_deposit_pm3_own(Geo G, cons
   const int nreg = nrx * nry * nrz;
   const int64_t j = blockIdx.x / nreg;
   const int r = (int)(blockIdx.x - j * nreg);
-  const int o[3] = {(r % nrx) * R, ((r / nrx) % nry) * R, (r / (nrx * nry)) * R};
-  const int e[3] = {min(R, nft - o[0]), min(R, nft - o[1]), min(R, nft - o[2])};
+  const int o[3] = {(r % nrx) * R, ((r / nrx) % nry) * R, (r / (nrx * nry)) * RZ};
+  const int e[3] = {min(R, nft - o[0]), min(R, nft - o[1]), min(RZ, nft - o[2])};
   // subtile of this box
   const int s = box_sub[j];
   const int nns3 = G.nns * G.nns * G.nns;
@@ -602,7 +604,7 @@ __global__ void __launch_bounds__(DEP3_THREADS, 2) k_deposit_pm3_own(Geo G, cons
   }
   {
     ulonglong2* a2 = reinterpret_cast<ulonglong2*>(acc);
-    for (int i = tid; i < R * R * R / 2; i += blockDim.x) a2[i] = make_ulonglong2(0ull, 0ull);
+    for (int i = tid; i < R * R * RZ / 2; i += blockDim.x) a2[i] = make_ulonglong2(0ull, 0ull);
   }
   __syncthreads();
   if (tid < 32) {  // prefix of the counts
