@@ -346,20 +346,18 @@ def main():
     vh[...] = cur[1]
     ph[...] = cur[2]
     rh[...] = cur[3]
-    from cube_nu_b200._lib import _check, _ptr
-    import ctypes
-
-    lib = ctx._lib
-    nplocal = ctypes.c_int64()
     e2e_steps = args.steps
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t_e2e = time.perf_counter()
     for _ in range(e2e_steps):
-        _check(lib.cube_gpu_upload(ctx._h, _ptr(xh), _ptr(vh), _ptr(ph), _ptr(rh), n), "upload")
-        one_step()
-        _check(lib.cube_gpu_download(ctx._h, _ptr(xh), _ptr(vh), _ptr(ph), _ptr(rh), ctypes.byref(nplocal)), "download")
+        # host-resident state: cube_gpu_step_host uploads it from the pinned arrays, steps,
+        # and writes the new state back (copies the step does not wait for overlap it)
+        cosmology.timestep(bg, S, zck)
+        so = ctx.step_host(xh, vh, ph, rh, S.dt, S.dt_old, S.a_mid, S.vz_max)
+        S.dt_pm1, S.dt_pm2, S.dt_pm3, S.dt_pp, S.dt_vmax = so.dt_pm1, so.dt_pm2, so.dt_pm3, so.dt_pp, so.dt_vmax
+        S.vz_max = so.vz_max
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t_e2e
     t_e2e = over_ranks([t_e2e], "max", dist)[0]

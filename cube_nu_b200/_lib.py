@@ -21,7 +21,7 @@ EXPORTS = (
     "cube_gpu_green_table", "cube_gpu_subtile_class", "cube_gpu_last_error", "cube_gpu_version",
     "cube_gpu_profile", "cube_gpu_profile_read", "cube_gpu_profile_name", "cube_gpu_kernel_launches",
     "cube_gpu_zipv_encode", "cube_gpu_zipv_decode", "cube_gpu_download_zipv", "cube_gpu_ic", "cube_gpu_power",
-    "cube_gpu_int2real",
+    "cube_gpu_int2real", "cube_gpu_step_host",
 )
 
 
@@ -103,6 +103,8 @@ def load():
     L.cube_gpu_download_zipv.argtypes = [vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_float]
     L.cube_gpu_power.argtypes = [vp, ctypes.POINTER(PowerIn), vp, ctypes.c_int64, vp, ctypes.POINTER(PowerOut)]
     L.cube_gpu_int2real.argtypes = [vp, vp, ctypes.c_int64]
+    L.cube_gpu_step_host.argtypes = [vp, ctypes.POINTER(StepIn), ctypes.POINTER(StepOut), vp, vp, vp, vp,
+                                     ctypes.c_int64]
     _LIB = L
     return L
 
@@ -187,6 +189,19 @@ class Context:
         si = StepIn(dt, dt_old, a_mid, vz_max)
         so = StepOut()
         _check(self._lib.cube_gpu_step(self._h, ctypes.byref(si), ctypes.byref(so)), "cube_gpu_step")
+        return so
+
+    def step_host(self, xp: np.ndarray, vp: np.ndarray, pid: np.ndarray, rhoc: np.ndarray, dt: float,
+                  dt_old: float, a_mid: float, vz_max: float) -> StepOut:
+        """One step on a host-resident state: the four arrays are uploaded, stepped and
+        overwritten with the new state (cube_gpu_step_host)."""
+        for a in (xp, vp, pid, rhoc):
+            if not a.flags.c_contiguous:
+                raise ValueError("step_host needs C-contiguous arrays")
+        si = StepIn(dt, dt_old, a_mid, vz_max)
+        so = StepOut()
+        _check(self._lib.cube_gpu_step_host(self._h, ctypes.byref(si), ctypes.byref(so), _ptr(xp), _ptr(vp),
+                                            _ptr(pid), _ptr(rhoc), ctypes.c_int64(xp.shape[0])), "cube_gpu_step_host")
         return so
 
     def capture(self, level: int, box: int, what: int) -> None:

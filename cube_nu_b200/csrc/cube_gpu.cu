@@ -117,6 +117,9 @@ struct cube_ctx {
   int64_t cap_n = 0;
   // timing
   cudaEvent_t ev[8];
+  // side stream of cube_gpu_step_host (copies that overlap the step), created at first use
+  cudaStream_t s2 = nullptr;
+  cudaEvent_t ev_ids = nullptr, ev_drift = nullptr;
   // 1: use the generic Stockham passes for every size (CUBE_FFT_GENERIC=1)
   int fft_generic = 0;
   // 1: fused plane FFT kernels for sides <= 144 (CUBE_FFT_FUSED, default 1)
@@ -696,6 +699,10 @@ int cube_gpu_destroy(cube_ctx* c) {
   for (int i = 0; i < 8; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
+  if (c->s2) cudaStreamSynchronize(c->s2);
+  if (c->ev_ids) cudaEventDestroy(c->ev_ids);
+  if (c->ev_drift) cudaEventDestroy(c->ev_drift);
+  if (c->s2) cudaStreamDestroy(c->s2);
   if (c->s) cudaStreamDestroy(c->s);
   delete c;
   return 0;
@@ -793,8 +800,10 @@ static int check_err(cube_ctx* c) {
   return 0;
 }
 
-// drift.f90.  Enqueues the drift; returns after the error word is checked.
-static int drift_enqueue(cube_ctx* c, const cube_step_in* in) {
+// drift.f90.  Enqueues the drift; returns after the error word is checked.  When
+// `ids_ready` is given, the gather (the first kernel that reads the particle ids) waits
+// for it, so the ids may still be in flight from the host while the rest runs.
+static int drift_enqueue(cube_ctx* c, const cube_step_in* in, cudaEvent_t ids_ready = nullptr) {
   const Geo& G = c->G;
   const float dt_mid = (in->dt_old + in->dt) / 2.f;
   const int nlayer = 2 * (int)std::ceil(dt_mid * in->vz_max / (float)G.rcs) + 2;
@@ -817,6 +826,7 @@ static int drift_enqueue(cube_ctx* c, const cube_step_in* in) {
   if (nb_host > 0)
     LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nb_host, 512, (size_t)max_seg * 12, c->s>>>(c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey,
                                                                     c->ssrc, max_seg, c->err));
+  if (ids_ready) CK(cudaStreamWaitEvent(c->s, ids_ready, 0));
   LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp, c->pid, dt_mid, c->xp2, c->vp2,
                                              c->pid2, c->pcell2));
   CK(cudaGetLastError());
@@ -1054,6 +1064,80 @@ int cube_gpu_step(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     out->tcat[5] += ms;
     cudaEventElapsedTime(&ms, c->ev[5], c->ev[7]);
     out->tcat[6] = ms;  // whole step on the device, host gaps included
+  }
+  return rc;
+}
+
+// One step on a host-resident particle state: upload, drift, kick, download, with the
+// copies that the step does not wait for moved onto a side stream.  The ids go up beside
+// the drift's first kernels (only its gather reads them); the drift's outputs (positions,
+// ids, cell counts) come down while the kick runs (the kick only reads them); the
+// velocities come down after the kick.  Same results as cube_gpu_upload +
+// cube_gpu_step + cube_gpu_download on the same arrays.
+int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, void* xp, float* vp, int64_t* pid,
+                       int32_t* rhoc, int64_t nplocal) {
+  if (!c || !in || !xp || !vp || !pid || !rhoc || nplocal <= 0) return fail(CUBE_E_ARG, "bad step_host arguments");
+  CK(cudaSetDevice(c->device));
+  const Geo& G = c->G;
+  if (!c->s2) {
+    CK(cudaStreamCreateWithFlags(&c->s2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_ids, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_drift, cudaEventDisableTiming));
+  }
+  // the copies the host arrays still feed must be done before the arrays are checked
+  // or reused by a failed call
+  auto drain = [&]() {
+    cudaStreamSynchronize(c->s2);
+    cudaStreamSynchronize(c->s);
+  };
+  int rc = alloc_particles(c, nplocal);
+  if (rc) return rc;
+  c->np = nplocal;
+  c->loaded = false;
+  CK(cudaMemcpyAsync(c->rhoc, rhoc, (size_t)G.ncells * 4, cudaMemcpyHostToDevice, c->s));
+  CK(cudaMemcpyAsync(c->xp, xp, (size_t)nplocal * 3 * c->xbytes, cudaMemcpyHostToDevice, c->s));
+  CK(cudaMemcpyAsync(c->vp, vp, (size_t)nplocal * 12, cudaMemcpyHostToDevice, c->s));
+  CK(cudaMemcpyAsync(c->pid, pid, (size_t)nplocal * 8, cudaMemcpyHostToDevice, c->s2));
+  CK(cudaEventRecord(c->ev_ids, c->s2));
+  // the cell counts are validated on the host while the copies run
+  int64_t sum = 0;
+  bool neg = false;
+  for (int64_t i = 0; i < G.ncells; ++i) {
+    neg |= rhoc[i] < 0;
+    sum += rhoc[i];
+  }
+  if (neg || sum != nplocal) {
+    drain();
+    return neg ? fail(CUBE_E_ARG, "negative rhoc") : fail(CUBE_E_COUNT, "sum(rhoc) != nplocal");
+  }
+  LAUNCH(c, K_SCAN, 3, exclusive_scan(c->rhoc, c->cstart, G.ncells, c->scan_tmp, c->s));
+  LAUNCH(c, K_FILL, 1, k_fill_pcell<<<nblk(G.ncells), 256, 0, c->s>>>(c->cstart, G.ncells, c->pcell));
+  CK(cudaGetLastError());
+  c->loaded = true;
+  CK(cudaEventRecord(c->ev[5], c->s));
+  rc = drift_enqueue(c, in, c->ev_ids);
+  if (rc) {
+    drain();
+    return rc;
+  }
+  CK(cudaEventRecord(c->ev[6], c->s));
+  CK(cudaEventRecord(c->ev_drift, c->s));
+  CK(cudaStreamWaitEvent(c->s2, c->ev_drift, 0));
+  CK(cudaMemcpyAsync(xp, c->xp, (size_t)c->np * 3 * c->xbytes, cudaMemcpyDeviceToHost, c->s2));
+  CK(cudaMemcpyAsync(pid, c->pid, (size_t)c->np * 8, cudaMemcpyDeviceToHost, c->s2));
+  CK(cudaMemcpyAsync(rhoc, c->rhoc, (size_t)G.ncells * 4, cudaMemcpyDeviceToHost, c->s2));
+  rc = cube_gpu_kick(c, in, out);
+  CK(cudaEventRecord(c->ev[7], c->s));
+  if (!rc) CK(cudaMemcpyAsync(vp, c->vp, (size_t)c->np * 12, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  CK(cudaStreamSynchronize(c->s2));
+  if (!rc && out) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]);
+    out->tcat[0] = ms;
+    out->tcat[5] += ms;
+    cudaEventElapsedTime(&ms, c->ev[5], c->ev[7]);
+    out->tcat[6] = ms;
   }
   return rc;
 }

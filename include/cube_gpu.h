@@ -190,6 +190,16 @@ int cube_gpu_drift(cube_ctx* ctx, const cube_step_in* in);
 int cube_gpu_kick(cube_ctx* ctx, const cube_step_in* in, cube_step_out* out);
 /* One loop body of main.f90:36-38 (drift, ghosts, kick, ghosts). */
 int cube_gpu_step(cube_ctx* ctx, const cube_step_in* in, cube_step_out* out);
+/* The same step for a caller whose particle state lives in host memory, as the
+ * reference's arrays xp, vp, PID, rhoc do between iterations of main.f90:30-59: uploads
+ * the state from the four arrays (`nplocal` particles, checked as in cube_gpu_upload),
+ * steps, and writes the new state back into the same arrays.  Equal to cube_gpu_upload +
+ * cube_gpu_step + cube_gpu_download on those arrays; the copies the step does not wait
+ * for overlap it (ids go up beside the drift's first kernels, positions, ids and counts
+ * come down during the kick), which needs page-locked arrays.  After a failed call the
+ * context holds no particles. */
+int cube_gpu_step_host(cube_ctx* ctx, const cube_step_in* in, cube_step_out* out, void* xp, float* vp,
+                       int64_t* pid, int32_t* rhoc, int64_t nplocal);
 
 /* Inspection for tests.  cube_gpu_capture arms a capture: during the next kick the
  * field `what` (0: density = deposited mass per cell, 1: potential phi after the
