@@ -883,7 +883,16 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     launch_fft(c, n, 1, m.real, fixed, G.mass_p, phi, m.ck, c->green1, (float)n, 3, 1);
     maybe_capture(c, 1, 0, 1, phi, n, false, (int64_t)m.pt.pf * 4, m.pt.psb);
     LAUNCH(c, K_F2_PM1, 1, k_f2max_periodic<<<(unsigned)std::min<int64_t>(1184, (int64_t)n * n / 8 + 1), 256, 0, c->s>>>(phi, n, f2 + 0, m.pt.pf, m.pt.plf));
-    LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, a_mid, dt, m.pt.pf, m.pt.plf));
+    // force mesh (float4 per coarse cell) in the arena after phi, when it fits
+    const size_t foff = (mesh_bytes(c, n, 1, fixed) + 255) & ~(size_t)255;
+    const int64_t n3 = (int64_t)n * n * n;
+    if (foff + (size_t)n3 * sizeof(float4) <= c->arena_bytes) {
+      float4* force = reinterpret_cast<float4*>(reinterpret_cast<char*>(c->arena) + foff);
+      LAUNCH(c, K_INT_PM1, 1, k_force_pm1<<<nblk(n3), 256, 0, c->s>>>(n, phi, m.pt.pf, m.pt.plf, force));
+      LAUNCH(c, K_INT_PM1, 1, k_interp_pm1_force<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, force, c->vp, a_mid, dt));
+    } else {
+      LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, a_mid, dt, m.pt.pf, m.pt.plf));
+    }
   }
   CK(cudaEventRecord(c->ev[1], c->s));
   // ---------------- PM2 (kick.f90:47-77) ----------------

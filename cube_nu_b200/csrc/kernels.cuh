@@ -989,6 +989,66 @@ __global__ void k_interp_pm1(Geo G, int64_t np, const void* __restrict__ xp, con
   apply_kick(vp, ip, dv, a_mid, dt, av);
 }
 
+// PM1 force mesh, as potential_to_force builds it before the interpolation
+// (particle_mesh.f90:224-247): at every coarse cell j (0-based, periodic) the three
+// components grad4(phi(j-2), phi(j-1), phi(j+1), phi(j+2)), with the same FP32
+// operations as tsc_gather_force, stored as float4 (fx, fy, fz, 0), x fastest.
+__global__ void k_force_pm1(int nc, const float* __restrict__ phi, int pf, int64_t pl, float4* __restrict__ force) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n3 = (int64_t)nc * nc * nc;
+  if (i >= n3) return;
+  const int x = (int)(i % nc), y = (int)((i / nc) % nc), z = (int)(i / ((int64_t)nc * nc));
+  const int64_t row = (int64_t)z * pl + (int64_t)y * pf, xl = (int64_t)z * pl + x;
+  const float* ph = phi;
+  auto X = [&](int d) { return __ldg(&ph[row + wrapi(x + d, nc)]); };
+  auto Y = [&](int d) { return __ldg(&ph[xl + (int64_t)wrapi(y + d, nc) * pf]); };
+  auto Z = [&](int d) { return __ldg(&ph[(int64_t)wrapi(z + d, nc) * pl + (int64_t)y * pf + x]); };
+  force[i] = make_float4(grad4(X(-2), X(-1), X(1), X(2)), grad4(Y(-2), Y(-1), Y(1), Y(2)),
+                         grad4(Z(-2), Z(-1), Z(1), Z(2)), 0.f);
+}
+
+// PM1 interpolation + kick from the force mesh: the 27 TSC points of a particle are the
+// cells fl-1..fl+1 around its coarse cell; each component is summed in the order of
+// tsc_gather_force (a3 outer, a2, a1 inner) with the same products, so the result is
+// bit-identical to differencing phi on the fly.
+__global__ void k_interp_pm1_force(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
+                                   const float4* __restrict__ force, float* __restrict__ vp, float a_mid, float dt) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= np) return;
+  int g[3];
+  cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+  int i2[3];
+  float w[3][3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double xpos = (double)g[d] + zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
+    i2[d] = tsc_weights(xpos, w[d]);
+  }
+  const int nc = G.nc;
+  int64_t jx[3], jy[3], jz[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    jx[a] = wrapi(i2[0] - 2 + a, nc);
+    jy[a] = (int64_t)wrapi(i2[1] - 2 + a, nc) * nc;
+    jz[a] = (int64_t)wrapi(i2[2] - 2 + a, nc) * nc * nc;
+  }
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+  for (int a3 = 0; a3 < 3; ++a3)
+#pragma unroll
+    for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+      for (int a1 = 0; a1 < 3; ++a1) {
+        const float4 F = __ldg(&force[jz[a3] + jy[a2] + jx[a1]]);
+        sx = __fadd_rn(sx, __fmul_rn(__fmul_rn(__fmul_rn(F.x, w[0][a1]), w[1][a2]), w[2][a3]));
+        sy = __fadd_rn(sy, __fmul_rn(__fmul_rn(__fmul_rn(F.y, w[0][a1]), w[1][a2]), w[2][a3]));
+        sz = __fadd_rn(sz, __fmul_rn(__fmul_rn(__fmul_rn(F.z, w[0][a1]), w[1][a2]), w[2][a3]));
+      }
+  const float dv[3] = {sx, sy, sz};
+  float av[3];
+  apply_kick(vp, ip, dv, a_mid, dt, av);
+}
+
 __global__ void __launch_bounds__(256, 3) k_interp_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                              const float* __restrict__ phi, int tile0, int ntile, float* __restrict__ vp, float a_mid,
                              float dt, float* vmax, unsigned* err, int pf, int64_t pl) {
