@@ -876,7 +876,9 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     const int n = G.nc;
     MeshPtrs m = mesh_ptrs(c, n, 1, fixed);
     CK(cudaMemsetAsync(m.real, 0, mesh_bytes(c, n, 1, fixed), c->s));
-    if (fixed) LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr, m.pt.plr));
+    if (fixed)
+      LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1_runs<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell,
+                                                                     reinterpret_cast<unsigned long long*>(m.real), m.pt.pr, m.pt.plr));
     else LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr, m.pt.plr));
     maybe_capture(c, 1, 0, 0, m.real, n, fixed, m.pt.rp, m.pt.psb);
     float* phi = reinterpret_cast<float*>(m.real);

@@ -355,6 +355,68 @@ __global__ void __launch_bounds__(256, 6) k_deposit_pm1(Geo G, int64_t np, const
   }
 }
 
+// Fixed-point PM1 deposit with the sums of a coarse cell's particles combined in the warp
+// first.  A particle of coarse cell g has floor(xpos) = g, so every particle of the cell
+// deposits into the same 27 cells; particles are stored cell by cell, so the lanes of a
+// warp form runs of equal cells.  For each of the 27 cells the int64 contributions are
+// summed over each run (a segmented suffix sum by shuffles) and the run's first lane
+// adds the sum with one reduction: about one reduction per cell and run instead of one
+// per particle.  Integer sums do not depend on the order, so the density is the one of
+// k_deposit_pm1<true>.
+__global__ void __launch_bounds__(256) k_deposit_pm1_runs(Geo G, int64_t np, const void* __restrict__ xp,
+                                                          const int32_t* __restrict__ pcell,
+                                                          unsigned long long* __restrict__ rho, int pr, int64_t pl) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  if ((ip - lane) >= np) return;  // warp-uniform: no live lane in this warp
+  const bool live = ip < np;
+  const int cell = live ? pcell[ip] : -1 - lane;  // dead lanes form runs of their own
+  // run structure: same[k] = lane + 2^k is in this lane's run
+  unsigned samebits = 0;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const int off = 1 << k;
+    const int other = __shfl_down_sync(0xffffffffu, cell, off);
+    if (lane + off < 32 && other == cell) samebits |= 1u << k;
+  }
+  const int prev = __shfl_up_sync(0xffffffffu, cell, 1);
+  const bool head = live && (lane == 0 || prev != cell);
+  // the longest run decides how many doubling steps are needed
+  const unsigned need8 = __ballot_sync(0xffffffffu, samebits & 8u), need16 = __ballot_sync(0xffffffffu, samebits & 16u);
+  int g[3] = {0, 0, 0};
+  float w[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+  if (live) {
+    cell_coords(G, cell, g[0], g[1], g[2]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double xpos = (double)g[d] + zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
+      tsc_weights(xpos, w[d]);  // floor(xpos) = g
+    }
+  }
+  const int nc = G.nc;
+#pragma unroll
+  for (int a3 = 0; a3 < 3; ++a3) {
+    const int64_t z = (int64_t)wrapi(g[2] - 1 + a3, nc) * pl;
+#pragma unroll
+    for (int a2 = 0; a2 < 3; ++a2) {
+      const int64_t y = (int64_t)wrapi(g[1] - 1 + a2, nc) * pr;
+#pragma unroll
+      for (int a1 = 0; a1 < 3; ++a1) {
+        const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
+        unsigned long long q = live ? (unsigned long long)__float2ll_rn(__fmul_rn(ww, FIXED_SCALE)) : 0ull;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          if (k == 3 && !need8) continue;
+          if (k == 4 && !need16) continue;
+          const unsigned long long o = __shfl_down_sync(0xffffffffu, q, 1 << k);
+          if (samebits & (1u << k)) q += o;
+        }
+        if (head) atomicAdd(rho + z + y + wrapi(g[0] - 1 + a1, nc), q);
+      }
+    }
+  }
+}
+
 // Candidate tiles along one dimension for a particle with global cell g: its own tile
 // and, within ncb of a tile face, the neighbour whose ghost region holds it.
 // Writes (tile, local coordinate i-1 in that tile) pairs; returns the count (1 or 2).
