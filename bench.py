@@ -40,8 +40,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # owner-computes deposit profiles/deposit_pm3_owner_proxy.md).  Traffic grows with the
 # number of boxes, so a launch over B such boxes moves B times these.
 PM3_TRAFFIC_PER_BOX = {
-    "deposit_pm3": (14870016 + 1470362368) / 64,
-    "fft_x_pm3": 2.271174e9 / 64,
+    "deposit_pm3": (15048960 + 707247360) / 64,
     "fft_z_green_pm3": 1.910046e9 / 64,
     "fft_c2r_pm3": 1.485638e9 / 64,
 }
@@ -148,7 +147,7 @@ def kernel_bytes(p, name: str, n_particles: int, napm, fixed: bool):
     bx = 3 * p.izipx
     rb = 8 if fixed else 4
 
-    def mesh(n, nbox, what):
+    def mesh(n, nbox, what, rb=rb):
         n3 = n ** 3 * nbox
         nh = n * n * (n // 2 + 1) * nbox
         return {"x": n3 * rb + nh * 8, "y": 2 * nh * 8, "z": 2 * nh * 8 + n * n * (n // 2 + 1) * 4,
@@ -159,15 +158,17 @@ def kernel_bytes(p, name: str, n_particles: int, napm, fixed: bool):
         n = p.nft(2)
         nb = int(napm[2]) if napm is not None else p.ns3
         what = {"fft_x_pm3": "x", "fft_y_pm3": "y", "fft_z_green_pm3": "z", "fft_c2r_pm3": "c"}[name]
-        return mesh(n, nb, what) * (2 if what == "y" else 1)
+        # the PM3 mesh is float in both deposit forms (the owner-computes fixed-point
+        # deposit writes the converted sums)
+        return mesh(n, nb, what, rb=4) * (2 if what == "y" else 1)
     if name.startswith("fft_") and name.endswith("_pm2"):
         what = {"fft_x_pm2": "x", "fft_y_pm2": "y", "fft_z_green_pm2": "z", "fft_c2r_pm2": "c"}[name]
         return mesh(p.ngt, p.ntiles, what) * (2 if what == "y" else 1)
     if name == "deposit_pm3" and fixed:
-        # owner-computes form: every cell of every box written once (no memset, no
-        # read-back), each particle's position code read once
+        # owner-computes form: every cell of every box written once as float (no memset,
+        # no read-back), each particle's position code read once
         nbs = napm if napm is not None else [0, 0, p.ns3, 0, 0, 0]
-        return int(sum(int(nbs[c]) * p.nft(c) ** 3 * 8 for c in range(2, 6)) + n_particles * bx)
+        return int(sum(int(nbs[c]) * p.nft(c) ** 3 * 4 for c in range(2, 6)) + n_particles * bx)
     if name in ("deposit_pm1", "deposit_pm2", "deposit_pm3"):
         # read position code + cell index per particle, one read-modify-write of 27 cells
         boxes = {"deposit_pm1": 1.0, "deposit_pm2": (1 + 2 * p.ncb / p.nt) ** 3, "deposit_pm3": (1 + 2 / p.ntt) ** 3}[name]

@@ -937,7 +937,10 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     for (int s = 0; s < c->ns3; ++s) lists[ires[s]].push_back(s);
     for (int cl = 2; cl <= 5; ++cl) {
       if (lists[cl].empty()) continue;
-      const int64_t per = std::min<int64_t>((int64_t)lists[cl].size(), boxes_fit(c, G.nft[cl], fixed));
+      // int64 mesh layout only where the particle-major fixed-point deposit runs; the
+      // owner-computes deposit writes floats
+      const bool lint = fixed && !dep3_own_fits(G, cl);
+      const int64_t per = std::min<int64_t>((int64_t)lists[cl].size(), boxes_fit(c, G.nft[cl], lint));
       for (int64_t f = 0; f < (int64_t)lists[cl].size(); f += per)
         chunks.push_back({cl, f, (int)std::min<int64_t>(per, (int64_t)lists[cl].size() - f)});
     }
@@ -972,16 +975,18 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       const float* g3 = green3(c, cl);
       if (!g3) return CUBE_E_CUDA;
       const int32_t* slots = c->box_slot + k * c->ns3;
-      MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
+      const bool own = fixed && dep3_own_fits(G, cl);
+      const bool lint = fixed && !own;  // int64 mesh layout
+      MeshPtrs m = mesh_ptrs(c, n, nb, lint);
       const int64_t boxb = (int64_t)n * m.pt.psb;
-      if (fixed && dep3_own_fits(G, cl)) {
-        // owner-computes deposit: writes every cell, no memset
+      if (own) {
+        // owner-computes deposit: writes every cell (as float), no memset
         const int nr = (n + DEP3_R - 1) / DEP3_R, nrz = (n + DEP3_RZ - 1) / DEP3_RZ;
         const size_t sm = (size_t)DEP3_R * DEP3_R * DEP3_RZ * 8;
         smem_optin(k_deposit_pm3_own, sm);
         LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3_own<<<(unsigned)((int64_t)nb * nr * nr * nrz), DEP3_THREADS, sm, c->s>>>(
                                     G, c->xp, c->cstart, c->box_slot + list_off[k], cl,
-                                    reinterpret_cast<unsigned long long*>(m.real), c->err, m.pt.pr, m.pt.plr, nr, nr, nrz));
+                                    reinterpret_cast<float*>(m.real), c->err, m.pt.pr, m.pt.plr, nr, nr, nrz));
       } else {
         CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
         if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));
@@ -990,9 +995,9 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       int cap_slot = -1;
       if (c->cap_level == 3 && c->cap_box >= 0 && c->cap_box < c->ns3 && ires[c->cap_box] == cl)
         cap_slot = c->h_slots[k * c->ns3 + c->cap_box];
-      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 0, (char*)m.real + cap_slot * boxb, n, fixed, m.pt.rp, m.pt.psb);
+      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 0, (char*)m.real + cap_slot * boxb, n, lint, m.pt.rp, m.pt.psb);
       float* phi = reinterpret_cast<float*>(m.real);
-      launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, g3, (float)n * (float)n * (float)n, 1, 3);
+      launch_fft(c, n, nb, m.real, lint, G.mass_p, phi, m.ck, g3, (float)n * (float)n * (float)n, 1, 3);
       if (cap_slot >= 0)
         maybe_capture(c, 3, c->cap_box, 1, (char*)m.real + cap_slot * boxb, n, false, (int64_t)m.pt.pf * 4, m.pt.psb);
       const int nf = G.nfp[cl];

@@ -600,11 +600,14 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
 // DEP3_R x DEP3_R x DEP3_RZ cells of one box.  The block sums, in shared memory, the contributions of the
 // particles of every coarse cell whose TSC footprint can reach the region, then writes
 // every cell of the region (zeros included) with plain stores, so the mesh needs no
-// memset and no cell is read back from DRAM.  Particle arithmetic is that of
+// memset and no cell is read back from DRAM.  Cells are written as the float the forward
+// FFT would convert the int64 sum to, (float)(q * 2^-40) (unscaled; the FFT multiplies by
+// the particle mass), into the float mesh layout: half the bytes of the int64 mesh, and
+// the FFT input is bit-identical.  Particle arithmetic is that of
 // k_deposit_pm3 (a box's candidate particles are those of coarse cells k = -1..ntt
 // around its subtile, with tile-local coordinate l = u*ntt + k), so the int64 sums are
-// identical.  Requires the int64 layouts (no padding between real rows) and at most
-// DEP3_MAXC candidate coarse cells per region (checked on the host).
+// identical.  Requires at most DEP3_MAXC candidate coarse cells per region (checked on
+// the host); the padding of the float layouts is left alone (the FFT never reads it).
 constexpr int DEP3_R = 24;   // region extent in x and y (cells)
 constexpr int DEP3_RZ = 24;  // region extent in z
 constexpr int DEP3_MAXC = 125;
@@ -626,7 +629,7 @@ __device__ __forceinline__ void dep3_krange(int o, int e, int nfb, int ntt, int&
 __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo G, const void* __restrict__ xp,
                                                                      const int64_t* __restrict__ cstart,
                                                                      const int32_t* __restrict__ box_sub, int iapm,
-                                                                     unsigned long long* __restrict__ rho, unsigned* err,
+                                                                     float* __restrict__ rho, unsigned* err,
                                                                      int pr, int64_t pl, int nrx, int nry, int nrz) {
   constexpr int R = DEP3_R, RZ = DEP3_RZ;
   static_assert(R % 2 == 0 && R / 2 <= 16, "a half warp writes one region row");
@@ -755,10 +758,10 @@ __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo
   if (split) visits(std::true_type{});
   else visits(std::false_type{});
   __syncthreads();
-  // every cell of the region: a half warp per row, two cells per 16-byte store (e[0] and
+  // every cell of the region: a half warp per row, two cells per 8-byte store (e[0] and
   // the pitches are even).  z = row / e[1] through a float reciprocal: (row + 0.5) / e[1]
   // is at least 0.5/e[1] from an integer, far above the rounding error for row < R*R.
-  unsigned long long* base = rho + j * (int64_t)nft * pl + (int64_t)o[2] * pl + (int64_t)o[1] * pr + o[0];
+  float* base = rho + j * (int64_t)nft * pl + (int64_t)o[2] * pl + (int64_t)o[1] * pr + o[0];
   const int hx = e[0] >> 1, nrow = e[1] * e[2], hl = tid & 15;
   const float inv_e1 = 1.f / (float)e[1];
   for (int row = tid >> 4; row < nrow; row += blockDim.x >> 4) {
@@ -770,7 +773,9 @@ __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo
         val.x = ((val.x >> 32) << 20) + (val.x & 0xffffffffull);
         val.y = ((val.y >> 32) << 20) + (val.y & 0xffffffffull);
       }
-      __stcs(reinterpret_cast<ulonglong2*>(base + (int64_t)z * pl + (int64_t)y * pr) + hl, val);
+      const float2 fv = make_float2((float)((double)(long long)val.x * 9.094947017729282e-13),  // 2^-40
+                                    (float)((double)(long long)val.y * 9.094947017729282e-13));
+      __stcs(reinterpret_cast<float2*>(base + (int64_t)z * pl + (int64_t)y * pr) + hl, fv);
     }
   }
 }
