@@ -119,7 +119,7 @@ struct cube_ctx {
   cudaEvent_t ev[8];
   // side stream of cube_gpu_step_host (copies that overlap the step), created at first use
   cudaStream_t s2 = nullptr;
-  cudaEvent_t ev_ids = nullptr, ev_drift = nullptr;
+  cudaEvent_t ev_up = nullptr, ev_drift = nullptr;
   // 1: use the generic Stockham passes for every size (CUBE_FFT_GENERIC=1)
   int fft_generic = 0;
   // 1: fused plane FFT kernels for sides <= 144 (CUBE_FFT_FUSED, default 1)
@@ -700,7 +700,7 @@ int cube_gpu_destroy(cube_ctx* c) {
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
   if (c->s2) cudaStreamSynchronize(c->s2);
-  if (c->ev_ids) cudaEventDestroy(c->ev_ids);
+  if (c->ev_up) cudaEventDestroy(c->ev_up);
   if (c->ev_drift) cudaEventDestroy(c->ev_drift);
   if (c->s2) cudaStreamDestroy(c->s2);
   if (c->s) cudaStreamDestroy(c->s);
@@ -800,10 +800,11 @@ static int check_err(cube_ctx* c) {
   return 0;
 }
 
-// drift.f90.  Enqueues the drift; returns after the error word is checked.  When
-// `ids_ready` is given, the gather (the first kernel that reads the particle ids) waits
-// for it, so the ids may still be in flight from the host while the rest runs.
-static int drift_enqueue(cube_ctx* c, const cube_step_in* in, cudaEvent_t ids_ready = nullptr) {
+// drift.f90.  Enqueues the drift; returns after the error word is checked.  With
+// `defer_ids` the gather leaves the particle ids alone (the new id array is not written):
+// the caller applies the drift's permutation (c->ssrc) to them later with k_permute_ids,
+// from c->pid2 (the ids before the drift) into c->pid.
+static int drift_enqueue(cube_ctx* c, const cube_step_in* in, bool defer_ids = false) {
   const Geo& G = c->G;
   const float dt_mid = (in->dt_old + in->dt) / 2.f;
   const int nlayer = 2 * (int)std::ceil(dt_mid * in->vz_max / (float)G.rcs) + 2;
@@ -826,8 +827,8 @@ static int drift_enqueue(cube_ctx* c, const cube_step_in* in, cudaEvent_t ids_re
   if (nb_host > 0)
     LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nb_host, 512, (size_t)max_seg * 12, c->s>>>(c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey,
                                                                     c->ssrc, max_seg, c->err));
-  if (ids_ready) CK(cudaStreamWaitEvent(c->s, ids_ready, 0));
-  LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp, c->pid, dt_mid, c->xp2, c->vp2,
+  LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp,
+                                                                        defer_ids ? nullptr : c->pid, dt_mid, c->xp2, c->vp2,
                                              c->pid2, c->pcell2));
   CK(cudaGetLastError());
   int rc = check_err(c);
@@ -1085,11 +1086,13 @@ int cube_gpu_step(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
 }
 
 // One step on a host-resident particle state: upload, drift, kick, download, with the
-// copies that the step does not wait for moved onto a side stream.  The ids go up beside
-// the drift's first kernels (only its gather reads them); the drift's outputs (positions,
-// ids, cell counts) come down while the kick runs (the kick only reads them); the
-// velocities come down after the kick.  Same results as cube_gpu_upload +
-// cube_gpu_step + cube_gpu_download on the same arrays.
+// copies that the step does not wait for moved onto a side stream.  Positions,
+// velocities and cell counts go up first; the ids follow on the side stream while the
+// drift runs (its gather leaves them alone) and are put in the drift's order there by
+// k_permute_ids; the drift's outputs (positions, ids, cell counts) come down on that
+// stream during the kick, which only reads them; the velocities come down after the
+// kick.  Same results as cube_gpu_upload + cube_gpu_step + cube_gpu_download on the
+// same arrays.
 int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, void* xp, float* vp, int64_t* pid,
                        int32_t* rhoc, int64_t nplocal) {
   if (!c || !in || !xp || !vp || !pid || !rhoc || nplocal <= 0) return fail(CUBE_E_ARG, "bad step_host arguments");
@@ -1097,7 +1100,7 @@ int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, 
   const Geo& G = c->G;
   if (!c->s2) {
     CK(cudaStreamCreateWithFlags(&c->s2, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&c->ev_ids, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_up, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&c->ev_drift, cudaEventDisableTiming));
   }
   // the copies the host arrays still feed must be done before the arrays are checked
@@ -1113,8 +1116,11 @@ int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, 
   CK(cudaMemcpyAsync(c->rhoc, rhoc, (size_t)G.ncells * 4, cudaMemcpyHostToDevice, c->s));
   CK(cudaMemcpyAsync(c->xp, xp, (size_t)nplocal * 3 * c->xbytes, cudaMemcpyHostToDevice, c->s));
   CK(cudaMemcpyAsync(c->vp, vp, (size_t)nplocal * 12, cudaMemcpyHostToDevice, c->s));
+  // the ids go up after the arrays the drift starts with (not sharing the link with
+  // them) and are permuted on the side stream once the drift is done
+  CK(cudaEventRecord(c->ev_up, c->s));
+  CK(cudaStreamWaitEvent(c->s2, c->ev_up, 0));
   CK(cudaMemcpyAsync(c->pid, pid, (size_t)nplocal * 8, cudaMemcpyHostToDevice, c->s2));
-  CK(cudaEventRecord(c->ev_ids, c->s2));
   // the cell counts are validated on the host while the copies run
   int64_t sum = 0;
   bool neg = false;
@@ -1131,22 +1137,27 @@ int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, 
   CK(cudaGetLastError());
   c->loaded = true;
   CK(cudaEventRecord(c->ev[5], c->s));
-  rc = drift_enqueue(c, in, c->ev_ids);
+  rc = drift_enqueue(c, in, true);
   if (rc) {
     drain();
+    c->loaded = false;
     return rc;
   }
   CK(cudaEventRecord(c->ev[6], c->s));
   CK(cudaEventRecord(c->ev_drift, c->s));
   CK(cudaStreamWaitEvent(c->s2, c->ev_drift, 0));
   CK(cudaMemcpyAsync(xp, c->xp, (size_t)c->np * 3 * c->xbytes, cudaMemcpyDeviceToHost, c->s2));
-  CK(cudaMemcpyAsync(pid, c->pid, (size_t)c->np * 8, cudaMemcpyDeviceToHost, c->s2));
   CK(cudaMemcpyAsync(rhoc, c->rhoc, (size_t)G.ncells * 4, cudaMemcpyDeviceToHost, c->s2));
+  k_permute_ids<<<nblk(c->np), 256, 0, c->s2>>>(c->np, c->ssrc, c->pid2, c->pid);  // after the id upload (s2 order)
+  CK(cudaGetLastError());
+  ++c->launches;
+  CK(cudaMemcpyAsync(pid, c->pid, (size_t)c->np * 8, cudaMemcpyDeviceToHost, c->s2));
   rc = cube_gpu_kick(c, in, out);
   CK(cudaEventRecord(c->ev[7], c->s));
   if (!rc) CK(cudaMemcpyAsync(vp, c->vp, (size_t)c->np * 12, cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
   CK(cudaStreamSynchronize(c->s2));
+  if (rc) c->loaded = false;
   if (!rc && out) {
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]);

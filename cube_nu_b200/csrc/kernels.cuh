@@ -305,8 +305,16 @@ __global__ void k_drift_gather(Geo G, int64_t np, const uint32_t* __restrict__ s
     store_code(xo, G.izipx, 3 * pos + d, (int)(code + (int)dn));
     vo[3 * pos + d] = v;
   }
-  po[pos] = pid[src];
+  if (pid) po[pos] = pid[src];  // null: the ids are permuted later (k_permute_ids)
   pcell_o[pos] = dest[src];
+}
+
+// The drift's permutation applied to the particle ids on their own: ids_out[pos] =
+// ids_in[ssrc[pos]], for a caller whose ids arrive after the rest of the drift has run.
+__global__ void k_permute_ids(int64_t np, const uint32_t* __restrict__ ssrc, const int64_t* __restrict__ ids_in,
+                              int64_t* __restrict__ ids_out) {
+  const int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos < np) ids_out[pos] = ids_in[ssrc[pos]];
 }
 
 // =================================================================================

@@ -195,9 +195,9 @@ int cube_gpu_step(cube_ctx* ctx, const cube_step_in* in, cube_step_out* out);
  * the state from the four arrays (`nplocal` particles, checked as in cube_gpu_upload),
  * steps, and writes the new state back into the same arrays.  Equal to cube_gpu_upload +
  * cube_gpu_step + cube_gpu_download on those arrays; the copies the step does not wait
- * for overlap it (ids go up beside the drift's first kernels, positions, ids and counts
- * come down during the kick), which needs page-locked arrays.  After a failed call the
- * context holds no particles. */
+ * for overlap it (the ids go up and are reordered while the drift runs; positions, ids
+ * and counts come down during the kick), which needs page-locked arrays.  After a failed
+ * call the context holds no particles. */
 int cube_gpu_step_host(cube_ctx* ctx, const cube_step_in* in, cube_step_out* out, void* xp, float* vp,
                        int64_t* pid, int32_t* rhoc, int64_t nplocal);
 
