@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libcube_gpu.so")
 SOURCES = ["cube_gpu.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "fft2.cuh", "ic.cuh", "kernels.cuh"]
+# every kernel header in csrc/ (cube_gpu.cu includes them all), so an edit to any rebuilds
+HEADERS = sorted(f for f in os.listdir(SRC) if f.endswith(".cuh"))
 
 
 def nvcc() -> str:

@@ -59,13 +59,13 @@ enum KClass {
   K_DRIFT_DEST, K_DRIFT_SCATTER, K_DRIFT_SORT, K_DRIFT_GATHER, K_SCAN, K_DEP_PM1, K_FFT_PM1, K_F2_PM1, K_INT_PM1,
   K_DEP_PM2, K_FFTX_PM2, K_FFTY_PM2, K_FFTZ_PM2, K_FFTC_PM2, K_F2_PM2, K_INT_PM2, K_DEP_PM3, K_FFTX_PM3, K_FFTY_PM3,
   K_FFTZ_PM3, K_FFTC_PM3, K_F2_PM3, K_INT_PM3, K_PP, K_CLASSIFY, K_GREEN, K_FILL, K_PK_DEP, K_PK_FFT, K_PK_BIN,
-  K_PK_ALIAS, K_NCLASS
+  K_PK_ALIAS, K_MOMENTUM, K_NCLASS
 };
 const char* const KNAMES[K_NCLASS] = {
     "drift_dest", "drift_scatter", "drift_sort", "drift_gather", "scan", "deposit_pm1", "fft_pm1", "f2max_pm1",
     "interp_pm1", "deposit_pm2", "fft_x_pm2", "fft_y_pm2", "fft_z_green_pm2", "fft_c2r_pm2", "f2max_pm2",
     "interp_pm2", "deposit_pm3", "fft_x_pm3", "fft_y_pm3", "fft_z_green_pm3", "fft_c2r_pm3", "f2max_pm3",
-    "interp_pm3", "pp", "classify", "green", "fill_pcell", "pk_deposit", "pk_fft", "pk_bin", "pk_alias"};
+    "interp_pm3", "pp", "classify", "green", "fill_pcell", "pk_deposit", "pk_fft", "pk_bin", "pk_alias", "momentum"};
 
 struct ProfRec {
   int cls;
@@ -99,6 +99,10 @@ struct cube_ctx {
   // reductions: f2max[4] (pm1, pm2, pm3, pp), vmax[3][3] (pm2, pm3, pp)
   float* red = nullptr;
   unsigned long long* pairs = nullptr;
+  // FP64 reductions: mass sums [level 1..3][MASS_SLOTS] (int64 or double by deposit form),
+  // momentum partials [MOM_BLOCKS][3]
+  unsigned long long* msum = nullptr;
+  double* mom = nullptr;
   unsigned* err = nullptr;
   int32_t *ires = nullptr, *napm = nullptr;
   int32_t* box_slot = nullptr;  // [nchunk][ns3]
@@ -666,6 +670,8 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
   CK(cudaMalloc(&c->scan_tmp, ((nc3 + 2047) / 2048 + 2) * 8));
   CK(cudaMalloc(&c->red, 64 * sizeof(float)));
   CK(cudaMalloc(&c->pairs, 8));
+  CK(cudaMalloc(&c->msum, 3 * MASS_SLOTS * 8));
+  CK(cudaMalloc(&c->mom, MOM_BLOCKS * 3 * sizeof(double)));
   CK(cudaMalloc(&c->err, 4));
   CK(cudaMemset(c->err, 0, 4));
   CK(cudaMalloc(&c->ires, c->ns3 * 4));
@@ -688,7 +694,7 @@ int cube_gpu_destroy(cube_ctx* c) {
   if (c->s) cudaStreamSynchronize(c->s);
   void* bufs[] = {c->xp, c->xp2, c->vp, c->vp2, c->pid, c->pid2, c->pcell, c->pcell2, c->rhoc, c->rhoc2,
                   c->fill, c->biglist, c->nbig, c->cstart, c->cstart2, c->scan_tmp, c->dest, c->key, c->skey,
-                  c->ssrc, c->red, c->pairs, c->err, c->ires, c->napm, c->box_slot, c->arena, c->green1,
+                  c->ssrc, c->red, c->pairs, c->msum, c->mom, c->err, c->ires, c->napm, c->box_slot, c->arena, c->green1,
                   c->green2, c->cap_buf};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -871,6 +877,10 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
   float* vm = c->red + 8;    // [pm2 0..2][pm3 3..5][pp 6..8]
   CK(cudaMemsetAsync(c->red, 0, 64 * sizeof(float), c->s));
   CK(cudaMemsetAsync(c->pairs, 0, 8, c->s));
+  CK(cudaMemsetAsync(c->msum, 0, 3 * MASS_SLOTS * 8, c->s));
+  unsigned long long* ms1 = c->msum;
+  unsigned long long* ms2 = c->msum + MASS_SLOTS;
+  unsigned long long* ms3 = c->msum + 2 * MASS_SLOTS;
   CK(cudaEventRecord(c->ev[0], c->s));
   // ---------------- PM1 (particle_mesh.f90) ----------------
   {
@@ -879,8 +889,8 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     CK(cudaMemsetAsync(m.real, 0, mesh_bytes(c, n, 1, fixed), c->s));
     if (fixed)
       LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1_runs<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell,
-                                                                     reinterpret_cast<unsigned long long*>(m.real), m.pt.pr, m.pt.plr));
-    else LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr, m.pt.plr));
+                                                                     reinterpret_cast<unsigned long long*>(m.real), m.pt.pr, m.pt.plr, ms1));
+    else LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr, m.pt.plr, ms1));
     maybe_capture(c, 1, 0, 0, m.real, n, fixed, m.pt.rp, m.pt.psb);
     float* phi = reinterpret_cast<float*>(m.real);
     launch_fft(c, n, 1, m.real, fixed, G.mass_p, phi, m.ck, c->green1, (float)n, 3, 1);
@@ -907,8 +917,8 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
       const int64_t boxb = (int64_t)n * m.pt.psb;
       CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
-      if (fixed) LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb, m.pt.pr, m.pt.plr));
-      else LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb, m.pt.pr, m.pt.plr));
+      if (fixed) LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb, m.pt.pr, m.pt.plr, ms2));
+      else LAUNCH(c, K_DEP_PM2, 1, k_deposit_pm2<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, t0, nb, m.pt.pr, m.pt.plr, ms2));
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
         maybe_capture(c, 2, c->cap_box, 0, (char*)m.real + (c->cap_box - t0) * boxb, n, fixed, m.pt.rp, m.pt.psb);
       float* phi = reinterpret_cast<float*>(m.real);
@@ -987,11 +997,11 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
         smem_optin(k_deposit_pm3_own, sm);
         LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3_own<<<(unsigned)((int64_t)nb * nr * nr * nrz), DEP3_THREADS, sm, c->s>>>(
                                     G, c->xp, c->cstart, c->box_slot + list_off[k], cl,
-                                    reinterpret_cast<float*>(m.real), c->err, m.pt.pr, m.pt.plr, nr, nr, nrz));
+                                    reinterpret_cast<float*>(m.real), c->err, m.pt.pr, m.pt.plr, nr, nr, nrz, ms3));
       } else {
         CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
-        if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));
-        else LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));
+        if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr, ms3));
+        else LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr, ms3));
       }
       int cap_slot = -1;
       if (c->cap_level == 3 && c->cap_box >= 0 && c->cap_box < c->ns3 && ires[c->cap_box] == cl)
@@ -1025,11 +1035,16 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
                                                                      mass_scale, v_scale, f2 + 3, vm + 6, c->pairs));
   }
   CK(cudaEventRecord(c->ev[4], c->s));
+  LAUNCH(c, K_MOMENTUM, 1, k_momentum<<<MOM_BLOCKS, MOM_THREADS, 0, c->s>>>(c->vp, np, c->mom));
   CK(cudaGetLastError());
   float red[64];
   unsigned long long pairs = 0;
+  std::vector<unsigned long long> msum(3 * MASS_SLOTS);
+  std::vector<double> mom(3 * MOM_BLOCKS);
   CK(cudaMemcpyAsync(red, c->red, sizeof(red), cudaMemcpyDeviceToHost, c->s));
   CK(cudaMemcpyAsync(&pairs, c->pairs, 8, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(msum.data(), c->msum, msum.size() * 8, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(mom.data(), c->mom, mom.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
   prof_collect(c);
   int rc = check_err(c);
@@ -1059,6 +1074,31 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     }
     cudaEventElapsedTime(&ms, c->ev[0], c->ev[4]);
     out->tcat[5] = ms;
+    double mass[3];
+    for (int l = 0; l < 3; ++l) {
+      const unsigned long long* q = msum.data() + l * MASS_SLOTS;
+      if (fixed) {
+        unsigned long long t = 0;  // exact: the slots hold sums of int64 contributions
+        for (int k = 0; k < MASS_SLOTS; ++k) t += q[k];
+        mass[l] = std::ldexp((double)t, -40);
+      } else {
+        double t = 0.0;
+        for (int k = 0; k < MASS_SLOTS; ++k) {
+          double v;
+          memcpy(&v, q + k, sizeof v);
+          t += v;
+        }
+        mass[l] = t;
+      }
+    }
+    out->mass_pm1 = mass[0];
+    out->mass_pm2 = mass[1];
+    out->mass_pm3 = mass[2];
+    for (int d = 0; d < 3; ++d) {
+      double t = 0.0;
+      for (int b = 0; b < MOM_BLOCKS; ++b) t += mom[3 * b + d];
+      out->momentum[d] = t;
+    }
   }
   return 0;
 }
@@ -1446,7 +1486,8 @@ constexpr size_t kNaAccOff = 0;                                                 
 constexpr size_t kNaStartOff = kNaAccOff + na_round(kNaCells * 8);               // int64 [cells+1]
 constexpr size_t kNaScanOff = kNaStartOff + na_round((kNaCells + 1) * 8);        // int64 [tiles+2]
 constexpr size_t kNaCellOff = kNaScanOff + na_round(((kNaCells + SCAN_TILE - 1) / SCAN_TILE + 2) * 8);  // int32 [np]
-constexpr size_t kNaBytes = kNaCellOff + na_round(kNaParticles * 4);
+constexpr size_t kNaFlagOff = kNaCellOff + na_round(kNaParticles * 4);           // uint32: negative count seen
+constexpr size_t kNaBytes = kNaFlagOff + 256;
 
 }  // namespace
 
@@ -1476,11 +1517,13 @@ int noalloc_scratch(unsigned char** out) {
 }
 
 // Particle -> cell index from the cell starts; indices at or beyond np are not written,
-// so a rhoc that does not sum to np cannot write past the scratch.
+// so a rhoc that does not sum to np cannot write past the scratch.  A negative count
+// (cstart decreasing) raises *bad, which the host turns into CUBE_E_COUNT.
 __global__ void k_na_fill_pcell(const int64_t* __restrict__ cstart, int64_t ncells, int64_t np,
-                                int32_t* __restrict__ pcell) {
+                                int32_t* __restrict__ pcell, unsigned* __restrict__ bad) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncells) return;
+  if (cstart[c + 1] < cstart[c]) atomicOr(bad, 1u);
   const int64_t b = cstart[c] > 0 ? cstart[c] : 0;
   const int64_t e = cstart[c + 1] < np ? cstart[c + 1] : np;
   for (int64_t i = b; i < e; ++i) pcell[i] = (int32_t)c;
@@ -1523,6 +1566,7 @@ extern "C" int cube_gpu_pm1_density_noalloc(const cube_params* p, const void* xp
   int64_t* cstart = reinterpret_cast<int64_t*>(base + kNaStartOff);
   int64_t* tmp = reinterpret_cast<int64_t*>(base + kNaScanOff);
   int32_t* pcell = reinterpret_cast<int32_t*>(base + kNaCellOff);
+  unsigned* bad = reinterpret_cast<unsigned*>(base + kNaFlagOff);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool fixed = p->deposit_mode == CUBE_DEPOSIT_FIXED;
   const int nc = G.nc;
@@ -1532,19 +1576,23 @@ extern "C" int cube_gpu_pm1_density_noalloc(const cube_params* p, const void* xp
   if (fixed) CK(cudaMemsetAsync(acc, 0, n3 * 8, s));
   else CK(cudaMemsetAsync(rho, 0, n3 * 4, s));
   if (np > 0) CK(cudaMemsetAsync(pcell, 0, np * 4, s));
+  CK(cudaMemsetAsync(bad, 0, sizeof(unsigned), s));
   exclusive_scan(rhoc, cstart, n3, tmp, s);
-  k_na_fill_pcell<<<nblk(n3), 256, 0, s>>>(cstart, n3, np, pcell);
+  k_na_fill_pcell<<<nblk(n3), 256, 0, s>>>(cstart, n3, np, pcell, bad);
   if (np > 0) {
-    if (fixed) k_deposit_pm1<true><<<nblk(np), 256, 0, s>>>(G, np, xp, pcell, acc, nc, (int64_t)nc * nc);
-    else k_deposit_pm1<false><<<nblk(np), 256, 0, s>>>(G, np, xp, pcell, rho, nc, (int64_t)nc * nc);
+    if (fixed) k_deposit_pm1<true><<<nblk(np), 256, 0, s>>>(G, np, xp, pcell, acc, nc, (int64_t)nc * nc, nullptr);
+    else k_deposit_pm1<false><<<nblk(np), 256, 0, s>>>(G, np, xp, pcell, rho, nc, (int64_t)nc * nc, nullptr);
   }
   if (fixed) k_na_fixed_to_density<<<nblk(n3), 256, 0, s>>>(acc, n3, G.mass_p, rho);
   else k_na_scale<<<nblk(n3), 256, 0, s>>>(rho, n3, G.mass_p);
   CK(cudaGetLastError());
   // every particle must belong to a cell (drift.f90:139-143 checks the same sum)
   int64_t total = -1;
+  unsigned negative = 0;
   CK(cudaMemcpyAsync(&total, cstart + n3, sizeof total, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&negative, bad, sizeof negative, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  if (negative) return fail(CUBE_E_COUNT, "rhoc holds a negative count");
   if (total != np) {
     char msg[160];
     snprintf(msg, sizeof msg, "rhoc sums to %lld particles but np is %lld", (long long)total, (long long)np);

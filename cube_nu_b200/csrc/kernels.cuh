@@ -332,11 +332,43 @@ __device__ __forceinline__ void dep_add(void* rho, int64_t i, float w) {
   }
 }
 
+// Mass sums of the deposited density over the physical cells of a level (the reference
+// forms them in real(8): particle_mesh.f90:106 testrho, kick.f90:687-688 ptotal), in
+// particle units.  The fixed-point form sums the int64 contributions exactly (order
+// independent, so deterministic); the FP32 form sums the float weights in FP64.  Warps
+// add into one of MASS_SLOTS accumulators picked by block, so the atomics do not all hit
+// one address; the host adds the slots.
+constexpr int MASS_SLOTS = 64;
+
+__device__ __forceinline__ void warp_sum_to(unsigned long long v, unsigned long long* out) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v && out) atomicAdd(out + (blockIdx.x & (MASS_SLOTS - 1)), v);
+}
+
+__device__ __forceinline__ void warp_sum_to(double v, double* out) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0.0 && out) atomicAdd(out + (blockIdx.x & (MASS_SLOTS - 1)), v);
+}
+
+// One thread's running mass sum in the arithmetic of its deposit form.
+template <bool FIXED>
+struct MassAcc {
+  using T = typename std::conditional<FIXED, unsigned long long, double>::type;
+  T v = 0;
+  __device__ __forceinline__ void add(float w) {
+    if constexpr (FIXED) v += (unsigned long long)__float2ll_rn(__fmul_rn(w, FIXED_SCALE));
+    else v += (double)w;
+  }
+  // out: MASS_SLOTS accumulators of type T (nullptr: no sum wanted)
+  __device__ __forceinline__ void flush(void* out) { warp_sum_to(v, static_cast<T*>(out)); }
+};
+
 template <bool FIXED>
 __global__ void __launch_bounds__(256, 6) k_deposit_pm1(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
-                              void* __restrict__ rho, int pr, int64_t pl) {
+                              void* __restrict__ rho, int pr, int64_t pl, void* msum) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (ip >= np) return;
+  MassAcc<FIXED> mass;
+  if (ip < np) {
   int g[3];
   cell_coords(G, pcell[ip], g[0], g[1], g[2]);
   int i2[3];
@@ -358,9 +390,12 @@ __global__ void __launch_bounds__(256, 6) k_deposit_pm1(Geo G, int64_t np, const
         const int x = wrapi(i2[0] - 2 + a1, nc);
         const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
         dep_add<FIXED>(rho, (int64_t)z * pl + (int64_t)y * pr + x, ww);
+        mass.add(ww);
       }
     }
   }
+  }
+  mass.flush(msum);
 }
 
 // Fixed-point PM1 deposit with the sums of a coarse cell's particles combined in the warp
@@ -373,7 +408,8 @@ __global__ void __launch_bounds__(256, 6) k_deposit_pm1(Geo G, int64_t np, const
 // k_deposit_pm1<true>.
 __global__ void __launch_bounds__(256) k_deposit_pm1_runs(Geo G, int64_t np, const void* __restrict__ xp,
                                                           const int32_t* __restrict__ pcell,
-                                                          unsigned long long* __restrict__ rho, int pr, int64_t pl) {
+                                                          unsigned long long* __restrict__ rho, int pr, int64_t pl,
+                                                          unsigned long long* msum) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   if ((ip - lane) >= np) return;  // warp-uniform: no live lane in this warp
@@ -402,6 +438,7 @@ __global__ void __launch_bounds__(256) k_deposit_pm1_runs(Geo G, int64_t np, con
     }
   }
   const int nc = G.nc;
+  unsigned long long mloc = 0;
 #pragma unroll
   for (int a3 = 0; a3 < 3; ++a3) {
     const int64_t z = (int64_t)wrapi(g[2] - 1 + a3, nc) * pl;
@@ -419,10 +456,14 @@ __global__ void __launch_bounds__(256) k_deposit_pm1_runs(Geo G, int64_t np, con
           const unsigned long long o = __shfl_down_sync(0xffffffffu, q, 1 << k);
           if (samebits & (1u << k)) q += o;
         }
-        if (head) atomicAdd(rho + z + y + wrapi(g[0] - 1 + a1, nc), q);
+        if (head) {
+          atomicAdd(rho + z + y + wrapi(g[0] - 1 + a1, nc), q);
+          mloc += q;
+        }
       }
     }
   }
+  warp_sum_to(mloc, msum);
 }
 
 // Candidate tiles along one dimension for a particle with global cell g: its own tile
@@ -442,9 +483,10 @@ __device__ __forceinline__ int tile_cands(const Geo& G, int g, int* t, int* li) 
 // PM2 tile meshes [tile - tile0][ngt^3]; fine index i maps to array i-(1-ngb).
 template <bool FIXED>
 __global__ void __launch_bounds__(256, 5) k_deposit_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
-                              void* __restrict__ rho, int tile0, int ntile, int pr, int64_t pl) {
+                              void* __restrict__ rho, int tile0, int ntile, int pr, int64_t pl, void* msum) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (ip >= np) return;
+  MassAcc<FIXED> mass;
+  if (ip < np) {
   int g[3];
   cell_coords(G, pcell[ip], g[0], g[1], g[2]);
   int tc[3][2], lc[3][2], nca[3];
@@ -490,10 +532,16 @@ __global__ void __launch_bounds__(256, 5) k_deposit_pm2(Geo G, int64_t np, const
               if (x < 0 || x >= ngt) continue;
               const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
               dep_add<FIXED>(base, (int64_t)z * pl + (int64_t)y * pr + x, ww);
+              // physical cells 1..ngp of the tile (array ngb..ngb+ngp-1)
+              if ((unsigned)(x - G.ngb) < (unsigned)G.ngp && (unsigned)(y - G.ngb) < (unsigned)G.ngp &&
+                  (unsigned)(z - G.ngb) < (unsigned)G.ngp)
+                mass.add(ww);
             }
           }
         }
       }
+  }
+  mass.flush(msum);
 }
 
 // Candidate subtiles along one dimension (PM3 nloop=1): own subtile and, in the
@@ -541,9 +589,10 @@ __device__ __forceinline__ double pm3_xpos(double lf, const Geo& G, double gs, i
 template <bool FIXED>
 __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                               const int32_t* __restrict__ box_slot, int iapm, void* __restrict__ rho,
-                              unsigned* err, int pr, int64_t pl) {
+                              unsigned* err, int pr, int64_t pl, void* msum) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (ip >= np) return;
+  MassAcc<FIXED> mass;
+  if (ip < np) {
   int g[3];
   cell_coords(G, pcell[ip], g[0], g[1], g[2]);
   int tc[3][2], uc[3][2], lc[3][2], nca[3];  // at most two candidate subtiles per dimension (ntt >= 2)
@@ -598,10 +647,16 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
               if (x < 0 || x >= nft) continue;
               const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
               dep_add<FIXED>(base, (int64_t)z * pl + (int64_t)y * pr + x, ww);
+              // physical cells 1..nfp of the subtile (array nfb..nfb+nfp-1)
+              if ((unsigned)(x - nfb) < (unsigned)nfp && (unsigned)(y - nfb) < (unsigned)nfp &&
+                  (unsigned)(z - nfb) < (unsigned)nfp)
+                mass.add(ww);
             }
           }
         }
       }
+  }
+  mass.flush(msum);
 }
 
 // Owner-computes form of the fixed-point PM3 deposit: one block per region of
@@ -638,7 +693,8 @@ __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo
                                                                      const int64_t* __restrict__ cstart,
                                                                      const int32_t* __restrict__ box_sub, int iapm,
                                                                      float* __restrict__ rho, unsigned* err,
-                                                                     int pr, int64_t pl, int nrx, int nry, int nrz) {
+                                                                     int pr, int64_t pl, int nrx, int nry, int nrz,
+                                                                     unsigned long long* msum) {
   constexpr int R = DEP3_R, RZ = DEP3_RZ;
   static_assert(R % 2 == 0 && R / 2 <= 16, "a half warp writes one region row");
   extern __shared__ __align__(16) unsigned long long acc[];  // [RZ][R][R]
@@ -772,6 +828,9 @@ __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo
   float* base = rho + j * (int64_t)nft * pl + (int64_t)o[2] * pl + (int64_t)o[1] * pr + o[0];
   const int hx = e[0] >> 1, nrow = e[1] * e[2], hl = tid & 15;
   const float inv_e1 = 1.f / (float)e[1];
+  // physical cells 1..nfp of the subtile are array nfb..nfb+nfp-1
+  const bool px0 = (unsigned)(o[0] + 2 * hl - nfb) < (unsigned)nfp, px1 = (unsigned)(o[0] + 2 * hl + 1 - nfb) < (unsigned)nfp;
+  unsigned long long mloc = 0;
   for (int row = tid >> 4; row < nrow; row += blockDim.x >> 4) {
     const int z = (int)(((float)row + 0.5f) * inv_e1);
     const int y = row - z * e[1];
@@ -781,11 +840,14 @@ __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo
         val.x = ((val.x >> 32) << 20) + (val.x & 0xffffffffull);
         val.y = ((val.y >> 32) << 20) + (val.y & 0xffffffffull);
       }
+      if ((unsigned)(o[1] + y - nfb) < (unsigned)nfp && (unsigned)(o[2] + z - nfb) < (unsigned)nfp)
+        mloc += (px0 ? val.x : 0ull) + (px1 ? val.y : 0ull);
       const float2 fv = make_float2((float)((double)(long long)val.x * 9.094947017729282e-13),  // 2^-40
                                     (float)((double)(long long)val.y * 9.094947017729282e-13));
       __stcs(reinterpret_cast<float2*>(base + (int64_t)z * pl + (int64_t)y * pr) + hl, fv);
     }
   }
+  warp_sum_to(mloc, msum);
 }
 
 // =================================================================================
@@ -1329,6 +1391,34 @@ __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32
   unsigned long long c = live ? cnt : 0ull;
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(npairs, c);
+}
+
+// =================================================================================
+// Total momentum (sum of vp over the particles, per component) in FP64, deterministic:
+// each block sums a fixed grid-stride share in a fixed order and a shared-memory tree,
+// and writes its partial; the host adds the partials in block order.  MOM_BLOCKS blocks.
+// =================================================================================
+constexpr int MOM_BLOCKS = 592, MOM_THREADS = 256;
+__global__ void __launch_bounds__(MOM_THREADS) k_momentum(const float* __restrict__ vp, int64_t np,
+                                                          double* __restrict__ partial) {
+  __shared__ double sh[3][MOM_THREADS];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * MOM_THREADS + threadIdx.x; i < np; i += (int64_t)gridDim.x * MOM_THREADS) {
+    s0 += (double)vp[3 * i];
+    s1 += (double)vp[3 * i + 1];
+    s2 += (double)vp[3 * i + 2];
+  }
+  sh[0][threadIdx.x] = s0;
+  sh[1][threadIdx.x] = s1;
+  sh[2][threadIdx.x] = s2;
+  __syncthreads();
+  for (int h = MOM_THREADS / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) sh[d][threadIdx.x] += sh[d][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) partial[3 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
 }
 
 // =================================================================================

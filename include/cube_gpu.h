@@ -99,6 +99,14 @@ typedef struct cube_step_out {
   int64_t nplocal;
   int64_t pp_pairs;                             /* in-range PP pairs evaluated (both orders)  */
   float tcat[16];                               /* stage ms: 0 drift,1 PM1,2 PM2,3 PM3,4 PP,5 sum, 6 step wall on device */
+  /* FP64 global reductions.  mass_pm*: the deposited density summed over the physical
+   * cells of each level, in particle units (particle_mesh.f90:106 testrho, kick.f90:687-688
+   * ptotal; the reference prints them at kick.f90:42,72,242): nplocal up to the rounding
+   * of the TSC weights.  Exact int64 sums with CUBE_DEPOSIT_FIXED, FP64 sums of the FP32
+   * weights otherwise.  mass_pm3 is 0 with PM3 off.  momentum: sum of vp over the
+   * particles after the kick, per component, in FP64 (deterministic order). */
+  double mass_pm1, mass_pm2, mass_pm3;
+  double momentum[3];
 } cube_step_out;
 
 typedef struct cube_ctx cube_ctx;
@@ -245,11 +253,17 @@ int cube_gpu_subtile_class(cube_ctx* ctx, int32_t* ires, int64_t n);
  * All scratch lives in one static device array sized for at most
  * CUBE_NOALLOC_MAX_CELLS coarse cells and CUBE_NOALLOC_MAX_PARTICLES particles (about
  * 12 MB, held by every device that loads the library until the process exits); larger
- * sizes return CUBE_E_CAPACITY.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  Every call shares the array: calls that overlap on the GPU (other
- * streams, other host threads) race; serialise them.  Each call clears what it
- * accumulates into.  Returns CUBE_E_COUNT when rhoc does not sum to np.
+ * sizes return CUBE_E_CAPACITY.  The 12 MB are committed when the library's device code
+ * is first loaded on a device (with lazy module loading, at the first call of any entry
+ * point there); a caller whose device memory a pool will later claim should make one
+ * call on each device before the pool grows.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and keeps it for the life of the
+ * process: do not use the library on a device after cudaDeviceReset.  The call waits for
+ * `stream` (it reads back a count), so it can never be recorded into a CUDA graph.  Every
+ * call shares the array: calls that overlap on the GPU (other streams, other host
+ * threads) race; serialise them.  Each call clears what it accumulates into.  Returns
+ * CUBE_E_COUNT when rhoc holds a negative count or does not sum to np; on any error the
+ * contents of rho are undefined.
  */
 #define CUBE_NOALLOC_MAX_CELLS 262144       /* 64^3 coarse cells */
 #define CUBE_NOALLOC_MAX_PARTICLES 2097152  /* 2^21 particles    */

@@ -351,7 +351,7 @@ static const float WEIGHT[4] = {(W_ALPHA - 1) / 4, -W_ALPHA / 2, W_ALPHA / 2, (1
 
 template <class T, class XT>
 static void box_density(const Geo& G, const Cells& C, const XT* xp, const Box& b, BoxWork<T>& w,
-                        bool fixed, int64_t& err) {
+                        bool fixed, int64_t& err, int64_t& mass_fx, double& mass_d) {
   const int64_t ne = b.nphy + 2 * b.nex;
   const int64_t o = 1 - b.nex;  // first index
   if (fixed) w.rho_fx.assign(ne * ne * ne, 0);
@@ -384,6 +384,14 @@ static void box_density(const Geo& G, const Cells& C, const XT* xp, const Box& b
                 }
           }
         }
+  // ptotal = sum(1d0*rho_th(1:nphy,1:nphy,1:nphy))  (kick.f90:687-688)
+  for (int64_t z = 1 - o; z <= b.nphy - o; ++z)
+    for (int64_t y = 1 - o; y <= b.nphy - o; ++y)
+      for (int64_t x = 1 - o; x <= b.nphy - o; ++x) {
+        const int64_t s = (z * ne + y) * ne + x;
+        if (fixed) mass_fx += w.rho_fx[s];
+        else mass_d += (double)w.rho_th[s];
+      }
   // density(nstart:nend) = rho_th(m1:m2)*mass_p_cdm  (kick.f90:686)
   const int64_t nw = b.nwork;
   w.dens.assign(nw * nw * nw, (T)0);
@@ -485,13 +493,14 @@ static void box_interp(const Geo& G, const Cells& C, const XT* xp, T* vp, const 
 template <class T, class XT>
 static void pm1(const Geo& G, const Cells& C, const XT* xp, T* vp, const float* green, bool fixed, float a_mid,
                 float dt, T& f2max, std::vector<T>* dbg_dens, std::vector<T>* dbg_phi, std::vector<T>* dbg_force,
-                int64_t& err) {
+                int64_t& err, double& mass) {
   const int64_t nc = G.nc, nt = G.nt;
   std::vector<T> rho(nc * nc * nc, (T)0);
   const int64_t ntiles = G.nnt * G.nnt * G.nnt;
   const int64_t nex = 2, ne = nt + 2 * nex;
-  int64_t e = 0;
-#pragma omp parallel for schedule(dynamic) reduction(| : e)
+  int64_t e = 0, mfx = 0;
+  double md = 0.0;
+#pragma omp parallel for schedule(dynamic) reduction(| : e) reduction(+ : mfx, md)
   for (int64_t t = 0; t < ntiles; ++t) {
     const int64_t tx = t % G.nnt, ty = (t / G.nnt) % G.nnt, tz = t / (G.nnt * G.nnt);
     std::vector<T> rex;
@@ -532,9 +541,13 @@ static void pm1(const Geo& G, const Cells& C, const XT* xp, T* vp, const float* 
           const int64_t s = ((k - 1 + nex) * ne + (j - 1 + nex)) * ne + (i - 1 + nex);
           T r = fixed ? (T)(float)std::ldexp((double)rfx[s], -FIXED_SHIFT) : rex[s];
           rho[((tz * nt + k - 1) * nc + (ty * nt + j - 1)) * nc + (tx * nt + i - 1)] = r * (T)G.mass_p;
+          // testrho = testrho + sum(1d0*rho_ex(1:nphy,1:nphy,1:nphy))  (particle_mesh.f90:106)
+          if (fixed) mfx += rfx[s];
+          else md += (double)rex[s];
         }
   }
   err |= e;
+  mass = fixed ? std::ldexp((double)mfx, -FIXED_SHIFT) : md;
   if (dbg_dens) *dbg_dens = rho;
   const int n = (int)nc, nh = n / 2 + 1;
   std::vector<std::complex<T>> ck((int64_t)n * n * nh);
@@ -793,6 +806,9 @@ typedef struct oracle_kick_out {
   int32_t napm[8];
   int64_t pp_pairs;
   int64_t err;
+  // sum of the density over each level's physical cells, particle units (particle_mesh.f90:106
+  // testrho, kick.f90:687-688 ptotal): exact int64 sums with the fixed-point deposit
+  double mass[3];
 } oracle_kick_out;
 
 int oracle_set_threads(int n) {
@@ -881,7 +897,7 @@ static int kick_impl(const Geo& G, const XT* xp, T* vp, const int32_t* rhoc, flo
     std::vector<T> dd, dp, df;
     const bool want = dbg_level == 1;
     pm1<T, XT>(G, C, xp, vp, g1.data(), fixed, a_mid, dt, f2, want && dbg_what == 0 ? &dd : nullptr,
-               want && dbg_what == 1 ? &dp : nullptr, want && dbg_what == 2 ? &df : nullptr, err);
+               want && dbg_what == 1 ? &dp : nullptr, want && dbg_what == 2 ? &df : nullptr, err, out->mass[0]);
     if (want) dump(dbg_what == 0 ? dd : dbg_what == 1 ? dp : df);
   }
   out->f2max_pm1 = (double)f2;
@@ -895,12 +911,13 @@ static int kick_impl(const Geo& G, const XT* xp, T* vp, const int32_t* rhoc, flo
     std::vector<float> g2(G.ngt * G.ngt * (G.ngt / 2 + 1));
     green_3d(g2.data(), G.ngt, G.apm2, G.apm1c * (float)G.rcs, 1.f);
     T f2m = 0, vm0 = 0, vm1 = 0, vm2 = 0;
-    int64_t e = 0;
-#pragma omp parallel for schedule(dynamic, 1) reduction(max : f2m, vm0, vm1, vm2) reduction(| : e)
+    int64_t e = 0, mfx = 0;
+    double md = 0.0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(max : f2m, vm0, vm1, vm2) reduction(| : e) reduction(+ : mfx, md)
     for (int64_t t = 0; t < ntile_run; ++t) {
       BoxWork<T> w;
       Box b = make_pm2_box(G, t);
-      box_density<T, XT>(G, C, xp, b, w, fixed, e);
+      box_density<T, XT>(G, C, xp, b, w, fixed, e, mfx, md);
       if (dbg_level == 2 && dbg_box == t && dbg_what == 0) dump(w.dens);
       T f2t = 0;
       box_force<T>(b, g2.data(), w, f2t);
@@ -914,6 +931,7 @@ static int kick_impl(const Geo& G, const XT* xp, T* vp, const int32_t* rhoc, flo
       vm2 = std::max(vm2, vm[2]);
     }
     err |= e;
+    out->mass[1] = fixed ? std::ldexp((double)mfx, -FIXED_SHIFT) : md;
     out->f2max_pm2 = (double)f2m;
     vmax[0] = vm0; vmax[1] = vm1; vmax[2] = vm2;
   }
@@ -933,12 +951,13 @@ static int kick_impl(const Geo& G, const XT* xp, T* vp, const int32_t* rhoc, flo
         green_3d(g3[c].data(), G.nft[c], G.apm3f, G.apm2 * (float)RSF[c], 1.f / (float)RSF[c]);
       }
     T f2m = 0, vm0 = 0, vm1 = 0, vm2 = 0;
-    int64_t e = 0;
-#pragma omp parallel for schedule(dynamic, 1) reduction(max : f2m, vm0, vm1, vm2) reduction(| : e)
+    int64_t e = 0, mfx = 0;
+    double md = 0.0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(max : f2m, vm0, vm1, vm2) reduction(| : e) reduction(+ : mfx, md)
     for (int64_t s = 0; s < ns_run; ++s) {
       BoxWork<T> w;
       Box b = make_pm3_box(G, s, ires[s]);
-      box_density<T, XT>(G, C, xp, b, w, fixed, e);
+      box_density<T, XT>(G, C, xp, b, w, fixed, e, mfx, md);
       if (dbg_level == 3 && dbg_box == s && dbg_what == 0) dump(w.dens);
       T f2t = 0;
       box_force<T>(b, g3[ires[s]].data(), w, f2t);
@@ -952,6 +971,7 @@ static int kick_impl(const Geo& G, const XT* xp, T* vp, const int32_t* rhoc, flo
       vm2 = std::max(vm2, vm[2]);
     }
     err |= e;
+    out->mass[2] = fixed ? std::ldexp((double)mfx, -FIXED_SHIFT) : md;
     out->f2max_pm3 = (double)f2m;
     vmax[0] = vm0; vmax[1] = vm1; vmax[2] = vm2;
   }

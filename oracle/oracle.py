@@ -28,13 +28,16 @@ class KickOut(ctypes.Structure):
         ("dt_pm1", ctypes.c_float), ("dt_pm2", ctypes.c_float), ("dt_pm3", ctypes.c_float),
         ("dt_pp", ctypes.c_float), ("dt_vmax", ctypes.c_float), ("vz_max", ctypes.c_float),
         ("napm", ctypes.c_int32 * 8), ("pp_pairs", ctypes.c_int64), ("err", ctypes.c_int64),
+        ("mass", ctypes.c_double * 3),
     ]
 
 
 def build(force: bool = False) -> str:
+    """(Re)build liboracle.so with its Makefile; make skips it when it is up to date."""
     path = os.path.join(_HERE, "liboracle.so")
-    if force or not os.path.exists(path):
-        subprocess.check_call(["make", "-s", "-C", _HERE])
+    if force and os.path.exists(path):
+        os.unlink(path)
+    subprocess.check_call(["make", "-s", "-C", _HERE])
     return path
 
 

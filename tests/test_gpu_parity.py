@@ -349,3 +349,34 @@ def test_int2real_matches_oracle(oracle_lib, izipx):
     assert xv.shape == ref.shape and xv.dtype == np.float32
     assert np.array_equal(xv, ref)
     assert xv.min() >= 0.0 and xv.max() < p.nc
+
+
+@pytest.mark.parametrize("fixed", [False, True])
+def test_fp64_mass_and_momentum(oracle_lib, fixed):
+    """FP64 global reductions of the step: the density summed over each level's physical
+    cells (particle_mesh.f90:106, kick.f90:687-688) equals the oracle's, exactly with the
+    fixed-point deposit (int64 sums) and to 1e-9 relative in FP32; it is the particle count
+    up to the rounding of the TSC weights.  Momentum is the FP64 sum of vp after the kick."""
+    p = _params(fixed=fixed)
+    n = 24000
+    st = clustered_state(p, n, seed=17)
+    p.mass_p_cdm = float(p.ng) ** 3 / n
+    ref = oracle_lib.kick(p, st[0], st[1].copy(), st[3], 0.1, 0.05, fixed=fixed)
+    with _ctx(p, st) as ctx:
+        so = ctx.kick(0.1, 0.05)
+        _, vp, _, _ = ctx.download()
+        so2 = ctx.kick(0.1, 0.05)
+    got = (so.mass_pm1, so.mass_pm2, so.mass_pm3)
+    for lvl in range(3):
+        assert abs(got[lvl] - n) < 1e-6 * n, (lvl, got[lvl])
+        if fixed:
+            assert got[lvl] == ref.mass[lvl], (lvl, got[lvl], ref.mass[lvl])
+        else:
+            assert abs(got[lvl] - ref.mass[lvl]) < 1e-9 * n, (lvl, got[lvl], ref.mass[lvl])
+    mom = vp.astype(np.float64).sum(axis=0)
+    scale = np.abs(vp).astype(np.float64).sum(axis=0)
+    for d in range(3):
+        assert abs(so.momentum[d] - mom[d]) <= 1e-12 * scale[d], (d, so.momentum[d], mom[d])
+    # deterministic: the same density gives the same sums on a second kick
+    if fixed:
+        assert (so2.mass_pm1, so2.mass_pm2, so2.mass_pm3) == got

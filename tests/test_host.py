@@ -71,3 +71,69 @@ def test_linear_power_shape():
     # growth scales as D^2
     assert np.allclose(cosmology.linear_power(k, 0.5, p) / P, (cosmology.growth_cpt(0.5, p.omega_m, p.omega_l)
                                                                / cosmology.growth_cpt(1.0, p.omega_m, p.omega_l)) ** 2)
+
+
+def _bg_at(a):
+    tab = cosmology.expansion_table(0.6817, 0.3013, 5.0467e-5)
+    bg = cosmology.Background.from_table(tab)
+    bg.init_cursor(a)
+    return bg
+
+
+def test_timestep_takes_the_smallest_criterion():
+    """timestep.f90:34: dt = min(dt_e, dt_pm1, dt_pm2, dt_pm3, dt_refine*dt_pp, dt_vmax); each
+    criterion in turn is made the smallest and must be the step taken, with dt_old the
+    previous dt, the step counter advanced and a_mid = a + da/2 (timestep.f90:14-15,65)."""
+    names = ("dt_pm1", "dt_pm2", "dt_pm3", "dt_pp", "dt_vmax")
+    for k, name in enumerate(names):
+        a0 = 1 / 40.0
+        bg = _bg_at(a0)
+        st = cosmology.StepState(a=a0, dt=0.0123)
+        for m, other in enumerate(names):
+            setattr(st, other, 0.5 + 0.1 * m)
+        setattr(st, name, 1.5e-3 * (k + 1))
+        cosmology.timestep(bg, st, [49.0, 0.0])
+        assert st.dt == np.float32(1.5e-3 * (k + 1)), name
+        assert st.dt_old == 0.0123 and st.timestep == 1
+        da = st.a - a0
+        assert da > 0 and abs(st.a_mid - (a0 + da / 2)) < 1e-7
+        assert not st.checkpoint_step
+
+
+def test_timestep_expansion_limit_matches_matter_era():
+    """With every force criterion loose the step is the expansion limit ra = da/(a+da) <=
+    ra_max = 0.1 (timestep.f90:20-33), below dt_max = 1.  In the code's time unit
+    da/dt = (2/3) a^1.5 in the matter era (the table's omHsq*H(a)*a^3 with
+    H = H0 sqrt(om) a^-1.5), so a^-1/2 falls by dt/3: ra = 0.1 (a1 = 10a/9) needs
+    dt = 3 a^-1/2 (1 - sqrt(9/10)).  At a = 0.1 that is 0.487; Lambda and radiation move it
+    by ~0.1%.  At a = 1/50 the same formula gives 1.09 > dt_max, so dt = dt_max there."""
+    for a0, want in ((0.1, 3 / np.sqrt(0.1) * (1 - np.sqrt(0.9))), (1 / 50.0, 1.0)):
+        bg = _bg_at(a0)
+        st = cosmology.StepState(a=a0)
+        cosmology.timestep(bg, st, [49.0, 0.0])
+        da = st.a - a0
+        ra = da / (a0 + da)
+        assert ra <= 0.1 + 1e-6
+        assert abs(st.dt - want) / want < 0.01, (a0, st.dt, want)
+        if want < 1.0:
+            assert ra > 0.099
+
+
+def test_timestep_snaps_to_the_checkpoint():
+    """A step that would pass the next checkpoint is shrunk until |(a+da)/a_next - 1| < 1e-6
+    (timestep.f90:47-61); reaching the last checkpoint sets final_step."""
+    a_next = 1 / 11.0
+    a0 = a_next * 0.999
+    bg = _bg_at(a0)
+    st = cosmology.StepState(a=a0, cur_checkpoint=2)
+    st.dt_pm1 = st.dt_pm2 = st.dt_pm3 = st.dt_pp = st.dt_vmax = 0.05
+    cosmology.timestep(bg, st, [49.0, 10.0])
+    assert st.checkpoint_step and st.final_step
+    assert abs(st.a / a_next - 1) < 2e-6
+    assert st.dt < 0.05
+    # one checkpoint still ahead: the snap happens but the run is not over
+    bg = _bg_at(a0)
+    st = cosmology.StepState(a=a0, cur_checkpoint=2)
+    st.dt_pm1 = st.dt_pm2 = st.dt_pm3 = st.dt_pp = st.dt_vmax = 0.05
+    cosmology.timestep(bg, st, [49.0, 10.0, 5.0])
+    assert st.checkpoint_step and not st.final_step

@@ -132,3 +132,20 @@ def test_power_spectrum_invariants(oracle_lib, nw):
     c = oracle_lib.power(p, lat[0], lat[3], nw)
     assert np.isnan(c.alpha) and c.n_done == 0
     assert np.array_equal(c.xi[1:, 4], c.xi[1:, 3])
+
+
+def test_oracle_mass_sums_are_particle_count(oracle_lib):
+    """The reference's mass check (kick.f90:42,72,242): each level's density summed over its
+    physical cells is the particle count, up to the rounding of the TSC weights."""
+    from cube_nu_b200.params import DEPOSIT_FIXED, config_small
+    from tests.helpers import clustered_state
+
+    p = config_small(ng=32, nnt=1, nns=2, np_nc=2, izipx=2)
+    p.deposit_mode = DEPOSIT_FIXED
+    n = 3000
+    st = clustered_state(p, n, seed=2)
+    p.mass_p_cdm = float(p.ng) ** 3 / n
+    for fixed in (False, True):
+        out = oracle_lib.kick(p, st[0], st[1].copy(), st[3], 0.1, 0.05, fixed=fixed)
+        for m in out.mass:
+            assert abs(m - n) < 1e-6 * n, (fixed, list(out.mass))

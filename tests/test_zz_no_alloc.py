@@ -133,6 +133,17 @@ def test_noalloc_density_rejects_oversize_and_bad_counts():
     p.mass_p_cdm = float(p.ng) ** 3 / 5000
     rc, _ = _noalloc_density(L, p, st, np_arg=4990)
     assert rc == CUBE_E_COUNT, _last_error(L)
+    # a negative count whose total still equals np: rejected, not deposited around cell 0
+    bad = list(st)
+    r = bad[3].astype(np.int32).copy()
+    r[np.flatnonzero(r > 0)[0]] += 3
+    zero = np.flatnonzero(r == 0)[0]
+    r[zero] = -3
+    assert r.sum() == 5000 and r.min() < 0
+    bad[3] = r
+    rc, _ = _noalloc_density(L, p, bad)
+    assert rc == CUBE_E_COUNT, _last_error(L)
+    assert "negative" in _last_error(L)
     # and a valid call right after still matches the context path
     ref = _context_density(p, st)
     rc, got = _noalloc_density(L, p, st)
