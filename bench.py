@@ -7,7 +7,11 @@ compressed coordinates, Zel'dovich ICs at z=49 (EH no-wiggle, A_s), reference
 adaptive timestep.  One JSON line on rank 0.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload 512|128] [--deposit fixed|plain]
+                  [--workload 512|128] [--deposit fixed|plain] [--graph on|off] [--compare on|off]
+
+The headline is the chosen form (int64 fixed-point deposit, each step one CUDA graph);
+the plain form (FP32 atomics, eager launches) is timed in the same run over the same steps
+and both are reported, with the relative P(k) difference of their final states.
 
 --impl reference times the CPU restatement of the reference path (oracle/, the
 reference Fortran cannot be built here) on the host cores over a bounded sample of
@@ -35,10 +39,10 @@ from cube_nu_b200.params import DEPOSIT_FIXED, DEPOSIT_FP32, config_512, config_
 
 METRIC = "particle-steps/s P3M KDK @512^3"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
-# DRAM bytes (read + write) per class-2 PM3 box of 144^3, measured with ncu on the proxy
-# workload (one launch over 64 boxes; profiles/pm3_kernels_proxy.md, and for the
-# owner-computes deposit profiles/deposit_pm3_owner_proxy.md).  Traffic grows with the
-# number of boxes, so a launch over B such boxes moves B times these.
+# DRAM bytes (read + write) per class-2 PM3 box of 144^3, measured once with ncu on the
+# proxy workload (one launch over 64 boxes) and kept here as constants: the 512^3 launch is
+# too large to capture.  Traffic grows with the number of boxes, so a launch over B such
+# boxes moves B times these.  The bench line labels the figure proxy_ncu_constant.
 PM3_TRAFFIC_PER_BOX = {
     "deposit_pm3": (15048960 + 707247360) / 64,
     "fft_z_green_pm3": 1.910046e9 / 64,
@@ -244,14 +248,99 @@ def pinned_like(a):
     return out, t
 
 
+def pinned_state(st):
+    """Pinned host copies of a particle state (for the end-to-end leg)."""
+    out = []
+    for a in st:
+        h, _ = pinned_like(a)
+        out.append(h)
+    return out
+
+
+def run_form(p, args, local, dist, rank, replay=None, timed=True, want_base=False):
+    """IC on the device, W warm-up steps and K timed steps of one form of the step.
+
+    replay: the (dt, dt_old, a_mid, vz_max) of every step of another run, replayed here so
+    both forms take the same steps; else the reference's adaptive timestep chooses them.
+    Returns the timing, the per-kernel profile, the step inputs and outputs, the context
+    (still open) and the state at the start of the timed steps when want_base."""
+    import torch
+
+    ctx, d = device_ic(p, seed=1 + rank, device=local)
+    n = d["nplocal"]
+    tab = cosmology.expansion_table(p.h0, p.omega_m, p.omega_r)
+    bg = cosmology.Background.from_table(tab)
+    S = cosmology.StepState(a=d["a"], dt_vmax=d["dt_vmax"], vz_max=d["vz_max"])
+    bg.init_cursor(S.a)
+    zck = [49.0, 0.0]
+    steps_in = []
+
+    def one_step(i):
+        if replay is not None:
+            dt, dt_old, a_mid, vz = replay[i]
+        else:
+            cosmology.timestep(bg, S, zck)
+            dt, dt_old, a_mid, vz = S.dt, S.dt_old, S.a_mid, S.vz_max
+        so = ctx.step(dt, dt_old, a_mid, vz)
+        steps_in.append((dt, dt_old, a_mid, vz))
+        S.dt_pm1, S.dt_pm2, S.dt_pm3, S.dt_pp, S.dt_vmax = so.dt_pm1, so.dt_pm2, so.dt_pm3, so.dt_pp, so.dt_vmax
+        S.vz_max = so.vz_max
+        return so
+
+    for i in range(args.warmup):
+        if i == args.warmup - 1:
+            ctx.profile(True)  # a graph is captured with its timer events before the timed steps
+        one_step(i)
+    base = ctx.download() if want_base else None
+    base_args = (S.dt, S.dt, S.a_mid, S.vz_max)
+    ctx.profile(True)
+    launches0 = ctx.launches()
+    clocks = Clocks(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_wall = time.perf_counter()
+    dev_ms = 0.0
+    stage = np.zeros(7)
+    sos = []
+    for i in range(args.steps):
+        so = one_step(args.warmup + i)
+        dev_ms += so.tcat[6]
+        stage += np.array(list(so.tcat)[:7])
+        sos.append(so)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = ctx.launches() - launches0
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    dev_s, t_wall = over_ranks([dev_ms / 1e3, t_wall], "max", dist)
+    return {"ctx": ctx, "n": n, "d": d, "S": S, "bg": bg, "zck": zck, "steps_in": steps_in, "sos": sos,
+            "dev_s": dev_s, "t_wall": t_wall, "stage": stage, "clk": clk, "launches": launches, "prof": prof,
+            "base": base, "base_args": base_args}
+
+
+def pk_grid(p):
+    """cicpower grid of the precision check: 2*ng as utilities/Makefile's FFTFINE builds it,
+    capped at 1024^3 (the 512^3 workload's 2048^3 grid would hold ~100 GB beside the step)."""
+    return min(2 * p.ng, 1024)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="512", choices=["512", "128", "proxy"])
     ap.add_argument("--deposit", default="fixed", choices=["fixed", "plain"])
+    ap.add_argument("--graph", default="on", choices=["on", "off"],
+                    help="replay each step as one captured CUDA graph (cube_params.step_graph)")
+    ap.add_argument("--compare", default="on", choices=["on", "off"],
+                    help="also time the plain form (FP32 atomics, eager) over the same steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-json", default="")
     ap.add_argument("--pk", type=int, default=0,
@@ -266,6 +355,7 @@ def main():
     p, desc = workload(args.workload)
     fixed = args.deposit == "fixed"
     p.deposit_mode = DEPOSIT_FIXED if fixed else DEPOSIT_FP32
+    p.step_graph = args.graph == "on"
 
     import torch
 
@@ -284,75 +374,20 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    ctx, d = device_ic(p, seed=1 + rank, device=local)
-    n = d["nplocal"]
-    st = ctx.download()
-    tab = cosmology.expansion_table(p.h0, p.omega_m, p.omega_r)
-    bg = cosmology.Background.from_table(tab)
-    S = cosmology.StepState(a=d["a"], dt_vmax=d["dt_vmax"], vz_max=d["vz_max"])
-    bg.init_cursor(S.a)
-    zck = [49.0, 0.0]
-
-    def one_step():
-        cosmology.timestep(bg, S, zck)
-        so = ctx.step(S.dt, S.dt_old, S.a_mid, S.vz_max)
-        S.dt_pm1, S.dt_pm2, S.dt_pm3, S.dt_pp, S.dt_vmax = so.dt_pm1, so.dt_pm2, so.dt_pm3, so.dt_pp, so.dt_vmax
-        S.vz_max = so.vz_max
-        return so
-
-    first = None
-    for _ in range(args.warmup):
-        so = one_step()
-        first = first or (S.dt, S.dt_old, S.a_mid, S.vz_max)
-    # state at the start of the timed region (for the CPU baseline sample)
-    base_state = ctx.download() if (rank == 0 and not args.no_cpu_baseline) else None
-    base_args = (S.dt, S.dt, S.a_mid, S.vz_max)
-
-    ctx.profile(True)
-    launches0 = ctx.launches()
-    clocks = Clocks(local)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    t_wall = time.perf_counter()
-    dev_ms = 0.0
-    stage = np.zeros(7)
-    sos = []
-    for _ in range(args.steps):
-        so = one_step()
-        dev_ms += so.tcat[6]
-        stage += np.array(list(so.tcat)[:7])
-        sos.append(so)
-    torch.cuda.synchronize()
-    t_wall = time.perf_counter() - t_wall
-    if dist:
-        dist.barrier()
-    clk = clocks.stop()
-    launches = ctx.launches() - launches0
-    prof = ctx.profile_read()
-    ctx.profile(False)
-    # max over ranks of the device time
-    dev_s, t_wall = over_ranks([dev_ms / 1e3, t_wall], "max", dist)
+    R = run_form(p, args, local, dist, rank, want_base=(rank == 0 and not args.no_cpu_baseline))
+    ctx, n, S, bg, zck = R["ctx"], R["n"], R["S"], R["bg"], R["zck"]
     total_particles = over_ranks([n], "sum", dist)[0]
-    value = job_rate(total_particles, args.steps, dev_s)
+    value = job_rate(total_particles, args.steps, R["dev_s"])
+    nw = pk_grid(p)
+    xi_chosen = ctx.power(nw, n_corr=0)[0]
 
     # ---------------- end to end through the C ABI with pinned host buffers ----------------
-    xh, xt = pinned_like(st[0])
-    vh, vt = pinned_like(st[1])
-    ph, pt = pinned_like(st[2])
-    rh, rt = pinned_like(st[3])
-    cur = ctx.download()
-    xh[...] = cur[0]
-    vh[...] = cur[1]
-    ph[...] = cur[2]
-    rh[...] = cur[3]
-    e2e_steps = args.steps
+    xh, vh, ph, rh = pinned_state(ctx.download())
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t_e2e = time.perf_counter()
-    for _ in range(e2e_steps):
+    for _ in range(args.steps):
         # host-resident state: cube_gpu_step_host uploads it from the pinned arrays, steps,
         # and writes the new state back (copies the step does not wait for overlap it)
         cosmology.timestep(bg, S, zck)
@@ -363,7 +398,7 @@ def main():
     t_e2e = time.perf_counter() - t_e2e
     t_e2e = over_ranks([t_e2e], "max", dist)[0]
     io_bytes = n * (3 * p.izipx + 12 + 8) + p.ncells * 4
-    e2e_value = job_rate(total_particles, e2e_steps, t_e2e)
+    e2e_value = job_rate(total_particles, args.steps, t_e2e)
 
     analysis = None
     if args.pk:
@@ -373,10 +408,26 @@ def main():
         xi, _, po = ctx.power(args.pk)
         analysis = {"pk_nw": args.pk, "pk_ms": round(po.ms, 3), "pk_alpha": float(po.alpha),
                     "pk_corrections": po.n_corr_done, "pk_nbin": int(po.nbin)}
+    ctx.close()
+
+    # ---------------- the plain form over the same steps ----------------
+    plain = None
+    if args.compare == "on" and (fixed or p.step_graph):
+        q, _ = workload(args.workload)
+        q.deposit_mode = DEPOSIT_FP32
+        q.step_graph = False
+        P = run_form(q, args, local, dist, rank, replay=R["steps_in"])
+        xi_plain = P["ctx"].power(nw, n_corr=0)[0]
+        P["ctx"].close()
+        plain = {"value": job_rate(total_particles, args.steps, P["dev_s"]),
+                 "ms_per_step": P["dev_s"] * 1e3 / args.steps, "xi": xi_plain,
+                 "stage": P["stage"] / args.steps}
 
     if rank == 0:
         peaks, peak_kind = load_peaks()
+        sos = R["sos"]
         napm = list(sos[-1].napm)
+        prof = R["prof"]
         # roofline of the dominant kernel class
         rows = []
         for name, (ms, cnt) in prof.items():
@@ -397,34 +448,73 @@ def main():
                 traffic = int(PM3_TRAFFIC_PER_BOX[dom[1]] * napm[2] / launches_per_step)
             roof = {"kernel": dom[1], "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                     "frac": round(ach / hbm, 4), "traffic": traffic,
-                    "traffic_source": ("ncu DRAM bytes of one 64-box launch (proxy workload), scaled by boxes"
-                                       if traffic else None), "peak_kind": peak_kind,
-                    "avg_launch_ms": round(dom[3], 4), "launches_per_step": launches_per_step,
+                    "traffic_source": ("proxy_ncu_constant: ncu DRAM bytes of one 64-box launch of the proxy "
+                                       "workload, scaled by boxes (not measured in this run)" if traffic else None),
+                    "peak_kind": peak_kind, "avg_launch_ms": round(dom[3], 4),
+                    "launches_per_step": launches_per_step,
                     "algorithmic_bytes_per_launch": int(dom[4] / launches_per_step)}
+        # PP on the FP32 pipe: 9 flops per candidate pair (dx 3, r^2 5, compare 1) and 35 more
+        # per pair within range (sqrt, divide, two degree-6 F_ra, scale, accumulate)
+        pp = None
+        pp_ms, pp_n = prof.get("pp", (0.0, 0))
+        if pp_n:
+            cand = sum(int(so.pp_candidates) for so in sos)
+            pairs = sum(int(so.pp_pairs) for so in sos)
+            flops = 9.0 * cand + 35.0 * pairs
+            mhz = R["clk"].get("sm_mhz") or 1965.0
+            fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12  # TFLOP/s at the sampled SM clock
+            tf = flops / (pp_ms / 1e3) / 1e12
+            pp = {"tflops": round(tf, 3), "fp32_peak_tflops": round(fp32_peak, 1), "frac": round(tf / fp32_peak, 4),
+                  "candidates_per_step": cand // args.steps, "pairs_per_step": pairs // args.steps,
+                  "ms_per_step": round(pp_ms / args.steps, 3)}
         cpu = None
-        if base_state is not None:
-            v, cores, sample, secs = cpu_baseline(p, base_state, *base_args)
+        if R["base"] is not None:
+            v, cores, sample, secs = cpu_baseline(p, R["base"], *R["base_args"])
             cpu = {"value": round(v, 1), "unit": "particle-steps/s", "cores": cores, "kind": "port",
-                   "sample": sample}
+                   "sample": sample, "sample_seconds": round(secs, 2), "extrapolated_to_full_step": True}
+        forms = {"chosen": {"value": round(value, 1), "ms_per_step": round(R["dev_s"] * 1e3 / args.steps, 3),
+                            "deposit": "int64 fixed-point" if fixed else "fp32 atomics",
+                            "graph": bool(p.step_graph)}}
+        precision = None
+        if plain:
+            forms["plain"] = {"value": round(plain["value"], 1), "ms_per_step": round(plain["ms_per_step"], 3),
+                              "deposit": "fp32 atomics", "graph": False,
+                              "stage_ms_per_step": {k: round(float(v), 3) for k, v in
+                                                    zip(("drift", "pm1", "pm2", "pm3", "pp", "kick", "step"),
+                                                        plain["stage"])}}
+            forms["chosen_over_plain"] = round(value / plain["value"], 4)
+            a, b = xi_chosen, plain["xi"]
+            knyq = math.pi * nw / p.box
+            sel = (b[:, 0] > 0) & (b[:, 1] > 0) & (b[:, 1] < knyq / 2)
+            rel = np.abs(a[sel, 2] / b[sel, 2] - 1)
+            precision = {"dP_over_P_max_chosen_vs_plain": float(rel.max()), "bins": int(sel.sum()),
+                         "grid": nw, "k_max_hmpc": round(knyq / 2, 4),
+                         "note": "both forms after the same steps; against the FP64 oracle see tests/test_precision.py"}
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "particle-steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_s * 1e3 / args.steps, 3),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(R["dev_s"] * 1e3 / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
             "data": "synthetic (Zel'dovich ICs z=49, EH no-wiggle, seeded)",
             "config": {"workload": desc, "particles_per_gpu": n, "ng": p.ng, "box": p.box,
                        "deposit": "int64 fixed-point" if fixed else "fp32 atomics",
+                       "step_graph": bool(p.step_graph),
                        "timestep": "reference adaptive (timestep.f90)", "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (%.1f GB particle state)" % (n * 26 / 1e9),
-                       "pm3_classes": napm[2:6], "a_end": S.a},
+                       "pm3_classes": napm[2:6], "a_end": R["S"].a},
             "e2e": {"value": round(e2e_value, 1), "unit": "particle-steps/s", "h2d_bytes_per_step": io_bytes,
                     "d2h_bytes_per_step": io_bytes},
-            "gpu_launches": int(launches),
+            "gpu_launches": int(R["launches"]),
             "roofline": roof,
+            "pp_fp32": pp,
+            "forms": forms,
+            "precision": precision,
             "cpu_baseline": cpu,
-            "clocks": clk,
-            "wall_s": round(t_wall, 3),
+            "clocks": R["clk"],
+            "wall_s": round(R["t_wall"], 3),
             "stage_ms_per_step": {k: round(float(v) / args.steps, 3) for k, v in
-                                  zip(("drift", "pm1", "pm2", "pm3", "pp", "kick", "step"), stage)},
+                                  zip(("drift", "pm1", "pm2", "pm3", "pp", "kick", "step"), R["stage"])},
+            "mass_check": {"pm1": sos[-1].mass_pm1, "pm2": sos[-1].mass_pm2, "pm3": sos[-1].mass_pm3,
+                           "particles": n},
         }
         if analysis:
             line["analysis"] = analysis
@@ -434,7 +524,6 @@ def main():
                                         "alg_bytes_per_step": r[4], "ms_per_step": r[5]} for r in rows],
                            "steps": args.steps}, f, indent=1)
         print(json.dumps(line), flush=True)
-    ctx.close()
     if dist:
         dist.destroy_process_group()
     return 0

@@ -61,7 +61,7 @@ class StepOut(ctypes.Structure):
         ("f2max_pp", ctypes.c_float), ("napm", ctypes.c_int32 * 8), ("nplocal", ctypes.c_int64),
         ("pp_pairs", ctypes.c_int64), ("tcat", ctypes.c_float * 16),
         ("mass_pm1", ctypes.c_double), ("mass_pm2", ctypes.c_double), ("mass_pm3", ctypes.c_double),
-        ("momentum", ctypes.c_double * 3),
+        ("momentum", ctypes.c_double * 3), ("pp_candidates", ctypes.c_int64),
     ]
 
 

@@ -232,3 +232,41 @@ def vfactor(a, om, ol) -> float:
     km = (1 - om - ol) / om
     H = 2 / (3 * math.sqrt(a ** 3)) * math.sqrt(1 + a * km + a ** 3 * lm)
     return a ** 2 * H
+
+
+def fixed_steps(bg: Background, a_start: float, a_end: float, nsteps: int):
+    """A fixed-step schedule: `nsteps` KDK steps of equal code time dt from a_start to
+    a_end, for runs quoted at a fixed step count (the reference's own timestep is
+    adaptive, timestep.f90:4-110).  Returns [(dt, dt_old, a_mid, a_next)] per step, with
+    a_mid = a + da/2 and da from the same table interpolation (power_nu.f90:8-35); the
+    closing half drift is (dt_old=0, dt=dt) as main.f90:39-41 does at a checkpoint."""
+    if nsteps < 1 or not (0 < a_start < a_end <= 1):
+        raise ValueError("need nsteps >= 1 and 0 < a_start < a_end <= 1")
+    f = np.float32
+    bg.init_cursor(a_start)
+    target = float(f(a_end) - f(a_start))
+    lo, hi = 0.0, 1.0
+    while float(bg.expansion(a_start, hi)) < target:
+        hi *= 2
+        if hi > 1e6:
+            raise ValueError("a_end not reached by the expansion table")
+    for _ in range(80):
+        mid = 0.5 * (lo + hi)
+        bg.init_cursor(a_start)
+        if float(bg.expansion(a_start, mid)) < target:
+            lo = mid
+        else:
+            hi = mid
+    dt = float(f(0.5 * (lo + hi) / nsteps))
+    out = []
+    a = float(f(a_start))
+    bg.init_cursor(a)
+    dt_old = 0.0
+    for _ in range(nsteps):
+        da = f(bg.expansion(a, dt))
+        a_mid = float(f(a) + da / f(2))
+        a_next = float(f(a) + da)
+        out.append((dt, dt_old, a_mid, a_next))
+        dt_old = dt
+        a = a_next
+    return out

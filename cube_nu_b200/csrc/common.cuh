@@ -27,6 +27,18 @@ struct Geo {
   int64_t ncells;    // nc^3
 };
 
+// Per-step scalars, written by the host into device memory at the start of every step
+// (one small copy, which a captured step graph replays), so that no kernel of the step
+// takes them by value.  The host derives dt_mid, nlayer and the PP factors exactly as the
+// reference does (drift.f90:21,26; kick.f90:283-285).
+struct StepDev {
+  float dt, dt_old, a_mid, vz_max;
+  float dt_mid;       // (dt_old + dt) / 2
+  int nlayer;         // 2*ceiling(dt_mid*vz_max/ratio_cs)+2
+  float pp_mass;      // PP force factor (mass_p, times (1-f_nu)^2 with neutrinos)
+  float pp_vscale;    // a_mid*dt/6/pi
+};
+
 __host__ __device__ inline int wrapi(int a, int n) {
   a %= n;
   return a < 0 ? a + n : a;

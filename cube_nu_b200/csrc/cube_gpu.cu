@@ -59,18 +59,51 @@ enum KClass {
   K_DRIFT_DEST, K_DRIFT_SCATTER, K_DRIFT_SORT, K_DRIFT_GATHER, K_SCAN, K_DEP_PM1, K_FFT_PM1, K_F2_PM1, K_INT_PM1,
   K_DEP_PM2, K_FFTX_PM2, K_FFTY_PM2, K_FFTZ_PM2, K_FFTC_PM2, K_F2_PM2, K_INT_PM2, K_DEP_PM3, K_FFTX_PM3, K_FFTY_PM3,
   K_FFTZ_PM3, K_FFTC_PM3, K_F2_PM3, K_INT_PM3, K_PP, K_CLASSIFY, K_GREEN, K_FILL, K_PK_DEP, K_PK_FFT, K_PK_BIN,
-  K_PK_ALIAS, K_MOMENTUM, K_NCLASS
+  K_PK_ALIAS, K_MOMENTUM, K_MASS, K_NCLASS
 };
 const char* const KNAMES[K_NCLASS] = {
     "drift_dest", "drift_scatter", "drift_sort", "drift_gather", "scan", "deposit_pm1", "fft_pm1", "f2max_pm1",
     "interp_pm1", "deposit_pm2", "fft_x_pm2", "fft_y_pm2", "fft_z_green_pm2", "fft_c2r_pm2", "f2max_pm2",
     "interp_pm2", "deposit_pm3", "fft_x_pm3", "fft_y_pm3", "fft_z_green_pm3", "fft_c2r_pm3", "f2max_pm3",
-    "interp_pm3", "pp", "classify", "green", "fill_pcell", "pk_deposit", "pk_fft", "pk_bin", "pk_alias", "momentum"};
+    "interp_pm3", "pp", "classify", "green", "fill_pcell", "pk_deposit", "pk_fft", "pk_bin", "pk_alias", "momentum", "mass_pm3"};
 
 struct ProfRec {
   int cls;
   int a, b;  // event pool indices
 };
+
+// Results of a step that the host reads back with one copy at its end.
+struct StepRes {
+  float red[64];  // f2max[4] (pm1, pm2, pm3, pp), vmax[3][3] at 8.. (pm2, pm3, pp)
+  unsigned long long pairs, cand;  // PP pairs within range, PP candidate pairs
+  unsigned err;       // device error word (CUBE_DEVERR_*)
+  unsigned overflow;  // a PM3 class outgrew the captured plan
+  int32_t napm[8];
+  int64_t total;      // particles placed by the drift
+  unsigned long long msum[3 * MASS_SLOTS * MASS_STRIDE];
+  double mom[3 * MOM_BLOCKS];
+};
+
+// One captured step (drift + kick) as an executable CUDA graph, for one particle-buffer
+// parity, particle count and PM3 plan.
+struct StepGraph {
+  cudaGraphExec_t exec = nullptr;
+  int parity = 0;
+  int64_t np = 0;
+  PM3Plan plan;
+  bool prof = false;
+  int64_t kernels = 0;                 // kernel launches in one replay
+  std::vector<cudaEvent_t> events;     // per-kernel timer events recorded by the graph
+  std::vector<ProfRec> recs;
+};
+
+bool same_plan(const PM3Plan& a, const PM3Plan& b) {
+  if (a.nk != b.nk || a.per_max != b.per_max) return false;
+  for (int i = 2; i <= 5; ++i)
+    if (a.cap[i] != b.cap[i] || a.per[i] != b.per[i] || a.kbase[i] != b.kbase[i] || a.skip[i] != b.skip[i])
+      return false;
+  return true;
+}
 
 }  // namespace
 
@@ -96,18 +129,35 @@ struct cube_ctx {
   int32_t* dest = nullptr;
   uint64_t *key = nullptr, *skey = nullptr;
   uint32_t* ssrc = nullptr;
-  // reductions: f2max[4] (pm1, pm2, pm3, pp), vmax[3][3] (pm2, pm3, pp)
+  // step results (device) and their pinned host copy; the pointers below point into rdev:
+  // reductions f2max[4] (pm1, pm2, pm3, pp) and vmax[3][3] (pm2, pm3, pp); FP64 mass sums
+  // [level 1..3][MASS_SLOTS] (int64 or double by deposit form); momentum partials
+  // [MOM_BLOCKS][3]; the error word, class histogram, drift total and plan overflow flag
+  StepRes* rdev = nullptr;
+  StepRes* rhost = nullptr;
   float* red = nullptr;
-  unsigned long long* pairs = nullptr;
-  // FP64 reductions: mass sums [level 1..3][MASS_SLOTS] (int64 or double by deposit form),
-  // momentum partials [MOM_BLOCKS][3]
+  unsigned long long* pairs = nullptr;  // pairs[0] in range, pairs[1] candidates
   unsigned long long* msum = nullptr;
   double* mom = nullptr;
   unsigned* err = nullptr;
-  int32_t *ires = nullptr, *napm = nullptr;
-  int32_t* box_slot = nullptr;  // [nchunk][ns3]
-  int32_t* h_slots = nullptr;   // pinned host copy
-  int64_t slot_chunks = 0;
+  unsigned* overflow = nullptr;
+  int32_t* napm = nullptr;
+  int64_t* total = nullptr;
+  int32_t* ires = nullptr;
+  int32_t* h_ires = nullptr;  // pinned
+  // per-step scalars (device) and their pinned host staging copy
+  StepDev* sd = nullptr;
+  StepDev* h_sd = nullptr;
+  // PM3 class lists: box_slot [nk][ns3], box_sub [nk][per_max]
+  int32_t* box_slot = nullptr;
+  int32_t* box_sub = nullptr;
+  int64_t slot_cap = 0, sub_cap = 0;  // allocated entries
+  // captured steps (cube_params.step_graph)
+  std::vector<StepGraph> graphs;
+  StepGraph* cap_graph = nullptr;  // the graph being captured (timers and launches go to it)
+  int32_t napm_est[8] = {0};       // class histogram of the last step (plan of the next capture)
+  bool have_est = false;
+  void* xp_base = nullptr;         // parity of the particle buffers: xp == xp_base or not
   // meshes
   void* arena = nullptr;
   size_t arena_bytes = 0;
@@ -149,20 +199,44 @@ int pool_event(cube_ctx* c) {
   return c->pool_used++;
 }
 
+// Timer events: during a capture they come from the graph's own list and are recorded as
+// graph event nodes (cudaEventRecordExternal); otherwise from the context pool.
+int timer_event(cube_ctx* c) {
+  if (c->cap_graph) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    c->cap_graph->events.push_back(e);
+    return (int)c->cap_graph->events.size() - 1;
+  }
+  return pool_event(c);
+}
+
+void record_timer(cube_ctx* c, int i) {
+  if (c->cap_graph) cudaEventRecordWithFlags(c->cap_graph->events[i], c->s, cudaEventRecordExternal);
+  else cudaEventRecord(c->pool[i], c->s);
+}
+
+// A context event (ev[]) marking a stage boundary; a graph event node while capturing.
+cudaError_t mark(cube_ctx* c, cudaEvent_t e) {
+  return c->cap_graph ? cudaEventRecordWithFlags(e, c->s, cudaEventRecordExternal) : cudaEventRecord(e, c->s);
+}
+
 void prof_begin(cube_ctx* c, int cls, int nlaunch, int& a) {
-  c->launches += nlaunch;
+  if (c->cap_graph) c->cap_graph->kernels += nlaunch;
+  else c->launches += nlaunch;
   a = -1;
   if (!c->prof) return;
-  a = pool_event(c);
-  cudaEventRecord(c->pool[a], c->s);
+  a = timer_event(c);
+  record_timer(c, a);
   (void)cls;
 }
 
 void prof_end(cube_ctx* c, int cls, int a) {
   if (!c->prof || a < 0) return;
-  const int b = pool_event(c);
-  cudaEventRecord(c->pool[b], c->s);
-  c->pending.push_back({cls, a, b});
+  const int b = timer_event(c);
+  record_timer(c, b);
+  if (c->cap_graph) c->cap_graph->recs.push_back({cls, a, b});
+  else c->pending.push_back({cls, a, b});
 }
 
 // After a stream synchronisation: fold the pending event pairs into the totals.
@@ -560,6 +634,16 @@ float* green3(cube_ctx* c, int iapm) {
   return c->green3[iapm];
 }
 
+void drop_graphs(cube_ctx* c) {
+  if (c->graphs.empty()) return;
+  if (c->s) cudaStreamSynchronize(c->s);
+  for (auto& g : c->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (cudaEvent_t e : g.events) cudaEventDestroy(e);
+  }
+  c->graphs.clear();
+}
+
 // Copy a box field (n planes of n rows of n values, row pitch `rp` and plane pitch `psb`
 // bytes) into a dense capture buffer when it is the one requested.
 void maybe_capture(cube_ctx* c, int level, int64_t box, int what, const void* src, int n, bool fixed_int,
@@ -668,14 +752,22 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
   CK(cudaMalloc(&c->cstart, (nc3 + 1) * 8));
   CK(cudaMalloc(&c->cstart2, (nc3 + 1) * 8));
   CK(cudaMalloc(&c->scan_tmp, ((nc3 + 2047) / 2048 + 2) * 8));
-  CK(cudaMalloc(&c->red, 64 * sizeof(float)));
-  CK(cudaMalloc(&c->pairs, 8));
-  CK(cudaMalloc(&c->msum, 3 * MASS_SLOTS * 8));
-  CK(cudaMalloc(&c->mom, MOM_BLOCKS * 3 * sizeof(double)));
-  CK(cudaMalloc(&c->err, 4));
-  CK(cudaMemset(c->err, 0, 4));
+  CK(cudaMalloc(&c->rdev, sizeof(StepRes)));
+  CK(cudaMemset(c->rdev, 0, sizeof(StepRes)));
+  CK(cudaMallocHost(&c->rhost, sizeof(StepRes)));
+  c->red = c->rdev->red;
+  c->pairs = &c->rdev->pairs;
+  c->msum = c->rdev->msum;
+  c->mom = c->rdev->mom;
+  c->err = &c->rdev->err;
+  c->overflow = &c->rdev->overflow;
+  c->napm = c->rdev->napm;
+  c->total = &c->rdev->total;
+  CK(cudaMalloc(&c->sd, sizeof(StepDev)));
+  CK(cudaMemset(c->sd, 0, sizeof(StepDev)));
+  CK(cudaMallocHost(&c->h_sd, sizeof(StepDev)));
   CK(cudaMalloc(&c->ires, c->ns3 * 4));
-  CK(cudaMalloc(&c->napm, 8 * 4));
+  CK(cudaMallocHost(&c->h_ires, c->ns3 * 4));
   // Green tables of PM1 and PM2 (initialize.f90:247-258); PM3 classes on first use.
   rc = build_green(c, &c->green1, G.nc, G.apm1c, 0.f, (float)G.rcs);
   if (!rc) rc = build_green(c, &c->green2, G.ngt, G.apm2, G.apm1c * (float)G.rcs, 1.f);
@@ -692,16 +784,19 @@ int cube_gpu_destroy(cube_ctx* c) {
   if (!c) return 0;
   cudaSetDevice(c->device);
   if (c->s) cudaStreamSynchronize(c->s);
+  drop_graphs(c);
   void* bufs[] = {c->xp, c->xp2, c->vp, c->vp2, c->pid, c->pid2, c->pcell, c->pcell2, c->rhoc, c->rhoc2,
                   c->fill, c->biglist, c->nbig, c->cstart, c->cstart2, c->scan_tmp, c->dest, c->key, c->skey,
-                  c->ssrc, c->red, c->pairs, c->msum, c->mom, c->err, c->ires, c->napm, c->box_slot, c->arena, c->green1,
-                  c->green2, c->cap_buf};
+                  c->ssrc, c->rdev, c->sd, c->ires, c->box_slot, c->box_sub, c->arena, c->green1, c->green2,
+                  c->cap_buf};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (int i = 0; i < 8; ++i)
     if (c->green3[i]) cudaFree(c->green3[i]);
   for (auto& t : c->ffts) cudaFree(t.tw);
-  if (c->h_slots) cudaFreeHost(c->h_slots);
+  if (c->rhost) cudaFreeHost(c->rhost);
+  if (c->h_sd) cudaFreeHost(c->h_sd);
+  if (c->h_ires) cudaFreeHost(c->h_ires);
   for (int i = 0; i < 8; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
@@ -716,6 +811,7 @@ int cube_gpu_destroy(cube_ctx* c) {
 
 static int alloc_particles(cube_ctx* c, int64_t np) {
   if (np <= c->cap) return 0;
+  drop_graphs(c);
   const int64_t cap = std::max<int64_t>(np, c->P.np_capacity);
   void** ps[] = {&c->xp, &c->xp2, (void**)&c->vp, (void**)&c->vp2, (void**)&c->pid, (void**)&c->pid2,
                  (void**)&c->pcell, (void**)&c->pcell2, (void**)&c->dest, (void**)&c->key, (void**)&c->skey,
@@ -729,6 +825,7 @@ static int alloc_particles(cube_ctx* c, int64_t np) {
     CK(cudaMalloc(ps[i], sz[i] + 16));
   }
   c->cap = cap;
+  c->xp_base = c->xp;
   // mesh arena: everything that fits of what the largest level needs, within 70% of free memory
   const Geo& G = c->G;
   const bool fixed = c->P.deposit_mode == CUBE_DEPOSIT_FIXED;
@@ -775,6 +872,7 @@ int cube_gpu_upload(cube_ctx* c, const void* xp, const float* vp, const int64_t*
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->s));
   c->loaded = true;
+  c->have_est = false;
   return 0;
 }
 
@@ -790,6 +888,16 @@ int cube_gpu_download(cube_ctx* c, void* xp, float* vp, int64_t* pid, int32_t* r
   return 0;
 }
 
+// Map a device error word to the reference's fatal conditions.
+static int err_code(unsigned e) {
+  if (e & CUBE_DEVERR_DRIFT_RANGE) return fail(CUBE_E_RANGE, "drift: particle moved beyond the ghost depth");
+  if (e & CUBE_DEVERR_SEGMENT) return fail(CUBE_E_CAPACITY, "drift: destination cell exceeds max_segment");
+  if (e & CUBE_DEVERR_DEPOSIT_RANGE) return fail(CUBE_E_RANGE, "mass assignment out of range");
+  if (e & CUBE_DEVERR_INTERP_RANGE) return fail(CUBE_E_RANGE, "update velocity out of range");
+  return fail(CUBE_E_RANGE, "device error word " + std::to_string(e));
+}
+
+// Read and clear the device error word (synchronises the stream).
 static int check_err(cube_ctx* c) {
   unsigned e = 0;
   CK(cudaMemcpyAsync(&e, c->err, 4, cudaMemcpyDeviceToHost, c->s));
@@ -797,67 +905,91 @@ static int check_err(cube_ctx* c) {
   if (e) {
     CK(cudaMemsetAsync(c->err, 0, 4, c->s));
     CK(cudaStreamSynchronize(c->s));
-    if (e & CUBE_DEVERR_DRIFT_RANGE) return fail(CUBE_E_RANGE, "drift: particle moved beyond the ghost depth");
-    if (e & CUBE_DEVERR_SEGMENT) return fail(CUBE_E_CAPACITY, "drift: destination cell exceeds max_segment");
-    if (e & CUBE_DEVERR_DEPOSIT_RANGE) return fail(CUBE_E_RANGE, "mass assignment out of range");
-    if (e & CUBE_DEVERR_INTERP_RANGE) return fail(CUBE_E_RANGE, "update velocity out of range");
-    return fail(CUBE_E_RANGE, "device error word " + std::to_string(e));
+    return err_code(e);
   }
   return 0;
 }
 
-// drift.f90.  Enqueues the drift; returns after the error word is checked.  With
-// `defer_ids` the gather leaves the particle ids alone (the new id array is not written):
-// the caller applies the drift's permutation (c->ssrc) to them later with k_permute_ids,
-// from c->pid2 (the ids before the drift) into c->pid.
-static int drift_enqueue(cube_ctx* c, const cube_step_in* in, bool defer_ids = false) {
+// The step scalars as the reference derives them (drift.f90:21,26; kick.f90:283-285),
+// written to the pinned staging copy; `drift` validates nlayer for a drift.
+static int make_scalars(cube_ctx* c, const cube_step_in* in, bool drift, StepDev& d) {
   const Geo& G = c->G;
-  const float dt_mid = (in->dt_old + in->dt) / 2.f;
-  const int nlayer = 2 * (int)std::ceil(dt_mid * in->vz_max / (float)G.rcs) + 2;
-  if (nlayer <= 0 || nlayer > 65535) return fail(CUBE_E_ARG, "bad nlayer from dt_mid*vz_max");
+  d.dt = in->dt;
+  d.dt_old = in->dt_old;
+  d.a_mid = in->a_mid;
+  d.vz_max = in->vz_max;
+  d.dt_mid = (in->dt_old + in->dt) / 2.f;
+  d.nlayer = 2 * (int)std::ceil(d.dt_mid * in->vz_max / (float)G.rcs) + 2;
+  if (drift && (d.nlayer <= 0 || d.nlayer > 65535)) return fail(CUBE_E_ARG, "bad nlayer from dt_mid*vz_max");
+  d.pp_mass = (G.f_nu > 0.f) ? (float)((double)G.mass_p * ((1.0 - (double)G.f_nu) * (1.0 - (double)G.f_nu))) : G.mass_p;
+  d.pp_vscale = (float)((double)(in->a_mid * in->dt / 6.f) / M_PI);
+  return 0;
+}
+
+// Stage the scalars and copy them to the device on the context stream (the previous
+// step's copy has completed: every step ends with a stream synchronisation).
+static int upload_scalars(cube_ctx* c, const StepDev& d) {
+  *c->h_sd = d;
+  CK(cudaMemcpyAsync(c->sd, c->h_sd, sizeof(StepDev), cudaMemcpyHostToDevice, c->s));
+  return 0;
+}
+
+// drift.f90, enqueued without any host synchronisation; the drifted arrays land in the
+// second buffers and the particle total in StepRes.total.  With `defer_ids` the gather
+// leaves the particle ids alone (the new id array is not written): the caller applies the
+// drift's permutation (c->ssrc) to them later with k_permute_ids, from c->pid (the ids
+// before the drift, c->pid2 after swap_drift) into c->pid2 (c->pid after it).
+static void enqueue_drift(cube_ctx* c, bool defer_ids) {
+  const Geo& G = c->G;
   const int64_t np = c->np;
-  CK(cudaMemsetAsync(c->rhoc2, 0, G.ncells * 4, c->s));
-  CK(cudaMemsetAsync(c->fill, 0, G.ncells * 4, c->s));
-  CK(cudaMemsetAsync(c->nbig, 0, 4, c->s));
-  LAUNCH(c, K_DRIFT_DEST, 1, k_drift_dest<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->vp, c->pcell, c->cstart, dt_mid, nlayer, c->dest, c->key,
-                                           c->rhoc2, c->err));
+  cudaMemsetAsync(c->rhoc2, 0, G.ncells * 4, c->s);
+  cudaMemsetAsync(c->fill, 0, G.ncells * 4, c->s);
+  cudaMemsetAsync(c->nbig, 0, 4, c->s);
+  LAUNCH(c, K_DRIFT_DEST, 1, k_drift_dest<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->vp, c->pcell, c->cstart, c->sd,
+                                                                     c->dest, c->key, c->rhoc2, c->err));
   LAUNCH(c, K_SCAN, 3, exclusive_scan(c->rhoc2, c->cstart2, G.ncells, c->scan_tmp, c->s));
   LAUNCH(c, K_DRIFT_SCATTER, 1, k_drift_scatter<<<nblk(np), 256, 0, c->s>>>(np, c->dest, c->key, c->cstart2, c->fill, c->skey, c->ssrc));
   LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_small<<<nblk((G.ncells + 1) / 2 * 32), 256, 0, c->s>>>(G.ncells, c->rhoc2, c->cstart2, c->skey, c->ssrc,
                                                             c->biglist, c->nbig));
+  // long segments: one block per SM, each looping over the listed cells
   const int max_seg = c->P.max_segment > 0 ? std::min(c->P.max_segment, 16384) : 16384;
-  // One block per listed long segment; the grid is bounded by the cell count.
-  int nb_host = 0;
-  CK(cudaMemcpyAsync(&nb_host, c->nbig, 4, cudaMemcpyDeviceToHost, c->s));
-  CK(cudaStreamSynchronize(c->s));
-  if (nb_host > 0)
-    LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nb_host, 512, (size_t)max_seg * 12, c->s>>>(c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey,
-                                                                    c->ssrc, max_seg, c->err));
+  const unsigned nbb = (unsigned)std::min<int64_t>(G.ncells, c->nsm);
+  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nbb, 512, (size_t)max_seg * 12, c->s>>>(c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey,
+                                                                   c->ssrc, max_seg, c->err));
   LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp,
-                                                                        defer_ids ? nullptr : c->pid, dt_mid, c->xp2, c->vp2,
-                                             c->pid2, c->pcell2));
-  CK(cudaGetLastError());
-  int rc = check_err(c);
-  if (rc) return rc;
-  int64_t total = 0;
-  CK(cudaMemcpyAsync(&total, c->cstart2 + G.ncells, 8, cudaMemcpyDeviceToHost, c->s));
-  CK(cudaStreamSynchronize(c->s));
-  prof_collect(c);
-  if (total != np) return fail(CUBE_E_COUNT, "drift: particle count not conserved");
+                                                                        defer_ids ? nullptr : c->pid, c->sd, c->xp2, c->vp2,
+                                                                        c->pid2, c->pcell2));
+  cudaMemcpyAsync(c->total, c->cstart2 + G.ncells, 8, cudaMemcpyDeviceToDevice, c->s);
+}
+
+// The drift's outputs become the current particle state (host pointers only).
+static void swap_drift(cube_ctx* c) {
   std::swap(c->xp, c->xp2);
   std::swap(c->vp, c->vp2);
   std::swap(c->pid, c->pid2);
   std::swap(c->pcell, c->pcell2);
   std::swap(c->rhoc, c->rhoc2);
   std::swap(c->cstart, c->cstart2);
-  return 0;
 }
 
 int cube_gpu_drift(cube_ctx* c, const cube_step_in* in) {
   if (!c || !in) return fail(CUBE_E_ARG, "null argument");
   if (!c->loaded) return fail(CUBE_E_STATE, "drift before upload");
   CK(cudaSetDevice(c->device));
-  return drift_enqueue(c, in);
+  StepDev d;
+  int rc = make_scalars(c, in, true, d);
+  if (!rc) rc = upload_scalars(c, d);
+  if (rc) return rc;
+  enqueue_drift(c, false);
+  CK(cudaGetLastError());
+  swap_drift(c);
+  int64_t total = 0;
+  CK(cudaMemcpyAsync(&total, c->total, 8, cudaMemcpyDeviceToHost, c->s));
+  rc = check_err(c);
+  prof_collect(c);
+  if (rc) return rc;
+  if (total != c->np) return fail(CUBE_E_COUNT, "drift: particle count not conserved");
+  return 0;
 }
 
 static float dt_crit(float coef, float f2max, float a_mid) {
@@ -865,23 +997,20 @@ static float dt_crit(float coef, float f2max, float a_mid) {
   return coef * std::sqrt(1.f / (std::sqrt(f2max) * a_mid * G_grid));
 }
 
-int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
-  if (!c || !in) return fail(CUBE_E_ARG, "null argument");
-  if (!c->loaded) return fail(CUBE_E_STATE, "kick before upload");
-  CK(cudaSetDevice(c->device));
+// ---- the kick in stages ----
+// PM1 and PM2, then the subtile classes.  Zeroes the kick's reductions first.
+static int enqueue_kick_a(cube_ctx* c) {
   const Geo& G = c->G;
   const int64_t np = c->np;
   const bool fixed = c->P.deposit_mode == CUBE_DEPOSIT_FIXED;
-  const float a_mid = in->a_mid, dt = in->dt;
   float* f2 = c->red;        // [0..3]
   float* vm = c->red + 8;    // [pm2 0..2][pm3 3..5][pp 6..8]
   CK(cudaMemsetAsync(c->red, 0, 64 * sizeof(float), c->s));
-  CK(cudaMemsetAsync(c->pairs, 0, 8, c->s));
-  CK(cudaMemsetAsync(c->msum, 0, 3 * MASS_SLOTS * 8, c->s));
+  CK(cudaMemsetAsync(c->pairs, 0, 16, c->s));
+  CK(cudaMemsetAsync(c->msum, 0, 3 * MASS_SLOTS * MASS_STRIDE * 8, c->s));
   unsigned long long* ms1 = c->msum;
-  unsigned long long* ms2 = c->msum + MASS_SLOTS;
-  unsigned long long* ms3 = c->msum + 2 * MASS_SLOTS;
-  CK(cudaEventRecord(c->ev[0], c->s));
+  unsigned long long* ms2 = c->msum + MASS_SLOTS * MASS_STRIDE;
+  CK(mark(c, c->ev[0]));
   // ---------------- PM1 (particle_mesh.f90) ----------------
   {
     const int n = G.nc;
@@ -902,12 +1031,12 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     if (foff + (size_t)n3 * sizeof(float4) <= c->arena_bytes) {
       float4* force = reinterpret_cast<float4*>(reinterpret_cast<char*>(c->arena) + foff);
       LAUNCH(c, K_INT_PM1, 1, k_force_pm1<<<nblk(n3), 256, 0, c->s>>>(n, phi, m.pt.pf, m.pt.plf, force));
-      LAUNCH(c, K_INT_PM1, 1, k_interp_pm1_force<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, force, c->vp, a_mid, dt));
+      LAUNCH(c, K_INT_PM1, 1, k_interp_pm1_force<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, force, c->vp, c->sd));
     } else {
-      LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, a_mid, dt, m.pt.pf, m.pt.plf));
+      LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, c->sd, m.pt.pf, m.pt.plf));
     }
   }
-  CK(cudaEventRecord(c->ev[1], c->s));
+  CK(mark(c, c->ev[1]));
   // ---------------- PM2 (kick.f90:47-77) ----------------
   {
     const int n = G.ngt;
@@ -926,68 +1055,118 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
         maybe_capture(c, 2, c->cap_box, 1, (char*)m.real + (c->cap_box - t0) * boxb, n, false, (int64_t)m.pt.pf * 4,
                       m.pt.psb);
-      LAUNCH(c, K_F2_PM2, 1, k_f2max_box2<<<f2max_box2_grid(G.ngp, nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1, m.pt.pf, m.pt.plf));
-      LAUNCH(c, K_INT_PM2, 1, k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, a_mid, dt, vm + 0, c->err, m.pt.pf, m.pt.plf));
+      LAUNCH(c, K_F2_PM2, 1, k_f2max_box2<<<f2max_box2_grid(G.ngp, nb), 256, 0, c->s>>>(phi, n, G.ngp, 1 - G.ngb, nb, f2 + 1, m.pt.pf, m.pt.plf, nullptr));
+      LAUNCH(c, K_INT_PM2, 1, k_interp_pm2<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, t0, nb, c->vp, c->sd, vm + 0, c->err, m.pt.pf, m.pt.plf));
     }
   }
-  CK(cudaEventRecord(c->ev[2], c->s));
+  CK(mark(c, c->ev[2]));
   // ---------------- subtile classes (kick.f90:108-138) ----------------
   CK(cudaMemsetAsync(c->napm, 0, 32, c->s));
   LAUNCH(c, K_CLASSIFY, 1, k_classify<<<nblk(c->ns3), 256, 0, c->s>>>(G, c->rhoc, c->ns3, c->ires, c->napm));
-  std::vector<int32_t> ires(c->ns3);
-  int32_t napm[8];
-  CK(cudaMemcpyAsync(ires.data(), c->ires, c->ns3 * 4, cudaMemcpyDeviceToHost, c->s));
-  CK(cudaMemcpyAsync(napm, c->napm, 32, cudaMemcpyDeviceToHost, c->s));
-  CK(cudaStreamSynchronize(c->s));
-  // ---------------- PM3 (kick.f90:203-276) ----------------
+  // PM3 mass over the boxes' physical cells, from the classes just found
   if (c->P.pm3_on) {
-    // chunks per class
-    struct Chunk { int iapm; int64_t first; int nb; };
-    std::vector<Chunk> chunks;
-    std::vector<std::vector<int>> lists(8);
-    for (int s = 0; s < c->ns3; ++s) lists[ires[s]].push_back(s);
-    for (int cl = 2; cl <= 5; ++cl) {
-      if (lists[cl].empty()) continue;
-      // int64 mesh layout only where the particle-major fixed-point deposit runs; the
-      // owner-computes deposit writes floats
-      const bool lint = fixed && !dep3_own_fits(G, cl);
-      const int64_t per = std::min<int64_t>((int64_t)lists[cl].size(), boxes_fit(c, G.nft[cl], lint));
-      for (int64_t f = 0; f < (int64_t)lists[cl].size(); f += per)
-        chunks.push_back({cl, f, (int)std::min<int64_t>(per, (int64_t)lists[cl].size() - f)});
+    unsigned long long* ms3 = c->msum + 2 * MASS_SLOTS * MASS_STRIDE;
+    if (fixed) LAUNCH(c, K_MASS, 1, k_mass_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, c->ires, ms3));
+    else LAUNCH(c, K_MASS, 1, k_mass_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, c->ires, ms3));
+  }
+  return 0;
+}
+
+// PM3 chunk plan for class counts `cnt`: exact (cap = count) or with headroom for a
+// captured step (present classes +1/32, at least 2 boxes; absent classes none: a padded
+// slot still costs its FFT).  `skip` (may be null) leaves out the first skip[c] subtiles
+// of each class, the ones a captured step already covered.
+static PM3Plan make_plan(cube_ctx* c, const int32_t cnt[8], bool headroom, const int* skip = nullptr) {
+  const Geo& G = c->G;
+  const bool fixed = c->P.deposit_mode == CUBE_DEPOSIT_FIXED;
+  PM3Plan pl;
+  memset(&pl, 0, sizeof(pl));
+  int k = 0;
+  pl.per_max = 1;
+  for (int cl = 2; cl <= 5; ++cl) {
+    pl.skip[cl] = skip ? skip[cl] : 0;
+    int64_t want = std::max<int64_t>(0, (int64_t)cnt[cl] - pl.skip[cl]);
+    if (headroom && want > 0) want = want + std::max<int64_t>(2, want / 32);
+    want = std::min<int64_t>(want, c->ns3);
+    pl.cap[cl] = (int)want;
+    if (want == 0 || !c->P.pm3_on) {
+      pl.cap[cl] = 0;
+      continue;
     }
-    const int64_t nch = (int64_t)chunks.size();
-    // [nch][ns3] subtile -> slot maps, then the chunks' slot -> subtile lists (ns3 in all)
-    if (nch > c->slot_chunks) {
-      if (c->box_slot) cudaFree(c->box_slot);
-      if (c->h_slots) cudaFreeHost(c->h_slots);
-      c->box_slot = nullptr;
-      c->h_slots = nullptr;
-      CK(cudaMalloc(&c->box_slot, (nch + 1) * c->ns3 * 4));
-      CK(cudaMallocHost(&c->h_slots, (nch + 1) * c->ns3 * 4));
-      c->slot_chunks = nch;
-    }
-    std::vector<int64_t> list_off(nch);
-    int64_t off = nch * c->ns3;
-    for (int64_t k = 0; k < nch; ++k) {
-      int32_t* hs = c->h_slots + k * c->ns3;
-      std::fill(hs, hs + c->ns3, -1);
-      list_off[k] = off;
-      for (int j = 0; j < chunks[k].nb; ++j) {
-        const int sub = lists[chunks[k].iapm][chunks[k].first + j];
-        hs[sub] = j;
-        c->h_slots[off + j] = sub;
-      }
-      off += chunks[k].nb;
-    }
-    if (nch) CK(cudaMemcpyAsync(c->box_slot, c->h_slots, off * 4, cudaMemcpyHostToDevice, c->s));
-    for (int64_t k = 0; k < nch; ++k) {
-      const int cl = chunks[k].iapm, nb = chunks[k].nb;
-      const int n = G.nft[cl];
-      const float* g3 = green3(c, cl);
-      if (!g3) return CUBE_E_CUDA;
-      const int32_t* slots = c->box_slot + k * c->ns3;
-      const bool own = fixed && dep3_own_fits(G, cl);
-      const bool lint = fixed && !own;  // int64 mesh layout
+    const bool lint = fixed && !dep3_own_fits(G, cl);
+    const int64_t per = std::min<int64_t>(want, boxes_fit(c, G.nft[cl], lint));
+    pl.per[cl] = (int)per;
+    pl.kbase[cl] = k;
+    k += (int)((want + per - 1) / per);
+    pl.per_max = std::max<int>(pl.per_max, (int)per);
+  }
+  pl.nk = k;
+  return pl;
+}
+
+// Room for a plan's lists.  Growing them invalidates captured steps (they hold the old
+// pointers); the stream has no work that uses them when this runs.
+static int ensure_plan_buffers(cube_ctx* c, const PM3Plan& pl) {
+  const int64_t ns = std::max<int64_t>(1, (int64_t)pl.nk) * c->ns3;
+  const int64_t nsub = std::max<int64_t>(1, (int64_t)pl.nk) * pl.per_max;
+  if (ns <= c->slot_cap && nsub <= c->sub_cap) return 0;
+  drop_graphs(c);
+  if (c->box_slot) cudaFree(c->box_slot);
+  if (c->box_sub) cudaFree(c->box_sub);
+  c->box_slot = c->box_sub = nullptr;
+  c->slot_cap = c->sub_cap = 0;
+  CK(cudaMalloc(&c->box_slot, ns * 4));
+  CK(cudaMalloc(&c->box_sub, nsub * 4));
+  c->slot_cap = ns;
+  c->sub_cap = nsub;
+  return 0;
+}
+
+// The class lists of a plan, built on the device from ires.
+static int enqueue_lists(cube_ctx* c, const PM3Plan& pl) {
+  if (pl.nk == 0) return 0;
+  CK(cudaMemsetAsync(c->box_slot, 0xff, (size_t)pl.nk * c->ns3 * 4, c->s));
+  CK(cudaMemsetAsync(c->box_sub, 0xff, (size_t)pl.nk * pl.per_max * 4, c->s));
+  LAUNCH(c, K_CLASSIFY, 1, k_build_lists<<<1, 1024, 0, c->s>>>(c->ires, c->ns3, pl, c->box_slot, c->box_sub, c->overflow));
+  return 0;
+}
+
+// Slot of subtile s in its chunk of a plan (host copy of ires), for test captures.
+static int host_slot(const cube_ctx* c, const PM3Plan& pl, int s, int& chunk) {
+  const int cl = c->h_ires[s];
+  int rank = -pl.skip[cl];
+  for (int t = 0; t < s; ++t) rank += c->h_ires[t] == cl;
+  if (rank < 0 || rank >= pl.cap[cl]) return -1;
+  chunk = pl.kbase[cl] + rank / pl.per[cl];
+  return rank % pl.per[cl];
+}
+
+// PM3 (kick.f90:203-276) over the plan's chunks.  Each particle takes its PM3 kick from
+// its own subtile's box only, so the boxes can be split over passes.  `host_ires` marks
+// that h_ires holds this step's classes (test captures of a PM3 box need it).
+static int enqueue_pm3(cube_ctx* c, const PM3Plan& pl, bool host_ires) {
+  if (!c->P.pm3_on) return 0;
+  const Geo& G = c->G;
+  const int64_t np = c->np;
+  const bool fixed = c->P.deposit_mode == CUBE_DEPOSIT_FIXED;
+  float* f2 = c->red;
+  float* vm = c->red + 8;
+  int cap_chunk = -1, cap_slot = -1;
+  if (host_ires && c->cap_level == 3 && c->cap_box >= 0 && c->cap_box < c->ns3)
+    cap_slot = host_slot(c, pl, c->cap_box, cap_chunk);
+  for (int cl = 2; cl <= 5; ++cl) {
+    if (pl.cap[cl] == 0) continue;
+    const int n = G.nft[cl];
+    const float* g3 = green3(c, cl);
+    if (!g3) return CUBE_E_CUDA;
+    const bool own = fixed && dep3_own_fits(G, cl);
+    const bool lint = fixed && !own;  // int64 mesh layout
+    const int nch = (pl.cap[cl] + pl.per[cl] - 1) / pl.per[cl];
+    for (int ch = 0; ch < nch; ++ch) {
+      const int k = pl.kbase[cl] + ch;
+      const int nb = std::min(pl.per[cl], pl.cap[cl] - ch * pl.per[cl]);
+      const int32_t* slots = c->box_slot + (int64_t)k * c->ns3;
+      const int32_t* subs = c->box_sub + (int64_t)k * pl.per_max;
       MeshPtrs m = mesh_ptrs(c, n, nb, lint);
       const int64_t boxb = (int64_t)n * m.pt.psb;
       if (own) {
@@ -996,109 +1175,282 @@ int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
         const size_t sm = (size_t)DEP3_R * DEP3_R * DEP3_RZ * 8;
         smem_optin(k_deposit_pm3_own, sm);
         LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3_own<<<(unsigned)((int64_t)nb * nr * nr * nrz), DEP3_THREADS, sm, c->s>>>(
-                                    G, c->xp, c->cstart, c->box_slot + list_off[k], cl,
-                                    reinterpret_cast<float*>(m.real), c->err, m.pt.pr, m.pt.plr, nr, nr, nrz, ms3));
+                                    G, c->xp, c->cstart, subs, cl, reinterpret_cast<float*>(m.real), c->err, m.pt.pr,
+                                    m.pt.plr, nr, nr, nrz));
       } else {
         CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
-        if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr, ms3));
-        else LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr, ms3));
+        if (fixed) LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));
+        else LAUNCH(c, K_DEP_PM3, 1, k_deposit_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, slots, cl, m.real, c->err, m.pt.pr, m.pt.plr));
       }
-      int cap_slot = -1;
-      if (c->cap_level == 3 && c->cap_box >= 0 && c->cap_box < c->ns3 && ires[c->cap_box] == cl)
-        cap_slot = c->h_slots[k * c->ns3 + c->cap_box];
-      if (cap_slot >= 0) maybe_capture(c, 3, c->cap_box, 0, (char*)m.real + cap_slot * boxb, n, lint, m.pt.rp, m.pt.psb);
+      const bool cap_here = cap_slot >= 0 && cap_chunk == k;
+      if (cap_here) maybe_capture(c, 3, c->cap_box, 0, (char*)m.real + cap_slot * boxb, n, lint, m.pt.rp, m.pt.psb);
       float* phi = reinterpret_cast<float*>(m.real);
       launch_fft(c, n, nb, m.real, lint, G.mass_p, phi, m.ck, g3, (float)n * (float)n * (float)n, 1, 3);
-      if (cap_slot >= 0)
+      if (cap_here)
         maybe_capture(c, 3, c->cap_box, 1, (char*)m.real + cap_slot * boxb, n, false, (int64_t)m.pt.pf * 4, m.pt.psb);
       const int nf = G.nfp[cl];
-      LAUNCH(c, K_F2_PM3, 1, k_f2max_box2<<<f2max_box2_grid(nf, nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2, m.pt.pf, m.pt.plf));
-      LAUNCH(c, K_INT_PM3, 1, k_interp_pm3<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp, a_mid, dt, vm + 3,
+      LAUNCH(c, K_F2_PM3, 1, k_f2max_box2<<<f2max_box2_grid(nf, nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2, m.pt.pf, m.pt.plf, subs));
+      LAUNCH(c, K_INT_PM3, 1, k_interp_pm3<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp, c->sd, vm + 3,
                                                 c->err, m.pt.pf, m.pt.plf));
     }
   }
-  CK(cudaEventRecord(c->ev[3], c->s));
-  // ---------------- PP (kick.f90:280-311) ----------------
+  return 0;
+}
+
+// PP (kick.f90:280-311), then the FP64 momentum sums of the kicked velocities.
+static void enqueue_pp_and_momentum(cube_ctx* c, const unsigned* abort) {
+  const Geo& G = c->G;
+  const int64_t np = c->np;
+  float* f2 = c->red;
+  float* vm = c->red + 8;
   if (c->P.pp_on) {
-    const float mass_scale = (G.f_nu > 0.f)
-                                 ? (float)((double)G.mass_p * ((1.0 - (double)G.f_nu) * (1.0 - (double)G.f_nu)))
-                                 : G.mass_p;
-    const float v_scale = (float)((double)(a_mid * dt / 6.f) / M_PI);
     // FP32 candidate positions are exact when lq + offset fits 24 bits: int8 codes, or
     // int16 codes with tile-local coordinates |lq| <= nt < 128
     const bool pp_fast = G.izipx == 1 || G.nt < 127;
     if (pp_fast)
       LAUNCH(c, K_PP, 1, k_pp<true><<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->xp, c->pcell, c->cstart, c->ires, c->vp,
-                                                                    mass_scale, v_scale, f2 + 3, vm + 6, c->pairs));
+                                                                    c->sd, f2 + 3, vm + 6, c->pairs, c->pairs + 1, abort));
     else
       LAUNCH(c, K_PP, 1, k_pp<false><<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->xp, c->pcell, c->cstart, c->ires, c->vp,
-                                                                     mass_scale, v_scale, f2 + 3, vm + 6, c->pairs));
+                                                                     c->sd, f2 + 3, vm + 6, c->pairs, c->pairs + 1, abort));
   }
-  CK(cudaEventRecord(c->ev[4], c->s));
+  mark(c, c->ev[4]);
   LAUNCH(c, K_MOMENTUM, 1, k_momentum<<<MOM_BLOCKS, MOM_THREADS, 0, c->s>>>(c->vp, np, c->mom));
+}
+
+// cube_step_out from the step results in c->rhost.
+static void fill_out(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
+  const StepRes& R = *c->rhost;
+  const float* red = R.red;
+  const float a_mid = in->a_mid;
+  const bool fixed = c->P.deposit_mode == CUBE_DEPOSIT_FIXED;
+  memset(out, 0, sizeof(*out));
+  out->f2max_pm1 = red[0];
+  out->f2max_pm2 = red[1];
+  out->f2max_pm3 = red[2];
+  out->f2max_pp = red[3];
+  out->dt_pm1 = dt_crit(0.5f, red[0], a_mid);  // kick.f90:39
+  out->dt_pm2 = dt_crit(0.5f, red[1], a_mid);  // kick.f90:69
+  out->dt_pm3 = dt_crit(0.5f, red[2], a_mid);  // kick.f90:239
+  out->dt_pp = dt_crit(0.05f, red[3], a_mid);  // kick.f90:298
+  const float* v = c->P.pp_on ? (red + 14) : (c->P.pm3_on ? red + 11 : red + 8);
+  for (int d = 0; d < 3; ++d) out->vmax[d] = v[d];
+  const float vmx = std::max(v[0], std::max(v[1], v[2]));
+  out->dt_vmax = 0.9f * 14 / vmx;  // kick.f90:314
+  out->vz_max = v[2];
+  for (int i = 0; i < 8; ++i) out->napm[i] = R.napm[i];
+  out->nplocal = c->np;
+  out->pp_pairs = (int64_t)R.pairs;
+  out->pp_candidates = (int64_t)R.cand;
+  float ms;
+  for (int i = 0; i < 4; ++i) {
+    ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]);
+    out->tcat[1 + i] = ms;
+  }
+  ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[4]);
+  out->tcat[5] = ms;
+  double mass[3];
+  for (int l = 0; l < 3; ++l) {
+    const unsigned long long* q = R.msum + l * MASS_SLOTS * MASS_STRIDE;
+    if (fixed) {
+      unsigned __int128 t = 0;  // exact: 128-bit slots (sum, carries) of int64 contributions
+      for (int k = 0; k < MASS_SLOTS; ++k)
+        t += ((unsigned __int128)q[k * MASS_STRIDE + 1] << 64) + q[k * MASS_STRIDE];
+      mass[l] = std::ldexp((double)(unsigned long long)(t >> 64), 24) + std::ldexp((double)(unsigned long long)t, -40);
+    } else {
+      double t = 0.0;
+      for (int k = 0; k < MASS_SLOTS; ++k) {
+        double x;
+        memcpy(&x, q + k * MASS_STRIDE, sizeof x);
+        t += x;
+      }
+      mass[l] = t;
+    }
+  }
+  out->mass_pm1 = mass[0];
+  out->mass_pm2 = mass[1];
+  out->mass_pm3 = mass[2];
+  for (int d = 0; d < 3; ++d) {
+    double t = 0.0;
+    for (int b = 0; b < MOM_BLOCKS; ++b) t += R.mom[3 * b + d];
+    out->momentum[d] = t;
+  }
+}
+
+// The kick (kick.f90:1-353) eagerly: PM1 and PM2, the classes read back, PM3 over exact
+// class lists, PP, and the results read back (two host synchronisations).
+static int kick_eager(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
+  int rc = enqueue_kick_a(c);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(c->h_ires, c->ires, c->ns3 * 4, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(c->rhost->napm, c->napm, 32, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  int32_t napm[8];
+  memcpy(napm, c->rhost->napm, sizeof napm);
+  const PM3Plan pl = make_plan(c, napm, false);
+  rc = ensure_plan_buffers(c, pl);
+  if (!rc) rc = enqueue_lists(c, pl);
+  if (!rc) rc = enqueue_pm3(c, pl, true);
+  if (rc) return rc;
+  CK(mark(c, c->ev[3]));
+  enqueue_pp_and_momentum(c, nullptr);
   CK(cudaGetLastError());
-  float red[64];
-  unsigned long long pairs = 0;
-  std::vector<unsigned long long> msum(3 * MASS_SLOTS);
-  std::vector<double> mom(3 * MOM_BLOCKS);
-  CK(cudaMemcpyAsync(red, c->red, sizeof(red), cudaMemcpyDeviceToHost, c->s));
-  CK(cudaMemcpyAsync(&pairs, c->pairs, 8, cudaMemcpyDeviceToHost, c->s));
-  CK(cudaMemcpyAsync(msum.data(), c->msum, msum.size() * 8, cudaMemcpyDeviceToHost, c->s));
-  CK(cudaMemcpyAsync(mom.data(), c->mom, mom.size() * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(c->rhost, c->rdev, sizeof(StepRes), cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
   prof_collect(c);
-  int rc = check_err(c);
+  memcpy(c->napm_est, c->rhost->napm, sizeof c->napm_est);
+  c->have_est = true;
+  if (c->rhost->err) {
+    CK(cudaMemsetAsync(c->err, 0, 4, c->s));
+    CK(cudaStreamSynchronize(c->s));
+    return err_code(c->rhost->err);
+  }
+  if (out) fill_out(c, in, out);
+  return 0;
+}
+
+int cube_gpu_kick(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
+  if (!c || !in) return fail(CUBE_E_ARG, "null argument");
+  if (!c->loaded) return fail(CUBE_E_STATE, "kick before upload");
+  CK(cudaSetDevice(c->device));
+  StepDev d;
+  int rc = make_scalars(c, in, false, d);
+  if (!rc) rc = upload_scalars(c, d);
   if (rc) return rc;
-  if (out) {
-    memset(out, 0, sizeof(*out));
-    out->f2max_pm1 = red[0];
-    out->f2max_pm2 = red[1];
-    out->f2max_pm3 = red[2];
-    out->f2max_pp = red[3];
-    out->dt_pm1 = dt_crit(0.5f, red[0], a_mid);  // kick.f90:39
-    out->dt_pm2 = dt_crit(0.5f, red[1], a_mid);  // kick.f90:69
-    out->dt_pm3 = dt_crit(0.5f, red[2], a_mid);  // kick.f90:239
-    out->dt_pp = dt_crit(0.05f, red[3], a_mid);  // kick.f90:298
-    const float* v = c->P.pp_on ? (red + 14) : (c->P.pm3_on ? red + 11 : red + 8);
-    for (int d = 0; d < 3; ++d) out->vmax[d] = v[d];
-    const float vmx = std::max(v[0], std::max(v[1], v[2]));
-    out->dt_vmax = 0.9f * 14 / vmx;  // kick.f90:314
-    out->vz_max = v[2];
-    for (int i = 0; i < 8; ++i) out->napm[i] = napm[i];
-    out->nplocal = np;
-    out->pp_pairs = (int64_t)pairs;
-    float ms;
-    for (int i = 0; i < 4; ++i) {
-      cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]);
-      out->tcat[1 + i] = ms;
+  return kick_eager(c, in, out);
+}
+
+// Timing of a finished step: drift (ev5..ev6) and the whole step (ev5..ev7).
+static void step_times(cube_ctx* c, cube_step_out* out) {
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]);
+  out->tcat[0] = ms;
+  out->tcat[5] += ms;
+  ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[5], c->ev[7]);
+  out->tcat[6] = ms;  // whole step on the device, host gaps included
+}
+
+// One step as one CUDA graph (cube_params.step_graph): scalars up, drift, PM1, PM2,
+// classes, device-built class lists, PM3, PP, momentum and the results copied back, with
+// no host synchronisation inside.  The PM3 chunks are laid out for the previous step's
+// class histogram with headroom.  When a step's classes outgrow them, the graph kicks the
+// particles of the listed subtiles and skips PP (device flag); the host then runs PM3 for
+// the unlisted subtiles and PP, which gives every particle the same operations in the
+// same order as the eager step.  Graphs are kept per particle-buffer parity, particle
+// count and plan, and captured on first use.
+static int step_graph(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
+  StepDev d;
+  int rc = make_scalars(c, in, true, d);
+  if (rc) return rc;
+  if (!c->have_est) {  // first step: classes of the current state
+    CK(cudaMemsetAsync(c->napm, 0, 32, c->s));
+    LAUNCH(c, K_CLASSIFY, 1, k_classify<<<nblk(c->ns3), 256, 0, c->s>>>(c->G, c->rhoc, c->ns3, c->ires, c->napm));
+    CK(cudaMemcpyAsync(c->napm_est, c->napm, 32, cudaMemcpyDeviceToHost, c->s));
+    CK(cudaStreamSynchronize(c->s));
+    c->have_est = true;
+  }
+  const PM3Plan pl = make_plan(c, c->napm_est, true);
+  rc = ensure_plan_buffers(c, pl);
+  if (rc) return rc;
+  for (int cl = 2; cl <= 5; ++cl)
+    if (pl.cap[cl] > 0 && !green3(c, cl)) return CUBE_E_CUDA;  // tables exist before any capture
+  const int parity = c->xp == c->xp_base ? 0 : 1;
+  StepGraph* g = nullptr;
+  for (auto& x : c->graphs)
+    if (x.parity == parity && x.np == c->np && x.prof == c->prof && same_plan(x.plan, pl)) g = &x;
+  if (!g) {
+    // one graph per parity: a new plan replaces the old one of this parity
+    for (size_t i = 0; i < c->graphs.size(); ++i)
+      if (c->graphs[i].parity == parity) {
+        CK(cudaStreamSynchronize(c->s));
+        cudaGraphExecDestroy(c->graphs[i].exec);
+        for (cudaEvent_t e : c->graphs[i].events) cudaEventDestroy(e);
+        c->graphs.erase(c->graphs.begin() + i);
+        break;
+      }
+    StepGraph ng;
+    ng.parity = parity;
+    ng.np = c->np;
+    ng.plan = pl;
+    ng.prof = c->prof;
+    c->cap_graph = &ng;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeRelaxed));
+    cudaMemcpyAsync(c->sd, c->h_sd, sizeof(StepDev), cudaMemcpyHostToDevice, c->s);
+    mark(c, c->ev[5]);
+    enqueue_drift(c, false);
+    swap_drift(c);
+    mark(c, c->ev[6]);
+    rc = enqueue_kick_a(c);
+    if (!rc) rc = enqueue_lists(c, pl);
+    if (!rc) rc = enqueue_pm3(c, pl, false);
+    if (!rc) {
+      mark(c, c->ev[3]);
+      enqueue_pp_and_momentum(c, c->overflow);
+      mark(c, c->ev[7]);
+      cudaMemcpyAsync(c->rhost, c->rdev, sizeof(StepRes), cudaMemcpyDeviceToHost, c->s);
     }
-    cudaEventElapsedTime(&ms, c->ev[0], c->ev[4]);
-    out->tcat[5] = ms;
-    double mass[3];
-    for (int l = 0; l < 3; ++l) {
-      const unsigned long long* q = msum.data() + l * MASS_SLOTS;
-      if (fixed) {
-        unsigned long long t = 0;  // exact: the slots hold sums of int64 contributions
-        for (int k = 0; k < MASS_SLOTS; ++k) t += q[k];
-        mass[l] = std::ldexp((double)t, -40);
-      } else {
-        double t = 0.0;
-        for (int k = 0; k < MASS_SLOTS; ++k) {
-          double v;
-          memcpy(&v, q + k, sizeof v);
-          t += v;
-        }
-        mass[l] = t;
+    const cudaError_t ce = cudaStreamEndCapture(c->s, &graph);
+    swap_drift(c);  // undo: the graph has not run yet
+    c->cap_graph = nullptr;
+    cudaError_t ie = cudaSuccess;
+    if (!rc && ce == cudaSuccess) ie = cudaGraphInstantiate(&ng.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (rc || ce != cudaSuccess || ie != cudaSuccess) {
+      for (cudaEvent_t e : ng.events) cudaEventDestroy(e);
+      cudaGetLastError();
+      if (rc) return rc;
+      return fail(CUBE_E_CUDA, std::string("step graph capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ie));
+    }
+    c->graphs.push_back(std::move(ng));
+    g = &c->graphs.back();
+  }
+  *c->h_sd = d;
+  CK(cudaGraphLaunch(g->exec, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  swap_drift(c);
+  c->launches += g->kernels;
+  if (c->prof)
+    for (const ProfRec& r : g->recs) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, g->events[r.a], g->events[r.b]) == cudaSuccess) {
+        c->prof_ms[r.cls] += ms;
+        c->prof_n[r.cls] += 1;
       }
     }
-    out->mass_pm1 = mass[0];
-    out->mass_pm2 = mass[1];
-    out->mass_pm3 = mass[2];
-    for (int d = 0; d < 3; ++d) {
-      double t = 0.0;
-      for (int b = 0; b < MOM_BLOCKS; ++b) t += mom[3 * b + d];
-      out->momentum[d] = t;
-    }
+  if (c->rhost->overflow) {
+    // the classes outgrew the plan: PM3 of the subtiles beyond each class's capacity, then
+    // PP (skipped by the graph).  The f2max, vmax and mass sums of PM3 accumulate over
+    // both passes; PP contributed nothing yet; the momentum is recomputed.
+    CK(cudaMemsetAsync(c->overflow, 0, 4, c->s));
+    int32_t napm[8];
+    memcpy(napm, c->rhost->napm, sizeof napm);
+    const PM3Plan rest = make_plan(c, napm, false, pl.cap);
+    rc = ensure_plan_buffers(c, rest);
+    if (!rc) rc = enqueue_lists(c, rest);
+    if (!rc) rc = enqueue_pm3(c, rest, false);
+    if (rc) return rc;
+    CK(mark(c, c->ev[3]));
+    enqueue_pp_and_momentum(c, nullptr);
+    CK(mark(c, c->ev[7]));
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->rhost, c->rdev, sizeof(StepRes), cudaMemcpyDeviceToHost, c->s));
+    CK(cudaStreamSynchronize(c->s));
+    prof_collect(c);
+  }
+  memcpy(c->napm_est, c->rhost->napm, sizeof c->napm_est);
+  if (c->rhost->err) {
+    CK(cudaMemsetAsync(c->err, 0, 4, c->s));
+    CK(cudaStreamSynchronize(c->s));
+    return err_code(c->rhost->err);
+  }
+  if (c->rhost->total != c->np) return fail(CUBE_E_COUNT, "drift: particle count not conserved");
+  if (out) {
+    fill_out(c, in, out);
+    step_times(c, out);
   }
   return 0;
 }
@@ -1107,22 +1459,25 @@ int cube_gpu_step(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
   if (!c || !in) return fail(CUBE_E_ARG, "null argument");
   if (!c->loaded) return fail(CUBE_E_STATE, "step before upload");
   CK(cudaSetDevice(c->device));
+  // graph replay unless a test capture is armed (it copies with host-side allocations)
+  if (c->P.step_graph && c->cap_level == 0) return step_graph(c, in, out);
+  StepDev d;
+  int rc = make_scalars(c, in, true, d);
+  if (!rc) rc = upload_scalars(c, d);
+  if (rc) return rc;
   // ev[5]: step start, ev[6]: drift end, ev[7]: step end (all on the context stream)
   CK(cudaEventRecord(c->ev[5], c->s));
-  int rc = drift_enqueue(c, in);
+  enqueue_drift(c, false);
+  CK(cudaGetLastError());
+  swap_drift(c);
   CK(cudaEventRecord(c->ev[6], c->s));
-  if (!rc) rc = cube_gpu_kick(c, in, out);
+  rc = kick_eager(c, in, out);
   CK(cudaEventRecord(c->ev[7], c->s));
   CK(cudaEventSynchronize(c->ev[7]));
-  if (!rc && out) {
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]);
-    out->tcat[0] = ms;
-    out->tcat[5] += ms;
-    cudaEventElapsedTime(&ms, c->ev[5], c->ev[7]);
-    out->tcat[6] = ms;  // whole step on the device, host gaps included
-  }
-  return rc;
+  if (rc) return rc;
+  if (c->rhost->total != c->np) return fail(CUBE_E_COUNT, "drift: particle count not conserved");
+  if (out) step_times(c, out);
+  return 0;
 }
 
 // One step on a host-resident particle state: upload, drift, kick, download, with the
@@ -1149,7 +1504,9 @@ int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, 
     cudaStreamSynchronize(c->s2);
     cudaStreamSynchronize(c->s);
   };
-  int rc = alloc_particles(c, nplocal);
+  StepDev d;
+  int rc = make_scalars(c, in, true, d);
+  if (!rc) rc = alloc_particles(c, nplocal);
   if (rc) return rc;
   c->np = nplocal;
   c->loaded = false;
@@ -1176,13 +1533,15 @@ int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, 
   LAUNCH(c, K_FILL, 1, k_fill_pcell<<<nblk(G.ncells), 256, 0, c->s>>>(c->cstart, G.ncells, c->pcell));
   CK(cudaGetLastError());
   c->loaded = true;
-  CK(cudaEventRecord(c->ev[5], c->s));
-  rc = drift_enqueue(c, in, true);
+  rc = upload_scalars(c, d);
   if (rc) {
     drain();
-    c->loaded = false;
     return rc;
   }
+  CK(cudaEventRecord(c->ev[5], c->s));
+  enqueue_drift(c, true);
+  CK(cudaGetLastError());
+  swap_drift(c);
   CK(cudaEventRecord(c->ev[6], c->s));
   CK(cudaEventRecord(c->ev_drift, c->s));
   CK(cudaStreamWaitEvent(c->s2, c->ev_drift, 0));
@@ -1192,20 +1551,14 @@ int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, 
   CK(cudaGetLastError());
   ++c->launches;
   CK(cudaMemcpyAsync(pid, c->pid, (size_t)c->np * 8, cudaMemcpyDeviceToHost, c->s2));
-  rc = cube_gpu_kick(c, in, out);
+  rc = kick_eager(c, in, out);
   CK(cudaEventRecord(c->ev[7], c->s));
   if (!rc) CK(cudaMemcpyAsync(vp, c->vp, (size_t)c->np * 12, cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
   CK(cudaStreamSynchronize(c->s2));
+  if (!rc && c->rhost->total != c->np) rc = fail(CUBE_E_COUNT, "drift: particle count not conserved");
   if (rc) c->loaded = false;
-  if (!rc && out) {
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]);
-    out->tcat[0] = ms;
-    out->tcat[5] += ms;
-    cudaEventElapsedTime(&ms, c->ev[5], c->ev[7]);
-    out->tcat[6] = ms;
-  }
+  if (!rc && out) step_times(c, out);
   return rc;
 }
 
@@ -1333,15 +1686,13 @@ int cube_gpu_ic(cube_ctx* c, const cube_ic_in* in, cube_ic_out* out) {
   LAUNCH(c, K_DRIFT_SCATTER, 1, k_drift_scatter<<<nblk(np), 256, 0, c->s>>>(np, c->dest, c->key, c->cstart2, c->fill, c->skey, c->ssrc));
   LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_small<<<nblk((G.ncells + 1) / 2 * 32), 256, 0, c->s>>>(G.ncells, c->rhoc2, c->cstart2, c->skey,
                                                                                      c->ssrc, c->biglist, c->nbig));
-  int nb_host = 0;
-  CK(cudaMemcpyAsync(&nb_host, c->nbig, 4, cudaMemcpyDeviceToHost, c->s));
-  CK(cudaStreamSynchronize(c->s));
   const int max_seg = c->P.max_segment > 0 ? std::min(c->P.max_segment, 16384) : 16384;
-  if (nb_host > 0)
-    LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nb_host, 512, (size_t)max_seg * 12, c->s>>>(
-                                   c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey, c->ssrc, max_seg, c->err));
+  const unsigned nbb = (unsigned)std::min<int64_t>(G.ncells, c->nsm);
+  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nbb, 512, (size_t)max_seg * 12, c->s>>>(
+                                 c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey, c->ssrc, max_seg, c->err));
   c->np = np;
-  LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp, c->pid, 0.f,
+  CK(cudaMemsetAsync(c->sd, 0, sizeof(StepDev), c->s));  // dt_mid = 0: the gather only sorts
+  LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp, c->pid, c->sd,
                                                                          c->xp2, c->vp2, c->pid2, c->pcell2));
   CK(cudaGetLastError());
   rc = check_err(c);
@@ -1357,6 +1708,7 @@ int cube_gpu_ic(cube_ctx* c, const cube_ic_in* in, cube_ic_out* out) {
   std::swap(c->rhoc, c->rhoc2);
   std::swap(c->cstart, c->cstart2);
   c->loaded = true;
+  c->have_est = false;
   prof_collect(c);
   if (out) {
     memset(out, 0, sizeof(*out));

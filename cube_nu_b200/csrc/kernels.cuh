@@ -117,12 +117,17 @@ __global__ void k_fill_pcell(const int64_t* __restrict__ cstart, int64_t ncells,
 // (ilayer, k, j, i, l) with ilayer=(k-(1-ncb)) mod nlayer (drift.f90:96-115).  The key
 // packs that order relative to the destination tile:
 //   ilayer:16 | k+ncb-1:8 | j+ncb-1:8 | i+ncb-1:8 | l:24.
+// A particle that would move beyond the ghost depth raises CUBE_DEVERR_DRIFT_RANGE (the
+// reference stops, drift.f90:64-73) and is kept in its own cell, so the drifted state stays
+// a consistent permutation that later kernels can read safely until the host sees the error.
 __global__ void k_drift_dest(Geo G, int64_t np, const void* __restrict__ xp, const float* __restrict__ vp,
-                             const int32_t* __restrict__ pcell, const int64_t* __restrict__ cstart, float dt_mid,
-                             int nlayer, int32_t* __restrict__ dest, uint64_t* __restrict__ key,
+                             const int32_t* __restrict__ pcell, const int64_t* __restrict__ cstart,
+                             const StepDev* __restrict__ sd, int32_t* __restrict__ dest, uint64_t* __restrict__ key,
                              int32_t* __restrict__ count_new, unsigned* err) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= np) return;
+  const float dt_mid = sd->dt_mid;
+  const int nlayer = sd->nlayer;
   const int c = pcell[ip];
   int g[3];
   cell_coords(G, c, g[0], g[1], g[2]);
@@ -152,15 +157,19 @@ __global__ void k_drift_dest(Geo G, int64_t np, const void* __restrict__ xp, con
     rel[d] = dloc - dn[d];
     if (rel[d] < -G.ncb || rel[d] >= G.nt + G.ncb) bad = true;  // source outside the dest tile's ghost region
   }
-  if (bad || l >= (1 << 24)) {
+  if (bad) {
     set_err(err, CUBE_DEVERR_DRIFT_RANGE);
-    dest[ip] = -1;
-    return;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      dst[d] = g[d];
+      rel[d] = g[d] % G.nt;
+    }
   }
   const int64_t dc = cell_index(G, dst[0], dst[1], dst[2]);
   const uint64_t kz = (uint64_t)(rel[2] + G.ncb), ky = (uint64_t)(rel[1] + G.ncb), kx = (uint64_t)(rel[0] + G.ncb);
   const uint64_t il = kz % (uint64_t)nlayer;
-  key[ip] = (il << 48) | (kz << 40) | (ky << 32) | (kx << 24) | (uint64_t)l;
+  // l < 2^24: a cell holds fewer particles than the capacity check on upload allows
+  key[ip] = (il << 48) | (kz << 40) | (ky << 32) | (kx << 24) | (uint64_t)(l & 0xffffff);
   dest[ip] = (int32_t)dc;
   atomicAdd(&count_new[dc], 1);
 }
@@ -248,12 +257,14 @@ __global__ void k_drift_sort_big(const int32_t* __restrict__ biglist, const int3
                                  uint64_t* __restrict__ skey, uint32_t* __restrict__ ssrc, int max_seg,
                                  unsigned* err) {
   extern __shared__ uint64_t smk[];
-  if ((int)blockIdx.x >= *nbig) return;
-  const int c = biglist[blockIdx.x];
+  const int nb = *nbig;
+  for (int b = blockIdx.x; b < nb; b += gridDim.x) {  // block-uniform loop over the listed cells
+  __syncthreads();  // the previous segment's write-out is done with the shared arrays
+  const int c = biglist[b];
   const int n = count_new[c];
   if (n > max_seg) {
     if (threadIdx.x == 0) set_err(err, CUBE_DEVERR_SEGMENT);
-    return;
+    continue;
   }
   int m = 1;
   while (m < n) m <<= 1;
@@ -286,16 +297,18 @@ __global__ void k_drift_sort_big(const int32_t* __restrict__ biglist, const int3
     skey[base + i] = smk[i];
     ssrc[base + i] = smv[i];
   }
+  }
 }
 
 // New arrays in the sorted order, with the ZIPX update xp+nint(dt_mid*vp/(x_res*ratio_cs))
 // in the integer kind (drift.f90:117).
 __global__ void k_drift_gather(Geo G, int64_t np, const uint32_t* __restrict__ ssrc, const int32_t* __restrict__ dest,
                                const void* __restrict__ xp, const float* __restrict__ vp,
-                               const int64_t* __restrict__ pid, float dt_mid, void* __restrict__ xo,
+                               const int64_t* __restrict__ pid, const StepDev* __restrict__ sd, void* __restrict__ xo,
                                float* __restrict__ vo, int64_t* __restrict__ po, int32_t* __restrict__ pcell_o) {
   const int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (pos >= np) return;
+  const float dt_mid = sd->dt_mid;
   const int64_t src = ssrc[pos];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -336,18 +349,24 @@ __device__ __forceinline__ void dep_add(void* rho, int64_t i, float w) {
 // forms them in real(8): particle_mesh.f90:106 testrho, kick.f90:687-688 ptotal), in
 // particle units.  The fixed-point form sums the int64 contributions exactly (order
 // independent, so deterministic); the FP32 form sums the float weights in FP64.  Warps
-// add into one of MASS_SLOTS accumulators picked by block, so the atomics do not all hit
-// one address; the host adds the slots.
-constexpr int MASS_SLOTS = 64;
+// add into one of MASS_SLOTS accumulators picked by block, each on its own 128-byte line
+// (MASS_STRIDE words apart), so the atomics spread over many L2 lines; the host adds the
+// slots.  A fixed-point slot is 128 bits: word 0 takes the sums, word 1 counts its carries
+// (2^40 per particle overflows 64 bits beyond 2^24 particles).
+constexpr int MASS_SLOTS = 64, MASS_STRIDE = 16;
 
 __device__ __forceinline__ void warp_sum_to(unsigned long long v, unsigned long long* out) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0 && v && out) atomicAdd(out + (blockIdx.x & (MASS_SLOTS - 1)), v);
+  if ((threadIdx.x & 31) == 0 && v && out) {
+    unsigned long long* slot = out + (blockIdx.x & (MASS_SLOTS - 1)) * MASS_STRIDE;
+    const unsigned long long old = atomicAdd(slot, v);
+    if (old + v < old) atomicAdd(slot + 1, 1ull);
+  }
 }
 
 __device__ __forceinline__ void warp_sum_to(double v, double* out) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0 && v != 0.0 && out) atomicAdd(out + (blockIdx.x & (MASS_SLOTS - 1)), v);
+  if ((threadIdx.x & 31) == 0 && v != 0.0 && out) atomicAdd(out + (blockIdx.x & (MASS_SLOTS - 1)) * MASS_STRIDE, v);
 }
 
 // One thread's running mass sum in the arithmetic of its deposit form.
@@ -589,10 +608,9 @@ __device__ __forceinline__ double pm3_xpos(double lf, const Geo& G, double gs, i
 template <bool FIXED>
 __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                               const int32_t* __restrict__ box_slot, int iapm, void* __restrict__ rho,
-                              unsigned* err, int pr, int64_t pl, void* msum) {
+                              unsigned* err, int pr, int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  MassAcc<FIXED> mass;
-  if (ip < np) {
+  if (ip >= np) return;
   int g[3];
   cell_coords(G, pcell[ip], g[0], g[1], g[2]);
   int tc[3][2], uc[3][2], lc[3][2], nca[3];  // at most two candidate subtiles per dimension (ntt >= 2)
@@ -647,14 +665,66 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
               if (x < 0 || x >= nft) continue;
               const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
               dep_add<FIXED>(base, (int64_t)z * pl + (int64_t)y * pr + x, ww);
-              // physical cells 1..nfp of the subtile (array nfb..nfb+nfp-1)
-              if ((unsigned)(x - nfb) < (unsigned)nfp && (unsigned)(y - nfb) < (unsigned)nfp &&
-                  (unsigned)(z - nfb) < (unsigned)nfp)
-                mass.add(ww);
             }
           }
         }
       }
+}
+
+// PM3 mass over the physical cells of every subtile box (kick.f90:687-688 ptotal), summed
+// per particle: for each box the deposit puts the particle in (its own subtile and, in the
+// first or last coarse cell of a subtile, the neighbour; each at that box's class), the
+// contributions that land in the box's physical cells.  The deposit adds exactly these
+// contributions to those cells, so with the fixed-point deposit this is the mesh sum
+// itself, exactly; the deposit kernels need no extra work for it.
+template <bool FIXED>
+__global__ void __launch_bounds__(256) k_mass_pm3(Geo G, int64_t np, const void* __restrict__ xp,
+                                                  const int32_t* __restrict__ pcell, const int32_t* __restrict__ ires,
+                                                  void* msum) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  MassAcc<FIXED> mass;
+  if (ip < np) {
+    int g[3];
+    cell_coords(G, pcell[ip], g[0], g[1], g[2]);
+    int tc[3][2], uc[3][2], lc[3][2], nca[3];
+    double f[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      nca[d] = sub_cands(G, g[d], tc[d], uc[d], lc[d]);
+      f[d] = zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
+    }
+#pragma unroll
+    for (int cz = 0; cz < 2; ++cz)
+#pragma unroll
+      for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+        for (int cx = 0; cx < 2; ++cx) {
+          if (cz >= nca[2] || cy >= nca[1] || cx >= nca[0]) continue;
+          const int t[3] = {tc[0][cx], tc[1][cy], tc[2][cz]};
+          const int u[3] = {uc[0][cx], uc[1][cy], uc[2][cz]};
+          const int iapm = ires[subtile_id(G, t, u)];
+          const int nfp = G.nfp[iapm], rsf = rsf_of(iapm);
+          const double gs = (double)(1.f / (float)rsf);
+          const int l[3] = {lc[0][cx], lc[1][cy], lc[2][cz]};
+          int i2[3];
+          float w[3][3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) i2[d] = tsc_weights(pm3_xpos((double)l[d] + f[d], G, gs, rsf, u[d] * nfp), w[d]);
+          // array index i2-1+a-(1-nfb) is physical when in nfb..nfb+nfp-1, i.e. i2-1+a in 1..nfp
+#pragma unroll
+          for (int a3 = 0; a3 < 3; ++a3) {
+            if ((unsigned)(i2[2] - 2 + a3) >= (unsigned)nfp) continue;
+#pragma unroll
+            for (int a2 = 0; a2 < 3; ++a2) {
+              if ((unsigned)(i2[1] - 2 + a2) >= (unsigned)nfp) continue;
+#pragma unroll
+              for (int a1 = 0; a1 < 3; ++a1) {
+                if ((unsigned)(i2[0] - 2 + a1) >= (unsigned)nfp) continue;
+                mass.add(__fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]));
+              }
+            }
+          }
+        }
   }
   mass.flush(msum);
 }
@@ -693,8 +763,7 @@ __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo
                                                                      const int64_t* __restrict__ cstart,
                                                                      const int32_t* __restrict__ box_sub, int iapm,
                                                                      float* __restrict__ rho, unsigned* err,
-                                                                     int pr, int64_t pl, int nrx, int nry, int nrz,
-                                                                     unsigned long long* msum) {
+                                                                     int pr, int64_t pl, int nrx, int nry, int nrz) {
   constexpr int R = DEP3_R, RZ = DEP3_RZ;
   static_assert(R % 2 == 0 && R / 2 <= 16, "a half warp writes one region row");
   extern __shared__ __align__(16) unsigned long long acc[];  // [RZ][R][R]
@@ -707,8 +776,9 @@ __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo
   const int r = (int)(blockIdx.x - j * nreg);
   const int o[3] = {(r % nrx) * R, ((r / nrx) % nry) * R, (r / (nrx * nry)) * RZ};
   const int e[3] = {min(R, nft - o[0]), min(R, nft - o[1]), min(RZ, nft - o[2])};
-  // subtile of this box
+  // subtile of this box; -1 pads a class list beyond its count (the slot is never read)
   const int s = box_sub[j];
+  if (s < 0) return;
   const int nns3 = G.nns * G.nns * G.nns;
   const int T = s / nns3, f = s - T * nns3;
   const int t[3] = {T % G.nnt, (T / G.nnt) % G.nnt, T / (G.nnt * G.nnt)};
@@ -828,9 +898,6 @@ __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo
   float* base = rho + j * (int64_t)nft * pl + (int64_t)o[2] * pl + (int64_t)o[1] * pr + o[0];
   const int hx = e[0] >> 1, nrow = e[1] * e[2], hl = tid & 15;
   const float inv_e1 = 1.f / (float)e[1];
-  // physical cells 1..nfp of the subtile are array nfb..nfb+nfp-1
-  const bool px0 = (unsigned)(o[0] + 2 * hl - nfb) < (unsigned)nfp, px1 = (unsigned)(o[0] + 2 * hl + 1 - nfb) < (unsigned)nfp;
-  unsigned long long mloc = 0;
   for (int row = tid >> 4; row < nrow; row += blockDim.x >> 4) {
     const int z = (int)(((float)row + 0.5f) * inv_e1);
     const int y = row - z * e[1];
@@ -840,14 +907,11 @@ __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo
         val.x = ((val.x >> 32) << 20) + (val.x & 0xffffffffull);
         val.y = ((val.y >> 32) << 20) + (val.y & 0xffffffffull);
       }
-      if ((unsigned)(o[1] + y - nfb) < (unsigned)nfp && (unsigned)(o[2] + z - nfb) < (unsigned)nfp)
-        mloc += (px0 ? val.x : 0ull) + (px1 ? val.y : 0ull);
       const float2 fv = make_float2((float)((double)(long long)val.x * 9.094947017729282e-13),  // 2^-40
                                     (float)((double)(long long)val.y * 9.094947017729282e-13));
       __stcs(reinterpret_cast<float2*>(base + (int64_t)z * pl + (int64_t)y * pr) + hl, fv);
     }
   }
-  warp_sum_to(mloc, msum);
 }
 
 // =================================================================================
@@ -925,11 +989,13 @@ __device__ __forceinline__ void f3_cp_async4(float* smem, const float* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __global__ void __launch_bounds__(256, 3) k_f2max_box2(const float* __restrict__ phi, int n, int nforce, int m1phi,
-                                                       int nbox, float* __restrict__ f2out, int pf, int64_t pl) {
+                                                       int nbox, float* __restrict__ f2out, int pf, int64_t pl,
+                                                       const int32_t* __restrict__ box_sub) {
   __shared__ float pln[F3_STAGES][F3_HALO];
   const int nt = (nforce + F3_T - 1) / F3_T;
   const int tile = blockIdx.x % (nt * nt);
   const int b = blockIdx.x / (nt * nt);
+  if (box_sub && box_sub[b] < 0) return;  // padding slot of a class list: block-uniform, nothing to reduce
   const int tx0 = (tile % nt) * F3_T + 1, ty0 = (tile / nt) * F3_T + 1;  // first physical x, y
   const float* pb = phi + (size_t)b * n * pl;
   const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
@@ -1096,10 +1162,11 @@ __device__ __forceinline__ void block_vmax(const float av[3], float* vmax) {
 }
 
 __global__ void k_interp_pm1(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
-                             const float* __restrict__ phi, float* __restrict__ vp, float a_mid, float dt, int pf,
-                             int64_t pl) {
+                             const float* __restrict__ phi, float* __restrict__ vp, const StepDev* __restrict__ sd,
+                             int pf, int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= np) return;
+  const float a_mid = sd->a_mid, dt = sd->dt;
   int g[3];
   cell_coords(G, pcell[ip], g[0], g[1], g[2]);
   int i2[3];
@@ -1149,9 +1216,11 @@ __global__ void k_force_pm1(int nc, const float* __restrict__ phi, int pf, int64
 // tsc_gather_force (a3 outer, a2, a1 inner) with the same products, so the result is
 // bit-identical to differencing phi on the fly.
 __global__ void k_interp_pm1_force(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
-                                   const float4* __restrict__ force, float* __restrict__ vp, float a_mid, float dt) {
+                                   const float4* __restrict__ force, float* __restrict__ vp,
+                                   const StepDev* __restrict__ sd) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= np) return;
+  const float a_mid = sd->a_mid, dt = sd->dt;
   int g[3];
   cell_coords(G, pcell[ip], g[0], g[1], g[2]);
   int i2[3];
@@ -1187,9 +1256,10 @@ __global__ void k_interp_pm1_force(Geo G, int64_t np, const void* __restrict__ x
 }
 
 __global__ void __launch_bounds__(256, 3) k_interp_pm2(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
-                             const float* __restrict__ phi, int tile0, int ntile, float* __restrict__ vp, float a_mid,
-                             float dt, float* vmax, unsigned* err, int pf, int64_t pl) {
+                             const float* __restrict__ phi, int tile0, int ntile, float* __restrict__ vp,
+                             const StepDev* __restrict__ sd, float* vmax, unsigned* err, int pf, int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const float a_mid = sd->a_mid, dt = sd->dt;
   float av[3] = {0.f, 0.f, 0.f};
   if (ip < np) {
     int g[3];
@@ -1223,9 +1293,10 @@ __global__ void __launch_bounds__(256, 3) k_interp_pm2(Geo G, int64_t np, const 
 
 __global__ void __launch_bounds__(256, 3) k_interp_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                              const float* __restrict__ phi, const int32_t* __restrict__ box_slot, int iapm,
-                             float* __restrict__ vp, float a_mid, float dt, float* vmax, unsigned* err, int pf,
-                             int64_t pl) {
+                             float* __restrict__ vp, const StepDev* __restrict__ sd, float* vmax, unsigned* err,
+                             int pf, int64_t pl) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const float a_mid = sd->a_mid, dt = sd->dt;
   float av[3] = {0.f, 0.f, 0.f};
   if (ip < np) {
     int g[3];
@@ -1290,6 +1361,61 @@ __global__ void k_classify(Geo G, const int32_t* __restrict__ rhoc, int ns3, int
   atomicAdd(&napm[r], 1);
 }
 
+// Chunk plan of the PM3 boxes: of the subtiles of class c (2..5) in ascending order, the
+// first skip[c] are left out and the next cap[c] at most are listed, in chunks of per[c]
+// boxes; chunk j of class c is list kbase[c] + j.  The host sizes it (exactly, or with
+// headroom for a captured step; skip > 0 lists what a captured step could not hold) and
+// the device fills it from ires.
+struct PM3Plan {
+  int cap[8], per[8], kbase[8], skip[8];
+  int nk, per_max;
+};
+
+// Class lists on the device (kick.f90:108-138 classes, kick.f90:141-201 order by class):
+// the subtiles of class c in ascending order take slots 0, 1, ... of the chunks of c.
+// box_sub[k][slot] = subtile (-1 pads unused slots), box_slot[k][s] = slot (-1: not in
+// list k); both arrays arrive filled with -1.  *overflow is set when a class has more
+// subtiles than skip + capacity (the ones beyond are not listed).  One block of 1024
+// threads; thread t owns a contiguous run of subtiles, so ranks follow subtile order.
+__global__ void __launch_bounds__(1024) k_build_lists(const int32_t* __restrict__ ires, int ns3, PM3Plan pl,
+                                                      int32_t* __restrict__ box_slot, int32_t* __restrict__ box_sub,
+                                                      unsigned* __restrict__ overflow) {
+  __shared__ int sc[4][1024];
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int per_t = (ns3 + T - 1) / T;
+  const int s0 = min(ns3, tid * per_t), s1 = min(ns3, s0 + per_t);
+  int cnt[4] = {0, 0, 0, 0};
+  for (int s = s0; s < s1; ++s) cnt[(ires[s] - 2) & 3] += 1;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) sc[k][tid] = cnt[k];
+  __syncthreads();
+  for (int off = 1; off < T; off <<= 1) {
+    int v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = tid >= off ? sc[k][tid - off] : 0;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) sc[k][tid] += v[k];
+    __syncthreads();
+  }
+  int r[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r[k] = sc[k][tid] - cnt[k];
+  for (int s = s0; s < s1; ++s) {
+    const int c = ires[s], k = (c - 2) & 3;
+    const int rank = r[k]++ - pl.skip[c];
+    if (rank >= 0 && rank < pl.cap[c]) {
+      const int chunk = rank / pl.per[c], slot = rank - chunk * pl.per[c];
+      const int64_t kk = pl.kbase[c] + chunk;
+      box_slot[kk * ns3 + s] = slot;
+      box_sub[kk * pl.per_max + slot] = s;
+    }
+  }
+  if (tid == 0)
+    for (int k = 0; k < 4; ++k)
+      if (sc[k][T - 1] > pl.skip[k + 2] + pl.cap[k + 2]) *overflow = 1u;
+}
+
 // =================================================================================
 // PP (kick.f90:376-588).  Each physical particle sums 0<r^2<range^2 pairs over the
 // coarse cells its range can reach; equivalent to the reference's PP-cell lists
@@ -1321,10 +1447,13 @@ __device__ __forceinline__ float pp_xq(const Geo& G, int lq, int code, float xre
 template <bool FAST>
 __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                      const int64_t* __restrict__ cstart, const int32_t* __restrict__ ires, float* __restrict__ vp,
-                     float mass_scale, float v_scale, float* f2max, float* vmax,
-                     unsigned long long* npairs) {
+                     const StepDev* __restrict__ sd, float* f2max, float* vmax,
+                     unsigned long long* npairs, unsigned long long* ncand, const unsigned* __restrict__ abort) {
   const int64_t ip0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = ip0 < np;
+  const float mass_scale = sd->pp_mass, v_scale = sd->pp_vscale;
+  // abort: the class lists of a captured step were too short; PM3 is finished for the
+  // unlisted subtiles afterwards and PP must follow it, so PP leaves vp alone here
+  const bool live = ip0 < np && !(abort && *abort);
   const int64_t ip = live ? ip0 : np - 1;
   int g[3];
   cell_coords(G, pcell[ip], g[0], g[1], g[2]);
@@ -1353,12 +1482,14 @@ __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32
     hi[d] = ((float)G.rcs - fin[d] < range) ? 1 : 0;
   }
   float acc[3] = {0.f, 0.f, 0.f};
-  unsigned long long cnt = 0;
+  unsigned long long cnt = 0, cand = 0;
+  if (live)
   for (int dz = lo[2]; dz <= hi[2]; ++dz)
     for (int dy = lo[1]; dy <= hi[1]; ++dy)
       for (int dx = lo[0]; dx <= hi[0]; ++dx) {
         const int64_t c = cell_index(G, g[0] + dx, g[1] + dy, g[2] + dz);
         const int64_t s = cstart[c], e = cstart[c + 1];
+        cand += (unsigned long long)(e - s);
         const int lq[3] = {l[0] + dx, l[1] + dy, l[2] + dz};
         for (int64_t q = s; q < e; ++q) {
           float rv[3];
@@ -1388,9 +1519,13 @@ __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32
   }
   block_max_to(f2, f2max);
   block_vmax(av, vmax);
-  unsigned long long c = live ? cnt : 0ull;
-  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  unsigned long long c = live ? cnt : 0ull, cd = live ? cand : 0ull;
+  for (int o = 16; o > 0; o >>= 1) {
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+    cd += __shfl_xor_sync(0xffffffffu, cd, o);
+  }
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(npairs, c);
+  if ((threadIdx.x & 31) == 0 && cd) atomicAdd(ncand, cd);
 }
 
 // =================================================================================

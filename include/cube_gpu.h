@@ -78,7 +78,7 @@ typedef struct cube_params {
   float f_nu;        /* neutrino mass fraction for the linear-response rescale (0: CDM) */
   int64_t np_capacity; /* particle capacity on device (0: derive from ng, np_nc)        */
   int32_t max_segment; /* largest destination cell the drift sorts (0: default 16384)   */
-  int32_t reserved;
+  int32_t step_graph;  /* 1: cube_gpu_step replays each step as one captured CUDA graph   */
 } cube_params;
 
 /* Per-step scalars chosen by the host timestep (timestep.f90:4-110). */
@@ -107,6 +107,7 @@ typedef struct cube_step_out {
    * particles after the kick, per component, in FP64 (deterministic order). */
   double mass_pm1, mass_pm2, mass_pm3;
   double momentum[3];
+  int64_t pp_candidates;                        /* PP candidate pairs tested (r^2 evaluated) */
 } cube_step_out;
 
 typedef struct cube_ctx cube_ctx;

@@ -355,8 +355,10 @@ def test_int2real_matches_oracle(oracle_lib, izipx):
 def test_fp64_mass_and_momentum(oracle_lib, fixed):
     """FP64 global reductions of the step: the density summed over each level's physical
     cells (particle_mesh.f90:106, kick.f90:687-688) equals the oracle's, exactly with the
-    fixed-point deposit (int64 sums) and to 1e-9 relative in FP32; it is the particle count
-    up to the rounding of the TSC weights.  Momentum is the FP64 sum of vp after the kick."""
+    fixed-point deposit (int64 sums) and to 1e-6 relative in FP32 (the oracle, as the
+    reference, sums cells that were accumulated in FP32, ~5e-8 relative off; the GPU sums
+    the FP32 weights in FP64); it is the particle count up to the rounding of the TSC
+    weights.  Momentum is the FP64 sum of vp after the kick."""
     p = _params(fixed=fixed)
     n = 24000
     st = clustered_state(p, n, seed=17)
@@ -372,7 +374,7 @@ def test_fp64_mass_and_momentum(oracle_lib, fixed):
         if fixed:
             assert got[lvl] == ref.mass[lvl], (lvl, got[lvl], ref.mass[lvl])
         else:
-            assert abs(got[lvl] - ref.mass[lvl]) < 1e-9 * n, (lvl, got[lvl], ref.mass[lvl])
+            assert abs(got[lvl] - ref.mass[lvl]) < 1e-6 * n, (lvl, got[lvl], ref.mass[lvl])
     mom = vp.astype(np.float64).sum(axis=0)
     scale = np.abs(vp).astype(np.float64).sum(axis=0)
     for d in range(3):

@@ -1,0 +1,225 @@
+"""End-to-end precision of the P3M step at the 128^3 configuration against the FP64 oracle.
+
+Workload: 128^3 CDM particles in a 200 Mpc/h box, fine mesh 256^3 (PM1 64^3, PM2 64 tiles
+of 96^3, PM3 4096 subtiles), int8 compressed coordinates (izipx=1), PP on, Zel'dovich ICs
+at z=49 from the device IC generator, 10 KDK steps of equal code time to z=10 and the
+closing half drift of a checkpoint (main.f90:39-41).  The reference's own timestep is
+adaptive and needs ~16 steps for this range (ra_max = 0.1), so the fixed schedule of
+cosmology.fixed_steps is fed to every arm.
+
+Arms: the GPU in its plain form (FP32 atomics) and its chosen form (int64 fixed-point
+deposit), and the oracle in FP32 (the reference's kinds) and FP64 (drift64 + kick64).
+What is compared with the FP64 arm (particles matched by PID):
+  * final positions: max and rms of the periodic distance, in fine cells;
+  * final velocities: rms |dv| / rms |v|;
+  * density, potential and per-particle force of one more kick evaluated on the FP64
+    arm's final state (so only that evaluation differs): PM1 density and potential and the
+    velocity change of the whole kick, relative to their largest values;
+  * the power spectrum of the final particles on the 2*ng = 512^3 CIC grid
+    (cicpower.f90 with FFTFINE), every arm through the same estimator (cube_gpu_power
+    with the fixed-point deposit): |dP/P| < 1e-3 for k < k_Nyq/2, k_Nyq = pi*512/200 h/Mpc.
+"""
+import json
+
+import numpy as np
+import pytest
+
+from cube_nu_b200 import cosmology
+from cube_nu_b200.params import DEPOSIT_FIXED, DEPOSIT_FP32, config_plain_128
+
+pytestmark = pytest.mark.gpu
+
+NSTEPS = 10
+Z_START, Z_END = 49.0, 10.0
+PK_TOL = 1e-3
+
+
+def _params(fixed):
+    p = config_plain_128()
+    p.nic = 1
+    p.deposit_mode = DEPOSIT_FIXED if fixed else DEPOSIT_FP32
+    return p
+
+
+def _schedule(p):
+    tab = cosmology.expansion_table(p.h0, p.omega_m, p.omega_r)
+    bg = cosmology.Background.from_table(tab)
+    return cosmology.fixed_steps(bg, 1 / (1 + Z_START), 1 / (1 + Z_END), NSTEPS)
+
+
+def _positions(p, xp, rhoc):
+    """Global positions in fine cells (float64), particles in storage order: the ZIPX
+    offset plus the coarse cell (int2real.f90:85-86) times ratio_cs."""
+    u = xp.astype(np.int64) & (0xFF if p.izipx == 1 else 0xFFFF)
+    frac = (u.astype(np.float64) + 0.5) * 2.0 ** (-8 * p.izipx)
+    nt, nnt = p.nt, p.nnt
+    s = np.arange(p.nc ** 3, dtype=np.int64)
+    i, j, k = s % nt, (s // nt) % nt, (s // nt ** 2) % nt
+    t = s // nt ** 3
+    cell = np.stack([(t % nnt) * nt + i, ((t // nnt) % nnt) * nt + j, (t // nnt ** 2) * nt + k], axis=-1)
+    g = np.repeat(cell, np.asarray(rhoc, dtype=np.int64), axis=0)
+    return (frac + g) * p.ratio_cs
+
+
+def _by_pid(pid, *arrays):
+    order = np.argsort(pid, kind="stable")
+    return [a[order] for a in arrays]
+
+
+def _run_gpu(p, st, sched, vz0):
+    from cube_nu_b200._lib import Context
+
+    with Context(p) as ctx:
+        ctx.upload(*st)
+        vz = vz0
+        outs = []
+        for dt, dt_old, a_mid, _ in sched:
+            so = ctx.step(dt, dt_old, a_mid, vz)
+            vz = so.vz_max
+            outs.append(so)
+        ctx.drift(sched[-1][0], 0.0, vz)
+        return ctx.download(), outs
+
+
+def _run_oracle(O, p, st, sched, vz0, fp64):
+    xp, vp, pid, rhoc = st
+    vp = vp.astype(np.float64) if fp64 else vp.copy()
+    vz = vz0
+    for dt, dt_old, a_mid, _ in sched:
+        xp, vp, pid, rhoc = O.drift(p, xp, vp, pid, rhoc, dt_old, dt, vz)
+        out = O.kick(p, xp, vp, rhoc, dt, a_mid, fixed=False)
+        vz = float(out.vz_max)
+    xp, vp, pid, rhoc = O.drift(p, xp, vp, pid, rhoc, 0.0, sched[-1][0], vz)
+    return xp, vp, pid, rhoc
+
+
+def _power(p, st, nw):
+    from cube_nu_b200._lib import Context
+
+    q = _params(True)
+    q.mass_p_cdm = p.mass_p_cdm
+    with Context(q) as ctx:
+        ctx.upload(st[0], st[1].astype(np.float32), st[2], st[3])
+        xi, _, _ = ctx.power(nw)
+    return xi
+
+
+@pytest.fixture(scope="module")
+def runs(oracle_lib):
+    from cube_nu_b200 import ic
+    from cube_nu_b200._lib import Context
+
+    p = _params(True)
+    p.mass_p_cdm = float(p.ng) ** 3 / float(p.npglobal)
+    with Context(p) as ctx:
+        d = ic.zeldovich_device(ctx, p, z_i=Z_START, seed=1)
+        st0 = ctx.download()
+    sched = _schedule(p)
+    res = {"p": p, "st0": st0, "sched": sched}
+    for name, fixed in (("gpu_fixed", True), ("gpu_plain", False)):
+        q = _params(fixed)
+        q.mass_p_cdm = p.mass_p_cdm
+        res[name], res[name + "_outs"] = _run_gpu(q, st0, sched, d["vz_max"])
+    oracle_lib.set_threads(0)
+    res["oracle32"] = _run_oracle(oracle_lib, p, st0, sched, d["vz_max"], fp64=False)
+    res["oracle64"] = _run_oracle(oracle_lib, p, st0, sched, d["vz_max"], fp64=True)
+    return res
+
+
+def _pos_vel_errors(p, st, ref):
+    x = _positions(p, st[0], st[3])
+    xr = _positions(p, ref[0], ref[3])
+    x, v = _by_pid(st[2], x, st[1].astype(np.float64))
+    xr, vr = _by_pid(ref[2], xr, ref[1].astype(np.float64))
+    L = p.ng
+    dx = (x - xr + L / 2) % L - L / 2
+    dist = np.sqrt((dx ** 2).sum(axis=1))
+    dv = np.sqrt(((v - vr) ** 2).sum(axis=1))
+    return {"pos_max_fine": float(dist.max()), "pos_rms_fine": float(np.sqrt((dist ** 2).mean())),
+            "vel_rel_rms": float(np.sqrt((dv ** 2).mean() / (vr ** 2).sum(axis=1).mean()))}
+
+
+def test_final_state_matches_fp64_oracle(runs):
+    p = runs["p"]
+    ref = runs["oracle64"]
+    assert np.array_equal(np.sort(runs["gpu_fixed"][2]), np.sort(ref[2]))
+    summary = {}
+    for arm in ("gpu_fixed", "gpu_plain", "oracle32"):
+        e = _pos_vel_errors(p, runs[arm], ref)
+        summary[arm] = e
+        # one ZIPX code of an int8 coordinate is 1/64 fine cell; the FP32 arms differ from
+        # FP64 by velocity rounding that flips a few codes
+        assert e["pos_rms_fine"] < 2e-3, (arm, e)
+        assert e["pos_max_fine"] < 0.1, (arm, e)
+        assert e["vel_rel_rms"] < 2e-4, (arm, e)
+    # the plain form against the FP32 restatement of the reference path
+    e = _pos_vel_errors(p, runs["gpu_plain"], runs["oracle32"])
+    summary["gpu_plain_vs_oracle32"] = e
+    assert e["pos_rms_fine"] < 2e-3 and e["vel_rel_rms"] < 2e-4, e
+    # mass conservation every step (kick.f90:42,72,242)
+    n = p.npglobal
+    for arm in ("gpu_fixed", "gpu_plain"):
+        for so in runs[arm + "_outs"]:
+            for m in (so.mass_pm1, so.mass_pm2, so.mass_pm3):
+                assert abs(m - n) < 1e-6 * n
+    print("PRECISION final-state " + json.dumps(summary))
+
+
+def test_fields_and_forces_match_fp64_oracle(runs, oracle_lib):
+    """One kick on the FP64 arm's final state: PM1 density and potential, and the velocity
+    change of the whole kick (PM1+PM2+PM3+PP) per particle, against the FP64 oracle's."""
+    from cube_nu_b200._lib import Context
+
+    p = runs["p"]
+    xp, vp, pid, rhoc = runs["oracle64"]
+    a_mid, dt = runs["sched"][-1][2], runs["sched"][-1][0]
+    v64 = vp.astype(np.float64).copy()
+    ref_out = oracle_lib.kick(p, xp, v64, rhoc, dt, a_mid)
+    dv_ref = v64 - vp
+    n1 = p.nc ** 3
+    _, dens_ref = oracle_lib.kick(p, xp, vp.astype(np.float64).copy(), rhoc, dt, a_mid, only=1, debug=(1, 0, 0, n1))
+    _, phi_ref = oracle_lib.kick(p, xp, vp.astype(np.float64).copy(), rhoc, dt, a_mid, only=1, debug=(1, 0, 1, n1))
+    summary = {}
+    for arm, fixed in (("gpu_fixed", True), ("gpu_plain", False)):
+        q = _params(fixed)
+        q.mass_p_cdm = p.mass_p_cdm
+        v32 = vp.astype(np.float32)
+        got = {}
+        for what in (0, 1):
+            with Context(q) as ctx:
+                ctx.upload(xp, v32, pid, rhoc)
+                ctx.capture(1, 0, what)
+                so = ctx.kick(dt, a_mid)
+                got[what] = ctx.captured(n1)
+                vnew = ctx.download()[1]
+        dv = vnew.astype(np.float64) - v32.astype(np.float64)
+        e = {
+            "density_rel_max": float(np.abs(got[0] - dens_ref).max() / np.abs(dens_ref).max()),
+            "potential_rel_max": float(np.abs(got[1] - phi_ref).max() / np.abs(phi_ref).max()),
+            "force_rel_max": float(np.abs(dv - dv_ref).max() / np.abs(dv_ref).max()),
+            "force_rel_rms": float(np.sqrt(((dv - dv_ref) ** 2).mean() / (dv_ref ** 2).mean())),
+            "dt_pp_rel": float(abs(so.dt_pp - ref_out.dt_pp) / ref_out.dt_pp),
+        }
+        summary[arm] = e
+        assert e["density_rel_max"] < 1e-5, (arm, e)
+        assert e["potential_rel_max"] < 1e-4, (arm, e)
+        assert e["force_rel_rms"] < 1e-4 and e["force_rel_max"] < 2e-3, (arm, e)
+    print("PRECISION fields " + json.dumps(summary))
+
+
+def test_power_spectrum_within_tenth_percent(runs):
+    """|dP/P| < 1e-3 for k < k_Nyq/2 on the 512^3 grid, each arm against the FP64 oracle."""
+    p = runs["p"]
+    nw = 2 * p.ng
+    ref = _power(p, runs["oracle64"], nw)
+    knyq = np.pi * nw / p.box
+    sel = (ref[:, 0] > 0) & (ref[:, 1] > 0) & (ref[:, 1] < knyq / 2)
+    assert sel.sum() > 100
+    summary = {"grid": nw, "k_nyq_half": knyq / 2, "bins": int(sel.sum())}
+    for arm in ("gpu_fixed", "gpu_plain", "oracle32"):
+        xi = _power(p, runs[arm], nw)
+        assert np.array_equal(xi[:, 0], ref[:, 0])
+        rel = np.abs(xi[sel, 2] / ref[sel, 2] - 1)
+        summary[arm] = {"dP_over_P_max": float(rel.max()), "dP_over_P_rms": float(np.sqrt((rel ** 2).mean()))}
+        assert rel.max() < PK_TOL, (arm, summary[arm])
+    print("PRECISION pk " + json.dumps(summary))
