@@ -339,6 +339,8 @@ def main():
     ap.add_argument("--deposit", default="fixed", choices=["fixed", "plain"])
     ap.add_argument("--graph", default="on", choices=["on", "off"],
                     help="replay each step as one captured CUDA graph (cube_params.step_graph)")
+    ap.add_argument("--pp", default="queue", choices=["queue", "thread"],
+                    help="PP as the autotuned cell work queue (cube_params.pp_queue) or a thread per particle")
     ap.add_argument("--compare", default="on", choices=["on", "off"],
                     help="also time the plain form (FP32 atomics, eager) over the same steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -356,6 +358,7 @@ def main():
     fixed = args.deposit == "fixed"
     p.deposit_mode = DEPOSIT_FIXED if fixed else DEPOSIT_FP32
     p.step_graph = args.graph == "on"
+    p.pp_queue = args.pp == "queue" and (p.izipx == 1 or p.nt < 127)
 
     import torch
 
@@ -412,10 +415,11 @@ def main():
 
     # ---------------- the plain form over the same steps ----------------
     plain = None
-    if args.compare == "on" and (fixed or p.step_graph):
+    if args.compare == "on" and (fixed or p.step_graph or p.pp_queue):
         q, _ = workload(args.workload)
         q.deposit_mode = DEPOSIT_FP32
         q.step_graph = False
+        q.pp_queue = False
         P = run_form(q, args, local, dist, rank, replay=R["steps_in"])
         xi_plain = P["ctx"].power(nw, n_corr=0)[0]
         P["ctx"].close()
@@ -474,11 +478,11 @@ def main():
                    "sample": sample, "sample_seconds": round(secs, 2), "extrapolated_to_full_step": True}
         forms = {"chosen": {"value": round(value, 1), "ms_per_step": round(R["dev_s"] * 1e3 / args.steps, 3),
                             "deposit": "int64 fixed-point" if fixed else "fp32 atomics",
-                            "graph": bool(p.step_graph)}}
+                            "graph": bool(p.step_graph), "pp": "queue" if p.pp_queue else "thread"}}
         precision = None
         if plain:
             forms["plain"] = {"value": round(plain["value"], 1), "ms_per_step": round(plain["ms_per_step"], 3),
-                              "deposit": "fp32 atomics", "graph": False,
+                              "deposit": "fp32 atomics", "graph": False, "pp": "thread",
                               "stage_ms_per_step": {k: round(float(v), 3) for k, v in
                                                     zip(("drift", "pm1", "pm2", "pm3", "pp", "kick", "step"),
                                                         plain["stage"])}}
@@ -497,7 +501,7 @@ def main():
             "data": "synthetic (Zel'dovich ICs z=49, EH no-wiggle, seeded)",
             "config": {"workload": desc, "particles_per_gpu": n, "ng": p.ng, "box": p.box,
                        "deposit": "int64 fixed-point" if fixed else "fp32 atomics",
-                       "step_graph": bool(p.step_graph),
+                       "step_graph": bool(p.step_graph), "pp": "queue" if p.pp_queue else "thread",
                        "timestep": "reference adaptive (timestep.f90)", "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (%.1f GB particle state)" % (n * 26 / 1e9),
                        "pm3_classes": napm[2:6], "a_end": R["S"].a},

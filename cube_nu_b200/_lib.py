@@ -21,7 +21,7 @@ EXPORTS = (
     "cube_gpu_green_table", "cube_gpu_subtile_class", "cube_gpu_last_error", "cube_gpu_version",
     "cube_gpu_profile", "cube_gpu_profile_read", "cube_gpu_profile_name", "cube_gpu_kernel_launches",
     "cube_gpu_zipv_encode", "cube_gpu_zipv_decode", "cube_gpu_download_zipv", "cube_gpu_ic", "cube_gpu_power",
-    "cube_gpu_int2real", "cube_gpu_step_host",
+    "cube_gpu_int2real", "cube_gpu_step_host", "cube_gpu_pp_shape", "cube_gpu_pp_shape_get",
 )
 
 
@@ -107,6 +107,9 @@ def load():
     L.cube_gpu_int2real.argtypes = [vp, vp, ctypes.c_int64]
     L.cube_gpu_step_host.argtypes = [vp, ctypes.POINTER(StepIn), ctypes.POINTER(StepOut), vp, vp, vp, vp,
                                      ctypes.c_int64]
+    L.cube_gpu_pp_shape.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.cube_gpu_pp_shape_get.argtypes = [vp, ctypes.c_int, ip, ip, ip, ctypes.POINTER(ctypes.c_double)]
     _LIB = L
     return L
 
@@ -278,6 +281,17 @@ class Context:
         out = np.empty((self.np, 3), dtype=np.float32)
         _check(self._lib.cube_gpu_int2real(self._h, _ptr(out), out.size), "cube_gpu_int2real")
         return out
+
+    def pp_shape(self, cls: int, T: int, B: int = 256, J: int = 512) -> None:
+        """Set the queue-PP shape of occupancy class cls (T <= 0: tune it again)."""
+        _check(self._lib.cube_gpu_pp_shape(self._h, cls, T, B, J), "cube_gpu_pp_shape")
+
+    def pp_shape_get(self, cls: int):
+        """(T, B, J, tuned ms) of occupancy class cls, or None when it has none yet."""
+        T, B, J, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        rc = _check(self._lib.cube_gpu_pp_shape_get(self._h, cls, ctypes.byref(T), ctypes.byref(B), ctypes.byref(J),
+                                                    ctypes.byref(ms)), "cube_gpu_pp_shape_get")
+        return (T.value, B.value, J.value, ms.value) if rc == 1 else None
 
     def subtile_class(self) -> np.ndarray:
         out = np.empty(self.params.ns3, dtype=np.int32)

@@ -22,6 +22,8 @@
 #include "kernels.cuh"
 #include "ic.cuh"
 #include "power.cuh"
+#include "pp.cuh"
+#include "dpm.cuh"
 
 using namespace cube;
 
@@ -79,18 +81,31 @@ struct StepRes {
   unsigned err;       // device error word (CUBE_DEVERR_*)
   unsigned overflow;  // a PM3 class outgrew the captured plan
   int32_t napm[8];
+  int32_t maxcount;   // largest coarse-cell occupancy (PP tuning class)
+  int32_t pad;
   int64_t total;      // particles placed by the drift
   unsigned long long msum[3 * MASS_SLOTS * MASS_STRIDE];
   double mom[3 * MOM_BLOCKS];
 };
 
+// Shape of the queue PP (pp.cuh): light-cell threshold T, items of B particles (the heavy
+// kernel's block), candidate chunks of J particles in shared memory.
+struct PPShape {
+  int T = 64, B = 256, J = 512;
+  bool operator==(const PPShape& o) const { return T == o.T && B == o.B && J == o.J; }
+};
+
+// PP tuning classes by the largest cell occupancy.
+int pp_class(int maxcount) { return maxcount <= 64 ? 0 : maxcount <= 512 ? 1 : maxcount <= 4096 ? 2 : 3; }
+
 // One captured step (drift + kick) as an executable CUDA graph, for one particle-buffer
-// parity, particle count and PM3 plan.
+// parity, particle count, PM3 plan and PP shape.
 struct StepGraph {
   cudaGraphExec_t exec = nullptr;
   int parity = 0;
   int64_t np = 0;
   PM3Plan plan;
+  PPShape pps;
   bool prof = false;
   int64_t kernels = 0;                 // kernel launches in one replay
   std::vector<cudaEvent_t> events;     // per-kernel timer events recorded by the graph
@@ -157,6 +172,18 @@ struct cube_ctx {
   StepGraph* cap_graph = nullptr;  // the graph being captured (timers and launches go to it)
   int32_t napm_est[8] = {0};       // class histogram of the last step (plan of the next capture)
   bool have_est = false;
+  int32_t maxcount_est = -1;       // largest cell occupancy of the last step (-1: unknown)
+  // queue PP (cube_params.pp_queue): decoded offsets, heavy-cell list and item prefix,
+  // queue counters; the autotuner's scratch velocities and reductions, and its winners
+  float4* pfin = nullptr;
+  int32_t* hlist = nullptr;
+  int* hpre = nullptr;
+  int* ppq = nullptr;
+  float* vtune = nullptr;
+  float* tune_red = nullptr;  // f2max, vmax[3] at 8, pairs (u64) at 16
+  PPShape pp_best[4];
+  bool pp_tuned[4] = {false, false, false, false};
+  double pp_tune_ms[4] = {0, 0, 0, 0};
   void* xp_base = nullptr;         // parity of the particle buffers: xp == xp_base or not
   // meshes
   void* arena = nullptr;
@@ -768,6 +795,16 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
   CK(cudaMallocHost(&c->h_sd, sizeof(StepDev)));
   CK(cudaMalloc(&c->ires, c->ns3 * 4));
   CK(cudaMallocHost(&c->h_ires, c->ns3 * 4));
+  if (c->P.pp_queue) {
+    if (!(G.izipx == 1 || G.nt < 127)) {
+      cube_gpu_destroy(c);
+      return fail(CUBE_E_ARG, "pp_queue needs int8 codes, or int16 with nt < 127 (exact FP32 candidates)");
+    }
+    CK(cudaMalloc(&c->hlist, nc3 * 4));
+    CK(cudaMalloc(&c->hpre, (nc3 + 1) * 4));
+    CK(cudaMalloc(&c->ppq, PPQ_Q * 4));
+    CK(cudaMalloc(&c->tune_red, 32 * 4));
+  }
   // Green tables of PM1 and PM2 (initialize.f90:247-258); PM3 classes on first use.
   rc = build_green(c, &c->green1, G.nc, G.apm1c, 0.f, (float)G.rcs);
   if (!rc) rc = build_green(c, &c->green2, G.ngt, G.apm2, G.apm1c * (float)G.rcs, 1.f);
@@ -788,7 +825,7 @@ int cube_gpu_destroy(cube_ctx* c) {
   void* bufs[] = {c->xp, c->xp2, c->vp, c->vp2, c->pid, c->pid2, c->pcell, c->pcell2, c->rhoc, c->rhoc2,
                   c->fill, c->biglist, c->nbig, c->cstart, c->cstart2, c->scan_tmp, c->dest, c->key, c->skey,
                   c->ssrc, c->rdev, c->sd, c->ires, c->box_slot, c->box_sub, c->arena, c->green1, c->green2,
-                  c->cap_buf};
+                  c->cap_buf, c->pfin, c->hlist, c->hpre, c->ppq, c->vtune, c->tune_red};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (int i = 0; i < 8; ++i)
@@ -826,6 +863,13 @@ static int alloc_particles(cube_ctx* c, int64_t np) {
   }
   c->cap = cap;
   c->xp_base = c->xp;
+  if (c->P.pp_queue) {
+    if (c->pfin) cudaFree(c->pfin);
+    if (c->vtune) cudaFree(c->vtune);
+    c->pfin = nullptr;
+    c->vtune = nullptr;
+    CK(cudaMalloc(&c->pfin, (size_t)cap * sizeof(float4)));
+  }
   // mesh arena: everything that fits of what the largest level needs, within 70% of free memory
   const Geo& G = c->G;
   const bool fixed = c->P.deposit_mode == CUBE_DEPOSIT_FIXED;
@@ -873,6 +917,7 @@ int cube_gpu_upload(cube_ctx* c, const void* xp, const float* vp, const int64_t*
   CK(cudaStreamSynchronize(c->s));
   c->loaded = true;
   c->have_est = false;
+  c->maxcount_est = -1;
   return 0;
 }
 
@@ -1063,6 +1108,11 @@ static int enqueue_kick_a(cube_ctx* c) {
   // ---------------- subtile classes (kick.f90:108-138) ----------------
   CK(cudaMemsetAsync(c->napm, 0, 32, c->s));
   LAUNCH(c, K_CLASSIFY, 1, k_classify<<<nblk(c->ns3), 256, 0, c->s>>>(G, c->rhoc, c->ns3, c->ires, c->napm));
+  if (c->P.pp_queue && c->P.pp_on) {  // the PP tuning class of this step
+    CK(cudaMemsetAsync(&c->rdev->maxcount, 0, 4, c->s));
+    LAUNCH(c, K_CLASSIFY, 1, k_ppq_maxcount<<<(unsigned)std::min<int64_t>(nblk(G.ncells), 4 * c->nsm), 256, 0, c->s>>>(
+                                c->cstart, G.ncells, &c->rdev->maxcount));
+  }
   // PM3 mass over the boxes' physical cells, from the classes just found
   if (c->P.pm3_on) {
     unsigned long long* ms3 = c->msum + 2 * MASS_SLOTS * MASS_STRIDE;
@@ -1197,13 +1247,112 @@ static int enqueue_pm3(cube_ctx* c, const PM3Plan& pl, bool host_ires) {
   return 0;
 }
 
-// PP (kick.f90:280-311), then the FP64 momentum sums of the kicked velocities.
-static void enqueue_pp_and_momentum(cube_ctx* c, const unsigned* abort) {
+// The queue PP (pp.cuh) with shape sh: offsets, light cells, heavy-cell queue, heavy
+// items.  Velocities go from c->vp to vout; f2 (PP f2max), vm (PP vmax[3]) and pairs
+// (in range, candidates) receive the reductions.
+static void enqueue_ppq(cube_ctx* c, const PPShape& sh, float* vout, float* f2, float* vm, unsigned long long* pairs,
+                        const unsigned* abort) {
+  const Geo& G = c->G;
+  const int64_t np = c->np;
+  LAUNCH(c, K_PP, 1, k_ppq_prep<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pfin));
+  LAUNCH(c, K_PP, 1, k_ppq_light<<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->pcell, c->cstart, c->ires, c->pfin, c->vp, vout,
+                                                                  c->sd, sh.T, f2, vm, pairs, pairs + 1, abort));
+  cudaMemsetAsync(c->ppq, 0, PPQ_Q * 4, c->s);
+  LAUNCH(c, K_PP, 1, k_ppq_bucket_count<<<nblk(G.ncells), 256, 0, c->s>>>(c->cstart, G.ncells, sh.T, c->ppq));
+  LAUNCH(c, K_PP, 1, k_ppq_bucket_scan<<<1, 32, 0, c->s>>>(c->ppq));
+  LAUNCH(c, K_PP, 1, k_ppq_bucket_fill<<<nblk(G.ncells), 256, 0, c->s>>>(c->cstart, G.ncells, sh.T, c->ppq, c->hlist));
+  LAUNCH(c, K_PP, 1, k_ppq_items<<<1, 1024, 0, c->s>>>(c->hlist, c->cstart, sh.B, c->ppq, c->hpre));
+  const unsigned grid = (unsigned)(c->nsm * std::max(1, 1024 / sh.B));
+  const size_t sm = (size_t)sh.J * sizeof(float4);
+  smem_optin(k_ppq_heavy, sm);
+  LAUNCH(c, K_PP, 1, k_ppq_heavy<<<grid, sh.B, sm, c->s>>>(G, c->hlist, c->hpre, c->ppq, c->cstart, c->ires, c->pfin,
+                                                            c->vp, vout, c->sd, sh.J, f2, vm, pairs, pairs + 1, abort));
+}
+
+// The autotuner of the queue PP: on the current particle state, time every shape of a
+// small sweep (light threshold T, item size B, chunk J), writing the velocities to a
+// scratch copy, and keep the fastest for occupancy class cls.  Results do not depend on
+// the shape (pp.cuh), only the time does.  Runs eagerly (never inside a capture).
+static int pp_tune(cube_ctx* c, int cls, int maxcount) {
+  if (!c->vtune) CK(cudaMalloc(&c->vtune, (size_t)c->cap * 12));
+  const bool prof = c->prof;
+  c->prof = false;  // the sweep is not part of any step's kernel profile
+  std::vector<PPShape> cands;
+  const int Ts[] = {16, 64, 256, 2048}, Bs[] = {128, 256, 512}, Js[] = {256, 1024};
+  bool all_light_done = false;
+  for (int T : Ts) {
+    const bool all_light = T >= maxcount;  // no heavy cells: B and J do not matter
+    if (all_light && all_light_done) continue;
+    all_light_done |= all_light;
+    for (int B : Bs)
+      for (int J : Js) {
+        if (all_light && (B != Bs[1] || J != Js[0])) continue;
+        PPShape sh;
+        sh.T = T;
+        sh.B = B;
+        sh.J = J;
+        cands.push_back(sh);
+      }
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  PPShape win;
+  for (const PPShape& sh : cands) {
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {  // the second run is timed
+      cudaMemsetAsync(c->tune_red, 0, 32 * 4, c->s);
+      cudaEventRecord(e0, c->s);
+      enqueue_ppq(c, sh, c->vtune, c->tune_red, c->tune_red + 8,
+                  reinterpret_cast<unsigned long long*>(c->tune_red + 16), nullptr);
+      cudaEventRecord(e1, c->s);
+    }
+    const cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) {
+      c->prof = prof;
+      return fail(CUBE_E_CUDA, std::string("PP tuning: ") + cudaGetErrorString(e));
+    }
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      win = sh;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->prof = prof;
+  c->pp_best[cls] = win;
+  c->pp_tuned[cls] = true;
+  c->pp_tune_ms[cls] = best;
+  const char* verbose = getenv("CUBE_VERBOSE");
+  if (verbose && verbose[0] == '1')
+    fprintf(stderr, "cube_gpu: PP tuned for class %d (max %d per cell): T=%d B=%d J=%d, %.3f ms (%zu shapes)\n", cls,
+            maxcount, win.T, win.B, win.J, best, cands.size());
+  return 0;
+}
+
+// The PP shape for a step whose largest cell holds maxcount particles (tuned on first use).
+static int pp_shape(cube_ctx* c, int maxcount, PPShape& sh) {
+  const int cls = pp_class(maxcount);
+  if (!c->pp_tuned[cls]) {
+    const int rc = pp_tune(c, cls, maxcount);
+    if (rc) return rc;
+  }
+  sh = c->pp_best[cls];
+  return 0;
+}
+
+// PP (kick.f90:280-311), then the FP64 momentum sums of the kicked velocities.  pps:
+// the queue PP's shape, or null for one thread per particle (k_pp).
+static void enqueue_pp_and_momentum(cube_ctx* c, const unsigned* abort, const PPShape* pps = nullptr) {
   const Geo& G = c->G;
   const int64_t np = c->np;
   float* f2 = c->red;
   float* vm = c->red + 8;
-  if (c->P.pp_on) {
+  if (c->P.pp_on && pps) {
+    enqueue_ppq(c, *pps, c->vp, f2 + 3, vm + 6, c->pairs, abort);
+  } else if (c->P.pp_on) {
     // FP32 candidate positions are exact when lq + offset fits 24 bits: int8 codes, or
     // int16 codes with tile-local coordinates |lq| <= nt < 128
     const bool pp_fast = G.izipx == 1 || G.nt < 127;
@@ -1285,7 +1434,7 @@ static int kick_eager(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
   int rc = enqueue_kick_a(c);
   if (rc) return rc;
   CK(cudaMemcpyAsync(c->h_ires, c->ires, c->ns3 * 4, cudaMemcpyDeviceToHost, c->s));
-  CK(cudaMemcpyAsync(c->rhost->napm, c->napm, 32, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(c->rhost->napm, c->napm, 36, cudaMemcpyDeviceToHost, c->s));  // napm and maxcount
   CK(cudaStreamSynchronize(c->s));
   int32_t napm[8];
   memcpy(napm, c->rhost->napm, sizeof napm);
@@ -1295,13 +1444,20 @@ static int kick_eager(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
   if (!rc) rc = enqueue_pm3(c, pl, true);
   if (rc) return rc;
   CK(mark(c, c->ev[3]));
-  enqueue_pp_and_momentum(c, nullptr);
+  PPShape pps;
+  const bool ppq = c->P.pp_queue && c->P.pp_on;
+  if (ppq) {
+    rc = pp_shape(c, c->rhost->maxcount, pps);
+    if (rc) return rc;
+  }
+  enqueue_pp_and_momentum(c, nullptr, ppq ? &pps : nullptr);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->rhost, c->rdev, sizeof(StepRes), cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
   prof_collect(c);
   memcpy(c->napm_est, c->rhost->napm, sizeof c->napm_est);
   c->have_est = true;
+  c->maxcount_est = c->rhost->maxcount;
   if (c->rhost->err) {
     CK(cudaMemsetAsync(c->err, 0, 4, c->s));
     CK(cudaStreamSynchronize(c->s));
@@ -1355,12 +1511,26 @@ static int step_graph(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
   const PM3Plan pl = make_plan(c, c->napm_est, true);
   rc = ensure_plan_buffers(c, pl);
   if (rc) return rc;
+  const bool ppq = c->P.pp_queue && c->P.pp_on;
+  PPShape pps;
+  if (ppq) {
+    if (c->maxcount_est < 0) {  // occupancy of the current state
+      CK(cudaMemsetAsync(&c->rdev->maxcount, 0, 4, c->s));
+      k_ppq_maxcount<<<(unsigned)std::min<int64_t>(nblk(c->G.ncells), 4 * c->nsm), 256, 0, c->s>>>(
+          c->cstart, c->G.ncells, &c->rdev->maxcount);
+      ++c->launches;
+      CK(cudaMemcpyAsync(&c->maxcount_est, &c->rdev->maxcount, 4, cudaMemcpyDeviceToHost, c->s));
+      CK(cudaStreamSynchronize(c->s));
+    }
+    rc = pp_shape(c, c->maxcount_est, pps);
+    if (rc) return rc;
+  }
   for (int cl = 2; cl <= 5; ++cl)
     if (pl.cap[cl] > 0 && !green3(c, cl)) return CUBE_E_CUDA;  // tables exist before any capture
   const int parity = c->xp == c->xp_base ? 0 : 1;
   StepGraph* g = nullptr;
   for (auto& x : c->graphs)
-    if (x.parity == parity && x.np == c->np && x.prof == c->prof && same_plan(x.plan, pl)) g = &x;
+    if (x.parity == parity && x.np == c->np && x.prof == c->prof && same_plan(x.plan, pl) && x.pps == pps) g = &x;
   if (!g) {
     // one graph per parity: a new plan replaces the old one of this parity
     for (size_t i = 0; i < c->graphs.size(); ++i)
@@ -1375,6 +1545,7 @@ static int step_graph(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     ng.parity = parity;
     ng.np = c->np;
     ng.plan = pl;
+    ng.pps = pps;
     ng.prof = c->prof;
     c->cap_graph = &ng;
     cudaGraph_t graph = nullptr;
@@ -1389,7 +1560,7 @@ static int step_graph(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     if (!rc) rc = enqueue_pm3(c, pl, false);
     if (!rc) {
       mark(c, c->ev[3]);
-      enqueue_pp_and_momentum(c, c->overflow);
+      enqueue_pp_and_momentum(c, c->overflow, ppq ? &pps : nullptr);
       mark(c, c->ev[7]);
       cudaMemcpyAsync(c->rhost, c->rdev, sizeof(StepRes), cudaMemcpyDeviceToHost, c->s);
     }
@@ -1434,7 +1605,7 @@ static int step_graph(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     if (!rc) rc = enqueue_pm3(c, rest, false);
     if (rc) return rc;
     CK(mark(c, c->ev[3]));
-    enqueue_pp_and_momentum(c, nullptr);
+    enqueue_pp_and_momentum(c, nullptr, ppq ? &pps : nullptr);
     CK(mark(c, c->ev[7]));
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->rhost, c->rdev, sizeof(StepRes), cudaMemcpyDeviceToHost, c->s));
@@ -1442,6 +1613,7 @@ static int step_graph(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     prof_collect(c);
   }
   memcpy(c->napm_est, c->rhost->napm, sizeof c->napm_est);
+  c->maxcount_est = c->rhost->maxcount;
   if (c->rhost->err) {
     CK(cudaMemsetAsync(c->err, 0, 4, c->s));
     CK(cudaStreamSynchronize(c->s));
@@ -1560,6 +1732,34 @@ int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, 
   if (rc) c->loaded = false;
   if (!rc && out) step_times(c, out);
   return rc;
+}
+
+int cube_gpu_pp_shape(cube_ctx* c, int cls, int T, int B, int J) {
+  if (!c || cls < 0 || cls > 3) return fail(CUBE_E_ARG, "bad PP class");
+  if (T <= 0) {
+    c->pp_tuned[cls] = false;
+    return 0;
+  }
+  if (B != 128 && B != 256 && B != 512) return fail(CUBE_E_ARG, "PP item size B must be 128, 256 or 512");
+  if (J < 32 || J > 4096) return fail(CUBE_E_ARG, "PP chunk J must be in 32..4096");
+  PPShape sh;
+  sh.T = T;
+  sh.B = B;
+  sh.J = J;
+  c->pp_best[cls] = sh;
+  c->pp_tuned[cls] = true;
+  c->pp_tune_ms[cls] = 0;
+  return 0;
+}
+
+int cube_gpu_pp_shape_get(cube_ctx* c, int cls, int* T, int* B, int* J, double* ms) {
+  if (!c || cls < 0 || cls > 3) return fail(CUBE_E_ARG, "bad PP class");
+  if (!c->pp_tuned[cls]) return 0;
+  if (T) *T = c->pp_best[cls].T;
+  if (B) *B = c->pp_best[cls].B;
+  if (J) *J = c->pp_best[cls].J;
+  if (ms) *ms = c->pp_tune_ms[cls];
+  return 1;
 }
 
 int cube_gpu_profile(cube_ctx* c, int enable) {
@@ -1709,6 +1909,7 @@ int cube_gpu_ic(cube_ctx* c, const cube_ic_in* in, cube_ic_out* out) {
   std::swap(c->cstart, c->cstart2);
   c->loaded = true;
   c->have_est = false;
+  c->maxcount_est = -1;
   prof_collect(c);
   if (out) {
     memset(out, 0, sizeof(*out));
@@ -2156,3 +2357,172 @@ extern "C" int cube_gpu_power(cube_ctx* c, const cube_power_in* in, float* xi, i
 #undef PK_CK
   return 0;
 }
+
+// =================================================================================
+// Differentiable PM step for the adjoint (dpm.cuh; cube_nu_b200/adjoint.py binds it).
+// =================================================================================
+struct cube_dpm {
+  cube_ctx* c = nullptr;  // stream, FFT tables and the Green table (green1)
+  int n = 0;
+  float mass = 0.f;
+  float* mesh = nullptr;  // in-place FFT mesh, layout pitch_of(c, n, false)
+  Pitch pt;
+  float4* fm = nullptr;   // force mesh, dense n^3
+  float4* lam = nullptr;  // adjoint force deposit, dense n^3
+};
+
+namespace {
+
+// Force mesh Fm = grad_h Gconv(rho) of the particles at x.
+int dpm_force_mesh(cube_dpm* d, const float* x, int64_t np) {
+  cube_ctx* c = d->c;
+  const int n = d->n;
+  CK(cudaMemsetAsync(d->mesh, 0, mesh_bytes(c, n, 1, false), c->s));
+  if (np > 0) k_dpm_deposit<<<nblk(np), 256, 0, c->s>>>(n, np, x, d->mass, d->mesh, d->pt.pr, d->pt.plr);
+  launch_fft(c, n, 1, d->mesh, false, 1.f, d->mesh, reinterpret_cast<float2*>(d->mesh), c->green1, (float)n, 3, 1);
+  const int64_t n3 = (int64_t)n * n * n;
+  k_force_pm1<<<nblk(n3), 256, 0, c->s>>>(n, d->mesh, d->pt.pf, d->pt.plf, d->fm);
+  c->launches += 7;
+  return 0;
+}
+
+int dpm_finish(cube_dpm* d) {
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(d->c->s));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cube_dpm_create(int n, float soft, float mass, int device, cube_dpm** out) {
+  if (!out) return fail(CUBE_E_ARG, "null argument");
+  *out = nullptr;
+  if (n < 16 || n % 2 || !smooth23(n)) return fail(CUBE_E_ARG, "dpm mesh side must be an even 2^a 3^b size >= 16");
+  if (!(soft >= 0.f) || !(mass > 0.f)) return fail(CUBE_E_ARG, "dpm needs soft >= 0 and mass > 0");
+  cube_dpm* d = new cube_dpm();
+  cube_ctx* c = new cube_ctx();
+  d->c = c;
+  d->n = n;
+  d->mass = mass;
+  c->device = device;
+  int rc = 0;
+  auto bail = [&](int code) {
+    cube_dpm_destroy(d);
+    return code;
+  };
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    return bail(fail(CUBE_E_CUDA, "dpm: device or stream setup failed"));
+  rc = add_fft(c, n);
+  if (!rc) rc = build_green(c, &c->green1, n, soft, 0.f, 1.f);  // Green.f90 without a range cut, gridsize 1
+  if (rc) return bail(rc);
+  const size_t big = 200 * 1024;
+  cudaFuncSetAttribute(k_fft_x_r2c<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(k_fft_y, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(k_fft_z_green, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  d->pt = pitch_of(c, n, false);
+  const int64_t n3 = (int64_t)n * n * n;
+  if (cudaMalloc(&d->mesh, mesh_bytes(c, n, 1, false)) != cudaSuccess || cudaMalloc(&d->fm, n3 * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(&d->lam, n3 * sizeof(float4)) != cudaSuccess)
+    return bail(fail(CUBE_E_CUDA, "dpm: out of device memory"));
+  if (cudaStreamSynchronize(c->s) != cudaSuccess) return bail(fail(CUBE_E_CUDA, "dpm: setup failed"));
+  *out = d;
+  return 0;
+}
+
+int cube_dpm_destroy(cube_dpm* d) {
+  if (!d) return 0;
+  if (d->c) {
+    cudaSetDevice(d->c->device);
+    if (d->c->s) cudaStreamSynchronize(d->c->s);
+  }
+  if (d->mesh) cudaFree(d->mesh);
+  if (d->fm) cudaFree(d->fm);
+  if (d->lam) cudaFree(d->lam);
+  if (d->c) cube_gpu_destroy(d->c);
+  delete d;
+  return 0;
+}
+
+int cube_dpm_density(cube_dpm* d, const float* x, int64_t np, float* rho) {
+  if (!d || !rho || np < 0 || (np > 0 && !x)) return fail(CUBE_E_ARG, "bad dpm density arguments");
+  CK(cudaSetDevice(d->c->device));
+  const int n = d->n;
+  CK(cudaMemsetAsync(rho, 0, (size_t)n * n * n * 4, d->c->s));
+  if (np > 0) k_dpm_deposit<<<nblk(np), 256, 0, d->c->s>>>(n, np, x, d->mass, rho, n, (int64_t)n * n);
+  ++d->c->launches;
+  return dpm_finish(d);
+}
+
+int cube_dpm_density_vjp(cube_dpm* d, const float* x, int64_t np, const float* lam, float* gx) {
+  if (!d || !lam || !gx || np < 0 || (np > 0 && !x)) return fail(CUBE_E_ARG, "bad dpm density_vjp arguments");
+  CK(cudaSetDevice(d->c->device));
+  const int n = d->n;
+  if (np > 0)
+    k_dpm_grad_gather<<<nblk(np), 256, 0, d->c->s>>>(n, np, x, nullptr, nullptr, lam, n, (int64_t)n * n, d->mass, gx);
+  ++d->c->launches;
+  return dpm_finish(d);
+}
+
+int cube_dpm_drift(cube_dpm* d, float* x, const float* v, int64_t np, float D) {
+  if (!d || np < 0 || (np > 0 && (!x || !v))) return fail(CUBE_E_ARG, "bad dpm drift arguments");
+  CK(cudaSetDevice(d->c->device));
+  if (np > 0) k_dpm_drift<<<nblk(3 * np), 256, 0, d->c->s>>>(d->n, 3 * np, x, v, D);
+  ++d->c->launches;
+  return dpm_finish(d);
+}
+
+int cube_dpm_kdk(cube_dpm* d, float* x, float* v, int64_t np, float D, float K) {
+  if (!d || np < 0 || (np > 0 && (!x || !v))) return fail(CUBE_E_ARG, "bad dpm kdk arguments");
+  CK(cudaSetDevice(d->c->device));
+  if (np > 0) k_dpm_drift<<<nblk(3 * np), 256, 0, d->c->s>>>(d->n, 3 * np, x, v, D);
+  int rc = dpm_force_mesh(d, x, np);
+  if (rc) return rc;
+  if (np > 0) k_dpm_kick<<<nblk(np), 256, 0, d->c->s>>>(d->n, np, x, d->fm, K, v);
+  d->c->launches += 2;
+  return dpm_finish(d);
+}
+
+int cube_dpm_force(cube_dpm* d, const float* x, int64_t np, float* f) {
+  if (!d || !f || np < 0 || (np > 0 && !x)) return fail(CUBE_E_ARG, "bad dpm force arguments");
+  CK(cudaSetDevice(d->c->device));
+  int rc = dpm_force_mesh(d, x, np);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(f, 0, (size_t)np * 12, d->c->s));
+  if (np > 0) k_dpm_kick<<<nblk(np), 256, 0, d->c->s>>>(d->n, np, x, d->fm, 1.f, f);
+  ++d->c->launches;
+  return dpm_finish(d);
+}
+
+int cube_dpm_force_vjp(cube_dpm* d, const float* x, int64_t np, const float* u, float* gx) {
+  if (!d || !u || !gx || np < 0 || (np > 0 && !x)) return fail(CUBE_E_ARG, "bad dpm force_vjp arguments");
+  CK(cudaSetDevice(d->c->device));
+  cube_ctx* c = d->c;
+  const int n = d->n;
+  const int64_t n3 = (int64_t)n * n * n;
+  int rc = dpm_force_mesh(d, x, np);  // Fm at these positions
+  if (rc) return rc;
+  CK(cudaMemsetAsync(d->lam, 0, n3 * sizeof(float4), c->s));
+  if (np > 0) k_dpm_deposit_vec<<<nblk(np), 256, 0, c->s>>>(n, np, x, u, d->lam);
+  k_dpm_grad_t<<<nblk(n3), 256, 0, c->s>>>(n, d->lam, d->mesh, d->pt.pr, d->pt.plr);
+  launch_fft(c, n, 1, d->mesh, false, 1.f, d->mesh, reinterpret_cast<float2*>(d->mesh), c->green1, (float)n, 3, 1);
+  if (np > 0)
+    k_dpm_grad_gather<<<nblk(np), 256, 0, c->s>>>(n, np, x, u, d->fm, d->mesh, d->pt.pf, d->pt.plf, d->mass, gx);
+  c->launches += 8;
+  return dpm_finish(d);
+}
+
+int cube_dpm_green(cube_dpm* d, float* out, int64_t nout) {
+  if (!d || !out) return fail(CUBE_E_ARG, "null argument");
+  const int n = d->n;
+  const int64_t cnt = (int64_t)n * n * (n / 2 + 1);
+  if (nout < cnt) return fail(CUBE_E_ARG, "buffer too small");
+  CK(cudaSetDevice(d->c->device));
+  CK(cudaMemcpy(out, d->c->green1, cnt * 4, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+}  // extern "C"

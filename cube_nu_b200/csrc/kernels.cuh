@@ -333,13 +333,11 @@ __global__ void k_permute_ids(int64_t np, const uint32_t* __restrict__ ssrc, con
 // =================================================================================
 // Deposit (particle_mesh.f90:20-109, kick.f90:611-691).
 // =================================================================================
-static constexpr float FIXED_SCALE = 1099511627776.f;  // 2^40
 
 template <bool FIXED>
 __device__ __forceinline__ void dep_add(void* rho, int64_t i, float w) {
   if (FIXED) {
-    const long long q = __float2ll_rn(__fmul_rn(w, FIXED_SCALE));
-    atomicAdd(reinterpret_cast<unsigned long long*>(rho) + i, (unsigned long long)q);
+    atomicAdd(reinterpret_cast<unsigned long long*>(rho) + i, fixed40(w));
   } else {
     atomicAdd(reinterpret_cast<float*>(rho) + i, w);
   }
@@ -375,7 +373,7 @@ struct MassAcc {
   using T = typename std::conditional<FIXED, unsigned long long, double>::type;
   T v = 0;
   __device__ __forceinline__ void add(float w) {
-    if constexpr (FIXED) v += (unsigned long long)__float2ll_rn(__fmul_rn(w, FIXED_SCALE));
+    if constexpr (FIXED) v += fixed40(w);
     else v += (double)w;
   }
   // out: MASS_SLOTS accumulators of type T (nullptr: no sum wanted)
@@ -467,7 +465,7 @@ __global__ void __launch_bounds__(256) k_deposit_pm1_runs(Geo G, int64_t np, con
 #pragma unroll
       for (int a1 = 0; a1 < 3; ++a1) {
         const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
-        unsigned long long q = live ? (unsigned long long)__float2ll_rn(__fmul_rn(ww, FIXED_SCALE)) : 0ull;
+        unsigned long long q = live ? fixed40(ww) : 0ull;
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
           if (k == 3 && !need8) continue;
@@ -677,6 +675,23 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
 // contributions that land in the box's physical cells.  The deposit adds exactly these
 // contributions to those cells, so with the fixed-point deposit this is the mesh sum
 // itself, exactly; the deposit kernels need no extra work for it.
+// A neighbour box of the same class has the own box's weights shifted by whole cells, so
+// its physical contributions are the own box's contributions that leave the own physical
+// region in its direction: the sum of all 27 own contributions covers both.  Only a
+// neighbour of another class (a class boundary, rare) needs its own weights: its share of
+// the 27 is replaced by its physical contributions at its class.
+template <bool FIXED>
+__device__ __forceinline__ void mass_box(const Geo& G, int iapm, const double lf[3], const int u[3], int i2[3],
+                                         float w[3][3]) {
+  const int rsf = rsf_of(iapm), nfp = G.nfp[iapm];
+  const double gs = (double)(1.f / (float)rsf);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) i2[d] = tsc_weights(pm3_xpos(lf[d], G, gs, rsf, u[d] * nfp), w[d]);
+}
+
+// direction (-1, 0, +1) of 0-based cell index i relative to the physical range 0..nfp-1
+__device__ __forceinline__ int mass_dir(int i, int nfp) { return i < 0 ? -1 : (i >= nfp ? 1 : 0); }
+
 template <bool FIXED>
 __global__ void __launch_bounds__(256) k_mass_pm3(Geo G, int64_t np, const void* __restrict__ xp,
                                                   const int32_t* __restrict__ pcell, const int32_t* __restrict__ ires,
@@ -693,38 +708,65 @@ __global__ void __launch_bounds__(256) k_mass_pm3(Geo G, int64_t np, const void*
       nca[d] = sub_cands(G, g[d], tc[d], uc[d], lc[d]);
       f[d] = zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
     }
+    // own box: all 27 contributions
+    const int t0[3] = {tc[0][0], tc[1][0], tc[2][0]}, u0[3] = {uc[0][0], uc[1][0], uc[2][0]};
+    const int own = ires[subtile_id(G, t0, u0)];
+    const double lf0[3] = {(double)lc[0][0] + f[0], (double)lc[1][0] + f[1], (double)lc[2][0] + f[2]};
+    int i2[3];
+    float w[3][3];
+    mass_box<FIXED>(G, own, lf0, u0, i2, w);
 #pragma unroll
-    for (int cz = 0; cz < 2; ++cz)
+    for (int a3 = 0; a3 < 3; ++a3)
 #pragma unroll
-      for (int cy = 0; cy < 2; ++cy)
+      for (int a2 = 0; a2 < 3; ++a2)
 #pragma unroll
-        for (int cx = 0; cx < 2; ++cx) {
-          if (cz >= nca[2] || cy >= nca[1] || cx >= nca[0]) continue;
-          const int t[3] = {tc[0][cx], tc[1][cy], tc[2][cz]};
-          const int u[3] = {uc[0][cx], uc[1][cy], uc[2][cz]};
-          const int iapm = ires[subtile_id(G, t, u)];
-          const int nfp = G.nfp[iapm], rsf = rsf_of(iapm);
-          const double gs = (double)(1.f / (float)rsf);
-          const int l[3] = {lc[0][cx], lc[1][cy], lc[2][cz]};
-          int i2[3];
-          float w[3][3];
+        for (int a1 = 0; a1 < 3; ++a1) mass.add(__fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]));
+    // neighbour boxes of another class (only particles in a face cell of their subtile)
+    if (nca[0] * nca[1] * nca[2] > 1) {
+      const int nfp0 = G.nfp[own];
+      for (int cz = 0; cz < nca[2]; ++cz)
+        for (int cy = 0; cy < nca[1]; ++cy)
+          for (int cx = 0; cx < nca[0]; ++cx) {
+            if (cx + cy + cz == 0) continue;
+            const int t[3] = {tc[0][cx], tc[1][cy], tc[2][cz]};
+            const int u[3] = {uc[0][cx], uc[1][cy], uc[2][cz]};
+            const int nb = ires[subtile_id(G, t, u)];
+            if (nb == own) continue;
+            // the box's direction from the own box, per dimension (0 where it is the own subtile)
+            int dir[3];
+            const int cc[3] = {cx, cy, cz};
 #pragma unroll
-          for (int d = 0; d < 3; ++d) i2[d] = tsc_weights(pm3_xpos((double)l[d] + f[d], G, gs, rsf, u[d] * nfp), w[d]);
-          // array index i2-1+a-(1-nfb) is physical when in nfb..nfb+nfp-1, i.e. i2-1+a in 1..nfp
+            for (int d = 0; d < 3; ++d)  // sub_cands: the first coarse cell of a subtile reaches down, the last up
+              dir[d] = cc[d] == 0 ? 0 : ((lc[d][0] % G.ntt) == 0 ? -1 : 1);
+            // the own contributions in that direction leave the sum ...
+            MassAcc<FIXED> sub;
 #pragma unroll
-          for (int a3 = 0; a3 < 3; ++a3) {
-            if ((unsigned)(i2[2] - 2 + a3) >= (unsigned)nfp) continue;
+            for (int a3 = 0; a3 < 3; ++a3)
 #pragma unroll
-            for (int a2 = 0; a2 < 3; ++a2) {
-              if ((unsigned)(i2[1] - 2 + a2) >= (unsigned)nfp) continue;
+              for (int a2 = 0; a2 < 3; ++a2)
 #pragma unroll
-              for (int a1 = 0; a1 < 3; ++a1) {
-                if ((unsigned)(i2[0] - 2 + a1) >= (unsigned)nfp) continue;
-                mass.add(__fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]));
-              }
-            }
+                for (int a1 = 0; a1 < 3; ++a1)
+                  if (mass_dir(i2[0] - 2 + a1, nfp0) == dir[0] && mass_dir(i2[1] - 2 + a2, nfp0) == dir[1] &&
+                      mass_dir(i2[2] - 2 + a3, nfp0) == dir[2])
+                    sub.add(__fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]));
+            mass.v -= sub.v;
+            // ... and the neighbour's own physical contributions at its class come in
+            const double lf[3] = {(double)lc[0][cx] + f[0], (double)lc[1][cy] + f[1], (double)lc[2][cz] + f[2]};
+            int j2[3];
+            float v[3][3];
+            mass_box<FIXED>(G, nb, lf, u, j2, v);
+            const int nfp = G.nfp[nb];
+#pragma unroll
+            for (int a3 = 0; a3 < 3; ++a3)
+#pragma unroll
+              for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+                for (int a1 = 0; a1 < 3; ++a1)
+                  if ((unsigned)(j2[0] - 2 + a1) < (unsigned)nfp && (unsigned)(j2[1] - 2 + a2) < (unsigned)nfp &&
+                      (unsigned)(j2[2] - 2 + a3) < (unsigned)nfp)
+                    mass.add(__fmul_rn(__fmul_rn(v[0][a1], v[1][a2]), v[2][a3]));
           }
-        }
+    }
   }
   mass.flush(msum);
 }
@@ -875,7 +917,7 @@ __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo
             const int x = c0[0] + a1;
             if (x < 0 || x >= e[0]) continue;
             const float ww = __fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]);
-            const unsigned long long q = (unsigned long long)__float2ll_rn(__fmul_rn(ww, FIXED_SCALE));
+            const unsigned long long q = fixed40(ww);
             unsigned long long* cell = &acc[(z * R + y) * R + x];
             if (SPLIT) {
               unsigned* h = reinterpret_cast<unsigned*>(cell);

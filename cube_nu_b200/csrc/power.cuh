@@ -52,7 +52,7 @@ __global__ void k_cic_deposit(Geo G, int64_t np, const void* __restrict__ xp, co
         const float w = __fmul_rn(__fmul_rn(a ? d2[0] : d1[0], b ? d2[1] : d1[1]), c ? d2[2] : d1[2]);
         const int64_t idx = (int64_t)zs[c] * pl + (int64_t)ys[b] * pr + xs[a];
         if (FIXED) {
-          const long long q = __float2ll_rn(__fmul_rn(w, 1099511627776.f));  // w * 2^40
+          const long long q = (long long)fixed40(w);  // round(w * 2^40)
           atomicAdd(reinterpret_cast<unsigned long long*>(rho) + idx, (unsigned long long)q);
         } else {
           atomicAdd(reinterpret_cast<float*>(rho) + idx, w);

@@ -41,6 +41,8 @@ class CParams(ctypes.Structure):
         ("np_capacity", ctypes.c_int64),
         ("max_segment", ctypes.c_int32),
         ("step_graph", ctypes.c_int32),
+        ("pp_queue", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -70,6 +72,7 @@ class Params:
     np_capacity: int = 0
     max_segment: int = 0
     step_graph: bool = False  # cube_gpu_step replays each step as one captured CUDA graph
+    pp_queue: bool = False    # PP as an autotuned work queue over cells (chosen form)
     # cosmology (parameters.f90:101-125; values of the benchmark configs)
     h0: float = 0.6817
     omega_c: float = 0.2532
@@ -159,7 +162,8 @@ class Params:
             pp_on=int(self.pp_on), deposit_mode=int(self.deposit_mode), box=self.box, app=self.app,
             apm1c=self.apm1c, apm2=self.apm2, apm3f=self.apm3f,
             mass_p_cdm=self.particle_mass(), f_nu=self.f_nu, np_capacity=self.np_capacity,
-            max_segment=self.max_segment, step_graph=int(self.step_graph),
+            max_segment=self.max_segment, step_graph=int(self.step_graph), pp_queue=int(self.pp_queue),
+            reserved=0,
         )
 
 

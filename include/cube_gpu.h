@@ -79,6 +79,9 @@ typedef struct cube_params {
   int64_t np_capacity; /* particle capacity on device (0: derive from ng, np_nc)        */
   int32_t max_segment; /* largest destination cell the drift sorts (0: default 16384)   */
   int32_t step_graph;  /* 1: cube_gpu_step replays each step as one captured CUDA graph   */
+  int32_t pp_queue;    /* 1: PP as an autotuned work queue over cells (needs int8 codes, or
+                          int16 with nt < 127); 0: one thread per particle                 */
+  int32_t reserved;
 } cube_params;
 
 /* Per-step scalars chosen by the host timestep (timestep.f90:4-110). */
@@ -225,6 +228,18 @@ int cube_gpu_captured(cube_ctx* ctx, float* out, int64_t n);
 int cube_gpu_profile(cube_ctx* ctx, int enable);
 int cube_gpu_profile_read(cube_ctx* ctx, double* ms, int64_t* count, int n);
 const char* cube_gpu_profile_name(int i);
+/* Queue PP shapes (cube_params.pp_queue).  The PP work is split by the occupancy of each
+ * particle's coarse cell: cells of at most T particles take one thread per particle, the
+ * others are cut into items of B particles that a persistent kernel pulls from a device
+ * queue (largest cells first), staging candidates in shared-memory chunks of J.  The
+ * library's autotuner times a sweep of shapes on the live state the first time a step
+ * falls in occupancy class cls (largest cell <= 64, <= 512, <= 4096, larger: 0..3; the
+ * reference's only tuning data is its PP timing, kick.f90:141-201) and keeps the fastest.
+ * Forces do not depend on the shape.  cube_gpu_pp_shape sets the shape of a class (T <= 0
+ * forgets it, so it is tuned again); cube_gpu_pp_shape_get returns 1 and the shape and
+ * its timed milliseconds when the class has one, else 0. */
+int cube_gpu_pp_shape(cube_ctx* ctx, int cls, int T, int B, int J);
+int cube_gpu_pp_shape_get(cube_ctx* ctx, int cls, int* T, int* B, int* J, double* ms);
 /* Number of kernels this context has launched since creation. */
 int64_t cube_gpu_kernel_launches(cube_ctx* ctx);
 
@@ -270,6 +285,34 @@ int cube_gpu_subtile_class(cube_ctx* ctx, int32_t* ires, int64_t n);
 #define CUBE_NOALLOC_MAX_PARTICLES 2097152  /* 2^21 particles    */
 int cube_gpu_pm1_density_noalloc(const cube_params* p, const void* xp, const int32_t* rhoc, int64_t np,
                                  float* rho, void* stream);
+
+/*
+ * Differentiable particle-mesh step, for the adjoint (the PyTorch binding
+ * cube_nu_b200/adjoint.py wraps it in torch.autograd.Function).  One periodic PM level on
+ * an n^3 mesh in fine-cell units with the reference's PM pieces: TSC mass assignment
+ * (particle_mesh.f90:56-62), the Green table of Green/Green.f90 with softening `soft` and
+ * no range cut, the 4-point gradient (particle_mesh.f90:224-247), TSC interpolation, and
+ * the KDK order of main.f90 (drift by D, then kick by K times the force).  Positions are
+ * real numbers (not ZIPX codes) so that the step is differentiable.  All arrays are device
+ * pointers on the context's device: x, v, u, gx are (np,3) floats, x in [0, n); rho and
+ * lam are n^3 floats, x fastest.  Each call returns when its work is done.
+ *   cube_dpm_kdk:         x += D v (wrapped), then v += K F(x)
+ *   cube_dpm_force:       f = F(x)
+ *   cube_dpm_force_vjp:   gx += d(sum_i u_i . F_i(x)) / dx   (the hand-written adjoint)
+ *   cube_dpm_density:     rho = mass * sum_i W(x_i - c)
+ *   cube_dpm_density_vjp: gx += d(sum_c lam(c) rho(c)) / dx
+ *   cube_dpm_green:       the Green table, n*n*(n/2+1) floats [kz][ky][kx]
+ */
+typedef struct cube_dpm cube_dpm;
+int cube_dpm_create(int n, float soft, float mass, int device, cube_dpm** out);
+int cube_dpm_destroy(cube_dpm* d);
+int cube_dpm_drift(cube_dpm* d, float* x, const float* v, int64_t np, float D);
+int cube_dpm_kdk(cube_dpm* d, float* x, float* v, int64_t np, float D, float K);
+int cube_dpm_force(cube_dpm* d, const float* x, int64_t np, float* f);
+int cube_dpm_force_vjp(cube_dpm* d, const float* x, int64_t np, const float* u, float* gx);
+int cube_dpm_density(cube_dpm* d, const float* x, int64_t np, float* rho);
+int cube_dpm_density_vjp(cube_dpm* d, const float* x, int64_t np, const float* lam, float* gx);
+int cube_dpm_green(cube_dpm* d, float* out, int64_t nout);
 
 /* Text of the last error on this thread. */
 int cube_gpu_last_error(char* buf, size_t n);
