@@ -35,7 +35,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from cube_nu_b200 import cosmology  # noqa: E402
-from cube_nu_b200.params import DEPOSIT_FIXED, DEPOSIT_FP32, config_512, config_plain_128  # noqa: E402
+from cube_nu_b200.params import DEPOSIT_FIXED, DEPOSIT_FP32, config_512, config_late_256, config_plain_128  # noqa: E402
 
 METRIC = "particle-steps/s P3M KDK @512^3"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
@@ -323,6 +323,86 @@ def run_form(p, args, local, dist, rank, replay=None, timed=True, want_base=Fals
             "base": base, "base_args": base_args}
 
 
+def late_leg(args, local, rank, a_stop=0.99, max_evolve=2000, steps=5):
+    """The clustered-PP configuration: 256^3 CDM in 100 Mpc/h (ng 256, 64 particles per
+    coarse cell), evolved from z=49 in the chosen form until a >= a_stop (outside any timed
+    region), then `steps` steps timed in the chosen form and the same steps replayed by
+    the plain form from the same state.  The evolution takes the reference's timestep with
+    only its expansion and velocity limits (timestep.f90:20-34 with the force criteria
+    left out): a few hundred steps instead of ~2000, which still collapses the haloes
+    (cells of ~10^4 particles); the timed steps use every criterion."""
+    import torch
+
+    from cube_nu_b200._lib import Context
+
+    p = config_late_256()
+    p.deposit_mode = DEPOSIT_FIXED
+    p.step_graph = True
+    p.pp_queue = True
+    ctx, d = device_ic(p, seed=3 + rank, device=local)
+    tab = cosmology.expansion_table(p.h0, p.omega_m, p.omega_r)
+    bg = cosmology.Background.from_table(tab)
+    S = cosmology.StepState(a=d["a"], dt_vmax=d["dt_vmax"], vz_max=d["vz_max"])
+    bg.init_cursor(S.a)
+    zck = [49.0, 0.0]
+    t0 = time.perf_counter()
+    nev = 0
+
+    def advance(evolve=False):
+        if evolve:  # expansion and velocity limits only
+            S.dt_pm1 = S.dt_pm2 = S.dt_pm3 = S.dt_pp = 1e3
+        cosmology.timestep(bg, S, zck)
+        si = (S.dt, S.dt_old, S.a_mid, S.vz_max)
+        so = ctx.step(*si)
+        S.dt_pm1, S.dt_pm2, S.dt_pm3, S.dt_pp, S.dt_vmax = so.dt_pm1, so.dt_pm2, so.dt_pm3, so.dt_pp, so.dt_vmax
+        S.vz_max = so.vz_max
+        return si, so
+
+    while S.a < a_stop and nev < max_evolve and not S.final_step:
+        advance(evolve=True)
+        nev += 1
+    t_evolve = time.perf_counter() - t0
+    state = ctx.download()
+    res = {"workload": "256^3 CDM, 100 Mpc/h, ng 256 (64 particles per coarse cell), int16 ZIPX",
+           "evolve_steps": nev, "evolve_s": round(t_evolve, 1), "a_start": S.a, "z_start": round(1 / S.a - 1, 4),
+           "max_cell": int(state[3].max())}
+    forms = {}
+    replay = []
+    ctx.profile(True)
+    torch.cuda.synchronize()
+    ms = 0.0
+    pairs = cand = 0
+    for _ in range(steps):
+        si, so = advance()
+        replay.append(si)
+        ms += so.tcat[6]
+        pairs += so.pp_pairs
+        cand += so.pp_candidates
+    prof = ctx.profile_read()
+    forms["chosen"] = {"ms_per_step": round(ms / steps, 3), "value": round(state[0].shape[0] * steps / (ms / 1e3), 1),
+                       "pp_ms_per_step": round(prof.get("pp", (0, 0))[0] / steps, 3),
+                       "pm3_classes": list(so.napm)[2:6], "pp_pairs_per_step": pairs // steps,
+                       "pp_candidates_per_step": cand // steps}
+    ctx.close()
+    q = config_late_256()
+    q.deposit_mode = DEPOSIT_FP32
+    q.mass_p_cdm = p.mass_p_cdm
+    with Context(q, device=local) as c2:
+        c2.upload(*state)
+        c2.profile(True)
+        ms = 0.0
+        for si in replay:
+            so = c2.step(*si)
+            ms += so.tcat[6]
+        prof = c2.profile_read()
+    forms["plain"] = {"ms_per_step": round(ms / steps, 3), "value": round(state[0].shape[0] * steps / (ms / 1e3), 1),
+                      "pp_ms_per_step": round(prof.get("pp", (0, 0))[0] / steps, 3)}
+    forms["chosen_over_plain"] = round(forms["plain"]["ms_per_step"] / forms["chosen"]["ms_per_step"], 4)
+    res["forms"] = forms
+    res["steps"] = steps
+    return res
+
+
 def pk_grid(p):
     """cicpower grid of the precision check: 2*ng as utilities/Makefile's FFTFINE builds it,
     capped at 1024^3 (the 512^3 workload's 2048^3 grid would hold ~100 GB beside the step)."""
@@ -343,6 +423,8 @@ def main():
                     help="PP as the autotuned cell work queue (cube_params.pp_queue) or a thread per particle")
     ap.add_argument("--compare", default="on", choices=["on", "off"],
                     help="also time the plain form (FP32 atomics, eager) over the same steps")
+    ap.add_argument("--late", default="on", choices=["on", "off"],
+                    help="also time the clustered-PP configuration (256^3, 100 Mpc/h) evolved to z~0, both forms")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-json", default="")
     ap.add_argument("--pk", type=int, default=0,
@@ -426,6 +508,10 @@ def main():
         plain = {"value": job_rate(total_particles, args.steps, P["dev_s"]),
                  "ms_per_step": P["dev_s"] * 1e3 / args.steps, "xi": xi_plain,
                  "stage": P["stage"] / args.steps}
+
+    late = None
+    if args.late == "on" and args.workload == "512" and world == 1:
+        late = late_leg(args, local, rank)
 
     if rank == 0:
         peaks, peak_kind = load_peaks()
@@ -520,6 +606,8 @@ def main():
             "mass_check": {"pm1": sos[-1].mass_pm1, "pm2": sos[-1].mass_pm2, "pm3": sos[-1].mass_pm3,
                            "particles": n},
         }
+        if late:
+            line["late_time"] = late
         if analysis:
             line["analysis"] = analysis
         if args.profile_json:

@@ -139,6 +139,7 @@ struct cube_ctx {
   int32_t *pcell = nullptr, *pcell2 = nullptr;
   // cells
   int32_t *rhoc = nullptr, *rhoc2 = nullptr, *fill = nullptr, *biglist = nullptr, *nbig = nullptr;
+  int32_t* hugelist = nullptr;  // segments beyond the shared-memory sorter; nbig[1] counts them
   int64_t *cstart = nullptr, *cstart2 = nullptr, *scan_tmp = nullptr;
   // drift scratch
   int32_t* dest = nullptr;
@@ -775,7 +776,8 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
   CK(cudaMalloc(&c->rhoc2, nc3 * 4));
   CK(cudaMalloc(&c->fill, nc3 * 4));
   CK(cudaMalloc(&c->biglist, nc3 * 4));
-  CK(cudaMalloc(&c->nbig, 4));
+  CK(cudaMalloc(&c->hugelist, nc3 * 4));
+  CK(cudaMalloc(&c->nbig, 8));
   CK(cudaMalloc(&c->cstart, (nc3 + 1) * 8));
   CK(cudaMalloc(&c->cstart2, (nc3 + 1) * 8));
   CK(cudaMalloc(&c->scan_tmp, ((nc3 + 2047) / 2048 + 2) * 8));
@@ -823,7 +825,7 @@ int cube_gpu_destroy(cube_ctx* c) {
   if (c->s) cudaStreamSynchronize(c->s);
   drop_graphs(c);
   void* bufs[] = {c->xp, c->xp2, c->vp, c->vp2, c->pid, c->pid2, c->pcell, c->pcell2, c->rhoc, c->rhoc2,
-                  c->fill, c->biglist, c->nbig, c->cstart, c->cstart2, c->scan_tmp, c->dest, c->key, c->skey,
+                  c->fill, c->biglist, c->hugelist, c->nbig, c->cstart, c->cstart2, c->scan_tmp, c->dest, c->key, c->skey,
                   c->ssrc, c->rdev, c->sd, c->ires, c->box_slot, c->box_sub, c->arena, c->green1, c->green2,
                   c->cap_buf, c->pfin, c->hlist, c->hpre, c->ppq, c->vtune, c->tune_red};
   for (void* b : bufs)
@@ -979,6 +981,17 @@ static int upload_scalars(cube_ctx* c, const StepDev& d) {
   return 0;
 }
 
+// Segments beyond the shared-memory sorter: ranked into the scratch arrays c->key (free
+// after the scatter) and c->pcell2 (written only by the gather that follows), then copied
+// back.  Both kernels exit at once when no segment is listed.
+static void enqueue_huge_sort(cube_ctx* c) {
+  uint32_t* tsrc = reinterpret_cast<uint32_t*>(c->pcell2);
+  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_rank_huge<<<(unsigned)c->nsm, HUGE_T, 0, c->s>>>(
+                                 c->hugelist, c->nbig + 1, c->rhoc2, c->cstart2, c->skey, c->ssrc, c->key, tsrc));
+  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_copy_huge<<<(unsigned)c->nsm, 256, 0, c->s>>>(
+                                 c->hugelist, c->nbig + 1, c->rhoc2, c->cstart2, c->key, tsrc, c->skey, c->ssrc));
+}
+
 // drift.f90, enqueued without any host synchronisation; the drifted arrays land in the
 // second buffers and the particle total in StepRes.total.  With `defer_ids` the gather
 // leaves the particle ids alone (the new id array is not written): the caller applies the
@@ -989,7 +1002,7 @@ static void enqueue_drift(cube_ctx* c, bool defer_ids) {
   const int64_t np = c->np;
   cudaMemsetAsync(c->rhoc2, 0, G.ncells * 4, c->s);
   cudaMemsetAsync(c->fill, 0, G.ncells * 4, c->s);
-  cudaMemsetAsync(c->nbig, 0, 4, c->s);
+  cudaMemsetAsync(c->nbig, 0, 8, c->s);
   LAUNCH(c, K_DRIFT_DEST, 1, k_drift_dest<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->vp, c->pcell, c->cstart, c->sd,
                                                                      c->dest, c->key, c->rhoc2, c->err));
   LAUNCH(c, K_SCAN, 3, exclusive_scan(c->rhoc2, c->cstart2, G.ncells, c->scan_tmp, c->s));
@@ -999,8 +1012,9 @@ static void enqueue_drift(cube_ctx* c, bool defer_ids) {
   // long segments: one block per SM, each looping over the listed cells
   const int max_seg = c->P.max_segment > 0 ? std::min(c->P.max_segment, 16384) : 16384;
   const unsigned nbb = (unsigned)std::min<int64_t>(G.ncells, c->nsm);
-  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nbb, 512, (size_t)max_seg * 12, c->s>>>(c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey,
-                                                                   c->ssrc, max_seg, c->err));
+  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nbb, 512, drift_sort_smem(max_seg), c->s>>>(c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey,
+                                                                   c->ssrc, max_seg, c->hugelist, c->nbig + 1));
+  enqueue_huge_sort(c);
   LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp,
                                                                         defer_ids ? nullptr : c->pid, c->sd, c->xp2, c->vp2,
                                                                         c->pid2, c->pcell2));
@@ -1879,7 +1893,7 @@ int cube_gpu_ic(cube_ctx* c, const cube_ic_in* in, cube_ic_out* out) {
   A.nlayer = 2 * (int)std::ceil(gm[2] * A.np_nc / (8.0 * A.nic * PI * G.rcs)) + 3;  // ic.f90:587
   CK(cudaMemsetAsync(c->rhoc2, 0, G.ncells * 4, c->s));
   CK(cudaMemsetAsync(c->fill, 0, G.ncells * 4, c->s));
-  CK(cudaMemsetAsync(c->nbig, 0, 4, c->s));
+  CK(cudaMemsetAsync(c->nbig, 0, 8, c->s));
   LAUNCH(c, K_FILL, 1, k_ic_particles<<<nblk(np), 256, 0, c->s>>>(G, phi, pt.pf, pt.plf, A, c->xp, c->vp, c->pid, c->dest,
                                                                   c->key, c->rhoc2, c->err));
   LAUNCH(c, K_SCAN, 3, exclusive_scan(c->rhoc2, c->cstart2, G.ncells, c->scan_tmp, c->s));
@@ -1888,8 +1902,10 @@ int cube_gpu_ic(cube_ctx* c, const cube_ic_in* in, cube_ic_out* out) {
                                                                                      c->ssrc, c->biglist, c->nbig));
   const int max_seg = c->P.max_segment > 0 ? std::min(c->P.max_segment, 16384) : 16384;
   const unsigned nbb = (unsigned)std::min<int64_t>(G.ncells, c->nsm);
-  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nbb, 512, (size_t)max_seg * 12, c->s>>>(
-                                 c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey, c->ssrc, max_seg, c->err));
+  LAUNCH(c, K_DRIFT_SORT, 1, k_drift_sort_big<<<nbb, 512, drift_sort_smem(max_seg), c->s>>>(
+                                 c->biglist, c->nbig, c->rhoc2, c->cstart2, c->skey, c->ssrc, max_seg, c->hugelist,
+                                 c->nbig + 1));
+  enqueue_huge_sort(c);
   c->np = np;
   CK(cudaMemsetAsync(c->sd, 0, sizeof(StepDev), c->s));  // dt_mid = 0: the gather only sorts
   LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp, c->pid, c->sd,

@@ -251,11 +251,13 @@ __global__ void k_drift_sort_small(int64_t ncells, const int32_t* __restrict__ c
   }
 }
 
-// Block per long segment: bitonic sort in shared memory (keys are unique).
+// Block per long segment: bitonic sort in shared memory (keys are unique), which holds
+// max_seg rounded up to a power of two keys and values (drift_sort_smem).  Segments
+// longer than max_seg are listed in hugelist for k_drift_rank_huge.
 __global__ void k_drift_sort_big(const int32_t* __restrict__ biglist, const int32_t* __restrict__ nbig,
                                  const int32_t* __restrict__ count_new, const int64_t* __restrict__ cstart_new,
                                  uint64_t* __restrict__ skey, uint32_t* __restrict__ ssrc, int max_seg,
-                                 unsigned* err) {
+                                 int32_t* __restrict__ hugelist, int32_t* __restrict__ nhuge) {
   extern __shared__ uint64_t smk[];
   const int nb = *nbig;
   for (int b = blockIdx.x; b < nb; b += gridDim.x) {  // block-uniform loop over the listed cells
@@ -263,12 +265,14 @@ __global__ void k_drift_sort_big(const int32_t* __restrict__ biglist, const int3
   const int c = biglist[b];
   const int n = count_new[c];
   if (n > max_seg) {
-    if (threadIdx.x == 0) set_err(err, CUBE_DEVERR_SEGMENT);
+    if (threadIdx.x == 0) hugelist[atomicAdd(nhuge, 1)] = c;
     continue;
   }
   int m = 1;
-  while (m < n) m <<= 1;
-  uint32_t* smv = reinterpret_cast<uint32_t*>(smk + max_seg);
+  while (m < n) m <<= 1;  // m <= max_seg rounded up to a power of two: the keys' capacity
+  int cap = 1;
+  while (cap < max_seg) cap <<= 1;
+  uint32_t* smv = reinterpret_cast<uint32_t*>(smk + cap);
   const int64_t base = cstart_new[c];
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
     smk[i] = (i < n) ? skey[base + i] : ~0ull;
@@ -297,6 +301,73 @@ __global__ void k_drift_sort_big(const int32_t* __restrict__ biglist, const int3
     skey[base + i] = smk[i];
     ssrc[base + i] = smv[i];
   }
+  }
+}
+
+// Dynamic shared memory of k_drift_sort_big for a given max_seg.
+inline size_t drift_sort_smem(int max_seg) {
+  size_t cap = 1;
+  while (cap < (size_t)max_seg) cap <<= 1;
+  return cap * 12;
+}
+
+// Segments longer than the shared-memory sorter holds (dense halo cores at late times):
+// the rank of each key is the number of smaller keys in its segment (keys are unique), so
+// it is written straight to its sorted place in (tkey, tsrc); k_drift_copy_huge copies the
+// segment back.  Every block walks the listed cells and takes the tiles of 512 elements
+// with index = blockIdx.x mod gridDim.x; the segment's keys stream through shared memory in
+// chunks.  Quadratic in the segment length (0.3 ms for 5e4 keys), and only such cells run.
+constexpr int HUGE_T = 512, HUGE_CHUNK = 4096;
+__global__ void __launch_bounds__(HUGE_T) k_drift_rank_huge(const int32_t* __restrict__ hugelist,
+                                                            const int32_t* __restrict__ nhuge,
+                                                            const int32_t* __restrict__ count_new,
+                                                            const int64_t* __restrict__ cstart_new,
+                                                            const uint64_t* __restrict__ skey,
+                                                            const uint32_t* __restrict__ ssrc,
+                                                            uint64_t* __restrict__ tkey, uint32_t* __restrict__ tsrc) {
+  __shared__ uint64_t chunk[HUGE_CHUNK];
+  const int nh = *nhuge;
+  int item = 0;  // running tile index over all listed cells
+  for (int h = 0; h < nh; ++h) {
+    const int c = hugelist[h];
+    const int n = count_new[c];
+    const int64_t base = cstart_new[c];
+    const int ntile = (n + HUGE_T - 1) / HUGE_T;
+    for (int t = 0; t < ntile; ++t, ++item) {
+      if (item % gridDim.x != blockIdx.x) continue;  // block-uniform
+      const int i = t * HUGE_T + threadIdx.x;
+      const bool live = i < n;
+      const uint64_t k = live ? skey[base + i] : 0ull;
+      int rank = 0;
+      for (int j0 = 0; j0 < n; j0 += HUGE_CHUNK) {
+        const int cnt = min(HUGE_CHUNK, n - j0);
+        __syncthreads();
+        for (int j = threadIdx.x; j < cnt; j += HUGE_T) chunk[j] = skey[base + j0 + j];
+        __syncthreads();
+        if (live)
+          for (int j = 0; j < cnt; ++j) rank += chunk[j] < k;
+      }
+      if (live) {
+        tkey[base + rank] = k;
+        tsrc[base + rank] = ssrc[base + i];
+      }
+    }
+  }
+}
+
+__global__ void k_drift_copy_huge(const int32_t* __restrict__ hugelist, const int32_t* __restrict__ nhuge,
+                                  const int32_t* __restrict__ count_new, const int64_t* __restrict__ cstart_new,
+                                  const uint64_t* __restrict__ tkey, const uint32_t* __restrict__ tsrc,
+                                  uint64_t* __restrict__ skey, uint32_t* __restrict__ ssrc) {
+  const int nh = *nhuge;
+  for (int h = 0; h < nh; ++h) {
+    const int c = hugelist[h];
+    const int64_t base = cstart_new[c];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count_new[c];
+         i += (int64_t)gridDim.x * blockDim.x) {
+      skey[base + i] = tkey[base + i];
+      ssrc[base + i] = tsrc[base + i];
+    }
   }
 }
 

@@ -177,6 +177,12 @@ def config_512() -> Params:
     return Params(ng=1024, nnt=4, nns=4, np_nc=2, izipx=2, box=1000.0, nic=1)
 
 
+def config_late_256() -> Params:
+    """256^3 particles, 100 Mpc/h, fine mesh 256^3 (np_nc = 4, the reference default),
+    int16 coordinates: the clustered-PP configuration, evolved to z ~ 0."""
+    return Params(ng=256, nnt=4, nns=4, np_nc=4, izipx=2, box=100.0, nic=1)
+
+
 def config_small(ng: int = 64, nnt: int = 2, nns: int = 2, np_nc: int = 2, izipx: int = 1,
                  box: float = 100.0) -> Params:
     """Small geometry the oracle finishes in seconds (parity tests)."""

@@ -77,7 +77,8 @@ typedef struct cube_params {
   float mass_p_cdm;  /* particle mass in fine-cell units (ic.f90:839)                   */
   float f_nu;        /* neutrino mass fraction for the linear-response rescale (0: CDM) */
   int64_t np_capacity; /* particle capacity on device (0: derive from ng, np_nc)        */
-  int32_t max_segment; /* largest destination cell the drift sorts (0: default 16384)   */
+  int32_t max_segment; /* largest destination cell the drift sorts in shared memory (0 or
+                          above 16384: 16384); longer cells take a rank sort in HBM       */
   int32_t step_graph;  /* 1: cube_gpu_step replays each step as one captured CUDA graph   */
   int32_t pp_queue;    /* 1: PP as an autotuned work queue over cells (needs int8 codes, or
                           int16 with nt < 127); 0: one thread per particle                 */

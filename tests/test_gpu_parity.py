@@ -65,10 +65,12 @@ def test_drift_bitexact(oracle_lib, izipx, kind):
             cur = ref
 
 
-def test_drift_long_segments(oracle_lib):
+@pytest.mark.parametrize("max_segment", [0, 40])
+def test_drift_long_segments(oracle_lib, max_segment):
     """Destination cells of every sorter class: 2..16 arrivals (half-warp sort), 17..32
-    (whole-warp sort) and more than 32 (block sorter)."""
-    p = _params()
+    (whole-warp sort), more than 32 (block sorter) and, with max_segment = 40, more than
+    max_segment (the rank sort that dense halo cores take beyond 16384)."""
+    p = _params(max_segment=max_segment)
     n = 30000
     st = clustered_state(p, n, seed=5, nblob=2, sigma=0.3, frac=0.8, vscale=1.0)
     assert st[3].max() > 32
