@@ -22,7 +22,13 @@ EXPORTS = (
     "cube_gpu_profile", "cube_gpu_profile_read", "cube_gpu_profile_name", "cube_gpu_kernel_launches",
     "cube_gpu_zipv_encode", "cube_gpu_zipv_decode", "cube_gpu_download_zipv", "cube_gpu_ic", "cube_gpu_power",
     "cube_gpu_int2real", "cube_gpu_step_host", "cube_gpu_pp_shape", "cube_gpu_pp_shape_get",
+    "cube_gpu_nu_transfer", "cube_gpu_kernel_table", "cube_gpu_checkpoint_async", "cube_gpu_checkpoint_wait",
 )
+
+
+class CkptFiles(ctypes.Structure):
+    _fields_ = [("info", ctypes.c_char_p), ("xp", ctypes.c_char_p), ("vp", ctypes.c_char_p), ("np", ctypes.c_char_p),
+                ("id", ctypes.c_char_p)]
 
 
 class StepIn(ctypes.Structure):
@@ -108,6 +114,10 @@ def load():
     L.cube_gpu_step_host.argtypes = [vp, ctypes.POINTER(StepIn), ctypes.POINTER(StepOut), vp, vp, vp, vp,
                                      ctypes.c_int64]
     L.cube_gpu_pp_shape.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.cube_gpu_nu_transfer.argtypes = [vp, vp, vp, ctypes.c_int]
+    L.cube_gpu_checkpoint_async.argtypes = [vp, ctypes.POINTER(CkptFiles), vp, ctypes.c_int64]
+    L.cube_gpu_checkpoint_wait.argtypes = [vp]
+    L.cube_gpu_kernel_table.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int64]
     ip = ctypes.POINTER(ctypes.c_int)
     L.cube_gpu_pp_shape_get.argtypes = [vp, ctypes.c_int, ip, ip, ip, ctypes.POINTER(ctypes.c_double)]
     _LIB = L
@@ -292,6 +302,38 @@ class Context:
         rc = _check(self._lib.cube_gpu_pp_shape_get(self._h, cls, ctypes.byref(T), ctypes.byref(B), ctypes.byref(J),
                                                     ctypes.byref(ms)), "cube_gpu_pp_shape_get")
         return (T.value, B.value, J.value, ms.value) if rc == 1 else None
+
+    def checkpoint_async(self, opath: str, image: int, z: float, header) -> None:
+        """Write the resident state as the checkpoint files of one image in the background
+        (cube_gpu_checkpoint_async); names as checkpoint.output_name, header a sim_header."""
+        import os
+
+        from . import checkpoint
+
+        os.makedirs(os.path.join(opath, "image%d" % image), exist_ok=True)
+        names = {k: checkpoint.output_name(opath, image, z, k).encode() for k in ("info", "xp", "vp", "np", "id")}
+        files = CkptFiles(names["info"], names["xp"], names["vp"], names["np"], names["id"])
+        hb = np.ascontiguousarray(np.asarray(header)).tobytes()
+        buf = ctypes.create_string_buffer(hb, len(hb))
+        _check(self._lib.cube_gpu_checkpoint_async(self._h, ctypes.byref(files), ctypes.cast(buf, ctypes.c_void_p),
+                                                   len(hb)), "cube_gpu_checkpoint_async")
+
+    def checkpoint_wait(self) -> None:
+        _check(self._lib.cube_gpu_checkpoint_wait(self._h), "cube_gpu_checkpoint_wait")
+
+    def nu_transfer(self, kh, tf) -> None:
+        """Neutrino transfer ratio tf_F(k) at kh (h/Mpc, increasing) for the next kicks
+        (cube_gpu_nu_transfer); an empty table drops it."""
+        kl = np.ascontiguousarray(np.log(np.asarray(kh, dtype=np.float64)), dtype=np.float32)
+        tl = np.ascontiguousarray(np.log(np.asarray(tf, dtype=np.float64)), dtype=np.float32)
+        _check(self._lib.cube_gpu_nu_transfer(self._h, _ptr(kl), _ptr(tl), kl.size), "cube_gpu_nu_transfer")
+
+    def kernel_table(self, level: int, iapm: int = 2) -> np.ndarray:
+        p = self.params
+        n = {1: p.nc, 2: p.ngt}.get(level) or p.nft(iapm)
+        out = np.empty((n, n, n // 2 + 1), dtype=np.float32)
+        _check(self._lib.cube_gpu_kernel_table(self._h, level, iapm, _ptr(out), out.size), "cube_gpu_kernel_table")
+        return out
 
     def subtile_class(self) -> np.ndarray:
         out = np.empty(self.params.ns3, dtype=np.int32)

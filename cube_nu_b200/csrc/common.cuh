@@ -99,22 +99,10 @@ __device__ __forceinline__ float kick_add(float v, float dv, float a_mid, float 
   return (float)__dadd_rn((double)v, __ddiv_rn((double)t, 3.141592653589793));
 }
 
-// Fixed-point weight round(w * 2^40), rounded half to even as a float -> int64
-// conversion of w * 2^40 would be, for 0 <= w <= 2^23, with 32-bit integer operations only
-// (the 64-bit conversion instruction has a low issue rate; weights of 2^-17 and more,
-// nearly all of them, take the exact shift): w * 2^40 = m * 2^(e - 110) for the biased
-// exponent e and the 24-bit significand m.
+// Fixed-point weight round(w * 2^40) (round half to even, as the oracle's llrint), for
+// 0 <= w <= 2^23: the scaling by 2^40 is exact in FP32 and one conversion rounds.
 __device__ __forceinline__ unsigned long long fixed40(float w) {
-  const unsigned b = __float_as_uint(w);
-  const int e = (int)(b >> 23);
-  if (e == 0) return 0ull;  // zero (or subnormal, below 2^-126)
-  const unsigned m = (b & 0x7fffffu) | 0x800000u;
-  const int s = e - 110;
-  if (s >= 0) return (unsigned long long)m << s;
-  const int r = -s;
-  if (r > 24) return 0ull;  // m * 2^-r < 1/2
-  const unsigned q = m >> r, rem = m & ((1u << r) - 1u), half = 1u << (r - 1);
-  return (unsigned long long)(q + (rem > half || (rem == half && (q & 1u))));
+  return (unsigned long long)__float2ll_rn(__fmul_rn(w, 1099511627776.f));
 }
 
 // Non-negative float max through integer atomics.

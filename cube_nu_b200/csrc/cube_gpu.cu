@@ -11,7 +11,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -191,6 +193,14 @@ struct cube_ctx {
   size_t arena_bytes = 0;
   float* green1 = nullptr;
   float* green2 = nullptr;
+  // neutrino linear response: force kernels tf = interp_tf_F(|k|) * Gk per level (or
+  // (1 - f_nu) * Gk without a table), rebuilt in place when the table changes
+  float* tf1 = nullptr;
+  float* tf2 = nullptr;
+  float* tf3[8] = {nullptr};
+  int tf_ver[10] = {0};       // table version each kernel was built from (1, 2, 3 + class)
+  float* nu_tab = nullptr;    // log k [nb] then log tf_F [nb]
+  int nu_nb = 0, nu_ver = 1;
   float* green3[8] = {nullptr};
   std::vector<FFTTable> ffts;
   // capture for tests
@@ -199,6 +209,16 @@ struct cube_ctx {
   int64_t cap_n = 0;
   // timing
   cudaEvent_t ev[8];
+  // asynchronous checkpoint: side stream, staging copies in pinned memory, the event that
+  // marks the copies done, and the writer thread with its status
+  cudaStream_t s3 = nullptr;
+  cudaEvent_t ev_ckpt = nullptr;
+  bool ckpt_pending = false;
+  void* ck_host = nullptr;
+  size_t ck_bytes = 0;
+  std::thread ck_thread;
+  int ck_status = 0;
+  std::string ck_error;
   // side stream of cube_gpu_step_host (copies that overlap the step), created at first use
   cudaStream_t s2 = nullptr;
   cudaEvent_t ev_up = nullptr, ev_drift = nullptr;
@@ -672,6 +692,39 @@ void drop_graphs(cube_ctx* c) {
   c->graphs.clear();
 }
 
+// The force kernel of a level: the Green table, or with neutrinos (f_nu > 0 or a
+// transfer table from cube_gpu_nu_transfer) the rescaled table of kick.f90:23-29,
+// rebuilt in place when the transfer table is newer than it (outside any capture: the
+// step graph calls this for every level it uses before capturing).
+const float* kernel_table(cube_ctx* c, int level, int iapm) {
+  const Geo& G = c->G;
+  const float* gk = level == 1 ? c->green1 : level == 2 ? c->green2 : green3(c, iapm);
+  if (!gk) return nullptr;
+  if (!(c->P.f_nu > 0.f) && c->nu_nb < 3) return gk;
+  float** tf = level == 1 ? &c->tf1 : level == 2 ? &c->tf2 : &c->tf3[iapm];
+  const int n = level == 1 ? G.nc : level == 2 ? G.ngt : G.nft[iapm];
+  const int slot = level == 3 ? 3 + iapm : level;
+  const int64_t cnt = (int64_t)n * n * (n / 2 + 1);
+  if (!*tf) {
+    if (cudaMalloc(tf, cnt * sizeof(float)) != cudaSuccess) {
+      fail(CUBE_E_CUDA, "out of device memory for a neutrino force kernel");
+      return nullptr;
+    }
+    c->tf_ver[slot] = 0;
+  }
+  if (c->tf_ver[slot] != c->nu_ver) {
+    // box sides of the levels (nu_correction_coarse and nu_correction, power_nu.f90)
+    const double size = level == 1 ? (double)c->P.box : level == 2 ? (double)c->P.box / G.nnt
+                                                                    : (double)c->P.box / G.nnt / G.nns;
+    const int nb = c->nu_nb >= 3 ? c->nu_nb : 0;
+    const float scale = (float)(1.0 - (double)c->P.f_nu);
+    LAUNCH(c, K_GREEN, 1, k_nu_rescale<<<nblk(cnt), 256, 0, c->s>>>(n, size, gk, *tf, c->nu_tab,
+                                                                   c->nu_tab ? c->nu_tab + c->nu_nb : nullptr, nb, scale));
+    c->tf_ver[slot] = c->nu_ver;
+  }
+  return *tf;
+}
+
 // Copy a box field (n planes of n rows of n values, row pitch `rp` and plane pitch `psb`
 // bytes) into a dense capture buffer when it is the one requested.
 void maybe_capture(cube_ctx* c, int level, int64_t box, int what, const void* src, int n, bool fixed_int,
@@ -822,18 +875,26 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
 int cube_gpu_destroy(cube_ctx* c) {
   if (!c) return 0;
   cudaSetDevice(c->device);
+  if (c->ck_thread.joinable()) c->ck_thread.join();
+  if (c->s3) cudaStreamSynchronize(c->s3);
   if (c->s) cudaStreamSynchronize(c->s);
   drop_graphs(c);
   void* bufs[] = {c->xp, c->xp2, c->vp, c->vp2, c->pid, c->pid2, c->pcell, c->pcell2, c->rhoc, c->rhoc2,
                   c->fill, c->biglist, c->hugelist, c->nbig, c->cstart, c->cstart2, c->scan_tmp, c->dest, c->key, c->skey,
                   c->ssrc, c->rdev, c->sd, c->ires, c->box_slot, c->box_sub, c->arena, c->green1, c->green2,
-                  c->cap_buf, c->pfin, c->hlist, c->hpre, c->ppq, c->vtune, c->tune_red};
+                  c->cap_buf, c->pfin, c->hlist, c->hpre, c->ppq, c->vtune, c->tune_red, c->tf1, c->tf2,
+                  c->nu_tab};
   for (void* b : bufs)
     if (b) cudaFree(b);
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 8; ++i) {
     if (c->green3[i]) cudaFree(c->green3[i]);
+    if (c->tf3[i]) cudaFree(c->tf3[i]);
+  }
   for (auto& t : c->ffts) cudaFree(t.tw);
   if (c->rhost) cudaFreeHost(c->rhost);
+  if (c->ck_host) cudaFreeHost(c->ck_host);
+  if (c->ev_ckpt) cudaEventDestroy(c->ev_ckpt);
+  if (c->s3) cudaStreamDestroy(c->s3);
   if (c->h_sd) cudaFreeHost(c->h_sd);
   if (c->h_ires) cudaFreeHost(c->h_ires);
   for (int i = 0; i < 8; ++i)
@@ -848,9 +909,17 @@ int cube_gpu_destroy(cube_ctx* c) {
   return 0;
 }
 
+// Work on the context stream that overwrites the particle buffers of a checkpoint still
+// being copied waits for those copies (a no-op once they are done).  Not inside a
+// capture: a replayed step graph waits before its launch instead.
+static void after_checkpoint_copy(cube_ctx* c) {
+  if (c->ckpt_pending && !c->cap_graph) cudaStreamWaitEvent(c->s, c->ev_ckpt, 0);
+}
+
 static int alloc_particles(cube_ctx* c, int64_t np) {
   if (np <= c->cap) return 0;
   drop_graphs(c);
+  if (c->ckpt_pending) cudaEventSynchronize(c->ev_ckpt);  // its copies read the buffers freed here
   const int64_t cap = std::max<int64_t>(np, c->P.np_capacity);
   void** ps[] = {&c->xp, &c->xp2, (void**)&c->vp, (void**)&c->vp2, (void**)&c->pid, (void**)&c->pid2,
                  (void**)&c->pcell, (void**)&c->pcell2, (void**)&c->dest, (void**)&c->key, (void**)&c->skey,
@@ -909,6 +978,7 @@ int cube_gpu_upload(cube_ctx* c, const void* xp, const float* vp, const int64_t*
   int rc = alloc_particles(c, nplocal);
   if (rc) return rc;
   c->np = nplocal;
+  after_checkpoint_copy(c);
   CK(cudaMemcpyAsync(c->xp, xp, (size_t)nplocal * 3 * c->xbytes, cudaMemcpyHostToDevice, c->s));
   CK(cudaMemcpyAsync(c->vp, vp, (size_t)nplocal * 12, cudaMemcpyHostToDevice, c->s));
   CK(cudaMemcpyAsync(c->pid, pid, (size_t)nplocal * 8, cudaMemcpyHostToDevice, c->s));
@@ -1000,6 +1070,7 @@ static void enqueue_huge_sort(cube_ctx* c) {
 static void enqueue_drift(cube_ctx* c, bool defer_ids) {
   const Geo& G = c->G;
   const int64_t np = c->np;
+  after_checkpoint_copy(c);
   cudaMemsetAsync(c->rhoc2, 0, G.ncells * 4, c->s);
   cudaMemsetAsync(c->fill, 0, G.ncells * 4, c->s);
   cudaMemsetAsync(c->nbig, 0, 8, c->s);
@@ -1081,7 +1152,9 @@ static int enqueue_kick_a(cube_ctx* c) {
     else LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr, m.pt.plr, ms1));
     maybe_capture(c, 1, 0, 0, m.real, n, fixed, m.pt.rp, m.pt.psb);
     float* phi = reinterpret_cast<float*>(m.real);
-    launch_fft(c, n, 1, m.real, fixed, G.mass_p, phi, m.ck, c->green1, (float)n, 3, 1);
+    const float* k1 = kernel_table(c, 1, 0);
+    if (!k1) return CUBE_E_CUDA;
+    launch_fft(c, n, 1, m.real, fixed, G.mass_p, phi, m.ck, k1, (float)n, 3, 1);
     maybe_capture(c, 1, 0, 1, phi, n, false, (int64_t)m.pt.pf * 4, m.pt.psb);
     LAUNCH(c, K_F2_PM1, 1, k_f2max_periodic<<<(unsigned)std::min<int64_t>(1184, (int64_t)n * n / 8 + 1), 256, 0, c->s>>>(phi, n, f2 + 0, m.pt.pf, m.pt.plf));
     // force mesh (float4 per coarse cell) in the arena after phi, when it fits
@@ -1110,7 +1183,9 @@ static int enqueue_kick_a(cube_ctx* c) {
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
         maybe_capture(c, 2, c->cap_box, 0, (char*)m.real + (c->cap_box - t0) * boxb, n, fixed, m.pt.rp, m.pt.psb);
       float* phi = reinterpret_cast<float*>(m.real);
-      launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, c->green2, (float)n * (float)n * (float)n, 1, 2);
+      const float* k2 = kernel_table(c, 2, 0);
+      if (!k2) return CUBE_E_CUDA;
+      launch_fft(c, n, nb, m.real, fixed, G.mass_p, phi, m.ck, k2, (float)n * (float)n * (float)n, 1, 2);
       if (c->cap_level == 2 && c->cap_box >= t0 && c->cap_box < t0 + nb)
         maybe_capture(c, 2, c->cap_box, 1, (char*)m.real + (c->cap_box - t0) * boxb, n, false, (int64_t)m.pt.pf * 4,
                       m.pt.psb);
@@ -1130,8 +1205,8 @@ static int enqueue_kick_a(cube_ctx* c) {
   // PM3 mass over the boxes' physical cells, from the classes just found
   if (c->P.pm3_on) {
     unsigned long long* ms3 = c->msum + 2 * MASS_SLOTS * MASS_STRIDE;
-    if (fixed) LAUNCH(c, K_MASS, 1, k_mass_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, c->ires, ms3));
-    else LAUNCH(c, K_MASS, 1, k_mass_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, c->ires, ms3));
+    if (fixed) LAUNCH(c, K_MASS, 1, k_mass_pm3<true><<<nblk(G.ncells), 256, 0, c->s>>>(G, c->cstart, c->xp, c->ires, ms3));
+    else LAUNCH(c, K_MASS, 1, k_mass_pm3<false><<<nblk(G.ncells), 256, 0, c->s>>>(G, c->cstart, c->xp, c->ires, ms3));
   }
   return 0;
 }
@@ -1221,7 +1296,7 @@ static int enqueue_pm3(cube_ctx* c, const PM3Plan& pl, bool host_ires) {
   for (int cl = 2; cl <= 5; ++cl) {
     if (pl.cap[cl] == 0) continue;
     const int n = G.nft[cl];
-    const float* g3 = green3(c, cl);
+    const float* g3 = kernel_table(c, 3, cl);
     if (!g3) return CUBE_E_CUDA;
     const bool own = fixed && dep3_own_fits(G, cl);
     const bool lint = fixed && !own;  // int64 mesh layout
@@ -1254,8 +1329,13 @@ static int enqueue_pm3(cube_ctx* c, const PM3Plan& pl, bool host_ires) {
         maybe_capture(c, 3, c->cap_box, 1, (char*)m.real + cap_slot * boxb, n, false, (int64_t)m.pt.pf * 4, m.pt.psb);
       const int nf = G.nfp[cl];
       LAUNCH(c, K_F2_PM3, 1, k_f2max_box2<<<f2max_box2_grid(nf, nb), 256, 0, c->s>>>(phi, n, nf, 1 - G.nfb[cl], nb, f2 + 2, m.pt.pf, m.pt.plf, subs));
-      LAUNCH(c, K_INT_PM3, 1, k_interp_pm3<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp, c->sd, vm + 3,
-                                                c->err, m.pt.pf, m.pt.plf));
+      unsigned long long* ms3 = c->msum + 2 * MASS_SLOTS * MASS_STRIDE;
+      if (fixed)
+        LAUNCH(c, K_INT_PM3, 1, k_interp_pm3<true><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp,
+                                                                               c->sd, vm + 3, c->err, m.pt.pf, m.pt.plf, ms3));
+      else
+        LAUNCH(c, K_INT_PM3, 1, k_interp_pm3<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, slots, cl, c->vp,
+                                                                                c->sd, vm + 3, c->err, m.pt.pf, m.pt.plf, ms3));
     }
   }
   return 0;
@@ -1540,7 +1620,8 @@ static int step_graph(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     if (rc) return rc;
   }
   for (int cl = 2; cl <= 5; ++cl)
-    if (pl.cap[cl] > 0 && !green3(c, cl)) return CUBE_E_CUDA;  // tables exist before any capture
+    if (pl.cap[cl] > 0 && !kernel_table(c, 3, cl)) return CUBE_E_CUDA;  // tables exist before any capture
+  if (!kernel_table(c, 1, 0) || !kernel_table(c, 2, 0)) return CUBE_E_CUDA;
   const int parity = c->xp == c->xp_base ? 0 : 1;
   StepGraph* g = nullptr;
   for (auto& x : c->graphs)
@@ -1594,6 +1675,7 @@ static int step_graph(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     g = &c->graphs.back();
   }
   *c->h_sd = d;
+  after_checkpoint_copy(c);
   CK(cudaGraphLaunch(g->exec, c->s));
   CK(cudaStreamSynchronize(c->s));
   swap_drift(c);
@@ -1696,6 +1778,7 @@ int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, 
   if (rc) return rc;
   c->np = nplocal;
   c->loaded = false;
+  after_checkpoint_copy(c);
   CK(cudaMemcpyAsync(c->rhoc, rhoc, (size_t)G.ncells * 4, cudaMemcpyHostToDevice, c->s));
   CK(cudaMemcpyAsync(c->xp, xp, (size_t)nplocal * 3 * c->xbytes, cudaMemcpyHostToDevice, c->s));
   CK(cudaMemcpyAsync(c->vp, vp, (size_t)nplocal * 12, cudaMemcpyHostToDevice, c->s));
@@ -2016,6 +2099,124 @@ int cube_gpu_green_table(cube_ctx* c, int level, int iapm, float* out, int64_t n
   if (!src) return fail(CUBE_E_ARG, "bad level/iapm");
   const int64_t cnt = (int64_t)m * m * (m / 2 + 1);
   if (n < cnt) return fail(CUBE_E_ARG, "buffer too small");
+  CK(cudaStreamSynchronize(c->s));
+  CK(cudaMemcpy(out, src, cnt * 4, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int cube_gpu_checkpoint_wait(cube_ctx* c) {
+  if (!c) return fail(CUBE_E_ARG, "null context");
+  if (c->ck_thread.joinable()) c->ck_thread.join();
+  c->ckpt_pending = false;
+  const int st = c->ck_status;
+  c->ck_status = 0;
+  if (st) return fail(st, c->ck_error);
+  return 0;
+}
+
+int cube_gpu_checkpoint_async(cube_ctx* c, const cube_ckpt_files* files, const void* header, int64_t header_bytes) {
+  if (!c || !files || !files->info || !files->xp || !files->vp || !files->np || !files->id || !header ||
+      header_bytes <= 0)
+    return fail(CUBE_E_ARG, "bad checkpoint arguments");
+  if (!c->loaded) return fail(CUBE_E_STATE, "checkpoint before upload");
+  int rc = cube_gpu_checkpoint_wait(c);  // one checkpoint in flight at a time
+  if (rc) return rc;
+  CK(cudaSetDevice(c->device));
+  if (!c->s3) {
+    CK(cudaStreamCreateWithFlags(&c->s3, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_ckpt, cudaEventDisableTiming));
+  }
+  const Geo& G = c->G;
+  const size_t bx = (size_t)c->np * 3 * c->xbytes, bv = (size_t)c->np * 12, bn = (size_t)G.ncells * 4,
+               bi = (size_t)c->np * 8;
+  const size_t need = bx + bv + bn + bi + 64;
+  if (need > c->ck_bytes) {
+    if (c->ck_host) cudaFreeHost(c->ck_host);
+    c->ck_host = nullptr;
+    c->ck_bytes = 0;
+    CK(cudaMallocHost(&c->ck_host, need));
+    c->ck_bytes = need;
+  }
+  char* hx = static_cast<char*>(c->ck_host);
+  char* hv = hx + bx;
+  char* hn = hv + bv;
+  char* hi = hn + bn;
+  // the state as the context stream leaves it, copied on the side stream
+  CK(cudaEventRecord(c->ev_ckpt, c->s));
+  CK(cudaStreamWaitEvent(c->s3, c->ev_ckpt, 0));
+  CK(cudaMemcpyAsync(hx, c->xp, bx, cudaMemcpyDeviceToHost, c->s3));
+  CK(cudaMemcpyAsync(hv, c->vp, bv, cudaMemcpyDeviceToHost, c->s3));
+  CK(cudaMemcpyAsync(hn, c->rhoc, bn, cudaMemcpyDeviceToHost, c->s3));
+  CK(cudaMemcpyAsync(hi, c->pid, bi, cudaMemcpyDeviceToHost, c->s3));
+  CK(cudaEventRecord(c->ev_ckpt, c->s3));
+  c->ckpt_pending = true;
+  struct Part {
+    std::string path;
+    const char* data;
+    size_t bytes;
+  };
+  std::vector<Part> parts = {{files->info, static_cast<const char*>(header), (size_t)header_bytes},
+                             {files->xp, hx, bx}, {files->vp, hv, bv}, {files->np, hn, bn}, {files->id, hi, bi}};
+  std::vector<char> hdr(static_cast<const char*>(header), static_cast<const char*>(header) + header_bytes);
+  const int dev = c->device;
+  cudaEvent_t ev = c->ev_ckpt;
+  c->ck_status = 0;
+  c->ck_error.clear();
+  c->ck_thread = std::thread([c, parts, hdr, dev, ev]() mutable {
+    parts[0].data = hdr.data();  // the caller's header may go away once the call returns
+    cudaSetDevice(dev);
+    if (cudaEventSynchronize(ev) != cudaSuccess) {
+      c->ck_status = CUBE_E_CUDA;
+      c->ck_error = "checkpoint copies failed";
+      return;
+    }
+    for (const Part& p : parts) {
+      FILE* f = fopen(p.path.c_str(), "wb");
+      if (!f || fwrite(p.data, 1, p.bytes, f) != p.bytes || fclose(f) != 0) {
+        c->ck_status = CUBE_E_ARG;
+        c->ck_error = "checkpoint: cannot write " + p.path;
+        return;
+      }
+    }
+  });
+  return 0;
+}
+
+int cube_gpu_nu_transfer(cube_ctx* c, const float* kh_log, const float* tf_log, int nb) {
+  if (!c || nb < 0 || (nb > 0 && (!kh_log || !tf_log))) return fail(CUBE_E_ARG, "bad neutrino transfer arguments");
+  if (nb > 0 && nb < 3) return fail(CUBE_E_ARG, "the transfer table needs at least three points");
+  for (int i = 1; i < nb; ++i)
+    if (!(kh_log[i] > kh_log[i - 1])) return fail(CUBE_E_ARG, "log k of the transfer table must increase");
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->s));  // the previous table may still be read
+  // captured steps name the force kernels: the Green tables or, with neutrinos, the
+  // rescaled copies (rebuilt in place before each step); switching between the two
+  // needs new captures
+  const bool before = c->P.f_nu > 0.f || c->nu_nb >= 3, after = c->P.f_nu > 0.f || nb >= 3;
+  if (before != after) drop_graphs(c);
+  if (c->nu_tab) cudaFree(c->nu_tab);
+  c->nu_tab = nullptr;
+  c->nu_nb = 0;
+  if (nb > 0) {
+    CK(cudaMalloc(&c->nu_tab, (size_t)2 * nb * sizeof(float)));
+    CK(cudaMemcpy(c->nu_tab, kh_log, nb * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->nu_tab + nb, tf_log, nb * sizeof(float), cudaMemcpyHostToDevice));
+    c->nu_nb = nb;
+  }
+  ++c->nu_ver;
+  return 0;
+}
+
+int cube_gpu_kernel_table(cube_ctx* c, int level, int iapm, float* out, int64_t n) {
+  if (!c || !out) return fail(CUBE_E_ARG, "null argument");
+  if (level < 1 || level > 3 || (level == 3 && (iapm < 2 || iapm > 5))) return fail(CUBE_E_ARG, "bad level/iapm");
+  CK(cudaSetDevice(c->device));
+  const Geo& G = c->G;
+  const int m = level == 1 ? G.nc : level == 2 ? G.ngt : G.nft[iapm];
+  const int64_t cnt = (int64_t)m * m * (m / 2 + 1);
+  if (n < cnt) return fail(CUBE_E_ARG, "buffer too small");
+  const float* src = kernel_table(c, level, iapm);
+  if (!src) return CUBE_E_CUDA;
   CK(cudaStreamSynchronize(c->s));
   CK(cudaMemcpy(out, src, cnt * 4, cudaMemcpyDeviceToHost));
   return 0;

@@ -748,9 +748,10 @@ __global__ void k_deposit_pm3(Geo G, int64_t np, const void* __restrict__ xp, co
 // itself, exactly; the deposit kernels need no extra work for it.
 // A neighbour box of the same class has the own box's weights shifted by whole cells, so
 // its physical contributions are the own box's contributions that leave the own physical
-// region in its direction: the sum of all 27 own contributions covers both.  Only a
-// neighbour of another class (a class boundary, rare) needs its own weights: its share of
-// the 27 is replaced by its physical contributions at its class.
+// region in its direction: the sum of all 27 own contributions covers both, and
+// k_interp_pm3 adds it while it holds the weights.  Only a neighbour of another class (a
+// class boundary, rare) needs its own weights: its share of the 27 is replaced by its
+// physical contributions at its class (k_mass_pm3).
 template <bool FIXED>
 __device__ __forceinline__ void mass_box(const Geo& G, int iapm, const double lf[3], const int u[3], int i2[3],
                                          float w[3][3]) {
@@ -763,38 +764,44 @@ __device__ __forceinline__ void mass_box(const Geo& G, int iapm, const double lf
 // direction (-1, 0, +1) of 0-based cell index i relative to the physical range 0..nfp-1
 __device__ __forceinline__ int mass_dir(int i, int nfp) { return i < 0 ? -1 : (i >= nfp ? 1 : 0); }
 
+// The class-boundary part: one thread per coarse cell; a cell in a face layer of its
+// subtile whose neighbour subtile across that face has another class corrects the own-box
+// sums that k_interp_pm3 added for its particles.  Every other cell returns at once.
 template <bool FIXED>
-__global__ void __launch_bounds__(256) k_mass_pm3(Geo G, int64_t np, const void* __restrict__ xp,
-                                                  const int32_t* __restrict__ pcell, const int32_t* __restrict__ ires,
+__global__ void __launch_bounds__(256) k_mass_pm3(Geo G, const int64_t* __restrict__ cstart,
+                                                  const void* __restrict__ xp, const int32_t* __restrict__ ires,
                                                   void* msum) {
-  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   MassAcc<FIXED> mass;
-  if (ip < np) {
-    int g[3];
-    cell_coords(G, pcell[ip], g[0], g[1], g[2]);
-    int tc[3][2], uc[3][2], lc[3][2], nca[3];
-    double f[3];
+  int g[3], tc[3][2], uc[3][2], lc[3][2], nca[3] = {1, 1, 1};
+  bool any = false;
+  int own = 0;
+  if (cell < G.ncells) {
+    cell_coords(G, cell, g[0], g[1], g[2]);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      nca[d] = sub_cands(G, g[d], tc[d], uc[d], lc[d]);
-      f[d] = zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
-    }
-    // own box: all 27 contributions
-    const int t0[3] = {tc[0][0], tc[1][0], tc[2][0]}, u0[3] = {uc[0][0], uc[1][0], uc[2][0]};
-    const int own = ires[subtile_id(G, t0, u0)];
-    const double lf0[3] = {(double)lc[0][0] + f[0], (double)lc[1][0] + f[1], (double)lc[2][0] + f[2]};
-    int i2[3];
-    float w[3][3];
-    mass_box<FIXED>(G, own, lf0, u0, i2, w);
-#pragma unroll
-    for (int a3 = 0; a3 < 3; ++a3)
-#pragma unroll
-      for (int a2 = 0; a2 < 3; ++a2)
-#pragma unroll
-        for (int a1 = 0; a1 < 3; ++a1) mass.add(__fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]));
-    // neighbour boxes of another class (only particles in a face cell of their subtile)
+    for (int d = 0; d < 3; ++d) nca[d] = sub_cands(G, g[d], tc[d], uc[d], lc[d]);
     if (nca[0] * nca[1] * nca[2] > 1) {
-      const int nfp0 = G.nfp[own];
+      const int t0[3] = {tc[0][0], tc[1][0], tc[2][0]}, u0[3] = {uc[0][0], uc[1][0], uc[2][0]};
+      own = ires[subtile_id(G, t0, u0)];
+      for (int cz = 0; cz < nca[2]; ++cz)
+        for (int cy = 0; cy < nca[1]; ++cy)
+          for (int cx = 0; cx < nca[0]; ++cx) {
+            const int t[3] = {tc[0][cx], tc[1][cy], tc[2][cz]}, u[3] = {uc[0][cx], uc[1][cy], uc[2][cz]};
+            any |= ires[subtile_id(G, t, u)] != own;
+          }
+    }
+  }
+  if (any) {
+    const int nfp0 = G.nfp[own];
+    const int u0[3] = {uc[0][0], uc[1][0], uc[2][0]};
+    for (int64_t ip = cstart[cell]; ip < cstart[cell + 1]; ++ip) {
+      double f[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) f[d] = zfrac(load_code(xp, G.izipx, 3 * ip + d), G);
+      const double lf0[3] = {(double)lc[0][0] + f[0], (double)lc[1][0] + f[1], (double)lc[2][0] + f[2]};
+      int i2[3];
+      float w[3][3];
+      mass_box<FIXED>(G, own, lf0, u0, i2, w);
       for (int cz = 0; cz < nca[2]; ++cz)
         for (int cy = 0; cy < nca[1]; ++cy)
           for (int cx = 0; cx < nca[0]; ++cx) {
@@ -803,7 +810,6 @@ __global__ void __launch_bounds__(256) k_mass_pm3(Geo G, int64_t np, const void*
             const int u[3] = {uc[0][cx], uc[1][cy], uc[2][cz]};
             const int nb = ires[subtile_id(G, t, u)];
             if (nb == own) continue;
-            // the box's direction from the own box, per dimension (0 where it is the own subtile)
             int dir[3];
             const int cc[3] = {cx, cy, cz};
 #pragma unroll
@@ -1404,13 +1410,17 @@ __global__ void __launch_bounds__(256, 3) k_interp_pm2(Geo G, int64_t np, const 
   block_vmax(av, vmax);
 }
 
+// msum: PM3 mass slots; each particle adds its own box's 27 contributions (the mass sums
+// described at k_mass_pm3), in the arithmetic of the deposit form.
+template <bool FIXED>
 __global__ void __launch_bounds__(256, 3) k_interp_pm3(Geo G, int64_t np, const void* __restrict__ xp, const int32_t* __restrict__ pcell,
                              const float* __restrict__ phi, const int32_t* __restrict__ box_slot, int iapm,
                              float* __restrict__ vp, const StepDev* __restrict__ sd, float* vmax, unsigned* err,
-                             int pf, int64_t pl) {
+                             int pf, int64_t pl, void* msum) {
   const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const float a_mid = sd->a_mid, dt = sd->dt;
   float av[3] = {0.f, 0.f, 0.f};
+  MassAcc<FIXED> mass;
   if (ip < np) {
     int g[3];
     cell_coords(G, pcell[ip], g[0], g[1], g[2]);
@@ -1444,10 +1454,17 @@ __global__ void __launch_bounds__(256, 3) k_interp_pm3(Geo G, int64_t np, const 
         float dv[3];
         tsc_gather_force(i2, w, P, dv);
         apply_kick(vp, ip, dv, a_mid, dt, av);
+#pragma unroll
+        for (int a3 = 0; a3 < 3; ++a3)
+#pragma unroll
+          for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+            for (int a1 = 0; a1 < 3; ++a1) mass.add(__fmul_rn(__fmul_rn(w[0][a1], w[1][a2]), w[2][a3]));
       }
     }
   }
   block_vmax(av, vmax);
+  mass.flush(msum);
 }
 
 // =================================================================================
@@ -1759,6 +1776,73 @@ __global__ void k_green(float* __restrict__ Gk, int n, float apm_soft, float apm
   const int h = n / 2;
   if ((k1 % h == 0) && (k2 % h == 0) && (k3 % h == 0)) val = 0.0;  // Green.f90:71
   Gk[i] = (float)val;
+}
+
+// =================================================================================
+// Neutrino linear response of the force kernels (kick.f90:23-29; power_nu.f90:179-219
+// interp_tf_F, :449-476 nu_correction): tf(k) = interp_tf_F(|k|) * Gk(k) for every mode
+// of a Green table, the zero mode set to 1 as nu_correction leaves it.  k of mode
+// (i, j, k) (1-based) is (mod(i + n/2, n) - n/2 - 1) * 2 pi / size with `size` the level's
+// box side in Mpc/h (box for PM1, box/nnt for PM2, box/nnt/nns for PM3), rounded to real
+// as the reference stores kx.  The interpolation is quadratic in log-log through the three
+// table points nearest log|k|, in FP32 as the reference computes it.
+// =================================================================================
+__device__ float nu_interp_tf(const float* __restrict__ klog, const float* __restrict__ tlog, int nb, float kr) {
+  const float kn = logf(kr);
+  int i1 = 1, i2 = nb;  // 1-based as the reference
+  while (i2 - i1 > 1) {
+    const int mid = (i1 + i2) / 2;
+    if (kn > klog[mid - 1]) i1 = mid;
+    else i2 = mid;
+  }
+  int i3;
+  if (kn - klog[i1 - 1] < klog[i2 - 1] - kn) {
+    i3 = i2;
+    i2 = i1;
+    i1 = i1 - 1;
+  } else {
+    i3 = i2 + 1;
+  }
+  if (i3 > nb) {
+    --i1;
+    --i2;
+    --i3;
+  }
+  if (i1 < 1) {  // |k| below the table's second point: the first three points
+    i1 = 1;
+    i2 = 2;
+    i3 = 3;
+  }
+  const float K1 = klog[i1 - 1], K2 = klog[i2 - 1], K3 = klog[i3 - 1];
+  const float T1 = tlog[i1 - 1], T2 = tlog[i2 - 1], T3 = tlog[i3 - 1];
+  const float a1 = (T1 - T2) / (K1 - K2);
+  const float a2 = (T2 - T3) / (K2 - K3);
+  const float k2 = (a1 - a2) / (K1 - K3);
+  const float b2 = a1 - k2 * (K1 + K2);
+  const float c2 = T1 - k2 * K1 * K1 - b2 * K1;
+  return expf(k2 * kn * kn + b2 * kn + c2);
+}
+
+__global__ void k_nu_rescale(int n, double size, const float* __restrict__ gk, float* __restrict__ tf,
+                             const float* __restrict__ klog, const float* __restrict__ tlog, int nb, float scale) {
+  const int nh = n / 2 + 1;
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= (int64_t)nh * n * n) return;
+  if (nb < 3) {  // no table: the constant (1 - f_nu) of initialize.f90:316-322
+    tf[m] = scale * gk[m];
+    return;
+  }
+  const int i = (int)(m % nh) + 1, j = (int)((m / nh) % n) + 1, k = (int)(m / ((int64_t)nh * n)) + 1;
+  if (i == 1 && j == 1 && k == 1) {  // zero frequency
+    tf[m] = 1.f;
+    return;
+  }
+  const double f = 2.0 * 3.141592653589793 / size;
+  const float kx = (float)(((i + n / 2) % n - n / 2 - 1) * f);
+  const float ky = (float)(((j + n / 2) % n - n / 2 - 1) * f);
+  const float kz = (float)(((k + n / 2) % n - n / 2 - 1) * f);
+  const float kr = sqrtf(kx * kx + ky * ky + kz * kz);
+  tf[m] = nu_interp_tf(klog, tlog, nb, kr) * gk[m];
 }
 
 }  // namespace cube

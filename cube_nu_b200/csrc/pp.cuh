@@ -40,7 +40,7 @@ struct PPi {
   int l[3], lo[3], hi[3];
   float range, range2;
   float acc[3];
-  unsigned long long pairs, cand;
+  unsigned pairs, cand;  // of this particle (item): well below 2^32
 
   __device__ __forceinline__ void init(const Geo& G, const int g[3], const float4 fin, int iapm) {
     const float fi[3] = {fin.x, fin.y, fin.z};
@@ -62,11 +62,11 @@ struct PPi {
   }
 
   // One candidate at in-cell offset p of the neighbour cell whose tile-local coarse
-  // coordinates are base (= l + d), already multiplied by ratio_cs.
-  __device__ __forceinline__ void pair(const float base[3], const float4 p, float app) {
-    const float rv0 = __fsub_rn(__fadd_rn(base[0], p.x), xf[0]);
-    const float rv1 = __fsub_rn(__fadd_rn(base[1], p.y), xf[1]);
-    const float rv2 = __fsub_rn(__fadd_rn(base[2], p.z), xf[2]);
+  // coordinates are (bx, by, bz) (= l + d), already multiplied by ratio_cs.
+  __device__ __forceinline__ void pair(float bx, float by, float bz, const float4 p, float app) {
+    const float rv0 = __fsub_rn(__fadd_rn(bx, p.x), xf[0]);
+    const float rv1 = __fsub_rn(__fadd_rn(by, p.y), xf[1]);
+    const float rv2 = __fsub_rn(__fadd_rn(bz, p.z), xf[2]);
     const float r2 = sumsq3(rv0, rv1, rv2);
     if (r2 > 0.f && r2 < range2) {
       const float rm = __fsqrt_rn(r2);
@@ -131,16 +131,16 @@ __global__ void __launch_bounds__(128) k_ppq_light(Geo G, int64_t np, const int3
         for (int dx = P.lo[0]; dx <= P.hi[0]; ++dx) {
           const int64_t n = cell_index(G, g[0] + dx, g[1] + dy, g[2] + dz);
           const int64_t s = cstart[n], e = cstart[n + 1];
-          P.cand += (unsigned long long)(e - s);
-          const float base[3] = {(float)((P.l[0] + dx) * G.rcs), (float)((P.l[1] + dy) * G.rcs),
-                                 (float)((P.l[2] + dz) * G.rcs)};
-          for (int64_t q = s; q < e; ++q) P.pair(base, pfin[q], G.app);
+          P.cand += (unsigned)(e - s);
+          const float bx = (float)((P.l[0] + dx) * G.rcs), by = (float)((P.l[1] + dy) * G.rcs),
+                      bz = (float)((P.l[2] + dz) * G.rcs);
+          for (int64_t q = s; q < e; ++q) P.pair(bx, by, bz, pfin[q], G.app);
         }
     f2 = ppq_apply(P, ip, vin, vout, sd->pp_mass, sd->pp_vscale, av);
   }
   block_max_to(f2, f2max);
   block_vmax(av, vmax);
-  unsigned long long a = P.pairs, b = P.cand;
+  unsigned long long a = P.pairs, b = P.cand;  // warp sums in 64 bits
   for (int o = 16; o > 0; o >>= 1) {
     a += __shfl_xor_sync(0xffffffffu, a, o);
     b += __shfl_xor_sync(0xffffffffu, b, o);
@@ -258,16 +258,16 @@ __global__ void k_ppq_heavy(Geo G, const int32_t* __restrict__ hlist, const int*
           if (!__syncthreads_or(need)) continue;  // block-uniform
           const int64_t n = cell_index(G, g[0] + dx, g[1] + dy, g[2] + dz);
           const int64_t s = cstart[n], e = cstart[n + 1];
-          if (need) P.cand += (unsigned long long)(e - s);
-          const float base[3] = {(float)((P.l[0] + dx) * G.rcs), (float)((P.l[1] + dy) * G.rcs),
-                                 (float)((P.l[2] + dz) * G.rcs)};
+          if (need) P.cand += (unsigned)(e - s);
+          const float bx = (float)((P.l[0] + dx) * G.rcs), by = (float)((P.l[1] + dy) * G.rcs),
+                      bz = (float)((P.l[2] + dz) * G.rcs);
           for (int64_t j0 = s; j0 < e; j0 += J) {
             const int cnt = (int)((e - j0) < (int64_t)J ? (e - j0) : (int64_t)J);
             __syncthreads();
             for (int k = threadIdx.x; k < cnt; k += B) sj[k] = pfin[j0 + k];
             __syncthreads();
             if (need)
-              for (int k = 0; k < cnt; ++k) P.pair(base, sj[k], G.app);
+              for (int k = 0; k < cnt; ++k) P.pair(bx, by, bz, sj[k], G.app);
           }
         }
     if (live) {

@@ -250,6 +250,35 @@ int64_t cube_gpu_kernel_launches(cube_ctx* ctx);
 int cube_gpu_int2real(cube_ctx* ctx, float* xv, int64_t n);
 /* Download the Green table of a level (1, 2, or 3 with class iapm 2..5). */
 int cube_gpu_green_table(cube_ctx* ctx, int level, int iapm, float* out, int64_t n);
+/* Asynchronous checkpoint (checkpoint.f90:11-39): the particle state as the context
+ * stream leaves it (after the work issued so far) is copied to pinned staging memory on
+ * a side stream, and a writer thread stores the five files of one image -- `info` gets
+ * the caller's sim_header bytes (224 in the reference), `xp` int(izipx)(3,np), `vp`
+ * real(4)(3,np), `np` int(4) rhoc, `id` int(8) PID -- while the host goes on stepping.
+ * Steps that would overwrite the copied buffers wait for the copies on the device; the
+ * host never waits.  One checkpoint is in flight at a time (a second call waits for the
+ * first); cube_gpu_checkpoint_wait joins the writer and returns its status. */
+typedef struct cube_ckpt_files {
+  const char* info;
+  const char* xp;
+  const char* vp;
+  const char* np;
+  const char* id;
+} cube_ckpt_files;
+int cube_gpu_checkpoint_async(cube_ctx* ctx, const cube_ckpt_files* files, const void* header,
+                              int64_t header_bytes);
+int cube_gpu_checkpoint_wait(cube_ctx* ctx);
+
+/* Neutrino linear response of the force kernels (kick.f90:23-29, get_tf_cb2matter).  The
+ * host computes the per-step transfer ratio tf_F(k) on its k table as the reference does
+ * (neutrinos/power_nu.f90:346-420) and passes log k (h/Mpc) and log tf_F, nb >= 3 points,
+ * k increasing; every level's force kernel becomes interp_tf_F(|k|) * Gk (power_nu.f90:
+ * 179-219, 449-498), rebuilt on the device before the next kick.  nb = 0 drops the table.
+ * Without a table and with cube_params.f_nu > 0 the kernels are (1 - f_nu) * Gk
+ * (initialize.f90:316-322), and PP uses (1 - f_nu)^2 (kick.f90:569).
+ * cube_gpu_kernel_table downloads the kernel a level uses (as cube_gpu_green_table). */
+int cube_gpu_nu_transfer(cube_ctx* ctx, const float* kh_log, const float* tf_log, int nb);
+int cube_gpu_kernel_table(cube_ctx* ctx, int level, int iapm, float* out, int64_t n);
 /* Download per-subtile PM3 class (ires, kick.f90:108-133), ns3 entries. */
 int cube_gpu_subtile_class(cube_ctx* ctx, int32_t* ires, int64_t n);
 
