@@ -23,7 +23,19 @@ EXPORTS = (
     "cube_gpu_zipv_encode", "cube_gpu_zipv_decode", "cube_gpu_download_zipv", "cube_gpu_ic", "cube_gpu_power",
     "cube_gpu_int2real", "cube_gpu_step_host", "cube_gpu_pp_shape", "cube_gpu_pp_shape_get",
     "cube_gpu_nu_transfer", "cube_gpu_kernel_table", "cube_gpu_checkpoint_async", "cube_gpu_checkpoint_wait",
+    "cube_gpu_set_comm", "cube_slab_cells", "cube_gpu_nplocal",
 )
+
+# cube_comm (include/cube_gpu.h): the collectives of a run split into z-slabs
+ALLREDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+                                ctypes.c_int32, ctypes.c_int32)
+SENDRECV_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                               ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                               ctypes.c_int32)
+
+
+class CComm(ctypes.Structure):
+    _fields_ = [("user", ctypes.c_void_p), ("allreduce", ALLREDUCE_FN), ("sendrecv", SENDRECV_FN)]
 
 
 class CkptFiles(ctypes.Structure):
@@ -118,6 +130,11 @@ def load():
     L.cube_gpu_checkpoint_async.argtypes = [vp, ctypes.POINTER(CkptFiles), vp, ctypes.c_int64]
     L.cube_gpu_checkpoint_wait.argtypes = [vp]
     L.cube_gpu_kernel_table.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int64]
+    L.cube_gpu_set_comm.argtypes = [vp, ctypes.POINTER(CComm)]
+    L.cube_slab_cells.argtypes = [P, ctypes.c_int, vp, ctypes.c_int64]
+    L.cube_slab_cells.restype = ctypes.c_int64
+    L.cube_gpu_nplocal.argtypes = [vp]
+    L.cube_gpu_nplocal.restype = ctypes.c_int64
     ip = ctypes.POINTER(ctypes.c_int)
     L.cube_gpu_pp_shape_get.argtypes = [vp, ctypes.c_int, ip, ip, ip, ctypes.POINTER(ctypes.c_double)]
     _LIB = L
@@ -179,8 +196,21 @@ class Context:
         _check(self._lib.cube_gpu_upload(self._h, _ptr(xp), _ptr(vp), _ptr(pid), _ptr(rhoc), n), "cube_gpu_upload")
         self.np = n
 
+    def nplocal(self) -> int:
+        """Particles this context holds for its rank (what download returns)."""
+        return int(_check(self._lib.cube_gpu_nplocal(self._h), "cube_gpu_nplocal"))
+
+    def set_comm(self, comm) -> None:
+        """The collectives of a run split into z-slabs (Params.nslab > 1): an object with
+        ``as_c()`` returning a CComm (cube_nu_b200.slabs.TorchComm); it must outlive the
+        context's steps."""
+        self._comm = comm
+        self._ccomm = comm.as_c()
+        _check(self._lib.cube_gpu_set_comm(self._h, ctypes.byref(self._ccomm)), "cube_gpu_set_comm")
+
     def download(self):
         p = self.params
+        self.np = self.nplocal()
         xp = np.empty((self.np, 3), dtype=p.xdtype)
         vp = np.empty((self.np, 3), dtype=np.float32)
         pid = np.empty(self.np, dtype=np.int64)

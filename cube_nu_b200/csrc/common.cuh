@@ -25,7 +25,25 @@ struct Geo {
   double inv_step;   // 1/(x_res*ratio_cs): code units per fine cell
   uint32_t zmask;    // 0xff or 0xffff
   int64_t ncells;    // nc^3
+  // The part of the box this context steps (cube_params.nslab/slab): tiles [tile0, tile1),
+  // their cells [c0, c1) in storage order and subtiles [s0, s1).  The whole box with one
+  // slab; other cells hold ghost copies (or nothing).
+  int nslab, tile0, tile1, s0, s1;
+  int64_t c0, c1;
 };
+
+// Whether storage cell c belongs to this context's slab.
+__host__ __device__ inline bool owned_cell(const Geo& G, int64_t c) { return c >= G.c0 && c < G.c1; }
+
+// Cell `slot` of a ghost-exchange layer: the ncb cell layers lz0 .. lz0+ncb-1 of every tile
+// of tile layer tz, in storage order.  Within a tile the cells of consecutive lz are
+// consecutive in storage, so the layer is nnt^2 runs of ncb*nt^2 cells.
+__host__ __device__ inline int64_t layer_cell(const Geo& G, int tz, int lz0, int64_t slot) {
+  const int64_t run = (int64_t)G.ncb * G.nt * G.nt;
+  const int64_t t = slot / run;
+  const int64_t T = (int64_t)tz * G.nnt * G.nnt + t;
+  return T * G.nt * G.nt * G.nt + (int64_t)lz0 * G.nt * G.nt + (slot - t * run);
+}
 
 // Per-step scalars, written by the host into device memory at the start of every step
 // (one small copy, which a captured step graph replays), so that no kernel of the step

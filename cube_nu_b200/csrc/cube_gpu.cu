@@ -26,6 +26,7 @@
 #include "power.cuh"
 #include "pp.cuh"
 #include "dpm.cuh"
+#include "slab.cuh"
 
 using namespace cube;
 
@@ -63,13 +64,14 @@ enum KClass {
   K_DRIFT_DEST, K_DRIFT_SCATTER, K_DRIFT_SORT, K_DRIFT_GATHER, K_SCAN, K_DEP_PM1, K_FFT_PM1, K_F2_PM1, K_INT_PM1,
   K_DEP_PM2, K_FFTX_PM2, K_FFTY_PM2, K_FFTZ_PM2, K_FFTC_PM2, K_F2_PM2, K_INT_PM2, K_DEP_PM3, K_FFTX_PM3, K_FFTY_PM3,
   K_FFTZ_PM3, K_FFTC_PM3, K_F2_PM3, K_INT_PM3, K_PP, K_CLASSIFY, K_GREEN, K_FILL, K_PK_DEP, K_PK_FFT, K_PK_BIN,
-  K_PK_ALIAS, K_MOMENTUM, K_MASS, K_NCLASS
+  K_PK_ALIAS, K_MOMENTUM, K_MASS, K_SLAB, K_NCLASS
 };
 const char* const KNAMES[K_NCLASS] = {
     "drift_dest", "drift_scatter", "drift_sort", "drift_gather", "scan", "deposit_pm1", "fft_pm1", "f2max_pm1",
     "interp_pm1", "deposit_pm2", "fft_x_pm2", "fft_y_pm2", "fft_z_green_pm2", "fft_c2r_pm2", "f2max_pm2",
     "interp_pm2", "deposit_pm3", "fft_x_pm3", "fft_y_pm3", "fft_z_green_pm3", "fft_c2r_pm3", "f2max_pm3",
-    "interp_pm3", "pp", "classify", "green", "fill_pcell", "pk_deposit", "pk_fft", "pk_bin", "pk_alias", "momentum", "mass_pm3"};
+    "interp_pm3", "pp", "classify", "green", "fill_pcell", "pk_deposit", "pk_fft", "pk_bin", "pk_alias", "momentum", "mass_pm3",
+    "slab_exchange"};
 
 struct ProfRec {
   int cls;
@@ -234,6 +236,18 @@ struct cube_ctx {
   double prof_ms[K_NCLASS] = {0};
   int64_t prof_n[K_NCLASS] = {0};
   int64_t launches = 0;
+  // a run split into z-slabs (cube_params.nslab > 1): the host's collectives; whether the
+  // store holds fresh ghost layers; this rank's particles [own0, own1) in the store;
+  // scratch of the layer exchange (counts and their prefixes: send down, send up, from
+  // below, from above; payloads)
+  cube_comm comm{};
+  bool have_comm = false;
+  bool ghosts = false;
+  int64_t own0 = 0, own1 = 0;
+  int32_t* lay_cnt = nullptr;
+  int64_t* lay_start = nullptr;
+  char* lay_buf = nullptr;
+  size_t lay_bytes = 0;
 };
 
 namespace {
@@ -368,6 +382,15 @@ Geo make_geo(const cube_params& p) {
   g.inv_step = 1.0 / (g.x_res * (double)g.rcs);
   g.zmask = (g.izipx == 1) ? 0xffu : 0xffffu;
   g.ncells = (int64_t)g.nc * g.nc * g.nc;
+  // this context's slab: tile layers [slab*L, (slab+1)*L) along z, L = nnt/nslab
+  g.nslab = p.nslab > 1 ? p.nslab : 1;
+  const int L = g.nnt / g.nslab, slab = g.nslab > 1 ? p.slab : 0;
+  g.tile0 = slab * L * g.nnt * g.nnt;
+  g.tile1 = (slab + 1) * L * g.nnt * g.nnt;
+  g.s0 = g.tile0 * g.nns * g.nns * g.nns;
+  g.s1 = g.tile1 * g.nns * g.nns * g.nns;
+  g.c0 = (int64_t)g.tile0 * g.nt * g.nt * g.nt;
+  g.c1 = (int64_t)g.tile1 * g.nt * g.nt * g.nt;
   return g;
 }
 
@@ -765,6 +788,7 @@ void cube_params_default(cube_params* p, int64_t ng) {
   p->apm2 = 3.5f;
   p->apm3f = 3.5f;
   p->mass_p_cdm = 0.f;
+  p->nslab = 1;
 }
 
 const char* cube_gpu_version(void) { return "cube-b200 0.1 (sm_100a)"; }
@@ -783,6 +807,8 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
     return fail(CUBE_E_ARG, "ng, nnt, nns must divide evenly (parameters.f90:57-59)");
   if (p->izipx != 1 && p->izipx != 2) return fail(CUBE_E_ARG, "izipx must be 1 or 2");
   if (p->mass_p_cdm <= 0.f) return fail(CUBE_E_ARG, "mass_p_cdm must be positive");
+  if (p->nslab < 0 || (p->nslab > 1 && (p->nnt % p->nslab || p->slab < 0 || p->slab >= p->nslab)))
+    return fail(CUBE_E_ARG, "nslab must divide nnt, and 0 <= slab < nslab");
   cube_ctx* c = new cube_ctx();
   c->P = *p;
   c->G = make_geo(*p);
@@ -850,6 +876,11 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
   CK(cudaMallocHost(&c->h_sd, sizeof(StepDev)));
   CK(cudaMalloc(&c->ires, c->ns3 * 4));
   CK(cudaMallocHost(&c->h_ires, c->ns3 * 4));
+  if (G.nslab > 1) {  // layer exchange: counts and prefixes of the four layers
+    const int64_t nlay = (int64_t)G.nnt * G.nnt * G.ncb * G.nt * G.nt;
+    CK(cudaMalloc(&c->lay_cnt, 4 * nlay * 4));
+    CK(cudaMalloc(&c->lay_start, 4 * (nlay + 1) * 8));
+  }
   if (c->P.pp_queue) {
     if (!(G.izipx == 1 || G.nt < 127)) {
       cube_gpu_destroy(c);
@@ -883,7 +914,7 @@ int cube_gpu_destroy(cube_ctx* c) {
                   c->fill, c->biglist, c->hugelist, c->nbig, c->cstart, c->cstart2, c->scan_tmp, c->dest, c->key, c->skey,
                   c->ssrc, c->rdev, c->sd, c->ires, c->box_slot, c->box_sub, c->arena, c->green1, c->green2,
                   c->cap_buf, c->pfin, c->hlist, c->hpre, c->ppq, c->vtune, c->tune_red, c->tf1, c->tf2,
-                  c->nu_tab};
+                  c->nu_tab, c->lay_cnt, c->lay_start, c->lay_buf};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (int i = 0; i < 8; ++i) {
@@ -920,7 +951,12 @@ static int alloc_particles(cube_ctx* c, int64_t np) {
   if (np <= c->cap) return 0;
   drop_graphs(c);
   if (c->ckpt_pending) cudaEventSynchronize(c->ev_ckpt);  // its copies read the buffers freed here
-  const int64_t cap = std::max<int64_t>(np, c->P.np_capacity);
+  int64_t cap = std::max<int64_t>(np, c->P.np_capacity);
+  if (c->G.nslab > 1) {  // room for the two ghost layers: 2 ncb of the slab's L*nt cell layers, with margin
+    const Geo& g = c->G;
+    const double frac = 2.0 * g.ncb / ((double)(g.nnt / g.nslab) * g.nt);
+    cap = (int64_t)((double)cap * (1.0 + 1.5 * frac)) + 4096;
+  }
   void** ps[] = {&c->xp, &c->xp2, (void**)&c->vp, (void**)&c->vp2, (void**)&c->pid, (void**)&c->pid2,
                  (void**)&c->pcell, (void**)&c->pcell2, (void**)&c->dest, (void**)&c->key, (void**)&c->skey,
                  (void**)&c->ssrc};
@@ -964,6 +1000,44 @@ static int alloc_particles(cube_ctx* c, int64_t np) {
   return 0;
 }
 
+// Grow the particle buffers to hold `need` particles, keeping the current state (the first
+// buffer set, c->np particles); the second set and the per-particle scratch come back
+// empty at the new size.
+static int grow_particles(cube_ctx* c, int64_t need) {
+  if (need <= c->cap) return 0;
+  drop_graphs(c);
+  if (c->ckpt_pending) cudaEventSynchronize(c->ev_ckpt);
+  CK(cudaStreamSynchronize(c->s));
+  const int64_t cap = need + need / 4 + 4096;
+  void** keep[] = {&c->xp, (void**)&c->vp, (void**)&c->pid, (void**)&c->pcell};
+  const size_t kper[] = {(size_t)3 * c->xbytes, 12, 8, 4};
+  for (int i = 0; i < 4; ++i) {
+    void* nb = nullptr;
+    CK(cudaMalloc(&nb, (size_t)cap * kper[i] + 16));
+    CK(cudaMemcpy(nb, *keep[i], (size_t)c->np * kper[i], cudaMemcpyDeviceToDevice));
+    cudaFree(*keep[i]);
+    *keep[i] = nb;
+  }
+  void** fresh[] = {&c->xp2, (void**)&c->vp2, (void**)&c->pid2, (void**)&c->pcell2, (void**)&c->dest,
+                    (void**)&c->key, (void**)&c->skey, (void**)&c->ssrc};
+  const size_t fper[] = {(size_t)3 * c->xbytes, 12, 8, 4, 4, 8, 8, 4};
+  for (int i = 0; i < 8; ++i) {
+    if (*fresh[i]) cudaFree(*fresh[i]);
+    *fresh[i] = nullptr;
+    CK(cudaMalloc(fresh[i], (size_t)cap * fper[i] + 16));
+  }
+  if (c->pfin) {
+    cudaFree(c->pfin);
+    c->pfin = nullptr;
+    CK(cudaMalloc(&c->pfin, (size_t)cap * sizeof(float4)));
+  }
+  if (c->vtune) cudaFree(c->vtune);
+  c->vtune = nullptr;  // reallocated by the PP tuner when it next runs
+  c->cap = cap;
+  c->xp_base = c->xp;
+  return 0;
+}
+
 int cube_gpu_upload(cube_ctx* c, const void* xp, const float* vp, const int64_t* pid, const int32_t* rhoc,
                     int64_t nplocal) {
   if (!c || !xp || !vp || !pid || !rhoc || nplocal <= 0) return fail(CUBE_E_ARG, "bad upload arguments");
@@ -972,12 +1046,16 @@ int cube_gpu_upload(cube_ctx* c, const void* xp, const float* vp, const int64_t*
   int64_t sum = 0;
   for (int64_t i = 0; i < G.ncells; ++i) {
     if (rhoc[i] < 0) return fail(CUBE_E_ARG, "negative rhoc");
+    if (rhoc[i] && !owned_cell(G, i)) return fail(CUBE_E_ARG, "rhoc holds particles outside this rank's slab");
     sum += rhoc[i];
   }
   if (sum != nplocal) return fail(CUBE_E_COUNT, "sum(rhoc) != nplocal");
   int rc = alloc_particles(c, nplocal);
   if (rc) return rc;
   c->np = nplocal;
+  c->own0 = 0;
+  c->own1 = nplocal;
+  c->ghosts = false;
   after_checkpoint_copy(c);
   CK(cudaMemcpyAsync(c->xp, xp, (size_t)nplocal * 3 * c->xbytes, cudaMemcpyHostToDevice, c->s));
   CK(cudaMemcpyAsync(c->vp, vp, (size_t)nplocal * 12, cudaMemcpyHostToDevice, c->s));
@@ -996,13 +1074,26 @@ int cube_gpu_upload(cube_ctx* c, const void* xp, const float* vp, const int64_t*
 int cube_gpu_download(cube_ctx* c, void* xp, float* vp, int64_t* pid, int32_t* rhoc, int64_t* nplocal) {
   if (!c || !c->loaded) return fail(CUBE_E_STATE, "no particles on device");
   CK(cudaSetDevice(c->device));
-  if (xp) CK(cudaMemcpyAsync(xp, c->xp, (size_t)c->np * 3 * c->xbytes, cudaMemcpyDeviceToHost, c->s));
-  if (vp) CK(cudaMemcpyAsync(vp, c->vp, (size_t)c->np * 12, cudaMemcpyDeviceToHost, c->s));
-  if (pid) CK(cudaMemcpyAsync(pid, c->pid, (size_t)c->np * 8, cudaMemcpyDeviceToHost, c->s));
+  // this rank's particles: all of them with one slab; the store may also hold ghosts
+  const bool slabs = c->G.nslab > 1;
+  const int64_t o = slabs ? c->own0 : 0, n = slabs ? c->own1 - c->own0 : c->np;
+  if (xp) CK(cudaMemcpyAsync(xp, (char*)c->xp + o * 3 * c->xbytes, (size_t)n * 3 * c->xbytes, cudaMemcpyDeviceToHost, c->s));
+  if (vp) CK(cudaMemcpyAsync(vp, c->vp + 3 * o, (size_t)n * 12, cudaMemcpyDeviceToHost, c->s));
+  if (pid) CK(cudaMemcpyAsync(pid, c->pid + o, (size_t)n * 8, cudaMemcpyDeviceToHost, c->s));
   if (rhoc) CK(cudaMemcpyAsync(rhoc, c->rhoc, (size_t)c->G.ncells * 4, cudaMemcpyDeviceToHost, c->s));
   CK(cudaStreamSynchronize(c->s));
-  if (nplocal) *nplocal = c->np;
+  if (rhoc && slabs) {  // ghost cells are other ranks' particles
+    memset(rhoc, 0, (size_t)c->G.c0 * 4);
+    memset(rhoc + c->G.c1, 0, (size_t)(c->G.ncells - c->G.c1) * 4);
+  }
+  if (nplocal) *nplocal = n;
   return 0;
+}
+
+int64_t cube_gpu_nplocal(cube_ctx* c) {
+  if (!c) return fail(CUBE_E_ARG, "null context");
+  if (!c->loaded) return 0;
+  return c->G.nslab > 1 ? c->own1 - c->own0 : c->np;
 }
 
 // Map a device error word to the reference's fatal conditions.
@@ -1088,7 +1179,7 @@ static void enqueue_drift(cube_ctx* c, bool defer_ids) {
   enqueue_huge_sort(c);
   LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp,
                                                                         defer_ids ? nullptr : c->pid, c->sd, c->xp2, c->vp2,
-                                                                        c->pid2, c->pcell2));
+                                                                        c->pid2, c->pcell2, c->cstart2 + G.ncells));
   cudaMemcpyAsync(c->total, c->cstart2 + G.ncells, 8, cudaMemcpyDeviceToDevice, c->s);
 }
 
@@ -1102,6 +1193,147 @@ static void swap_drift(cube_ctx* c) {
   std::swap(c->cstart, c->cstart2);
 }
 
+// ---- runs split into z-slabs (cube_params.nslab > 1) ----
+static int comm_allreduce(cube_ctx* c, void* buf, int64_t count, int dtype, int op, int device) {
+  if (!c->have_comm || !c->comm.allreduce) return fail(CUBE_E_STATE, "nslab > 1 needs cube_gpu_set_comm first");
+  if (device) CK(cudaStreamSynchronize(c->s));
+  const int r = c->comm.allreduce(c->comm.user, buf, count, dtype, op, device);
+  if (r) return fail(CUBE_E_COMM, "cube_comm allreduce returned " + std::to_string(r));
+  return 0;
+}
+
+static int comm_sendrecv(cube_ctx* c, const void* up, int64_t sn_up, const void* down, int64_t sn_down, void* below,
+                         int64_t rn_below, void* above, int64_t rn_above, int device) {
+  if (!c->have_comm || !c->comm.sendrecv) return fail(CUBE_E_STATE, "nslab > 1 needs cube_gpu_set_comm first");
+  if (device) CK(cudaStreamSynchronize(c->s));
+  const int r = c->comm.sendrecv(c->comm.user, up, sn_up, down, sn_down, below, rn_below, above, rn_above, device);
+  if (r) return fail(CUBE_E_COMM, "cube_comm sendrecv returned " + std::to_string(r));
+  return 0;
+}
+
+// The four ghost-exchange layers of this slab: 0 the layer it sends down (its lowest ncb
+// cell layers), 1 the layer it sends up (its highest), 2 its ghosts from below (the slab
+// below's highest layers), 3 its ghosts from above (the slab above's lowest).
+static void slab_layer(const Geo& G, int k, int& tz, int& lz0) {
+  const int L = G.nnt / G.nslab, tlo = G.tile0 / (G.nnt * G.nnt), thi = tlo + L - 1;
+  if (k == 0) {
+    tz = tlo;
+    lz0 = 0;
+  } else if (k == 1) {
+    tz = thi;
+    lz0 = G.nt - G.ncb;
+  } else if (k == 2) {
+    tz = (tlo - 1 + G.nnt) % G.nnt;
+    lz0 = G.nt - G.ncb;
+  } else {
+    tz = (thi + 1) % G.nnt;
+    lz0 = 0;
+  }
+}
+
+// Rebuild the store as this rank's particles plus fresh ghost layers from both neighbours
+// (the buffer_x/buffer_v step of main.f90:36-38); ghosts of an earlier exchange are
+// dropped.  The store keeps the global storage order over the slab's cells and both
+// layers, so every kernel reads a ghost cell like any other.  Host synchronisations: the
+// layer sizes and the new cell starts are read back.
+static int slab_exchange(cube_ctx* c) {
+  const Geo& G = c->G;
+  const int64_t nlay = (int64_t)G.nnt * G.nnt * G.ncb * G.nt * G.nt;
+  int32_t* cnt[4];
+  int64_t* st[4];
+  int tz[4], lz[4];
+  for (int k = 0; k < 4; ++k) {
+    cnt[k] = c->lay_cnt + k * nlay;
+    st[k] = c->lay_start + k * (nlay + 1);
+    slab_layer(G, k, tz[k], lz[k]);
+  }
+  after_checkpoint_copy(c);
+  for (int k = 0; k < 2; ++k) {  // outgoing counts and their prefixes
+    LAUNCH(c, K_SLAB, 1, k_layer_counts<<<nblk(nlay), 256, 0, c->s>>>(G, tz[k], lz[k], nlay, c->rhoc, cnt[k]));
+    LAUNCH(c, K_SLAB, 3, exclusive_scan(cnt[k], st[k], nlay, c->scan_tmp, c->s));
+  }
+  int64_t nout[2] = {0, 0}, nin[2] = {0, 0}, own[2] = {0, 0};
+  CK(cudaMemcpyAsync(&nout[0], st[0] + nlay, 8, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(&nout[1], st[1] + nlay, 8, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(&own[0], c->cstart + G.c0, 8, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(&own[1], c->cstart + G.c1, 8, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  // sizes, counts, then the particles
+  int rc = comm_sendrecv(c, &nout[1], 8, &nout[0], 8, &nin[0], 8, &nin[1], 8, 0);
+  if (!rc) rc = comm_sendrecv(c, cnt[1], nlay * 4, cnt[0], nlay * 4, cnt[2], nlay * 4, cnt[3], nlay * 4, 1);
+  if (rc) return rc;
+  const LayerBuf lb[4] = {layer_buf(nout[0], c->xbytes), layer_buf(nout[1], c->xbytes), layer_buf(nin[0], c->xbytes),
+                          layer_buf(nin[1], c->xbytes)};
+  size_t off[5] = {0, 0, 0, 0, 0};
+  for (int k = 0; k < 4; ++k) off[k + 1] = off[k] + (((size_t)lb[k].bytes + 255) & ~(size_t)255);
+  if (off[4] > c->lay_bytes) {
+    if (c->lay_buf) cudaFree(c->lay_buf);
+    c->lay_buf = nullptr;
+    c->lay_bytes = 0;
+    const size_t want = off[4] + off[4] / 4 + 4096;
+    CK(cudaMalloc(&c->lay_buf, want));
+    c->lay_bytes = want;
+  }
+  for (int k = 0; k < 2; ++k)
+    LAUNCH(c, K_SLAB, 1, k_layer_pack<<<nblk(nlay), 256, 0, c->s>>>(G, tz[k], lz[k], nlay, c->cstart, st[k], c->xp, c->vp,
+                                                                     c->pid, c->lay_buf + off[k], nout[k]));
+  rc = comm_sendrecv(c, c->lay_buf + off[1], lb[1].bytes, c->lay_buf + off[0], lb[0].bytes, c->lay_buf + off[2],
+                     lb[2].bytes, c->lay_buf + off[3], lb[3].bytes, 1);
+  if (rc) return rc;
+  // the new cell counts: the slab's own, then both ghost layers
+  CK(cudaMemsetAsync(c->rhoc2, 0, G.ncells * 4, c->s));
+  CK(cudaMemcpyAsync(c->rhoc2 + G.c0, c->rhoc + G.c0, (size_t)(G.c1 - G.c0) * 4, cudaMemcpyDeviceToDevice, c->s));
+  for (int k = 2; k < 4; ++k) {
+    LAUNCH(c, K_SLAB, 3, exclusive_scan(cnt[k], st[k], nlay, c->scan_tmp, c->s));
+    LAUNCH(c, K_SLAB, 1, k_layer_set_counts<<<nblk(nlay), 256, 0, c->s>>>(G, tz[k], lz[k], nlay, cnt[k], c->rhoc2));
+  }
+  LAUNCH(c, K_SCAN, 3, exclusive_scan(c->rhoc2, c->cstart2, G.ncells, c->scan_tmp, c->s));
+  int64_t total = 0, own0 = 0;
+  CK(cudaMemcpyAsync(&total, c->cstart2 + G.ncells, 8, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(&own0, c->cstart2 + G.c0, 8, cudaMemcpyDeviceToHost, c->s));
+  CK(cudaStreamSynchronize(c->s));
+  const int64_t nown = own[1] - own[0];
+  if (total != nown + nin[0] + nin[1]) return fail(CUBE_E_COUNT, "slab exchange: received counts and particles disagree");
+  rc = grow_particles(c, total);
+  if (rc) return rc;
+  // this rank's particles move as one block; the ghosts go to their cells' starts
+  CK(cudaMemcpyAsync((char*)c->xp2 + own0 * 3 * c->xbytes, (char*)c->xp + own[0] * 3 * c->xbytes,
+                     (size_t)nown * 3 * c->xbytes, cudaMemcpyDeviceToDevice, c->s));
+  CK(cudaMemcpyAsync(c->vp2 + 3 * own0, c->vp + 3 * own[0], (size_t)nown * 12, cudaMemcpyDeviceToDevice, c->s));
+  CK(cudaMemcpyAsync(c->pid2 + own0, c->pid + own[0], (size_t)nown * 8, cudaMemcpyDeviceToDevice, c->s));
+  for (int k = 2; k < 4; ++k)
+    LAUNCH(c, K_SLAB, 1, k_layer_unpack<<<nblk(nlay), 256, 0, c->s>>>(G, tz[k], lz[k], nlay, c->cstart2, st[k],
+                                                                       c->lay_buf + off[k], nin[k - 2], c->xp2, c->vp2,
+                                                                       c->pid2));
+  LAUNCH(c, K_FILL, 1, k_fill_pcell<<<nblk(G.ncells), 256, 0, c->s>>>(c->cstart2, G.ncells, c->pcell2));
+  CK(cudaGetLastError());
+  std::swap(c->xp, c->xp2);
+  std::swap(c->vp, c->vp2);
+  std::swap(c->pid, c->pid2);
+  std::swap(c->pcell, c->pcell2);
+  std::swap(c->rhoc, c->rhoc2);
+  std::swap(c->cstart, c->cstart2);
+  c->np = total;
+  c->own0 = own0;
+  c->own1 = own0 + nown;
+  c->ghosts = true;
+  return 0;
+}
+
+// After a drift of a split run: the store holds only the particles that landed in this
+// slab; the total over the slabs must not change (drift.f90:139-143 checks it per image).
+static int slab_after_drift(cube_ctx* c, int64_t nown_before, int64_t total) {
+  c->np = total;
+  c->own0 = 0;
+  c->own1 = total;
+  c->ghosts = false;
+  int64_t n[2] = {nown_before, total};
+  const int rc = comm_allreduce(c, n, 2, CUBE_DT_I64, CUBE_OP_SUM, 0);
+  if (rc) return rc;
+  if (n[0] != n[1]) return fail(CUBE_E_COUNT, "drift: particle count not conserved over the slabs");
+  return 0;
+}
+
 int cube_gpu_drift(cube_ctx* c, const cube_step_in* in) {
   if (!c || !in) return fail(CUBE_E_ARG, "null argument");
   if (!c->loaded) return fail(CUBE_E_STATE, "drift before upload");
@@ -1109,7 +1341,9 @@ int cube_gpu_drift(cube_ctx* c, const cube_step_in* in) {
   StepDev d;
   int rc = make_scalars(c, in, true, d);
   if (!rc) rc = upload_scalars(c, d);
+  if (!rc && c->G.nslab > 1 && !c->ghosts) rc = slab_exchange(c);
   if (rc) return rc;
+  const int64_t nown = c->own1 - c->own0;
   enqueue_drift(c, false);
   CK(cudaGetLastError());
   swap_drift(c);
@@ -1118,6 +1352,7 @@ int cube_gpu_drift(cube_ctx* c, const cube_step_in* in) {
   rc = check_err(c);
   prof_collect(c);
   if (rc) return rc;
+  if (c->G.nslab > 1) return slab_after_drift(c, nown, total);
   if (total != c->np) return fail(CUBE_E_COUNT, "drift: particle count not conserved");
   return 0;
 }
@@ -1143,13 +1378,25 @@ static int enqueue_kick_a(cube_ctx* c) {
   CK(mark(c, c->ev[0]));
   // ---------------- PM1 (particle_mesh.f90) ----------------
   {
+    // this rank's particles: all of them with one slab; a split run sums the density of
+    // every rank's particles over the whole box (exact in the fixed-point form) and solves
+    // PM1 on each rank
+    const int64_t o = G.nslab > 1 ? c->own0 : 0, npo = G.nslab > 1 ? c->own1 - c->own0 : np;
+    const void* xpo = static_cast<const char*>(c->xp) + o * 3 * c->xbytes;
+    const int32_t* pco = c->pcell + o;
+    float* vpo = c->vp + 3 * o;
     const int n = G.nc;
     MeshPtrs m = mesh_ptrs(c, n, 1, fixed);
     CK(cudaMemsetAsync(m.real, 0, mesh_bytes(c, n, 1, fixed), c->s));
     if (fixed)
-      LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1_runs<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell,
+      LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1_runs<<<nblk(npo), 256, 0, c->s>>>(G, npo, xpo, pco,
                                                                      reinterpret_cast<unsigned long long*>(m.real), m.pt.pr, m.pt.plr, ms1));
-    else LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<false><<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, m.real, m.pt.pr, m.pt.plr, ms1));
+    else LAUNCH(c, K_DEP_PM1, 1, k_deposit_pm1<false><<<nblk(npo), 256, 0, c->s>>>(G, npo, xpo, pco, m.real, m.pt.pr, m.pt.plr, ms1));
+    if (G.nslab > 1) {
+      const int64_t nel = (int64_t)(mesh_bytes(c, n, 1, fixed) / (fixed ? 8 : 4));
+      const int rc = comm_allreduce(c, m.real, nel, fixed ? CUBE_DT_I64 : CUBE_DT_F32, CUBE_OP_SUM, 1);
+      if (rc) return rc;
+    }
     maybe_capture(c, 1, 0, 0, m.real, n, fixed, m.pt.rp, m.pt.psb);
     float* phi = reinterpret_cast<float*>(m.real);
     const float* k1 = kernel_table(c, 1, 0);
@@ -1163,18 +1410,18 @@ static int enqueue_kick_a(cube_ctx* c) {
     if (foff + (size_t)n3 * sizeof(float4) <= c->arena_bytes) {
       float4* force = reinterpret_cast<float4*>(reinterpret_cast<char*>(c->arena) + foff);
       LAUNCH(c, K_INT_PM1, 1, k_force_pm1<<<nblk(n3), 256, 0, c->s>>>(n, phi, m.pt.pf, m.pt.plf, force));
-      LAUNCH(c, K_INT_PM1, 1, k_interp_pm1_force<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, force, c->vp, c->sd));
+      LAUNCH(c, K_INT_PM1, 1, k_interp_pm1_force<<<nblk(npo), 256, 0, c->s>>>(G, npo, xpo, pco, force, vpo, c->sd));
     } else {
-      LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pcell, phi, c->vp, c->sd, m.pt.pf, m.pt.plf));
+      LAUNCH(c, K_INT_PM1, 1, k_interp_pm1<<<nblk(npo), 256, 0, c->s>>>(G, npo, xpo, pco, phi, vpo, c->sd, m.pt.pf, m.pt.plf));
     }
   }
   CK(mark(c, c->ev[1]));
   // ---------------- PM2 (kick.f90:47-77) ----------------
   {
     const int n = G.ngt;
-    const int64_t per = std::min<int64_t>(c->ntiles, boxes_fit(c, n, fixed));
-    for (int t0 = 0; t0 < c->ntiles; t0 += (int)per) {
-      const int nb = (int)std::min<int64_t>(per, c->ntiles - t0);
+    const int64_t per = std::min<int64_t>(G.tile1 - G.tile0, boxes_fit(c, n, fixed));
+    for (int t0 = G.tile0; t0 < G.tile1; t0 += (int)per) {  // this rank's tiles
+      const int nb = (int)std::min<int64_t>(per, G.tile1 - t0);
       MeshPtrs m = mesh_ptrs(c, n, nb, fixed);
       const int64_t boxb = (int64_t)n * m.pt.psb;
       CK(cudaMemsetAsync(m.real, 0, nb * boxb, c->s));
@@ -1197,10 +1444,14 @@ static int enqueue_kick_a(cube_ctx* c) {
   // ---------------- subtile classes (kick.f90:108-138) ----------------
   CK(cudaMemsetAsync(c->napm, 0, 32, c->s));
   LAUNCH(c, K_CLASSIFY, 1, k_classify<<<nblk(c->ns3), 256, 0, c->s>>>(G, c->rhoc, c->ns3, c->ires, c->napm));
+  if (G.nslab > 1) {  // every rank's classes (the PM3 mass needs its neighbours')
+    const int rc = comm_allreduce(c, c->ires, c->ns3, CUBE_DT_I32, CUBE_OP_MAX, 1);
+    if (rc) return rc;
+  }
   if (c->P.pp_queue && c->P.pp_on) {  // the PP tuning class of this step
     CK(cudaMemsetAsync(&c->rdev->maxcount, 0, 4, c->s));
-    LAUNCH(c, K_CLASSIFY, 1, k_ppq_maxcount<<<(unsigned)std::min<int64_t>(nblk(G.ncells), 4 * c->nsm), 256, 0, c->s>>>(
-                                c->cstart, G.ncells, &c->rdev->maxcount));
+    LAUNCH(c, K_CLASSIFY, 1, k_ppq_maxcount<<<(unsigned)std::min<int64_t>(nblk(G.c1 - G.c0), 4 * c->nsm), 256, 0, c->s>>>(
+                                c->cstart, G.c0, G.c1, &c->rdev->maxcount));
   }
   // PM3 mass over the boxes' physical cells, from the classes just found
   if (c->P.pm3_on) {
@@ -1266,7 +1517,8 @@ static int enqueue_lists(cube_ctx* c, const PM3Plan& pl) {
   if (pl.nk == 0) return 0;
   CK(cudaMemsetAsync(c->box_slot, 0xff, (size_t)pl.nk * c->ns3 * 4, c->s));
   CK(cudaMemsetAsync(c->box_sub, 0xff, (size_t)pl.nk * pl.per_max * 4, c->s));
-  LAUNCH(c, K_CLASSIFY, 1, k_build_lists<<<1, 1024, 0, c->s>>>(c->ires, c->ns3, pl, c->box_slot, c->box_sub, c->overflow));
+  LAUNCH(c, K_CLASSIFY, 1, k_build_lists<<<1, 1024, 0, c->s>>>(c->ires, c->ns3, c->G.s0, c->G.s1, pl, c->box_slot,
+                                                               c->box_sub, c->overflow));
   return 0;
 }
 
@@ -1352,9 +1604,9 @@ static void enqueue_ppq(cube_ctx* c, const PPShape& sh, float* vout, float* f2, 
   LAUNCH(c, K_PP, 1, k_ppq_light<<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->pcell, c->cstart, c->ires, c->pfin, c->vp, vout,
                                                                   c->sd, sh.T, f2, vm, pairs, pairs + 1, abort));
   cudaMemsetAsync(c->ppq, 0, PPQ_Q * 4, c->s);
-  LAUNCH(c, K_PP, 1, k_ppq_bucket_count<<<nblk(G.ncells), 256, 0, c->s>>>(c->cstart, G.ncells, sh.T, c->ppq));
+  LAUNCH(c, K_PP, 1, k_ppq_bucket_count<<<nblk(G.c1 - G.c0), 256, 0, c->s>>>(c->cstart, G.c0, G.c1, sh.T, c->ppq));
   LAUNCH(c, K_PP, 1, k_ppq_bucket_scan<<<1, 32, 0, c->s>>>(c->ppq));
-  LAUNCH(c, K_PP, 1, k_ppq_bucket_fill<<<nblk(G.ncells), 256, 0, c->s>>>(c->cstart, G.ncells, sh.T, c->ppq, c->hlist));
+  LAUNCH(c, K_PP, 1, k_ppq_bucket_fill<<<nblk(G.c1 - G.c0), 256, 0, c->s>>>(c->cstart, G.c0, G.c1, sh.T, c->ppq, c->hlist));
   LAUNCH(c, K_PP, 1, k_ppq_items<<<1, 1024, 0, c->s>>>(c->hlist, c->cstart, sh.B, c->ppq, c->hpre));
   const unsigned grid = (unsigned)(c->nsm * std::max(1, 1024 / sh.B));
   const size_t sm = (size_t)sh.J * sizeof(float4);
@@ -1458,7 +1710,8 @@ static void enqueue_pp_and_momentum(cube_ctx* c, const unsigned* abort, const PP
                                                                      c->sd, f2 + 3, vm + 6, c->pairs, c->pairs + 1, abort));
   }
   mark(c, c->ev[4]);
-  LAUNCH(c, K_MOMENTUM, 1, k_momentum<<<MOM_BLOCKS, MOM_THREADS, 0, c->s>>>(c->vp, np, c->mom));
+  const int64_t o = G.nslab > 1 ? c->own0 : 0, npo = G.nslab > 1 ? c->own1 - c->own0 : np;
+  LAUNCH(c, K_MOMENTUM, 1, k_momentum<<<MOM_BLOCKS, MOM_THREADS, 0, c->s>>>(c->vp + 3 * o, npo, c->mom));
 }
 
 // cube_step_out from the step results in c->rhost.
@@ -1482,7 +1735,7 @@ static void fill_out(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
   out->dt_vmax = 0.9f * 14 / vmx;  // kick.f90:314
   out->vz_max = v[2];
   for (int i = 0; i < 8; ++i) out->napm[i] = R.napm[i];
-  out->nplocal = c->np;
+  out->nplocal = c->G.nslab > 1 ? c->own1 - c->own0 : c->np;
   out->pp_pairs = (int64_t)R.pairs;
   out->pp_candidates = (int64_t)R.cand;
   float ms;
@@ -1524,8 +1777,12 @@ static void fill_out(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
 
 // The kick (kick.f90:1-353) eagerly: PM1 and PM2, the classes read back, PM3 over exact
 // class lists, PP, and the results read back (two host synchronisations).
+static int slab_reduce_out(cube_ctx* c, const cube_step_in* in, cube_step_out* out);
+
 static int kick_eager(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
-  int rc = enqueue_kick_a(c);
+  int rc = 0;
+  if (c->G.nslab > 1 && !c->ghosts) rc = slab_exchange(c);  // ghosts with this step's positions
+  if (!rc) rc = enqueue_kick_a(c);
   if (rc) return rc;
   CK(cudaMemcpyAsync(c->h_ires, c->ires, c->ns3 * 4, cudaMemcpyDeviceToHost, c->s));
   CK(cudaMemcpyAsync(c->rhost->napm, c->napm, 36, cudaMemcpyDeviceToHost, c->s));  // napm and maxcount
@@ -1557,7 +1814,47 @@ static int kick_eager(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     CK(cudaStreamSynchronize(c->s));
     return err_code(c->rhost->err);
   }
+  if (c->G.nslab > 1) {
+    c->ghosts = false;  // the ghosts' velocities are their owners' business, stale now
+    cube_step_out local;
+    cube_step_out* o = out ? out : &local;  // every rank takes part in the reductions
+    fill_out(c, in, o);
+    return slab_reduce_out(c, in, o);
+  }
   if (out) fill_out(c, in, out);
+  return 0;
+}
+
+// The step results over all ranks of a split run (kick.f90:316-346 reduces the dt
+// criteria over images): maxima of the f2max and |v| values, sums of the PP pair counts,
+// the level masses and the momentum; the dt criteria from the global maxima.
+static int slab_reduce_out(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
+  float mx[8] = {out->f2max_pm1, out->f2max_pm2, out->f2max_pm3, out->f2max_pp, out->vmax[0], out->vmax[1],
+                 out->vmax[2], 0.f};
+  int64_t si[2] = {out->pp_pairs, out->pp_candidates};
+  double sd[6] = {out->mass_pm1, out->mass_pm2, out->mass_pm3, out->momentum[0], out->momentum[1], out->momentum[2]};
+  int rc = comm_allreduce(c, mx, 8, CUBE_DT_F32, CUBE_OP_MAX, 0);
+  if (!rc) rc = comm_allreduce(c, si, 2, CUBE_DT_I64, CUBE_OP_SUM, 0);
+  if (!rc) rc = comm_allreduce(c, sd, 6, CUBE_DT_F64, CUBE_OP_SUM, 0);
+  if (rc) return rc;
+  const float a_mid = in->a_mid;
+  out->f2max_pm1 = mx[0];
+  out->f2max_pm2 = mx[1];
+  out->f2max_pm3 = mx[2];
+  out->f2max_pp = mx[3];
+  out->dt_pm1 = dt_crit(0.5f, mx[0], a_mid);
+  out->dt_pm2 = dt_crit(0.5f, mx[1], a_mid);
+  out->dt_pm3 = dt_crit(0.5f, mx[2], a_mid);
+  out->dt_pp = dt_crit(0.05f, mx[3], a_mid);
+  for (int d = 0; d < 3; ++d) out->vmax[d] = mx[4 + d];
+  out->dt_vmax = 0.9f * 14 / std::max(mx[4], std::max(mx[5], mx[6]));
+  out->vz_max = mx[6];
+  out->pp_pairs = si[0];
+  out->pp_candidates = si[1];
+  out->mass_pm1 = sd[0];
+  out->mass_pm2 = sd[1];
+  out->mass_pm3 = sd[2];
+  for (int d = 0; d < 3; ++d) out->momentum[d] = sd[3 + d];
   return 0;
 }
 
@@ -1611,7 +1908,7 @@ static int step_graph(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
     if (c->maxcount_est < 0) {  // occupancy of the current state
       CK(cudaMemsetAsync(&c->rdev->maxcount, 0, 4, c->s));
       k_ppq_maxcount<<<(unsigned)std::min<int64_t>(nblk(c->G.ncells), 4 * c->nsm), 256, 0, c->s>>>(
-          c->cstart, c->G.ncells, &c->rdev->maxcount);
+          c->cstart, c->G.c0, c->G.c1, &c->rdev->maxcount);
       ++c->launches;
       CK(cudaMemcpyAsync(&c->maxcount_est, &c->rdev->maxcount, 4, cudaMemcpyDeviceToHost, c->s));
       CK(cudaStreamSynchronize(c->s));
@@ -1727,14 +2024,34 @@ int cube_gpu_step(cube_ctx* c, const cube_step_in* in, cube_step_out* out) {
   if (!c || !in) return fail(CUBE_E_ARG, "null argument");
   if (!c->loaded) return fail(CUBE_E_STATE, "step before upload");
   CK(cudaSetDevice(c->device));
-  // graph replay unless a test capture is armed (it copies with host-side allocations)
-  if (c->P.step_graph && c->cap_level == 0) return step_graph(c, in, out);
+  // graph replay unless a test capture is armed (it copies with host-side allocations); a
+  // split run steps eagerly (its collectives run on the host between the stages)
+  if (c->P.step_graph && c->cap_level == 0 && c->G.nslab == 1) return step_graph(c, in, out);
   StepDev d;
   int rc = make_scalars(c, in, true, d);
   if (!rc) rc = upload_scalars(c, d);
   if (rc) return rc;
   // ev[5]: step start, ev[6]: drift end, ev[7]: step end (all on the context stream)
   CK(cudaEventRecord(c->ev[5], c->s));
+  if (c->G.nslab > 1) {  // ghosts, drift, the count check over the slabs, then the kick
+    if (!c->ghosts) rc = slab_exchange(c);
+    if (rc) return rc;
+    const int64_t nown = c->own1 - c->own0;
+    enqueue_drift(c, false);
+    CK(cudaGetLastError());
+    swap_drift(c);
+    CK(cudaEventRecord(c->ev[6], c->s));
+    int64_t total = 0;
+    CK(cudaMemcpyAsync(&total, c->total, 8, cudaMemcpyDeviceToHost, c->s));
+    CK(cudaStreamSynchronize(c->s));
+    rc = slab_after_drift(c, nown, total);
+    if (!rc) rc = kick_eager(c, in, out);
+    CK(cudaEventRecord(c->ev[7], c->s));
+    CK(cudaEventSynchronize(c->ev[7]));
+    if (rc) return rc;
+    if (out) step_times(c, out);
+    return 0;
+  }
   enqueue_drift(c, false);
   CK(cudaGetLastError());
   swap_drift(c);
@@ -1761,6 +2078,8 @@ int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, 
   if (!c || !in || !xp || !vp || !pid || !rhoc || nplocal <= 0) return fail(CUBE_E_ARG, "bad step_host arguments");
   CK(cudaSetDevice(c->device));
   const Geo& G = c->G;
+  if (G.nslab > 1)  // the arrays hold nplocal particles, and a split run's count changes in the step
+    return fail(CUBE_E_ARG, "cube_gpu_step_host takes nslab = 1; split runs use upload, step and download");
   if (!c->s2) {
     CK(cudaStreamCreateWithFlags(&c->s2, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&c->ev_up, cudaEventDisableTiming));
@@ -1915,6 +2234,7 @@ int cube_gpu_captured(cube_ctx* c, float* out, int64_t n) {
 
 int cube_gpu_ic(cube_ctx* c, const cube_ic_in* in, cube_ic_out* out) {
   if (!c || !in || !in->pk_k || !in->pk_p || in->npk < 2 || in->nic < 1) return fail(CUBE_E_ARG, "bad IC arguments");
+  if (c->G.nslab > 1) return fail(CUBE_E_ARG, "cube_gpu_ic generates the whole box: nslab must be 1");
   CK(cudaSetDevice(c->device));
   const Geo& G = c->G;
   const int nw = in->nic * G.ng;
@@ -1992,7 +2312,7 @@ int cube_gpu_ic(cube_ctx* c, const cube_ic_in* in, cube_ic_out* out) {
   c->np = np;
   CK(cudaMemsetAsync(c->sd, 0, sizeof(StepDev), c->s));  // dt_mid = 0: the gather only sorts
   LAUNCH(c, K_DRIFT_GATHER, 1, k_drift_gather<<<nblk(np), 256, 0, c->s>>>(G, np, c->ssrc, c->dest, c->xp, c->vp, c->pid, c->sd,
-                                                                         c->xp2, c->vp2, c->pid2, c->pcell2));
+                                                                         c->xp2, c->vp2, c->pid2, c->pcell2, nullptr));
   CK(cudaGetLastError());
   rc = check_err(c);
   cudaFree(gtab);
@@ -2127,8 +2447,10 @@ int cube_gpu_checkpoint_async(cube_ctx* c, const cube_ckpt_files* files, const v
     CK(cudaEventCreateWithFlags(&c->ev_ckpt, cudaEventDisableTiming));
   }
   const Geo& G = c->G;
-  const size_t bx = (size_t)c->np * 3 * c->xbytes, bv = (size_t)c->np * 12, bn = (size_t)G.ncells * 4,
-               bi = (size_t)c->np * 8;
+  // this rank's particles (a split run's store may also hold ghosts)
+  const bool slabs = G.nslab > 1;
+  const int64_t o = slabs ? c->own0 : 0, n = slabs ? c->own1 - c->own0 : c->np;
+  const size_t bx = (size_t)n * 3 * c->xbytes, bv = (size_t)n * 12, bn = (size_t)G.ncells * 4, bi = (size_t)n * 8;
   const size_t need = bx + bv + bn + bi + 64;
   if (need > c->ck_bytes) {
     if (c->ck_host) cudaFreeHost(c->ck_host);
@@ -2144,10 +2466,10 @@ int cube_gpu_checkpoint_async(cube_ctx* c, const cube_ckpt_files* files, const v
   // the state as the context stream leaves it, copied on the side stream
   CK(cudaEventRecord(c->ev_ckpt, c->s));
   CK(cudaStreamWaitEvent(c->s3, c->ev_ckpt, 0));
-  CK(cudaMemcpyAsync(hx, c->xp, bx, cudaMemcpyDeviceToHost, c->s3));
-  CK(cudaMemcpyAsync(hv, c->vp, bv, cudaMemcpyDeviceToHost, c->s3));
+  CK(cudaMemcpyAsync(hx, (char*)c->xp + o * 3 * c->xbytes, bx, cudaMemcpyDeviceToHost, c->s3));
+  CK(cudaMemcpyAsync(hv, c->vp + 3 * o, bv, cudaMemcpyDeviceToHost, c->s3));
   CK(cudaMemcpyAsync(hn, c->rhoc, bn, cudaMemcpyDeviceToHost, c->s3));
-  CK(cudaMemcpyAsync(hi, c->pid, bi, cudaMemcpyDeviceToHost, c->s3));
+  CK(cudaMemcpyAsync(hi, c->pid + o, bi, cudaMemcpyDeviceToHost, c->s3));
   CK(cudaEventRecord(c->ev_ckpt, c->s3));
   c->ckpt_pending = true;
   struct Part {
@@ -2162,13 +2484,18 @@ int cube_gpu_checkpoint_async(cube_ctx* c, const cube_ckpt_files* files, const v
   cudaEvent_t ev = c->ev_ckpt;
   c->ck_status = 0;
   c->ck_error.clear();
-  c->ck_thread = std::thread([c, parts, hdr, dev, ev]() mutable {
+  const int64_t c0 = G.c0, c1 = G.c1, ncells = G.ncells;
+  c->ck_thread = std::thread([c, parts, hdr, dev, ev, slabs, hn, c0, c1, ncells]() mutable {
     parts[0].data = hdr.data();  // the caller's header may go away once the call returns
     cudaSetDevice(dev);
     if (cudaEventSynchronize(ev) != cudaSuccess) {
       c->ck_status = CUBE_E_CUDA;
       c->ck_error = "checkpoint copies failed";
       return;
+    }
+    if (slabs) {  // ghost cells are other ranks' particles
+      memset(hn, 0, (size_t)c0 * 4);
+      memset(hn + c1 * 4, 0, (size_t)(ncells - c1) * 4);
     }
     for (const Part& p : parts) {
       FILE* f = fopen(p.path.c_str(), "wb");
@@ -2220,6 +2547,35 @@ int cube_gpu_kernel_table(cube_ctx* c, int level, int iapm, float* out, int64_t 
   CK(cudaStreamSynchronize(c->s));
   CK(cudaMemcpy(out, src, cnt * 4, cudaMemcpyDeviceToHost));
   return 0;
+}
+
+int cube_gpu_set_comm(cube_ctx* c, const cube_comm* comm) {
+  if (!c || !comm || !comm->allreduce || !comm->sendrecv) return fail(CUBE_E_ARG, "cube_gpu_set_comm: null callback");
+  c->comm = *comm;
+  c->have_comm = true;
+  return 0;
+}
+
+int64_t cube_slab_cells(const cube_params* p, int which, int64_t* out, int64_t n) {
+  if (!p || which < 0 || which > 4 || n < 0) return fail(CUBE_E_ARG, "bad cube_slab_cells arguments");
+  if (p->ratio_cs <= 0 || p->nnt <= 0 || p->ng % p->ratio_cs || (p->ng / p->ratio_cs) % p->nnt)
+    return fail(CUBE_E_ARG, "ng, ratio_cs, nnt must divide evenly");
+  const int nslab = p->nslab > 1 ? p->nslab : 1;
+  if (p->nnt % nslab || (nslab > 1 && (p->slab < 0 || p->slab >= nslab)))
+    return fail(CUBE_E_ARG, "nslab must divide nnt, and 0 <= slab < nslab");
+  const Geo G = make_geo(*p);
+  if (G.ncb > G.nt) return fail(CUBE_E_ARG, "ghost layers deeper than a tile");
+  if (which == 0) {
+    const int64_t m = G.c1 - G.c0;
+    for (int64_t i = 0; i < m && i < n && out; ++i) out[i] = G.c0 + i;
+    return m;
+  }
+  if (nslab == 1) return 0;  // one slab: periodic, no layers to exchange
+  int tz, lz0;
+  slab_layer(G, which - 1, tz, lz0);
+  const int64_t nlay = (int64_t)G.nnt * G.nnt * G.ncb * G.nt * G.nt;
+  for (int64_t i = 0; i < nlay && i < n && out; ++i) out[i] = layer_cell(G, tz, lz0, i);
+  return nlay;
 }
 
 int cube_gpu_subtile_class(cube_ctx* c, int32_t* ires, int64_t n) {
@@ -2414,6 +2770,7 @@ extern "C" int cube_gpu_power(cube_ctx* c, const cube_power_in* in, float* xi, i
                               cube_power_out* out) {
   if (!c || !in || !xi) return fail(CUBE_E_ARG, "null argument");
   if (!c->loaded) return fail(CUBE_E_STATE, "power spectrum before upload");
+  if (c->G.nslab > 1) return fail(CUBE_E_ARG, "cube_gpu_power needs the whole box: nslab must be 1");
   const int nw = in->nw;
   if (nw < 16 || nw > 4096 || !smooth23(nw) || nw % 2)
     return fail(CUBE_E_ARG, "nw must be an even 2^a 3^b size in 16..4096");

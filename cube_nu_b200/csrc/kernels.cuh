@@ -166,6 +166,10 @@ __global__ void k_drift_dest(Geo G, int64_t np, const void* __restrict__ xp, con
     }
   }
   const int64_t dc = cell_index(G, dst[0], dst[1], dst[2]);
+  if (!owned_cell(G, dc)) {  // lands in another rank's slab, which keeps it
+    dest[ip] = -1;
+    return;
+  }
   const uint64_t kz = (uint64_t)(rel[2] + G.ncb), ky = (uint64_t)(rel[1] + G.ncb), kx = (uint64_t)(rel[0] + G.ncb);
   const uint64_t il = kz % (uint64_t)nlayer;
   // l < 2^24: a cell holds fewer particles than the capacity check on upload allows
@@ -376,9 +380,11 @@ __global__ void k_drift_copy_huge(const int32_t* __restrict__ hugelist, const in
 __global__ void k_drift_gather(Geo G, int64_t np, const uint32_t* __restrict__ ssrc, const int32_t* __restrict__ dest,
                                const void* __restrict__ xp, const float* __restrict__ vp,
                                const int64_t* __restrict__ pid, const StepDev* __restrict__ sd, void* __restrict__ xo,
-                               float* __restrict__ vo, int64_t* __restrict__ po, int32_t* __restrict__ pcell_o) {
+                               float* __restrict__ vo, int64_t* __restrict__ po, int32_t* __restrict__ pcell_o,
+                               const int64_t* __restrict__ ntot) {
+  // ntot: particles the drift kept (fewer than np when some left this rank's slab)
   const int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (pos >= np) return;
+  if (pos >= (ntot ? *ntot : np)) return;
   const float dt_mid = sd->dt_mid;
   const int64_t src = ssrc[pos];
 #pragma unroll
@@ -776,7 +782,7 @@ __global__ void __launch_bounds__(256) k_mass_pm3(Geo G, const int64_t* __restri
   int g[3], tc[3][2], uc[3][2], lc[3][2], nca[3] = {1, 1, 1};
   bool any = false;
   int own = 0;
-  if (cell < G.ncells) {
+  if (cell < G.ncells && owned_cell(G, cell)) {
     cell_coords(G, cell, g[0], g[1], g[2]);
 #pragma unroll
     for (int d = 0; d < 3; ++d) nca[d] = sub_cands(G, g[d], tc[d], uc[d], lc[d]);
@@ -1474,6 +1480,10 @@ __global__ void k_classify(Geo G, const int32_t* __restrict__ rhoc, int ns3, int
                            int32_t* __restrict__ napm) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns3) return;
+  if (s < G.s0 || s >= G.s1) {  // another rank's subtile: its class arrives by a max-reduction
+    ires[s] = 0;
+    return;
+  }
   const int nns3 = G.nns * G.nns * G.nns;
   const int T = s / nns3, f = s - T * nns3;
   const int tx = T % G.nnt, ty = (T / G.nnt) % G.nnt, tz = T / (G.nnt * G.nnt);
@@ -1507,13 +1517,14 @@ struct PM3Plan {
 // list k); both arrays arrive filled with -1.  *overflow is set when a class has more
 // subtiles than skip + capacity (the ones beyond are not listed).  One block of 1024
 // threads; thread t owns a contiguous run of subtiles, so ranks follow subtile order.
-__global__ void __launch_bounds__(1024) k_build_lists(const int32_t* __restrict__ ires, int ns3, PM3Plan pl,
-                                                      int32_t* __restrict__ box_slot, int32_t* __restrict__ box_sub,
-                                                      unsigned* __restrict__ overflow) {
+__global__ void __launch_bounds__(1024) k_build_lists(const int32_t* __restrict__ ires, int ns3, int s_lo, int s_hi,
+                                                      PM3Plan pl, int32_t* __restrict__ box_slot,
+                                                      int32_t* __restrict__ box_sub, unsigned* __restrict__ overflow) {
   __shared__ int sc[4][1024];
   const int T = blockDim.x, tid = threadIdx.x;
-  const int per_t = (ns3 + T - 1) / T;
-  const int s0 = min(ns3, tid * per_t), s1 = min(ns3, s0 + per_t);
+  const int nown = s_hi - s_lo;  // this rank's subtiles [s_lo, s_hi)
+  const int per_t = (nown + T - 1) / T;
+  const int s0 = s_lo + min(nown, tid * per_t), s1 = s_lo + min(nown, tid * per_t + per_t);
   int cnt[4] = {0, 0, 0, 0};
   for (int s = s0; s < s1; ++s) cnt[(ires[s] - 2) & 3] += 1;
 #pragma unroll
@@ -1583,7 +1594,7 @@ __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32
   const float mass_scale = sd->pp_mass, v_scale = sd->pp_vscale;
   // abort: the class lists of a captured step were too short; PM3 is finished for the
   // unlisted subtiles afterwards and PP must follow it, so PP leaves vp alone here
-  const bool live = ip0 < np && !(abort && *abort);
+  const bool live = ip0 < np && !(abort && *abort) && owned_cell(G, pcell[ip0]);
   const int64_t ip = live ? ip0 : np - 1;
   int g[3];
   cell_coords(G, pcell[ip], g[0], g[1], g[2]);

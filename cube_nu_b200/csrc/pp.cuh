@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(128) k_ppq_light(Geo G, int64_t np, const int3
   int c = 0;
   if (live) {
     c = pcell[ip];
-    live = cstart[c + 1] - cstart[c] <= heavy_t;
+    live = owned_cell(G, c) && cstart[c + 1] - cstart[c] <= heavy_t;
   }
   float f2 = 0.f, av[3] = {0.f, 0.f, 0.f};
   PPi P;
@@ -158,10 +158,11 @@ constexpr int PPQ_Q = 72;
 // bucket of a count n >= 1: floor(log2 n), 0..31
 __device__ __forceinline__ int ppq_bucket(int64_t n) { return 63 - __clzll((unsigned long long)n); }
 
-__global__ void k_ppq_bucket_count(const int64_t* __restrict__ cstart, int64_t ncells, int heavy_t,
+// Cells [c0, c1): this rank's slab.
+__global__ void k_ppq_bucket_count(const int64_t* __restrict__ cstart, int64_t c0, int64_t c1, int heavy_t,
                                    int* __restrict__ q) {
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncells) return;
+  const int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= c1) return;
   const int64_t n = cstart[c + 1] - cstart[c];
   if (n > heavy_t) atomicAdd(&q[ppq_bucket(n)], 1);
 }
@@ -177,10 +178,10 @@ __global__ void k_ppq_bucket_scan(int* __restrict__ q) {
   q[64] = off;
 }
 
-__global__ void k_ppq_bucket_fill(const int64_t* __restrict__ cstart, int64_t ncells, int heavy_t, int* __restrict__ q,
-                                  int32_t* __restrict__ hlist) {
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncells) return;
+__global__ void k_ppq_bucket_fill(const int64_t* __restrict__ cstart, int64_t c0, int64_t c1, int heavy_t,
+                                  int* __restrict__ q, int32_t* __restrict__ hlist) {
+  const int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= c1) return;
   const int64_t n = cstart[c + 1] - cstart[c];
   if (n > heavy_t) hlist[atomicAdd(&q[32 + ppq_bucket(n)], 1)] = (int32_t)c;
 }
@@ -289,10 +290,11 @@ __global__ void k_ppq_heavy(Geo G, const int32_t* __restrict__ hlist, const int*
   if ((threadIdx.x & 31) == 0 && tc) atomicAdd(ncand, tc);
 }
 
-// Largest cell occupancy (the autotuner's class key), one atomicMax per block.
-__global__ void k_ppq_maxcount(const int64_t* __restrict__ cstart, int64_t ncells, int* __restrict__ out) {
+// Largest occupancy of the cells [c0, c1) (the autotuner's class key), one atomicMax per
+// block.
+__global__ void k_ppq_maxcount(const int64_t* __restrict__ cstart, int64_t c0, int64_t c1, int* __restrict__ out) {
   int m = 0;
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += (int64_t)gridDim.x * blockDim.x)
+  for (int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += (int64_t)gridDim.x * blockDim.x)
     m = max(m, (int)(cstart[c + 1] - cstart[c]));
   for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);

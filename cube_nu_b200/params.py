@@ -42,7 +42,9 @@ class CParams(ctypes.Structure):
         ("max_segment", ctypes.c_int32),
         ("step_graph", ctypes.c_int32),
         ("pp_queue", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("nslab", ctypes.c_int32),
+        ("slab", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
 
@@ -73,6 +75,8 @@ class Params:
     max_segment: int = 0
     step_graph: bool = False  # cube_gpu_step replays each step as one captured CUDA graph
     pp_queue: bool = False    # PP as an autotuned work queue over cells (chosen form)
+    nslab: int = 1            # z-slabs of tile layers the box is split into, one rank each
+    slab: int = 0             # this rank's slab
     # cosmology (parameters.f90:101-125; values of the benchmark configs)
     h0: float = 0.6817
     omega_c: float = 0.2532
@@ -153,6 +157,8 @@ class Params:
             raise ValueError("izipx must be 1 or 2")
         if self.nt < self.ncb:
             raise ValueError("tiles must be at least ncb coarse cells wide")
+        if self.nslab < 1 or self.nnt % self.nslab or not 0 <= self.slab < self.nslab:
+            raise ValueError("nslab must divide nnt, and 0 <= slab < nslab")
 
     def to_c(self) -> CParams:
         self.validate()
@@ -163,7 +169,7 @@ class Params:
             apm1c=self.apm1c, apm2=self.apm2, apm3f=self.apm3f,
             mass_p_cdm=self.particle_mass(), f_nu=self.f_nu, np_capacity=self.np_capacity,
             max_segment=self.max_segment, step_graph=int(self.step_graph), pp_queue=int(self.pp_queue),
-            reserved=0,
+            nslab=self.nslab, slab=self.slab,
         )
 
 

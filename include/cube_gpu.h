@@ -1,5 +1,6 @@
 /*
- * cube_gpu.h -- C ABI of the B200 P3M gravity step for one CUBE image (nn=1).
+ * cube_gpu.h -- C ABI of the B200 P3M gravity step of CUBE: one image (nn=1), or
+ * the box split into z-slabs over ranks (cube_params.nslab).
  *
  * The reference drives its step with zero-argument Fortran subroutines that share
  * module globals (main.f90:33-38: timestep, drift, buffer_grid, buffer_x, kick,
@@ -39,6 +40,7 @@ extern "C" {
 #define CUBE_E_COUNT (-5)      /* particle count not conserved (drift.f90:139-143)         */
 #define CUBE_E_STATE (-6)      /* call out of order (e.g. step before upload)              */
 #define CUBE_E_TIMEOUT (-7)    /* a bounded device-side wait gave up                       */
+#define CUBE_E_COMM (-8)       /* a cube_comm callback failed (nslab > 1)                   */
 
 /* Device error-word bits (set by kernels, read back by the host after a step). */
 #define CUBE_DEVERR_DRIFT_RANGE 0x1u
@@ -82,7 +84,11 @@ typedef struct cube_params {
   int32_t step_graph;  /* 1: cube_gpu_step replays each step as one captured CUDA graph   */
   int32_t pp_queue;    /* 1: PP as an autotuned work queue over cells (needs int8 codes, or
                           int16 with nt < 127); 0: one thread per particle                 */
-  int32_t reserved;
+  int32_t nslab;       /* z-slabs the periodic box is split into, one rank each (0 or 1: one
+                          rank holds the whole box); nnt must be a multiple of nslab      */
+  int32_t slab;        /* this rank's slab: tile layers [slab*L, (slab+1)*L) along z with
+                          L = nnt/nslab; every other coarse cell is another rank's        */
+  int32_t reserved[3];
 } cube_params;
 
 /* Per-step scalars chosen by the host timestep (timestep.f90:4-110). */
@@ -131,6 +137,9 @@ int cube_gpu_upload(cube_ctx* ctx, const void* xp, const float* vp, const int64_
 /* Copy particles out (checkpoint.f90:24-33). `nplocal` receives the count. */
 int cube_gpu_download(cube_ctx* ctx, void* xp, float* vp, int64_t* pid, int32_t* rhoc,
                       int64_t* nplocal);
+/* Particles the context holds for its rank (sim%nplocal), the count a download returns;
+ * negative on error. */
+int64_t cube_gpu_nplocal(cube_ctx* ctx);
 
 /* Zel'dovich initial conditions generated on the device (utilities/ic.f90), left as the
  * context's particle state (replaces reading the IC checkpoint).  The noise comes from
@@ -315,6 +324,61 @@ int cube_gpu_subtile_class(cube_ctx* ctx, int32_t* ires, int64_t n);
 #define CUBE_NOALLOC_MAX_PARTICLES 2097152  /* 2^21 particles    */
 int cube_gpu_pm1_density_noalloc(const cube_params* p, const void* xp, const int32_t* rhoc, int64_t np,
                                  float* rho, void* stream);
+
+/*
+ * Runs split over ranks (cube_params.nslab > 1).  The reference decomposes the box into
+ * nn^3 images that exchange ncb-deep ghost layers of particles (buffer_particle.f90:29-375,
+ * buffer_x / buffer_v in main.f90:36-38), transpose PM1 pencils (pencil_fft.f90:81-325) and
+ * reduce the dt criteria over images (kick.f90:316-346).  Here the box is split along z
+ * into nslab slabs of whole tile layers, one rank each.  A rank holds its own particles
+ * plus ghost copies of the ncb coarse-cell layers next to its slab (refreshed before each
+ * drift and each kick), runs PM2, PM3 and PP on its own tiles, drifts its own and ghost
+ * particles and keeps the ones that land in its slab, and reduces the PM1 density over
+ * ranks before a replicated PM1 solve.  With CUBE_DEPOSIT_FIXED every rank's particles end
+ * up bit-identical to the nslab = 1 run of the whole box (integer sums do not depend on
+ * their order); cube_step_out holds the global reductions on every rank (maxima, and sums
+ * of pairs, masses and momentum; nplocal and napm stay per rank).
+ *
+ * The host supplies the two collectives through cube_comm (MPI, NCCL through
+ * torch.distributed, ...).  Every rank makes the same library calls in the same order, so
+ * the collectives match; a callback returning non-zero fails the call with CUBE_E_COMM.
+ *  allreduce: in place over all ranks, `count` elements of `dtype` (CUBE_DT_*) with `op`
+ *    (CUBE_OP_*).  device = 1: `buf` is device memory of the context's GPU (the library
+ *    has synchronised its stream and reads the result when the call returns); 0: host.
+ *  sendrecv: with the slab below (slab-1 mod nslab) and the slab above (slab+1 mod nslab):
+ *    send `up` (sn_up bytes) to the slab above and `down` to the slab below; receive into
+ *    `from_below` what the slab below sent up (rn_below bytes) and into `from_above` what
+ *    the slab above sent down.  Sizes agree pairwise (the library exchanges them first);
+ *    a zero-byte message may be skipped by both sides.  With nslab = 2 both neighbours
+ *    are one rank: post the sends in the order up, down and the receives in the order
+ *    from_below, from_above, so that messages pair up in order.
+ * cube_gpu_set_comm copies the struct; it must be set before the first drift or kick of a
+ * run with nslab > 1.  Such runs step eagerly (cube_params.step_graph is ignored), and
+ * cube_gpu_ic and cube_gpu_power do not take them.  Upload and download carry the rank's
+ * own particles: rhoc is the global array with zeros outside the slab.
+ */
+#define CUBE_DT_F32 0
+#define CUBE_DT_I64 1
+#define CUBE_DT_F64 2
+#define CUBE_DT_I32 3
+#define CUBE_OP_SUM 0
+#define CUBE_OP_MAX 1
+typedef struct cube_comm {
+  void* user;
+  int (*allreduce)(void* user, void* buf, int64_t count, int32_t dtype, int32_t op, int32_t device);
+  int (*sendrecv)(void* user, const void* up, int64_t sn_up, const void* down, int64_t sn_down,
+                  void* from_below, int64_t rn_below, void* from_above, int64_t rn_above,
+                  int32_t device);
+} cube_comm;
+int cube_gpu_set_comm(cube_ctx* ctx, const cube_comm* comm);
+
+/* Coarse-cell sets of slab p->slab of p->nslab as global storage indices of rhoc (the
+ * order above), ascending; host arithmetic only, no device needed.  which: 0 the slab's
+ * own cells, 1 the layer it sends down (its lowest ncb cell layers), 2 the layer it sends
+ * up (its highest ncb), 3 its ghost layer from below (the slab below's highest ncb
+ * layers), 4 its ghost layer from above.  Writes at most n indices (out may be NULL) and
+ * returns the size of the set, or a negative CUBE_E_* code. */
+int64_t cube_slab_cells(const cube_params* p, int which, int64_t* out, int64_t n);
 
 /*
  * Differentiable particle-mesh step, for the adjoint (the PyTorch binding
