@@ -73,15 +73,27 @@ __host__ __device__ inline int64_t cell_index(const Geo& G, int gx, int gy, int 
   return ((((int64_t)(tz * G.nnt + ty) * G.nnt + tx) * G.nt + lz) * G.nt + ly) * G.nt + lx;
 }
 
-// Inverse of cell_index: global coarse cell coordinates (0-based).
+// Inverse of cell_index: global coarse cell coordinates (0-based).  In 32-bit unsigned
+// arithmetic: contexts hold fewer than 2^32 coarse cells (checked at creation).
 __host__ __device__ inline void cell_coords(const Geo& G, int64_t c, int& gx, int& gy, int& gz) {
-  const int64_t nt3 = (int64_t)G.nt * G.nt * G.nt;
-  const int64_t t = c / nt3, r = c - t * nt3;
-  const int lz = (int)(r / (G.nt * G.nt)), ly = (int)((r / G.nt) % G.nt), lx = (int)(r % G.nt);
-  const int tx = (int)(t % G.nnt), ty = (int)((t / G.nnt) % G.nnt), tz = (int)(t / (G.nnt * G.nnt));
-  gx = tx * G.nt + lx;
-  gy = ty * G.nt + ly;
-  gz = tz * G.nt + lz;
+  const unsigned nt = (unsigned)G.nt, nt2 = nt * nt, nnt = (unsigned)G.nnt;
+  const unsigned cc = (unsigned)c;
+  const unsigned t = cc / (nt2 * nt), r = cc - t * (nt2 * nt);
+  const unsigned lz = r / nt2, r2 = r - lz * nt2, ly = r2 / nt, lx = r2 - ly * nt;
+  const unsigned t1 = t / nnt, tx = t - t1 * nnt, tz = t1 / nnt, ty = t1 - tz * nnt;
+  gx = (int)(tx * nt + lx);
+  gy = (int)(ty * nt + ly);
+  gz = (int)(tz * nt + lz);
+}
+
+// Storage index of the neighbour (dx, dy, dz) of storage cell c, whose tile-local
+// coordinates are l: an offset within the tile, cell_index across a tile face.
+__host__ __device__ inline int64_t nbr_cell(const Geo& G, int64_t c, const int l[3], const int g[3], int dx, int dy,
+                                            int dz) {
+  if ((unsigned)(l[0] + dx) < (unsigned)G.nt && (unsigned)(l[1] + dy) < (unsigned)G.nt &&
+      (unsigned)(l[2] + dz) < (unsigned)G.nt)
+    return c + ((int64_t)dz * G.nt + dy) * G.nt + dx;
+  return cell_index(G, g[0] + dx, g[1] + dy, g[2] + dz);
 }
 
 // ZIPX decode, kick.f90:627-628: (int(xp+ishift,izipx)+rshift)*x_resolution equals

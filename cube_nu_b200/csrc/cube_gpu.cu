@@ -96,7 +96,8 @@ struct StepRes {
 // kernel's block), candidate chunks of J particles in shared memory.
 struct PPShape {
   int T = 64, B = 256, J = 512;
-  bool operator==(const PPShape& o) const { return T == o.T && B == o.B && J == o.J; }
+  int L = 1;  // light cells: 0 one thread per particle (k_ppq_light), 1 the warp scan (k_ppq_lightw)
+  bool operator==(const PPShape& o) const { return T == o.T && B == o.B && J == o.J && L == o.L; }
 };
 
 // PP tuning classes by the largest cell occupancy.
@@ -809,6 +810,8 @@ int cube_gpu_create(const cube_params* p, int device, cube_ctx** out) {
   if (p->mass_p_cdm <= 0.f) return fail(CUBE_E_ARG, "mass_p_cdm must be positive");
   if (p->nslab < 0 || (p->nslab > 1 && (p->nnt % p->nslab || p->slab < 0 || p->slab >= p->nslab)))
     return fail(CUBE_E_ARG, "nslab must divide nnt, and 0 <= slab < nslab");
+  if ((double)(p->ng / p->ratio_cs) * (p->ng / p->ratio_cs) * (p->ng / p->ratio_cs) >= 4294967296.0)
+    return fail(CUBE_E_ARG, "at most 2^32 - 1 coarse cells (ng/ratio_cs < 1626)");
   cube_ctx* c = new cube_ctx();
   c->P = *p;
   c->G = make_geo(*p);
@@ -1601,15 +1604,20 @@ static void enqueue_ppq(cube_ctx* c, const PPShape& sh, float* vout, float* f2, 
   const Geo& G = c->G;
   const int64_t np = c->np;
   LAUNCH(c, K_PP, 1, k_ppq_prep<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pfin));
-  LAUNCH(c, K_PP, 1, k_ppq_light<<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->pcell, c->cstart, c->ires, c->pfin, c->vp, vout,
-                                                                  c->sd, sh.T, f2, vm, pairs, pairs + 1, abort));
+  if (sh.L == 1)
+    LAUNCH(c, K_PP, 1, k_ppq_lightw<<<nblk(np, 32 * PPW_WARPS), 32 * PPW_WARPS, PPW_WARPS * sizeof(PPWarp), c->s>>>(
+                           G, np, c->pcell, c->cstart, c->ires, c->pfin, c->vp, vout, c->sd, sh.T, f2, vm, pairs,
+                           pairs + 1, abort));
+  else
+    LAUNCH(c, K_PP, 1, k_ppq_light<<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->pcell, c->cstart, c->ires, c->pfin, c->vp,
+                                                                    vout, c->sd, sh.T, f2, vm, pairs, pairs + 1, abort));
   cudaMemsetAsync(c->ppq, 0, PPQ_Q * 4, c->s);
   LAUNCH(c, K_PP, 1, k_ppq_bucket_count<<<nblk(G.c1 - G.c0), 256, 0, c->s>>>(c->cstart, G.c0, G.c1, sh.T, c->ppq));
   LAUNCH(c, K_PP, 1, k_ppq_bucket_scan<<<1, 32, 0, c->s>>>(c->ppq));
   LAUNCH(c, K_PP, 1, k_ppq_bucket_fill<<<nblk(G.c1 - G.c0), 256, 0, c->s>>>(c->cstart, G.c0, G.c1, sh.T, c->ppq, c->hlist));
   LAUNCH(c, K_PP, 1, k_ppq_items<<<1, 1024, 0, c->s>>>(c->hlist, c->cstart, sh.B, c->ppq, c->hpre));
   const unsigned grid = (unsigned)(c->nsm * std::max(1, 1024 / sh.B));
-  const size_t sm = (size_t)sh.J * sizeof(float4);
+  const size_t sm = ppq_heavy_smem(sh.B, sh.J);
   smem_optin(k_ppq_heavy, sm);
   LAUNCH(c, K_PP, 1, k_ppq_heavy<<<grid, sh.B, sm, c->s>>>(G, c->hlist, c->hpre, c->ppq, c->cstart, c->ires, c->pfin,
                                                             c->vp, vout, c->sd, sh.J, f2, vm, pairs, pairs + 1, abort));
@@ -1645,6 +1653,8 @@ static int pp_tune(cube_ctx* c, int cls, int maxcount) {
   CK(cudaEventCreate(&e1));
   float best = 1e30f;
   PPShape win;
+  const char* vstr = getenv("CUBE_VERBOSE");
+  const bool verbose2 = vstr && vstr[0] == '2';
   for (const PPShape& sh : cands) {
     float ms = 0.f;
     for (int rep = 0; rep < 2; ++rep) {  // the second run is timed
@@ -1660,9 +1670,35 @@ static int pp_tune(cube_ctx* c, int cls, int maxcount) {
       return fail(CUBE_E_CUDA, std::string("PP tuning: ") + cudaGetErrorString(e));
     }
     cudaEventElapsedTime(&ms, e0, e1);
+    if (verbose2)
+      fprintf(stderr, "cube_gpu: PP shape T=%d B=%d J=%d L=%d: %.3f ms\n", sh.T, sh.B, sh.J, sh.L, ms);
     if (ms < best) {
       best = ms;
       win = sh;
+    }
+  }
+  {  // the thread-per-particle light form with the winning (T, B, J)
+    PPShape alt = win;
+    alt.L = 0;
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      cudaMemsetAsync(c->tune_red, 0, 32 * 4, c->s);
+      cudaEventRecord(e0, c->s);
+      enqueue_ppq(c, alt, c->vtune, c->tune_red, c->tune_red + 8,
+                  reinterpret_cast<unsigned long long*>(c->tune_red + 16), nullptr);
+      cudaEventRecord(e1, c->s);
+    }
+    const cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) {
+      c->prof = prof;
+      return fail(CUBE_E_CUDA, std::string("PP tuning: ") + cudaGetErrorString(e));
+    }
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (verbose2)
+      fprintf(stderr, "cube_gpu: PP shape T=%d B=%d J=%d L=%d: %.3f ms\n", alt.T, alt.B, alt.J, alt.L, ms);
+    if (ms < best) {
+      best = ms;
+      win = alt;
     }
   }
   cudaEventDestroy(e0);
@@ -1671,10 +1707,9 @@ static int pp_tune(cube_ctx* c, int cls, int maxcount) {
   c->pp_best[cls] = win;
   c->pp_tuned[cls] = true;
   c->pp_tune_ms[cls] = best;
-  const char* verbose = getenv("CUBE_VERBOSE");
-  if (verbose && verbose[0] == '1')
-    fprintf(stderr, "cube_gpu: PP tuned for class %d (max %d per cell): T=%d B=%d J=%d, %.3f ms (%zu shapes)\n", cls,
-            maxcount, win.T, win.B, win.J, best, cands.size());
+  if (vstr && (vstr[0] == '1' || verbose2))
+    fprintf(stderr, "cube_gpu: PP tuned for class %d (max %d per cell): T=%d B=%d J=%d L=%d, %.3f ms (%zu shapes)\n",
+            cls, maxcount, win.T, win.B, win.J, win.L, best, cands.size() + 1);
   return 0;
 }
 
@@ -2150,7 +2185,7 @@ int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, 
   return rc;
 }
 
-int cube_gpu_pp_shape(cube_ctx* c, int cls, int T, int B, int J) {
+int cube_gpu_pp_shape(cube_ctx* c, int cls, int T, int B, int J, int L) {
   if (!c || cls < 0 || cls > 3) return fail(CUBE_E_ARG, "bad PP class");
   if (T <= 0) {
     c->pp_tuned[cls] = false;
@@ -2158,22 +2193,25 @@ int cube_gpu_pp_shape(cube_ctx* c, int cls, int T, int B, int J) {
   }
   if (B != 128 && B != 256 && B != 512) return fail(CUBE_E_ARG, "PP item size B must be 128, 256 or 512");
   if (J < 32 || J > 4096) return fail(CUBE_E_ARG, "PP chunk J must be in 32..4096");
+  if (L != 0 && L != 1) return fail(CUBE_E_ARG, "PP light form L must be 0 or 1");
   PPShape sh;
   sh.T = T;
   sh.B = B;
   sh.J = J;
+  sh.L = L;
   c->pp_best[cls] = sh;
   c->pp_tuned[cls] = true;
   c->pp_tune_ms[cls] = 0;
   return 0;
 }
 
-int cube_gpu_pp_shape_get(cube_ctx* c, int cls, int* T, int* B, int* J, double* ms) {
+int cube_gpu_pp_shape_get(cube_ctx* c, int cls, int* T, int* B, int* J, int* L, double* ms) {
   if (!c || cls < 0 || cls > 3) return fail(CUBE_E_ARG, "bad PP class");
   if (!c->pp_tuned[cls]) return 0;
   if (T) *T = c->pp_best[cls].T;
   if (B) *B = c->pp_best[cls].B;
   if (J) *J = c->pp_best[cls].J;
+  if (L) *L = c->pp_best[cls].L;
   if (ms) *ms = c->pp_tune_ms[cls];
   return 1;
 }

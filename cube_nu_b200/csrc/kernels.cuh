@@ -1628,7 +1628,7 @@ __global__ void k_pp(Geo G, int64_t np, const void* __restrict__ xp, const int32
   for (int dz = lo[2]; dz <= hi[2]; ++dz)
     for (int dy = lo[1]; dy <= hi[1]; ++dy)
       for (int dx = lo[0]; dx <= hi[0]; ++dx) {
-        const int64_t c = cell_index(G, g[0] + dx, g[1] + dy, g[2] + dz);
+        const int64_t c = nbr_cell(G, pcell[ip], l, g, dx, dy, dz);
         const int64_t s = cstart[c], e = cstart[c + 1];
         cand += (unsigned long long)(e - s);
         const int lq[3] = {l[0] + dx, l[1] + dy, l[2] + dz};
