@@ -125,7 +125,7 @@ def load():
     L.cube_gpu_int2real.argtypes = [vp, vp, ctypes.c_int64]
     L.cube_gpu_step_host.argtypes = [vp, ctypes.POINTER(StepIn), ctypes.POINTER(StepOut), vp, vp, vp, vp,
                                      ctypes.c_int64]
-    L.cube_gpu_pp_shape.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.cube_gpu_pp_shape.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.cube_gpu_nu_transfer.argtypes = [vp, vp, vp, ctypes.c_int]
     L.cube_gpu_checkpoint_async.argtypes = [vp, ctypes.POINTER(CkptFiles), vp, ctypes.c_int64]
     L.cube_gpu_checkpoint_wait.argtypes = [vp]
@@ -136,7 +136,7 @@ def load():
     L.cube_gpu_nplocal.argtypes = [vp]
     L.cube_gpu_nplocal.restype = ctypes.c_int64
     ip = ctypes.POINTER(ctypes.c_int)
-    L.cube_gpu_pp_shape_get.argtypes = [vp, ctypes.c_int, ip, ip, ip, ip, ctypes.POINTER(ctypes.c_double)]
+    L.cube_gpu_pp_shape_get.argtypes = [vp, ctypes.c_int, ip, ip, ip, ctypes.POINTER(ctypes.c_double)]
     _LIB = L
     return L
 
@@ -322,17 +322,16 @@ class Context:
         _check(self._lib.cube_gpu_int2real(self._h, _ptr(out), out.size), "cube_gpu_int2real")
         return out
 
-    def pp_shape(self, cls: int, T: int, B: int = 256, J: int = 512, L: int = 1) -> None:
-        """Set the queue-PP shape of occupancy class cls (T <= 0: tune it again); L is the
-        light-cell form (0 a thread per particle, 1 the warp scan)."""
-        _check(self._lib.cube_gpu_pp_shape(self._h, cls, T, B, J, L), "cube_gpu_pp_shape")
+    def pp_shape(self, cls: int, T: int, B: int = 256, J: int = 512) -> None:
+        """Set the queue-PP shape of occupancy class cls (T <= 0: tune it again)."""
+        _check(self._lib.cube_gpu_pp_shape(self._h, cls, T, B, J), "cube_gpu_pp_shape")
 
     def pp_shape_get(self, cls: int):
-        """(T, B, J, L, tuned ms) of occupancy class cls, or None when it has none yet."""
-        T, B, J, L, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        """(T, B, J, tuned ms) of occupancy class cls, or None when it has none yet."""
+        T, B, J, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
         rc = _check(self._lib.cube_gpu_pp_shape_get(self._h, cls, ctypes.byref(T), ctypes.byref(B), ctypes.byref(J),
-                                                    ctypes.byref(L), ctypes.byref(ms)), "cube_gpu_pp_shape_get")
-        return (T.value, B.value, J.value, L.value, ms.value) if rc == 1 else None
+                                                    ctypes.byref(ms)), "cube_gpu_pp_shape_get")
+        return (T.value, B.value, J.value, ms.value) if rc == 1 else None
 
     def checkpoint_async(self, opath: str, image: int, z: float, header) -> None:
         """Write the resident state as the checkpoint files of one image in the background

@@ -96,8 +96,7 @@ struct StepRes {
 // kernel's block), candidate chunks of J particles in shared memory.
 struct PPShape {
   int T = 64, B = 256, J = 512;
-  int L = 1;  // light cells: 0 one thread per particle (k_ppq_light), 1 the warp scan (k_ppq_lightw)
-  bool operator==(const PPShape& o) const { return T == o.T && B == o.B && J == o.J && L == o.L; }
+  bool operator==(const PPShape& o) const { return T == o.T && B == o.B && J == o.J; }
 };
 
 // PP tuning classes by the largest cell occupancy.
@@ -1604,13 +1603,9 @@ static void enqueue_ppq(cube_ctx* c, const PPShape& sh, float* vout, float* f2, 
   const Geo& G = c->G;
   const int64_t np = c->np;
   LAUNCH(c, K_PP, 1, k_ppq_prep<<<nblk(np), 256, 0, c->s>>>(G, np, c->xp, c->pfin));
-  if (sh.L == 1)
-    LAUNCH(c, K_PP, 1, k_ppq_lightw<<<nblk(np, 32 * PPW_WARPS), 32 * PPW_WARPS, PPW_WARPS * sizeof(PPWarp), c->s>>>(
-                           G, np, c->pcell, c->cstart, c->ires, c->pfin, c->vp, vout, c->sd, sh.T, f2, vm, pairs,
-                           pairs + 1, abort));
-  else
-    LAUNCH(c, K_PP, 1, k_ppq_light<<<nblk(np, 128), 128, 0, c->s>>>(G, np, c->pcell, c->cstart, c->ires, c->pfin, c->vp,
-                                                                    vout, c->sd, sh.T, f2, vm, pairs, pairs + 1, abort));
+  LAUNCH(c, K_PP, 1, k_ppq_light<<<nblk(np, PPL_T), PPL_T, 0, c->s>>>(G, np, c->pcell, c->cstart, c->ires, c->pfin,
+                                                                      c->vp, vout, c->sd, sh.T, f2, vm, pairs, pairs + 1,
+                                                                      abort));
   cudaMemsetAsync(c->ppq, 0, PPQ_Q * 4, c->s);
   LAUNCH(c, K_PP, 1, k_ppq_bucket_count<<<nblk(G.c1 - G.c0), 256, 0, c->s>>>(c->cstart, G.c0, G.c1, sh.T, c->ppq));
   LAUNCH(c, K_PP, 1, k_ppq_bucket_scan<<<1, 32, 0, c->s>>>(c->ppq));
@@ -1632,7 +1627,7 @@ static int pp_tune(cube_ctx* c, int cls, int maxcount) {
   const bool prof = c->prof;
   c->prof = false;  // the sweep is not part of any step's kernel profile
   std::vector<PPShape> cands;
-  const int Ts[] = {16, 64, 256, 2048}, Bs[] = {128, 256, 512}, Js[] = {256, 1024};
+  const int Ts[] = {2048, 256, 64, 16}, Bs[] = {128, 256, 512}, Js[] = {256, 1024};  // T descending
   bool all_light_done = false;
   for (int T : Ts) {
     const bool all_light = T >= maxcount;  // no heavy cells: B and J do not matter
@@ -1670,35 +1665,12 @@ static int pp_tune(cube_ctx* c, int cls, int maxcount) {
       return fail(CUBE_E_CUDA, std::string("PP tuning: ") + cudaGetErrorString(e));
     }
     cudaEventElapsedTime(&ms, e0, e1);
-    if (verbose2)
-      fprintf(stderr, "cube_gpu: PP shape T=%d B=%d J=%d L=%d: %.3f ms\n", sh.T, sh.B, sh.J, sh.L, ms);
-    if (ms < best) {
+    if (verbose2) fprintf(stderr, "cube_gpu: PP shape T=%d B=%d J=%d: %.3f ms\n", sh.T, sh.B, sh.J, ms);
+    // shapes come with the light threshold T descending; a smaller T (more of the particles
+    // in the heavy queue) must win clearly, because cells grow between tunings of a class
+    if (ms < best * 0.97f) {
       best = ms;
       win = sh;
-    }
-  }
-  {  // the thread-per-particle light form with the winning (T, B, J)
-    PPShape alt = win;
-    alt.L = 0;
-    float ms = 0.f;
-    for (int rep = 0; rep < 2; ++rep) {
-      cudaMemsetAsync(c->tune_red, 0, 32 * 4, c->s);
-      cudaEventRecord(e0, c->s);
-      enqueue_ppq(c, alt, c->vtune, c->tune_red, c->tune_red + 8,
-                  reinterpret_cast<unsigned long long*>(c->tune_red + 16), nullptr);
-      cudaEventRecord(e1, c->s);
-    }
-    const cudaError_t e = cudaEventSynchronize(e1);
-    if (e != cudaSuccess) {
-      c->prof = prof;
-      return fail(CUBE_E_CUDA, std::string("PP tuning: ") + cudaGetErrorString(e));
-    }
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (verbose2)
-      fprintf(stderr, "cube_gpu: PP shape T=%d B=%d J=%d L=%d: %.3f ms\n", alt.T, alt.B, alt.J, alt.L, ms);
-    if (ms < best) {
-      best = ms;
-      win = alt;
     }
   }
   cudaEventDestroy(e0);
@@ -1708,8 +1680,8 @@ static int pp_tune(cube_ctx* c, int cls, int maxcount) {
   c->pp_tuned[cls] = true;
   c->pp_tune_ms[cls] = best;
   if (vstr && (vstr[0] == '1' || verbose2))
-    fprintf(stderr, "cube_gpu: PP tuned for class %d (max %d per cell): T=%d B=%d J=%d L=%d, %.3f ms (%zu shapes)\n",
-            cls, maxcount, win.T, win.B, win.J, win.L, best, cands.size() + 1);
+    fprintf(stderr, "cube_gpu: PP tuned for class %d (max %d per cell): T=%d B=%d J=%d, %.3f ms (%zu shapes)\n", cls,
+            maxcount, win.T, win.B, win.J, best, cands.size());
   return 0;
 }
 
@@ -2185,7 +2157,7 @@ int cube_gpu_step_host(cube_ctx* c, const cube_step_in* in, cube_step_out* out, 
   return rc;
 }
 
-int cube_gpu_pp_shape(cube_ctx* c, int cls, int T, int B, int J, int L) {
+int cube_gpu_pp_shape(cube_ctx* c, int cls, int T, int B, int J) {
   if (!c || cls < 0 || cls > 3) return fail(CUBE_E_ARG, "bad PP class");
   if (T <= 0) {
     c->pp_tuned[cls] = false;
@@ -2193,25 +2165,22 @@ int cube_gpu_pp_shape(cube_ctx* c, int cls, int T, int B, int J, int L) {
   }
   if (B != 128 && B != 256 && B != 512) return fail(CUBE_E_ARG, "PP item size B must be 128, 256 or 512");
   if (J < 32 || J > 4096) return fail(CUBE_E_ARG, "PP chunk J must be in 32..4096");
-  if (L != 0 && L != 1) return fail(CUBE_E_ARG, "PP light form L must be 0 or 1");
   PPShape sh;
   sh.T = T;
   sh.B = B;
   sh.J = J;
-  sh.L = L;
   c->pp_best[cls] = sh;
   c->pp_tuned[cls] = true;
   c->pp_tune_ms[cls] = 0;
   return 0;
 }
 
-int cube_gpu_pp_shape_get(cube_ctx* c, int cls, int* T, int* B, int* J, int* L, double* ms) {
+int cube_gpu_pp_shape_get(cube_ctx* c, int cls, int* T, int* B, int* J, double* ms) {
   if (!c || cls < 0 || cls > 3) return fail(CUBE_E_ARG, "bad PP class");
   if (!c->pp_tuned[cls]) return 0;
   if (T) *T = c->pp_best[cls].T;
   if (B) *B = c->pp_best[cls].B;
   if (J) *J = c->pp_best[cls].J;
-  if (L) *L = c->pp_best[cls].L;
   if (ms) *ms = c->pp_tune_ms[cls];
   return 1;
 }

@@ -127,8 +127,15 @@ __device__ __forceinline__ int ppq_iapm(const Geo& G, const int g[3], const int3
 }
 
 // Particles of light cells (count <= T), one thread each.  vin/vout: velocities before and
-// after (the same array in a step; the tuner writes a scratch copy).
-__global__ void __launch_bounds__(128) k_ppq_light(Geo G, int64_t np, const int32_t* __restrict__ pcell,
+// after (the same array in a step; the tuner writes a scratch copy).  Pairs in range are
+// deferred as in k_ppq_heavy: a thread keeps up to PPL_H of them (rv, r2) in its own
+// shared-memory column and adds them with PPi::accum in candidate order when the column
+// is full and at the end, so a warp runs the force of a pair once per PPL_H pairs of a
+// lane rather than once per candidate that any of its lanes has in range.
+constexpr int PPL_T = 128;  // threads per block
+constexpr int PPL_H = 8;    // deferred pairs per thread
+
+__global__ void __launch_bounds__(PPL_T) k_ppq_light(Geo G, int64_t np, const int32_t* __restrict__ pcell,
                                                    const int64_t* __restrict__ cstart, const int32_t* __restrict__ ires,
                                                    const float4* __restrict__ pfin, const float* vin, float* vout,
                                                    const StepDev* __restrict__ sd, int heavy_t, float* f2max,
@@ -141,6 +148,7 @@ __global__ void __launch_bounds__(128) k_ppq_light(Geo G, int64_t np, const int3
     c = pcell[ip];
     live = owned_cell(G, c) && cstart[c + 1] - cstart[c] <= heavy_t;
   }
+  __shared__ float4 hb[PPL_H][PPL_T];
   float f2 = 0.f, av[3] = {0.f, 0.f, 0.f};
   PPi P;
   P.pairs = P.cand = 0;
@@ -148,7 +156,41 @@ __global__ void __launch_bounds__(128) k_ppq_light(Geo G, int64_t np, const int3
     int g[3];
     cell_coords(G, c, g[0], g[1], g[2]);
     P.init(G, g, pfin[ip], ppq_iapm(G, g, ires));
-    P.all_cells(G, c, g, cstart, pfin);
+    int nh = 0;
+    for (int dz = P.lo[2]; dz <= P.hi[2]; ++dz)
+      for (int dy = P.lo[1]; dy <= P.hi[1]; ++dy)
+        for (int dx = P.lo[0]; dx <= P.hi[0]; ++dx) {
+          const int64_t n = nbr_cell(G, c, P.l, g, dx, dy, dz);
+          const int64_t s = cstart[n], e = cstart[n + 1];
+          P.cand += (unsigned)(e - s);
+          const float bx = (float)((P.l[0] + dx) * G.rcs), by = (float)((P.l[1] + dy) * G.rcs),
+                      bz = (float)((P.l[2] + dz) * G.rcs);
+          for (int64_t q = s; q < e; ++q) {
+            const float4 p = pfin[q];
+            const float rv0 = __fsub_rn(__fadd_rn(bx, p.x), P.xf[0]);
+            const float rv1 = __fsub_rn(__fadd_rn(by, p.y), P.xf[1]);
+            const float rv2 = __fsub_rn(__fadd_rn(bz, p.z), P.xf[2]);
+            const float r2 = sumsq3(rv0, rv1, rv2);
+            if (r2 > 0.f && r2 < P.range2) {
+              if (nh == PPL_H) {
+#pragma unroll 1
+                for (int h = 0; h < PPL_H; ++h) {
+                  const float4 r = hb[h][threadIdx.x];
+                  P.accum(r.x, r.y, r.z, r.w, G.app);
+                }
+                nh = 0;
+              }
+              hb[nh][threadIdx.x] = make_float4(rv0, rv1, rv2, r2);
+              ++nh;
+              ++P.pairs;
+            }
+          }
+        }
+#pragma unroll 1
+    for (int h = 0; h < nh; ++h) {
+      const float4 r = hb[h][threadIdx.x];
+      P.accum(r.x, r.y, r.z, r.w, G.app);
+    }
     f2 = ppq_apply(P, ip, vin, vout, sd->pp_mass, sd->pp_vscale, av);
   }
   block_max_to(f2, f2max);
@@ -160,202 +202,6 @@ __global__ void __launch_bounds__(128) k_ppq_light(Geo G, int64_t np, const int3
   }
   if ((threadIdx.x & 31) == 0 && a) atomicAdd(npairs, a);
   if ((threadIdx.x & 31) == 0 && b) atomicAdd(ncand, b);
-}
-
-// ---- light cells, warp scan ----
-// The same pairs as k_ppq_light, laid out for coherent loads.  A warp takes 32 consecutive
-// particles.  Each lane lists its particle's candidate cells (the cells its range reaches,
-// in the order dz, dy, dx, without the empty ones and the ones whose nearest face is
-// beyond the range) as chunks of one flat sequence of candidates: particle after
-// particle, cell after cell, candidates in storage order.  The warp then walks that
-// sequence 32 candidates at a time, lane i on element c+i: consecutive lanes read
-// consecutive candidates of the same cells, and every lane does useful work until the
-// end.  Pairs in range are deferred to a short list per particle, in sequence order, and
-// after the walk each lane adds its particle's list with PPi::accum, so the sums are
-// k_pp's bit for bit.  A particle with more than PPW_H pairs in range, or a warp whose
-// chunks overflow PPW_CAP, falls back to the thread-per-particle loop (same sums).
-//
-// A cell is left out only when it cannot hold a pair: with exact FP32 candidate
-// coordinates (the queue PP's condition) a candidate in the cell below has |rv_x| >= the
-// particle's offset x and one in the cell above |rv_x| >= ratio_cs - x, so r2 is at least
-// sumsq3 of those face distances (rounding is monotone); when that is >= range^2 no
-// candidate of the cell is in range.  The candidate count still covers every reached
-// cell, as the other paths count it.
-constexpr int PPW_WARPS = 4;  // warps per block
-constexpr int PPW_CAP = 256;  // chunks per warp (at most 8 per particle when range < ratio_cs/2)
-constexpr int PPW_H = 6;      // deferred pairs per particle
-
-struct PPWarp {
-  float4 base[PPW_CAP];      // (l + d) * ratio_cs per dimension; .w: particle lane (int bits)
-  float4 hit[PPW_H][32];     // rv and r2 of the deferred pairs, [slot][lane]
-  float4 part[32];           // xf and range^2 of each lane's particle
-  long long jd[PPW_CAP];     // candidate index = element + jd
-  int pre[PPW_CAP + 36];     // first element of each chunk; PPW_CAP+33 sentinels = total
-  int nh[32];                // pairs in range per particle (may exceed PPW_H)
-};
-
-__device__ __forceinline__ unsigned lanemask_lt() {
-  unsigned m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
-// Face distance of the particle to neighbour cell d (-1, 0, 1) along one dimension.
-__device__ __forceinline__ float ppw_gap(int d, float fin, float rcs) {
-  return d < 0 ? fin : (d > 0 ? __fsub_rn(rcs, fin) : 0.f);
-}
-
-__global__ void __launch_bounds__(32 * PPW_WARPS) k_ppq_lightw(Geo G, int64_t np, const int32_t* __restrict__ pcell,
-                                                             const int64_t* __restrict__ cstart,
-                                                             const int32_t* __restrict__ ires,
-                                                             const float4* __restrict__ pfin, const float* vin,
-                                                             float* vout, const StepDev* __restrict__ sd, int heavy_t,
-                                                             float* f2max, float* vmax, unsigned long long* npairs,
-                                                             unsigned long long* ncand,
-                                                             const unsigned* __restrict__ abort) {
-  extern __shared__ __align__(16) unsigned char ppw_smem[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  PPWarp& S = reinterpret_cast<PPWarp*>(ppw_smem)[wid];
-  const int64_t ip = ((int64_t)blockIdx.x * PPW_WARPS + wid) * 32 + lane;
-  bool live = ip < np && !(abort && *abort);
-  int c = 0;
-  if (live) {
-    c = pcell[ip];
-    live = owned_cell(G, c) && cstart[c + 1] - cstart[c] <= heavy_t;
-  }
-  const float rcs = (float)G.rcs;
-  PPi P;
-  P.pairs = P.cand = 0;
-  int g[3] = {0, 0, 0};
-  float fin[3] = {0.f, 0.f, 0.f};
-  // pass 1: chunks and elements of this lane's particle
-  int nch = 0, nel = 0;
-  if (live) {
-    cell_coords(G, c, g[0], g[1], g[2]);
-    const float4 f = pfin[ip];
-    fin[0] = f.x;
-    fin[1] = f.y;
-    fin[2] = f.z;
-    P.init(G, g, f, ppq_iapm(G, g, ires));
-    for (int dz = P.lo[2]; dz <= P.hi[2]; ++dz)
-      for (int dy = P.lo[1]; dy <= P.hi[1]; ++dy)
-        for (int dx = P.lo[0]; dx <= P.hi[0]; ++dx) {
-          const int64_t n = nbr_cell(G, c, P.l, g, dx, dy, dz);
-          const int m = (int)(cstart[n + 1] - cstart[n]);
-          P.cand += (unsigned)m;
-          const float dmin = sumsq3(ppw_gap(dx, fin[0], rcs), ppw_gap(dy, fin[1], rcs), ppw_gap(dz, fin[2], rcs));
-          if (m > 0 && dmin < P.range2) {
-            ++nch;
-            nel += m;
-          }
-        }
-  }
-  // exclusive prefixes over the warp
-  int cofs = nch, eofs = nel;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int a = __shfl_up_sync(0xffffffffu, cofs, o), b = __shfl_up_sync(0xffffffffu, eofs, o);
-    if (lane >= o) {
-      cofs += a;
-      eofs += b;
-    }
-  }
-  const int nchT = __shfl_sync(0xffffffffu, cofs, 31), nelT = __shfl_sync(0xffffffffu, eofs, 31);
-  cofs -= nch;
-  eofs -= nel;
-  const bool fits = nchT <= PPW_CAP;  // warp-uniform
-  if (fits) {
-    // pass 2: the chunks, in sequence order
-    if (live) {
-      int k = cofs, e0 = eofs;
-      for (int dz = P.lo[2]; dz <= P.hi[2]; ++dz)
-        for (int dy = P.lo[1]; dy <= P.hi[1]; ++dy)
-          for (int dx = P.lo[0]; dx <= P.hi[0]; ++dx) {
-            const int64_t n = nbr_cell(G, c, P.l, g, dx, dy, dz);
-            const int64_t s0 = cstart[n];
-            const int m = (int)(cstart[n + 1] - s0);
-            const float dmin = sumsq3(ppw_gap(dx, fin[0], rcs), ppw_gap(dy, fin[1], rcs), ppw_gap(dz, fin[2], rcs));
-            if (m > 0 && dmin < P.range2) {
-              S.pre[k] = e0;
-              S.jd[k] = (long long)(s0 - e0);
-              S.base[k] = make_float4((float)((P.l[0] + dx) * G.rcs), (float)((P.l[1] + dy) * G.rcs),
-                                      (float)((P.l[2] + dz) * G.rcs), __int_as_float(lane));
-              ++k;
-              e0 += m;
-            }
-          }
-    }
-    S.pre[nchT + lane] = nelT;
-    if (lane == 0) S.pre[nchT + 32] = nelT;
-    S.part[lane] = make_float4(P.xf[0], P.xf[1], P.xf[2], P.range2);
-    S.nh[lane] = 0;
-    __syncwarp();
-    // the walk: element e = c0 + lane lies in chunk ci; cb is the chunk holding element c0
-    const unsigned lt = lanemask_lt();
-    int cb = 0;
-    for (int c0 = 0; c0 < nelT; c0 += 32) {
-      const int tp = S.pre[cb + 1 + lane] - c0;  // >= 1: the chunks after cb start beyond c0
-      const unsigned starts = __reduce_or_sync(0xffffffffu, tp < 32 ? (1u << tp) : 0u);
-      const int ci = cb + __popc(starts & (lt | (1u << lane)));
-      const int nin = __popc(starts);
-      const int tpn = __shfl_sync(0xffffffffu, tp, nin);
-      cb += nin + (tpn == 32 ? 1 : 0);
-      const int e = c0 + lane;
-      const bool valid = e < nelT;
-      const int cj = valid ? ci : 0;
-      const float4 b = S.base[cj];
-      const int L = __float_as_int(b.w);
-      bool hit = false;
-      float rv0 = 0.f, rv1 = 0.f, rv2 = 0.f, r2 = 0.f;
-      if (valid) {
-        const float4 pi = S.part[L];
-        const float4 p = pfin[(int64_t)e + S.jd[cj]];
-        rv0 = __fsub_rn(__fadd_rn(b.x, p.x), pi.x);
-        rv1 = __fsub_rn(__fadd_rn(b.y, p.y), pi.y);
-        rv2 = __fsub_rn(__fadd_rn(b.z, p.z), pi.z);
-        r2 = sumsq3(rv0, rv1, rv2);
-        hit = r2 > 0.f && r2 < pi.w;
-      }
-      const unsigned hm = __ballot_sync(0xffffffffu, hit);
-      if (hm) {  // warp-uniform, rare
-        const unsigned same = __match_any_sync(0xffffffffu, L) & hm;
-        const int base_n = hit ? S.nh[L] : 0;
-        __syncwarp();
-        if (hit) {
-          const int slot = base_n + __popc(same & lt);
-          if (slot < PPW_H) S.hit[slot][L] = make_float4(rv0, rv1, rv2, r2);
-          if ((same >> lane) == 1u) S.nh[L] = base_n + __popc(same);  // the last of its particle
-        }
-        __syncwarp();
-      }
-    }
-    __syncwarp();
-  }
-  float f2 = 0.f, av[3] = {0.f, 0.f, 0.f};
-  if (live) {
-    const int nh = fits ? S.nh[lane] : PPW_H + 1;
-    if (nh <= PPW_H) {
-      for (int h = 0; h < nh; ++h) {
-        const float4 r = S.hit[h][lane];
-        P.accum(r.x, r.y, r.z, r.w, G.app);
-      }
-      P.pairs = (unsigned)nh;
-    } else {  // the thread-per-particle loop: same pairs in the same order
-      const unsigned cand = P.cand;
-      P.all_cells(G, c, g, cstart, pfin);
-      P.cand = cand;
-    }
-    f2 = ppq_apply(P, ip, vin, vout, sd->pp_mass, sd->pp_vscale, av);
-  }
-  block_max_to(f2, f2max);
-  block_vmax(av, vmax);
-  unsigned long long a = P.pairs, b = P.cand;
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_xor_sync(0xffffffffu, a, o);
-    b += __shfl_xor_sync(0xffffffffu, b, o);
-  }
-  if (lane == 0 && a) atomicAdd(npairs, a);
-  if (lane == 0 && b) atomicAdd(ncand, b);
 }
 
 // ---- the heavy-cell queue ----
@@ -475,6 +321,7 @@ __global__ void k_ppq_heavy(Geo G, const int32_t* __restrict__ hlist, const int*
     P.init(G, g, pfin[live ? ip : s0], ppq_iapm(G, g, ires));
     int nh = 0;
     auto flush = [&]() {
+#pragma unroll 1
       for (int h = 0; h < nh; ++h) {
         const float4 r = hb[h * B + threadIdx.x];
         P.accum(r.x, r.y, r.z, r.w, G.app);

@@ -239,18 +239,17 @@ int cube_gpu_profile(cube_ctx* ctx, int enable);
 int cube_gpu_profile_read(cube_ctx* ctx, double* ms, int64_t* count, int n);
 const char* cube_gpu_profile_name(int i);
 /* Queue PP shapes (cube_params.pp_queue).  The PP work is split by the occupancy of each
- * particle's coarse cell: cells of at most T particles are light, the others are cut into
- * items of B particles that a persistent kernel pulls from a device queue (largest cells
- * first), staging candidates in shared-memory chunks of J.  Light cells take one thread
- * per particle (L = 0) or a warp scan over the candidates of 32 particles (L = 1).  The
+ * particle's coarse cell: cells of at most T particles take one thread per particle, the
+ * others are cut into items of B particles that a persistent kernel pulls from a device
+ * queue (largest cells first), staging candidates in shared-memory chunks of J.  The
  * library's autotuner times a sweep of shapes on the live state the first time a step
  * falls in occupancy class cls (largest cell <= 64, <= 512, <= 4096, larger: 0..3; the
  * reference's only tuning data is its PP timing, kick.f90:141-201) and keeps the fastest.
  * Forces do not depend on the shape.  cube_gpu_pp_shape sets the shape of a class (T <= 0
  * forgets it, so it is tuned again); cube_gpu_pp_shape_get returns 1 and the shape and
  * its timed milliseconds when the class has one, else 0. */
-int cube_gpu_pp_shape(cube_ctx* ctx, int cls, int T, int B, int J, int L);
-int cube_gpu_pp_shape_get(cube_ctx* ctx, int cls, int* T, int* B, int* J, int* L, double* ms);
+int cube_gpu_pp_shape(cube_ctx* ctx, int cls, int T, int B, int J);
+int cube_gpu_pp_shape_get(cube_ctx* ctx, int cls, int* T, int* B, int* J, double* ms);
 /* Number of kernels this context has launched since creation. */
 int64_t cube_gpu_kernel_launches(cube_ctx* ctx);
 
