@@ -323,14 +323,14 @@ def run_form(p, args, local, dist, rank, replay=None, timed=True, want_base=Fals
             "base": base, "base_args": base_args}
 
 
-def late_leg(args, local, rank, a_stop=0.99, max_evolve=2000, steps=5):
+def late_leg(args, local, rank, z_late=0.05, max_evolve=2000, steps=5):
     """The clustered-PP configuration: 256^3 CDM in 100 Mpc/h (ng 256, 64 particles per
-    coarse cell), evolved from z=49 in the chosen form until a >= a_stop (outside any timed
-    region), then `steps` steps timed in the chosen form and the same steps replayed by
-    the plain form from the same state.  The evolution takes the reference's timestep with
-    only its expansion and velocity limits (timestep.f90:20-34 with the force criteria
-    left out): a few hundred steps instead of ~2000, which still collapses the haloes
-    (cells of ~10^4 particles); the timed steps use every criterion."""
+    coarse cell), evolved from z=49 in the chosen form to a checkpoint at z_late (outside
+    any timed region), then `steps` steps toward z=0 timed in the chosen form and the same
+    steps replayed by the plain form from the same state.  The evolution takes the
+    reference's timestep with only its expansion and velocity limits (timestep.f90:20-34
+    with the force criteria left out, ra_max = 0.1: about 40 steps), which still collapses
+    the haloes (cells of ~10^4 particles); the timed steps use every criterion."""
     import torch
 
     from cube_nu_b200._lib import Context
@@ -344,7 +344,7 @@ def late_leg(args, local, rank, a_stop=0.99, max_evolve=2000, steps=5):
     bg = cosmology.Background.from_table(tab)
     S = cosmology.StepState(a=d["a"], dt_vmax=d["dt_vmax"], vz_max=d["vz_max"])
     bg.init_cursor(S.a)
-    zck = [49.0, 0.0]
+    zck = [49.0, z_late]
     t0 = time.perf_counter()
     nev = 0
 
@@ -358,10 +358,14 @@ def late_leg(args, local, rank, a_stop=0.99, max_evolve=2000, steps=5):
         S.vz_max = so.vz_max
         return si, so
 
-    while S.a < a_stop and nev < max_evolve and not S.final_step:
+    while nev < max_evolve and not S.final_step:
         advance(evolve=True)
         nev += 1
     t_evolve = time.perf_counter() - t0
+    # the timed steps head for z = 0 from the checkpoint at z_late
+    zck.append(0.0)
+    S.cur_checkpoint = len(zck)
+    S.final_step = False
     state = ctx.download()
     res = {"workload": "256^3 CDM, 100 Mpc/h, ng 256 (64 particles per coarse cell), int16 ZIPX",
            "evolve_steps": nev, "evolve_s": round(t_evolve, 1), "a_start": S.a, "z_start": round(1 / S.a - 1, 4),
@@ -403,6 +407,75 @@ def late_leg(args, local, rank, a_stop=0.99, max_evolve=2000, steps=5):
     return res
 
 
+def full_run_leg(args, local, rank, nsteps=100):
+    """The 512^3 configuration as its run is defined: 512^3 CDM in 1000 Mpc/h from the
+    z=49 Zel'dovich ICs to z=0 in `nsteps` KDK steps of equal code time
+    (cosmology.fixed_steps, with the closing half drift at z=0), once in the chosen form and
+    once in the plain form from the same ICs.  Per form: the device time of every step (the
+    library's step events; the chosen form's PP tuning and graph captures run between
+    steps), the wall time of the whole run, the per-stage split, the occupancy the run
+    reaches, and the P(k) of the final particles on the 1024^3 grid; the two spectra are
+    compared for k < k_Nyq/2."""
+    import torch
+
+    nw = None
+    forms = {}
+    xis = {}
+    for form in ("chosen", "plain"):
+        q = config_512()
+        fixed = form == "chosen"
+        q.deposit_mode = DEPOSIT_FIXED if fixed else DEPOSIT_FP32
+        q.step_graph = fixed
+        q.pp_queue = fixed and (q.izipx == 1 or q.nt < 127)
+        nw = pk_grid(q)
+        ctx, d = device_ic(q, seed=1 + rank, device=local)
+        tab = cosmology.expansion_table(q.h0, q.omega_m, q.omega_r)
+        bg = cosmology.Background.from_table(tab)
+        sched = cosmology.fixed_steps(bg, d["a"], 1.0, nsteps)
+        vz = d["vz_max"]
+        ctx.profile(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        per = []
+        stage = np.zeros(7)
+        pairs = cand = 0
+        for dt, dt_old, a_mid, _ in sched:
+            so = ctx.step(dt, dt_old, a_mid, vz)
+            vz = so.vz_max
+            per.append(so.tcat[6])
+            stage += np.array(list(so.tcat)[:7])
+            pairs += so.pp_pairs
+            cand += so.pp_candidates
+        ctx.drift(sched[-1][0], 0.0, vz)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        ctx.profile(False)
+        n = d["nplocal"]
+        st = ctx.download()
+        xis[form] = ctx.power(nw, n_corr=0)[0]
+        ctx.close()
+        dev_s = sum(per) / 1e3
+        q10 = max(1, nsteps // 10)
+        forms[form] = {"value": round(n * nsteps / dev_s, 1), "ms_per_step": round(sum(per) / nsteps, 3),
+                       "wall_s": round(wall, 2),
+                       "ms_per_step_first_last_tenth": [round(float(np.mean(per[:q10])), 3),
+                                                        round(float(np.mean(per[-q10:])), 3)],
+                       "stage_ms_per_step": {k: round(float(v) / nsteps, 3) for k, v in
+                                             zip(("drift", "pm1", "pm2", "pm3", "pp", "kick", "step"), stage)},
+                       "pm3_classes_end": list(so.napm)[2:6], "max_cell_end": int(st[3].max()),
+                       "pp_pairs_per_step": pairs // nsteps, "pp_candidates_per_step": cand // nsteps,
+                       "deposit": "int64 fixed-point" if fixed else "fp32 atomics", "graph": fixed,
+                       "pp": "queue" if q.pp_queue else "thread"}
+    a, b = xis["chosen"], xis["plain"]
+    knyq = math.pi * nw / 1000.0
+    sel = (b[:, 0] > 0) & (b[:, 1] > 0) & (b[:, 1] < knyq / 2)
+    forms["chosen_over_plain"] = round(forms["plain"]["ms_per_step"] / forms["chosen"]["ms_per_step"], 4)
+    return {"workload": "512^3 CDM, 1000 Mpc/h, ng 1024, int16 ZIPX, z=49 -> 0 in %d equal code-time KDK steps" % nsteps,
+            "steps": nsteps, "forms": forms,
+            "dP_over_P_max_chosen_vs_plain": float(np.abs(a[sel, 2] / b[sel, 2] - 1).max()), "pk_grid": nw,
+            "pk_bins": int(sel.sum())}
+
+
 def pk_grid(p):
     """cicpower grid of the precision check: 2*ng as utilities/Makefile's FFTFINE builds it,
     capped at 1024^3 (the 512^3 workload's 2048^3 grid would hold ~100 GB beside the step)."""
@@ -425,6 +498,8 @@ def main():
                     help="also time the plain form (FP32 atomics, eager) over the same steps")
     ap.add_argument("--late", default="on", choices=["on", "off"],
                     help="also time the clustered-PP configuration (256^3, 100 Mpc/h) evolved to z~0, both forms")
+    ap.add_argument("--full-run", default="on", choices=["on", "off"],
+                    help="also run the 512^3 configuration z=49 -> 0 in 100 KDK steps, both forms")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-json", default="")
     ap.add_argument("--pk", type=int, default=0,
@@ -512,6 +587,12 @@ def main():
     late = None
     if args.late == "on" and args.workload == "512" and world == 1:
         late = late_leg(args, local, rank)
+    full = None
+    if args.full_run == "on" and args.workload == "512" and world == 1:
+        try:
+            full = full_run_leg(args, local, rank)
+        except Exception as e:  # reported in the line; the headline above stands
+            full = {"error": str(e)[:300]}
 
     if rank == 0:
         peaks, peak_kind = load_peaks()
@@ -608,6 +689,8 @@ def main():
         }
         if late:
             line["late_time"] = late
+        if full:
+            line["full_run"] = full
         if analysis:
             line["analysis"] = analysis
         if args.profile_json:

@@ -1017,23 +1017,42 @@ __global__ void __launch_bounds__(DEP3_THREADS, DEP3_MINB) k_deposit_pm3_own(Geo
   if (split) visits(std::true_type{});
   else visits(std::false_type{});
   __syncthreads();
-  // every cell of the region: a half warp per row, two cells per 8-byte store (e[0] and
-  // the pitches are even).  z = row / e[1] through a float reciprocal: (row + 0.5) / e[1]
-  // is at least 0.5/e[1] from an integer, far above the rounding error for row < R*R.
+  // every cell of the region.  Sums to floats: q * 2^-40 rounded once to FP32 (the int64
+  // to float conversion rounds the exact integer, and scaling by 2^-40 is exact), the value
+  // the FFT's conversion of the int64 mesh gives.
+  auto tofloat = [&](unsigned long long v) {
+    if (split) v = ((v >> 32) << 20) + (v & 0xffffffffull);
+    return __fmul_rn(__ll2float_rn((long long)v), 9.094947017729282e-13f);  // 2^-40
+  };
   float* base = rho + j * (int64_t)nft * pl + (int64_t)o[2] * pl + (int64_t)o[1] * pr + o[0];
+  if (e[0] == R && e[1] == R && e[2] == RZ && (pr & 3) == 0 && (pl & 3) == 0 &&
+      ((uintptr_t)base & 15) == 0) {
+    // a full region (every region of a class-2 box): four cells per 16-byte store, row and
+    // plane from compile-time divisions
+    constexpr int QX = R / 4;
+    static_assert(R % 4 == 0, "rows of whole float4s");
+    for (int i = tid; i < RZ * R * QX; i += blockDim.x) {
+      const int row = i / QX, qx = i - row * QX;
+      const int z = row / R, y = row - z * R;
+      const unsigned long long* a = &acc[(z * R + y) * R + 4 * qx];
+      const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(a);
+      const ulonglong2 v1 = *reinterpret_cast<const ulonglong2*>(a + 2);
+      __stcs(reinterpret_cast<float4*>(base + (int64_t)z * pl + (int64_t)y * pr) + qx,
+             make_float4(tofloat(v0.x), tofloat(v0.y), tofloat(v1.x), tofloat(v1.y)));
+    }
+    return;
+  }
+  // a partial region: a half warp per row, two cells per 8-byte store (e[0] and the
+  // pitches are even).  z = row / e[1] through a float reciprocal: (row + 0.5) / e[1]
+  // is at least 0.5/e[1] from an integer, far above the rounding error for row < R*R.
   const int hx = e[0] >> 1, nrow = e[1] * e[2], hl = tid & 15;
   const float inv_e1 = 1.f / (float)e[1];
   for (int row = tid >> 4; row < nrow; row += blockDim.x >> 4) {
     const int z = (int)(((float)row + 0.5f) * inv_e1);
     const int y = row - z * e[1];
     if (hl < hx) {
-      ulonglong2 val = *reinterpret_cast<const ulonglong2*>(&acc[(z * R + y) * R + 2 * hl]);
-      if (split) {
-        val.x = ((val.x >> 32) << 20) + (val.x & 0xffffffffull);
-        val.y = ((val.y >> 32) << 20) + (val.y & 0xffffffffull);
-      }
-      const float2 fv = make_float2((float)((double)(long long)val.x * 9.094947017729282e-13),  // 2^-40
-                                    (float)((double)(long long)val.y * 9.094947017729282e-13));
+      const ulonglong2 val = *reinterpret_cast<const ulonglong2*>(&acc[(z * R + y) * R + 2 * hl]);
+      const float2 fv = make_float2(tofloat(val.x), tofloat(val.y));
       __stcs(reinterpret_cast<float2*>(base + (int64_t)z * pl + (int64_t)y * pr) + hl, fv);
     }
   }
