@@ -181,6 +181,7 @@ struct cube_ctx {
   // queue PP (cube_params.pp_queue): decoded offsets, heavy-cell list and item prefix,
   // queue counters; the autotuner's scratch velocities and reductions, and its winners
   float4* pfin = nullptr;
+  int32_t* hperm = nullptr;  // heavy cells' particles ordered by neighbour-set code (pp.cuh)
   int32_t* hlist = nullptr;
   int* hpre = nullptr;
   int* ppq = nullptr;
@@ -915,7 +916,7 @@ int cube_gpu_destroy(cube_ctx* c) {
   void* bufs[] = {c->xp, c->xp2, c->vp, c->vp2, c->pid, c->pid2, c->pcell, c->pcell2, c->rhoc, c->rhoc2,
                   c->fill, c->biglist, c->hugelist, c->nbig, c->cstart, c->cstart2, c->scan_tmp, c->dest, c->key, c->skey,
                   c->ssrc, c->rdev, c->sd, c->ires, c->box_slot, c->box_sub, c->arena, c->green1, c->green2,
-                  c->cap_buf, c->pfin, c->hlist, c->hpre, c->ppq, c->vtune, c->tune_red, c->tf1, c->tf2,
+                  c->cap_buf, c->pfin, c->hperm, c->hlist, c->hpre, c->ppq, c->vtune, c->tune_red, c->tf1, c->tf2,
                   c->nu_tab, c->lay_cnt, c->lay_start, c->lay_buf};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -975,9 +976,12 @@ static int alloc_particles(cube_ctx* c, int64_t np) {
   if (c->P.pp_queue) {
     if (c->pfin) cudaFree(c->pfin);
     if (c->vtune) cudaFree(c->vtune);
+    if (c->hperm) cudaFree(c->hperm);
     c->pfin = nullptr;
     c->vtune = nullptr;
+    c->hperm = nullptr;
     CK(cudaMalloc(&c->pfin, (size_t)cap * sizeof(float4)));
+    CK(cudaMalloc(&c->hperm, (size_t)cap * sizeof(int32_t)));
   }
   // mesh arena: everything that fits of what the largest level needs, within 70% of free memory
   const Geo& G = c->G;
@@ -1611,11 +1615,14 @@ static void enqueue_ppq(cube_ctx* c, const PPShape& sh, float* vout, float* f2, 
   LAUNCH(c, K_PP, 1, k_ppq_bucket_scan<<<1, 32, 0, c->s>>>(c->ppq));
   LAUNCH(c, K_PP, 1, k_ppq_bucket_fill<<<nblk(G.c1 - G.c0), 256, 0, c->s>>>(c->cstart, G.c0, G.c1, sh.T, c->ppq, c->hlist));
   LAUNCH(c, K_PP, 1, k_ppq_items<<<1, 1024, 0, c->s>>>(c->hlist, c->cstart, sh.B, c->ppq, c->hpre));
+  LAUNCH(c, K_PP, 1, k_ppq_sort_codes<<<(unsigned)(4 * c->nsm), 256, 0, c->s>>>(G, c->hlist, c->ppq, c->cstart, c->ires,
+                                                                                c->pfin, c->hperm));
   const unsigned grid = (unsigned)(c->nsm * std::max(1, 1024 / sh.B));
   const size_t sm = ppq_heavy_smem(sh.B, sh.J);
   smem_optin(k_ppq_heavy, sm);
   LAUNCH(c, K_PP, 1, k_ppq_heavy<<<grid, sh.B, sm, c->s>>>(G, c->hlist, c->hpre, c->ppq, c->cstart, c->ires, c->pfin,
-                                                            c->vp, vout, c->sd, sh.J, f2, vm, pairs, pairs + 1, abort));
+                                                            c->hperm, c->vp, vout, c->sd, sh.J, f2, vm, pairs,
+                                                            pairs + 1, abort));
 }
 
 // The autotuner of the queue PP: on the current particle state, time every shape of a

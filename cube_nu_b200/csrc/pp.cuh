@@ -270,9 +270,65 @@ __global__ void __launch_bounds__(1024) k_ppq_items(const int32_t* __restrict__ 
   }
 }
 
-// Persistent: each block pulls items (B particles of one heavy cell) from the queue.  The
-// block's particles share their cell, so the candidate cells are the 27 around it; a cell
-// that no thread of the block needs is skipped, the others are staged in chunks of J.
+// Neighbour-set code of a particle: per dimension whether its range reaches the cell below
+// (1) or above (2), two bits each.
+__device__ __forceinline__ int ppq_code(const PPi& P) {
+  int code = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) code |= ((P.lo[d] < 0 ? 1 : 0) | (P.hi[d] > 0 ? 2 : 0)) << (2 * d);
+  return code;
+}
+
+// The particles of every heavy cell as indices ordered by neighbour-set code, in the
+// cell's own index range of hperm (a counting sort per cell; the order within a code is
+// arbitrary).  The items of B consecutive entries then hold one or two codes, so that a
+// block stages, and a warp computes, only the cells their particles reach.  Each
+// particle's sums do not depend on the item or thread that computes them.
+__global__ void __launch_bounds__(256) k_ppq_sort_codes(Geo G, const int32_t* __restrict__ hlist,
+                                                        const int* __restrict__ q, const int64_t* __restrict__ cstart,
+                                                        const int32_t* __restrict__ ires,
+                                                        const float4* __restrict__ pfin, int32_t* __restrict__ hperm) {
+  __shared__ int cnt[64];
+  const int nh = q[64];
+  for (int h = blockIdx.x; h < nh; h += gridDim.x) {
+    const int c = hlist[h];
+    const int64_t s0 = cstart[c], e0 = cstart[c + 1];
+    int g[3];
+    cell_coords(G, c, g[0], g[1], g[2]);
+    const int iapm = ppq_iapm(G, g, ires);
+    __syncthreads();  // cnt is free again
+    if (threadIdx.x < 64) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (int64_t ip = s0 + threadIdx.x; ip < e0; ip += blockDim.x) {
+      PPi P;
+      P.init(G, g, pfin[ip], iapm);
+      atomicAdd(&cnt[ppq_code(P)], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // exclusive offsets, two codes per lane
+      const int a = cnt[2 * threadIdx.x], b = cnt[2 * threadIdx.x + 1];
+      int incl = a + b;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((int)threadIdx.x >= o) incl += u;
+      }
+      cnt[2 * threadIdx.x] = incl - a - b;
+      cnt[2 * threadIdx.x + 1] = incl - b;
+    }
+    __syncthreads();
+    for (int64_t ip = s0 + threadIdx.x; ip < e0; ip += blockDim.x) {
+      PPi P;
+      P.init(G, g, pfin[ip], iapm);
+      hperm[s0 + atomicAdd(&cnt[ppq_code(P)], 1)] = (int32_t)ip;
+    }
+  }
+}
+
+// Persistent: each block pulls items (B entries of one heavy cell's code-ordered indices)
+// from the queue.  The block's particles share their cell, so the candidate cells are the
+// 27 around it; a cell that no thread of the block needs is skipped, the others are staged
+// in chunks of J, and a warp none of whose particles reaches a cell skips its candidates.
 // Pairs in range are deferred: each thread keeps up to PPH_H of them (rv, r2) in its own
 // shared-memory column and adds them with PPi::accum, in candidate order, whenever a
 // thread of its warp may run out of room; so the force of a pair is evaluated by the lanes
@@ -286,8 +342,8 @@ __host__ __device__ inline size_t ppq_heavy_smem(int B, int J) {
 
 __global__ void k_ppq_heavy(Geo G, const int32_t* __restrict__ hlist, const int* __restrict__ hpre, int* q,
                             const int64_t* __restrict__ cstart, const int32_t* __restrict__ ires,
-                            const float4* __restrict__ pfin, const float* vin, float* vout,
-                            const StepDev* __restrict__ sd, int J, float* f2max, float* vmax,
+                            const float4* __restrict__ pfin, const int32_t* __restrict__ hperm, const float* vin,
+                            float* vout, const StepDev* __restrict__ sd, int J, float* f2max, float* vmax,
                             unsigned long long* npairs, unsigned long long* ncand, const unsigned* __restrict__ abort) {
   extern __shared__ float4 sj[];  // J candidates, then the deferred pairs [PPH_H][B]
   __shared__ int s_item;
@@ -313,8 +369,9 @@ __global__ void k_ppq_heavy(Geo G, const int32_t* __restrict__ hlist, const int*
     }
     const int c = hlist[lo];
     const int64_t s0 = cstart[c], e0 = cstart[c + 1];
-    const int64_t ip = s0 + (int64_t)(item - hpre[lo]) * B + threadIdx.x;
-    const bool live = ip < e0;
+    const int64_t slot = s0 + (int64_t)(item - hpre[lo]) * B + threadIdx.x;
+    const bool live = slot < e0;
+    const int64_t ip = live ? (int64_t)hperm[slot] : s0;
     int g[3];
     cell_coords(G, c, g[0], g[1], g[2]);
     PPi P;
@@ -343,6 +400,7 @@ __global__ void k_ppq_heavy(Geo G, const int32_t* __restrict__ hlist, const int*
             __syncthreads();
             for (int k = threadIdx.x; k < cnt; k += B) sj[k] = pfin[j0 + k];
             __syncthreads();
+            if (__any_sync(0xffffffffu, need))  // warp-uniform
             for (int k0 = 0; k0 < cnt; k0 += PPH_U) {
               const int kn = min(cnt, k0 + PPH_U);
               if (need)
