@@ -495,7 +495,7 @@ void fz_green(cube_ctx* c, int64_t nbox, float2* ck, const float* green, const f
 
 template <int N, int R1, int R2>
 void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out, float2* ck,
-              const float* green, float norm, int reps, int kx, int ky, int kz, int kc, const Pitch& pt) {
+              const float* green, float inv, int kx, int ky, int kz, int kc, const Pitch& pt) {
   constexpr int T = f2::TPS<R1, R2>::T, NH = N / 2 + 1;
   const float2* tw = fft_desc(c, N)->tw;
   const int64_t nrows = nbox * (int64_t)N * N;
@@ -521,7 +521,7 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
       LAUNCH(c, kz, 1, f2::k_fcol3<N, R1, R2, 2, 2><<<gc, W * T, smg, c->s>>>(ck, green, tw, W, pt.pc, pt.plc));
       smem_optin(f2::k_fyx3_c2r<N, R1, R2>, smi);
       LAUNCH(c, kc, 1, f2::k_fyx3_c2r<N, R1, R2><<<planes, f2::PLANE3_THREADS, smi, c->s>>>(
-                           ck, phi_out, tw, norm, reps, pt.pc, pt.pf, pt.plc, pt.plf));
+                           ck, phi_out, tw, inv, pt.pc, pt.pf, pt.plc, pt.plf));
       return;
     }
   }
@@ -543,7 +543,7 @@ void fft2_run(cube_ctx* c, int64_t nbox, const void* real_in, bool fixed, float 
   LAUNCH(c, ky, 1, f2::k_fcol3<N, R1, R2, 1, 0><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
   fz_green<N, R1, R2>(c, nbox, ck, green, tw, pt, kz);
   LAUNCH(c, ky, 1, f2::k_fcol3<N, R1, R2, 1, 1><<<gc, W * T, smc, c->s>>>(ck, nullptr, tw, W, pt.pc, pt.plc));
-  LAUNCH(c, kc, 1, f2::k_fx_c2r<N, R1, R2><<<gx, S * T, smx, c->s>>>(ck, phi_out, nrows, tw, norm, reps, pt.pc, pt.pf));
+  LAUNCH(c, kc, 1, f2::k_fx_c2r<N, R1, R2><<<gx, S * T, smx, c->s>>>(ck, phi_out, nrows, tw, inv, pt.pc, pt.pf));
 }
 
 bool fft2_size(int n) {
@@ -559,9 +559,9 @@ bool fft2_size(int n) {
 bool fused_layout(const cube_ctx* c, int n) { return !c->fft_generic && c->fft_fused && n <= 144 && fft2_size(n); }
 
 bool fft2_dispatch(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixed, float scale, float* phi_out,
-                   float2* ck, const float* green, float norm, int reps, int kx, int ky, int kz, int kc, const Pitch& pt) {
+                   float2* ck, const float* green, float inv, int kx, int ky, int kz, int kc, const Pitch& pt) {
 #define CUBE_FFT2(N, R1, R2) \
-  case N: fft2_run<N, R1, R2>(c, nbox, real_in, fixed, scale, phi_out, ck, green, norm, reps, kx, ky, kz, kc, pt); return true;
+  case N: fft2_run<N, R1, R2>(c, nbox, real_in, fixed, scale, phi_out, ck, green, inv, kx, ky, kz, kc, pt); return true;
   switch (n) {
     CUBE_FFT2(16, 4, 4)
     CUBE_FFT2(32, 4, 8)
@@ -664,8 +664,11 @@ void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixe
   const int kz = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTZ_PM2 : K_FFTZ_PM3;
   const int kc = level == 1 ? K_FFT_PM1 : level == 2 ? K_FFTC_PM2 : K_FFTC_PM3;
   const Pitch pt = pitch_of(c, n, fixed);
+  // the backward transform's normalisation (phi/real(nwork)**3, kick.f90:846; PM1 divides
+  // by n three times) as one multiplication by the reciprocal, rounded once from double
+  const float inv = (float)(1.0 / std::pow((double)norm, (double)reps));
   if (c->fft_generic == 0 &&
-      fft2_dispatch(c, n, nbox, real_in, fixed, scale, phi_out, ck, green, norm, reps, kx, ky, kz, kc, pt))
+      fft2_dispatch(c, n, nbox, real_in, fixed, scale, phi_out, ck, green, inv, kx, ky, kz, kc, pt))
     return;
   const FFTDesc& D = *fft_desc(c, n);
   const int nh = n / 2 + 1;
@@ -685,7 +688,7 @@ void launch_fft(cube_ctx* c, int n, int64_t nbox, const void* real_in, bool fixe
   LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, -1, pt.pc, pt.plc));
   LAUNCH(c, kz, 1, k_fft_z_green<<<gy, 256, smy, c->s>>>(ck, green, D, W, pt.pc, pt.plc));
   LAUNCH(c, ky, 1, k_fft_y<<<gy, 256, smy, c->s>>>(ck, D, W, +1, pt.pc, pt.plc));
-  LAUNCH(c, kc, 1, k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, norm, reps, pt.pc, pt.pf));
+  LAUNCH(c, kc, 1, k_fft_x_c2r<<<gx, 256, smx, c->s>>>(ck, phi_out, nrows, D, rpb, inv, pt.pc, pt.pf));
 }
 
 inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }

@@ -196,7 +196,7 @@ __global__ void k_fft_z_green(float2* __restrict__ c, const float* __restrict__ 
 
 // ---- X' pass: half spectrum rows -> real rows, divided `reps` times by `norm`
 // (PM1: three times by nw, pencil_fft.f90:77; PM2/PM3: once by nwork^3, kick.f90:846).
-__global__ void k_fft_x_c2r(const float2* c, float* r, int64_t nrows, FFTDesc D, int rpb, float norm, int reps,
+__global__ void k_fft_x_c2r(const float2* c, float* r, int64_t nrows, FFTDesc D, int rpb, float inv,
                             int pc, int pf) {
   extern __shared__ float2 sm[];
   const int n = D.n, nh = n / 2 + 1;
@@ -221,8 +221,7 @@ __global__ void k_fft_x_c2r(const float2* c, float* r, int64_t nrows, FFTDesc D,
   __syncthreads();
   float2* res = fft_smem<false>(a, b, n, nr, n, 1, tw, D, +1);
   for (int t = threadIdx.x; t < nr * n; t += blockDim.x) {
-    float v = res[t].x;
-    for (int q = 0; q < reps; ++q) v = __fdiv_rn(v, norm);
+    const float v = __fmul_rn(res[t].x, inv);
     const int rr = t / n, x = t - rr * n;
     r[(row0 + rr) * pf + x] = v;
   }

@@ -488,7 +488,7 @@ __host__ inline int fcol_width(int N, int T) {
 // ---------------------------------------------------------------------------------
 template <int N, int R1, int R2>
 __global__ void __launch_bounds__(256) k_fx_c2r(const float2* c, float* r, int64_t nrows, const float2* __restrict__ gtw,
-                                                float norm, int reps, int pc, int pf) {
+                                                float inv, int pc, int pf) {
   constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1;
   extern __shared__ float2 sm[];
   float2* tw = sm;
@@ -515,8 +515,7 @@ __global__ void __launch_bounds__(256) k_fx_c2r(const float2* c, float* r, int64
     if (row >= nr) continue;
     const float2 z = Z[(row >> 1) * N + x];
     float v = (row & 1) ? z.y : z.x;
-    for (int q = 0; q < reps; ++q) v = __fdiv_rn(v, norm);
-    r[(row0 + row) * pf + x] = v;
+    r[(row0 + row) * pf + x] = __fmul_rn(v, inv);
   }
 }
 
@@ -664,7 +663,7 @@ __global__ void __launch_bounds__(PLANE3_THREADS, 2) k_fxy3_r2c(const IN* __rest
 
 template <int N, int R1, int R2>
 __global__ void __launch_bounds__(PLANE3_THREADS, 2) k_fyx3_c2r(const float2* __restrict__ c, float* __restrict__ r,
-                                                               const float2* __restrict__ gtw, float norm, int reps,
+                                                               const float2* __restrict__ gtw, float inv,
                                                                int pc, int pf, int64_t plc, int64_t plf) {
   constexpr int T = TPS<R1, R2>::T, NH = N / 2 + 1, NP = N / 2;
   static_assert(T <= 16, "two sequences per warp");
@@ -748,13 +747,8 @@ __global__ void __launch_bounds__(PLANE3_THREADS, 2) k_fyx3_c2r(const float2* __
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) {
           const int x = t + R1 * k2;
-          float a = w[k2].x, b = w[k2].y;
-          for (int q = 0; q < reps; ++q) {
-            a = __fdiv_rn(a, norm);
-            b = __fdiv_rn(b, norm);
-          }
-          rp[(2 * p) * pf + x] = a;
-          rp[(2 * p + 1) * pf + x] = b;
+          rp[(2 * p) * pf + x] = __fmul_rn(w[k2].x, inv);
+          rp[(2 * p + 1) * pf + x] = __fmul_rn(w[k2].y, inv);
         }
       }
       __syncwarp();
