@@ -421,7 +421,10 @@ def full_run_leg(args, local, rank, nsteps=100):
     nw = None
     forms = {}
     xis = {}
-    for form in ("chosen", "plain"):
+    # plain_repeat: the plain form once more from the same ICs; its FP32 atomics sum in a
+    # different order, so its P(k) against the first plain run measures how far rounding
+    # differences alone carry the particles apart over the run
+    for form in ("chosen", "plain", "plain_repeat"):
         q = config_512()
         fixed = form == "chosen"
         q.deposit_mode = DEPOSIT_FIXED if fixed else DEPOSIT_FP32
@@ -454,26 +457,35 @@ def full_run_leg(args, local, rank, nsteps=100):
         st = ctx.download()
         xis[form] = ctx.power(nw, n_corr=0)[0]
         ctx.close()
+        if form == "plain_repeat":
+            continue
         dev_s = sum(per) / 1e3
         q10 = max(1, nsteps // 10)
         forms[form] = {"value": round(n * nsteps / dev_s, 1), "ms_per_step": round(sum(per) / nsteps, 3),
                        "wall_s": round(wall, 2),
                        "ms_per_step_first_last_tenth": [round(float(np.mean(per[:q10])), 3),
                                                         round(float(np.mean(per[-q10:])), 3)],
+                       "ms_first_steps": [round(float(x), 2) for x in per[:q10]],
                        "stage_ms_per_step": {k: round(float(v) / nsteps, 3) for k, v in
                                              zip(("drift", "pm1", "pm2", "pm3", "pp", "kick", "step"), stage)},
                        "pm3_classes_end": list(so.napm)[2:6], "max_cell_end": int(st[3].max()),
                        "pp_pairs_per_step": pairs // nsteps, "pp_candidates_per_step": cand // nsteps,
                        "deposit": "int64 fixed-point" if fixed else "fp32 atomics", "graph": fixed,
                        "pp": "queue" if q.pp_queue else "thread"}
-    a, b = xis["chosen"], xis["plain"]
     knyq = math.pi * nw / 1000.0
-    sel = (b[:, 0] > 0) & (b[:, 1] > 0) & (b[:, 1] < knyq / 2)
+    b = xis["plain"]
+
+    def dpp(x, kmax):
+        sel = (b[:, 0] > 0) & (b[:, 1] > 0) & (b[:, 1] < kmax)
+        return float(np.abs(x[sel, 2] / b[sel, 2] - 1).max())
+
     forms["chosen_over_plain"] = round(forms["plain"]["ms_per_step"] / forms["chosen"]["ms_per_step"], 4)
     return {"workload": "512^3 CDM, 1000 Mpc/h, ng 1024, int16 ZIPX, z=49 -> 0 in %d equal code-time KDK steps" % nsteps,
-            "steps": nsteps, "forms": forms,
-            "dP_over_P_max_chosen_vs_plain": float(np.abs(a[sel, 2] / b[sel, 2] - 1).max()), "pk_grid": nw,
-            "pk_bins": int(sel.sum())}
+            "steps": nsteps, "forms": forms, "pk_grid": nw, "k_nyq_hmpc": round(knyq, 4),
+            "dP_over_P_max": {"chosen_vs_plain_k_lt_knyq_2": dpp(xis["chosen"], knyq / 2),
+                              "chosen_vs_plain_k_lt_knyq_4": dpp(xis["chosen"], knyq / 4),
+                              "plain_repeat_vs_plain_k_lt_knyq_2": dpp(xis["plain_repeat"], knyq / 2),
+                              "plain_repeat_vs_plain_k_lt_knyq_4": dpp(xis["plain_repeat"], knyq / 4)}}
 
 
 def pk_grid(p):

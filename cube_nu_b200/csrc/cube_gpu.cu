@@ -472,9 +472,14 @@ int64_t boxes_fit(cube_ctx* c, int n, bool fixed) {
   return std::max<int64_t>(1, (int64_t)(c->arena_bytes / per));
 }
 
+// Raise a kernel's dynamic shared-memory limit when `bytes` plus its static shared memory
+// pass the 48 KB default and the limit set so far is lower.
 template <typename K>
 void smem_optin(K kernel, size_t bytes) {
-  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncAttributes a;
+  if (cudaFuncGetAttributes(&a, kernel) != cudaSuccess) return;
+  if (bytes + a.sharedSizeBytes > 48 * 1024 && bytes > (size_t)a.maxDynamicSharedSizeBytes)
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 // Size-specialised passes (fft2.cuh) for N = R1*R2.  N <= 144 runs the fused plane
@@ -1637,7 +1642,10 @@ static int pp_tune(cube_ctx* c, int cls, int maxcount) {
   const bool prof = c->prof;
   c->prof = false;  // the sweep is not part of any step's kernel profile
   std::vector<PPShape> cands;
-  const int Ts[] = {2048, 256, 64, 16}, Bs[] = {128, 256, 512}, Js[] = {256, 1024};  // T descending
+  // T descending; B = 512 (one block per SM at the heavy kernel's registers) and J = 1024
+  // (the chunk length changes no time measured on 512^3 and 256^3 runs, z = 49 to 0) were
+  // never chosen and are left out of the sweep, which runs on the live state
+  const int Ts[] = {2048, 256, 64, 16}, Bs[] = {128, 256}, Js[] = {256};
   bool all_light_done = false;
   for (int T : Ts) {
     const bool all_light = T >= maxcount;  // no heavy cells: B and J do not matter
