@@ -488,6 +488,103 @@ def full_run_leg(args, local, rank, nsteps=100):
                               "plain_repeat_vs_plain_k_lt_knyq_4": dpp(xis["plain_repeat"], knyq / 4)}}
 
 
+def small_configs_leg(args, local, rank, cpu=True):
+    """The two smaller configurations of the benchmark set at full size.
+    128^3: 128^3 CDM in 200 Mpc/h, ng 256, int8 ZIPX, PP on, z=49 -> 10 in 10 equal
+    code-time KDK steps from the device ICs, in both forms (device time per step); and,
+    when cpu, one whole step of the oracle in FP32 on all host cores from the same state
+    (a measured step, not a sample scaled up).
+    adjoint: 128^3 particles on a 256^3 mesh in 256 Mpc/h, PM only, 20 KDK steps z=20 -> 0,
+    loss = mean squared difference of the final TSC density from a second seed's, gradient
+    with respect to the 128^3 white-noise modes by the hand-written adjoint with a checkpoint
+    every 5 steps; forward and backward timed on the device (the third evaluation of
+    three)."""
+    import torch
+
+    from cube_nu_b200 import adjoint as A
+    from cube_nu_b200.params import config_plain_128
+
+    out = {}
+    forms = {}
+    state = None
+    for form in ("chosen", "plain"):
+        q = config_plain_128()
+        q.nic = 1
+        fixed = form == "chosen"
+        q.deposit_mode = DEPOSIT_FIXED if fixed else DEPOSIT_FP32
+        q.step_graph = fixed
+        q.pp_queue = fixed
+        ctx, d = device_ic(q, seed=1 + rank, device=local)
+        tab = cosmology.expansion_table(q.h0, q.omega_m, q.omega_r)
+        bg = cosmology.Background.from_table(tab)
+        sched = cosmology.fixed_steps(bg, d["a"], 1 / 11.0, 10)
+        vz = d["vz_max"]
+        if state is None:
+            state = (ctx.download(), sched, vz, q)
+        ctx.profile(True)
+        ms = 0.0
+        for dt, dt_old, a_mid, _ in sched:
+            so = ctx.step(dt, dt_old, a_mid, vz)
+            vz = so.vz_max
+            ms += so.tcat[6]
+        ctx.profile(False)
+        n = d["nplocal"]
+        ctx.close()
+        forms[form] = {"ms_per_step": round(ms / len(sched), 3), "value": round(n * len(sched) / (ms / 1e3), 1)}
+    forms["chosen_over_plain"] = round(forms["plain"]["ms_per_step"] / forms["chosen"]["ms_per_step"], 4)
+    out["config_128"] = {"workload": "128^3 CDM, 200 Mpc/h, ng 256, int8 ZIPX, z=49 -> 10 in 10 KDK steps",
+                         "forms": forms}
+    if cpu:
+        from oracle import oracle as O
+
+        (xp, vp, pid, rhoc), sched, vz, q = state
+        cores = os.cpu_count() or 1
+        O.set_threads(cores)
+        dt, dt_old, a_mid, _ = sched[0]
+        t0 = time.perf_counter()
+        xp2, vp2, pid2, rhoc2 = O.drift(q, xp, vp, pid, rhoc, dt_old, dt, vz)
+        O.kick(q, xp2, vp2, rhoc2, dt, a_mid, fixed=False)
+        secs = time.perf_counter() - t0
+        out["config_128"]["cpu_oracle"] = {"value": round(xp.shape[0] / secs, 1), "unit": "particle-steps/s",
+                                           "cores": cores, "kind": "port",
+                                           "sample": "one whole step (drift + kick with PM1, PM2, PM3, PP) of "
+                                                     "the oracle in FP32, first step of the run",
+                                           "seconds": round(secs, 2)}
+    # the adjoint
+    p = config_plain_128()
+    p.box = 256.0
+    n, n_lat, m = 256, 128, 8.0
+    steps, d_close = A.kdk_schedule(p, 20.0, 0.0, 20)
+    a0 = 1 / 21.0
+    dpm = A.DPM(n, 1.5, m, device=local)
+    op = A.ic_operator(p, n_lat, a0)
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    w = torch.randn((n_lat,) * 3, generator=gen, device="cuda")
+    w2 = torch.randn((n_lat,) * 3, generator=gen, device="cuda")
+    with torch.no_grad():
+        x0, v0 = A.zeldovich(w2, p, a0, op)
+        target = dpm.density(A.Simulate.apply(x0.contiguous(), v0.contiguous(), dpm, steps, d_close, 5))
+    fw = bw = 0.0
+    for _ in range(3):
+        wg = w.clone().requires_grad_(True)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        loss = A.density_loss(wg, target, dpm, p, a0, steps, d_close, every=5, op=op)
+        e1.record()
+        loss.backward()
+        e2.record()
+        torch.cuda.synchronize()
+        fw, bw = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    dpm.close()
+    np3 = n_lat ** 3
+    out["adjoint"] = {"workload": "128^3 particles, mesh 256^3, 256 Mpc/h, PM only, 20 KDK steps z=20 -> 0, "
+                                  "density MSE loss, gradient w.r.t. the 128^3 noise modes, checkpoint every 5",
+                      "forward_ms": round(fw, 2), "backward_ms": round(bw, 2),
+                      "forward_particle_steps_per_s": round(np3 * 20 / (fw / 1e3), 1),
+                      "gradient_particle_steps_per_s": round(np3 * 20 / ((fw + bw) / 1e3), 1)}
+    return out
+
+
 def pk_grid(p):
     """cicpower grid of the precision check: 2*ng as utilities/Makefile's FFTFINE builds it,
     capped at 1024^3 (the 512^3 workload's 2048^3 grid would hold ~100 GB beside the step)."""
@@ -510,6 +607,8 @@ def main():
                     help="also time the plain form (FP32 atomics, eager) over the same steps")
     ap.add_argument("--late", default="on", choices=["on", "off"],
                     help="also time the clustered-PP configuration (256^3, 100 Mpc/h) evolved to z~0, both forms")
+    ap.add_argument("--small", default="on", choices=["on", "off"],
+                    help="also time the 128^3 configuration (both forms, and one oracle step) and the adjoint")
     ap.add_argument("--full-run", default="on", choices=["on", "off"],
                     help="also run the 512^3 configuration z=49 -> 0 in 100 KDK steps, both forms")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -599,6 +698,12 @@ def main():
     late = None
     if args.late == "on" and args.workload == "512" and world == 1:
         late = late_leg(args, local, rank)
+    small = None
+    if args.small == "on" and args.workload == "512" and world == 1:
+        try:
+            small = small_configs_leg(args, local, rank, cpu=not args.no_cpu_baseline)
+        except Exception as e:  # reported in the line; the headline above stands
+            small = {"error": str(e)[:300]}
     full = None
     if args.full_run == "on" and args.workload == "512" and world == 1:
         try:
@@ -703,6 +808,8 @@ def main():
             line["late_time"] = late
         if full:
             line["full_run"] = full
+        if small:
+            line["small_configs"] = small
         if analysis:
             line["analysis"] = analysis
         if args.profile_json:
