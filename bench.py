@@ -7,11 +7,16 @@ compressed coordinates, Zel'dovich ICs at z=49 (EH no-wiggle, A_s), reference
 adaptive timestep.  One JSON line on rank 0.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload 512|128] [--deposit fixed|plain] [--graph on|off] [--compare on|off]
+                  [--workload 512|128|proxy] [--deposit fixed|plain] [--graph on|off] [--pp queue|thread]
+                  [--compare on|off] [--late on|off] [--full-run on|off] [--small on|off]
 
-The headline is the chosen form (int64 fixed-point deposit, each step one CUDA graph);
-the plain form (FP32 atomics, eager launches) is timed in the same run over the same steps
-and both are reported, with the relative P(k) difference of their final states.
+The headline is the chosen form (int64 fixed-point deposit, queue PP, each step one CUDA
+graph) over K adaptive steps after W warm-up steps from z=49; the plain form (FP32 atomics,
+thread-per-particle PP, eager launches) is timed in the same run over the same steps and
+both are reported, with the relative P(k) difference of their final states.  On one GPU
+the line also carries: the 512^3 run z=49 -> 0 in 100 steps in both forms (full_run), the
+clustered 256^3 configuration evolved to z~0 (late_time), and the 128^3 configuration with
+one oracle step on the host cores plus the adjoint's forward and backward (small_configs).
 
 --impl reference times the CPU restatement of the reference path (oracle/, the
 reference Fortran cannot be built here) on the host cores over a bounded sample of
