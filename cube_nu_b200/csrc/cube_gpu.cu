@@ -1644,8 +1644,9 @@ static int pp_tune(cube_ctx* c, int cls, int maxcount) {
   std::vector<PPShape> cands;
   // T descending; B = 512 (one block per SM at the heavy kernel's registers) and J = 1024
   // (the chunk length changes no time measured on 512^3 and 256^3 runs, z = 49 to 0) were
-  // never chosen and are left out of the sweep, which runs on the live state
-  const int Ts[] = {2048, 256, 64, 16}, Bs[] = {128, 256}, Js[] = {256};
+  // never chosen and are left out of the sweep, which runs on the live state; B = 32 (an
+  // item of one warp) serves cells of a few dozen particles
+  const int Ts[] = {2048, 256, 64, 16}, Bs[] = {32, 128, 256}, Js[] = {256};
   bool all_light_done = false;
   for (int T : Ts) {
     const bool all_light = T >= maxcount;  // no heavy cells: B and J do not matter
@@ -1653,7 +1654,7 @@ static int pp_tune(cube_ctx* c, int cls, int maxcount) {
     all_light_done |= all_light;
     for (int B : Bs)
       for (int J : Js) {
-        if (all_light && (B != Bs[1] || J != Js[0])) continue;
+        if (all_light && (B != Bs[2] || J != Js[0])) continue;
         PPShape sh;
         sh.T = T;
         sh.B = B;
@@ -2181,7 +2182,8 @@ int cube_gpu_pp_shape(cube_ctx* c, int cls, int T, int B, int J) {
     c->pp_tuned[cls] = false;
     return 0;
   }
-  if (B != 128 && B != 256 && B != 512) return fail(CUBE_E_ARG, "PP item size B must be 128, 256 or 512");
+  if (B != 32 && B != 64 && B != 128 && B != 256 && B != 512)
+    return fail(CUBE_E_ARG, "PP item size B must be 32, 64, 128, 256 or 512");
   if (J < 32 || J > 4096) return fail(CUBE_E_ARG, "PP chunk J must be in 32..4096");
   PPShape sh;
   sh.T = T;

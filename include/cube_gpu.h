@@ -246,8 +246,9 @@ const char* cube_gpu_profile_name(int i);
  * falls in occupancy class cls (largest cell <= 64, <= 512, <= 4096, larger: 0..3; the
  * reference's only tuning data is its PP timing, kick.f90:141-201) and keeps the fastest.
  * Forces do not depend on the shape.  cube_gpu_pp_shape sets the shape of a class (T <= 0
- * forgets it, so it is tuned again); cube_gpu_pp_shape_get returns 1 and the shape and
- * its timed milliseconds when the class has one, else 0. */
+ * forgets it, so it is tuned again; B in {32, 64, 128, 256, 512}, J in 32..4096);
+ * cube_gpu_pp_shape_get returns 1 and the shape and its timed milliseconds when the class
+ * has one, else 0. */
 int cube_gpu_pp_shape(cube_ctx* ctx, int cls, int T, int B, int J);
 int cube_gpu_pp_shape_get(cube_ctx* ctx, int cls, int* T, int* B, int* J, double* ms);
 /* Number of kernels this context has launched since creation. */

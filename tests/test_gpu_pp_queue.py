@@ -79,7 +79,7 @@ def test_queue_pp_is_shape_independent():
     p.mass_p_cdm = float(p.ng) ** 3 / st[0].shape[0]
     assert st[3].max() > 256
     ref, so_ref, _ = _kick(p, st, shape=(4096, 256, 512))
-    for shape in ((4, 128, 256), (16, 256, 1024), (64, 512, 32), (256, 128, 4096)):
+    for shape in ((4, 128, 256), (16, 256, 1024), (64, 512, 32), (256, 128, 4096), (4, 32, 256), (16, 64, 64)):
         v, so, _ = _kick(p, st, shape=shape)
         assert np.array_equal(v, ref), shape
         assert so.pp_pairs == so_ref.pp_pairs and so.pp_candidates == so_ref.pp_candidates
