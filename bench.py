@@ -446,12 +446,16 @@ def full_run_leg(args, local, rank, nsteps=100):
         t0 = time.perf_counter()
         per = []
         stage = np.zeros(7)
+        stage_first = np.zeros(7)
         pairs = cand = 0
-        for dt, dt_old, a_mid, _ in sched:
+        q10 = max(1, nsteps // 10)
+        for i, (dt, dt_old, a_mid, _) in enumerate(sched):
             so = ctx.step(dt, dt_old, a_mid, vz)
             vz = so.vz_max
             per.append(so.tcat[6])
             stage += np.array(list(so.tcat)[:7])
+            if i < q10:
+                stage_first += np.array(list(so.tcat)[:7])
             pairs += so.pp_pairs
             cand += so.pp_candidates
         ctx.drift(sched[-1][0], 0.0, vz)
@@ -465,7 +469,6 @@ def full_run_leg(args, local, rank, nsteps=100):
         if form == "plain_repeat":
             continue
         dev_s = sum(per) / 1e3
-        q10 = max(1, nsteps // 10)
         forms[form] = {"value": round(n * nsteps / dev_s, 1), "ms_per_step": round(sum(per) / nsteps, 3),
                        "wall_s": round(wall, 2),
                        "ms_per_step_first_last_tenth": [round(float(np.mean(per[:q10])), 3),
@@ -473,6 +476,9 @@ def full_run_leg(args, local, rank, nsteps=100):
                        "ms_first_steps": [round(float(x), 2) for x in per[:q10]],
                        "stage_ms_per_step": {k: round(float(v) / nsteps, 3) for k, v in
                                              zip(("drift", "pm1", "pm2", "pm3", "pp", "kick", "step"), stage)},
+                       "stage_ms_per_step_first_tenth": {k: round(float(v) / q10, 3) for k, v in
+                                                         zip(("drift", "pm1", "pm2", "pm3", "pp", "kick", "step"),
+                                                             stage_first)},
                        "pm3_classes_end": list(so.napm)[2:6], "max_cell_end": int(st[3].max()),
                        "pp_pairs_per_step": pairs // nsteps, "pp_candidates_per_step": cand // nsteps,
                        "deposit": "int64 fixed-point" if fixed else "fp32 atomics", "graph": fixed,
