@@ -134,6 +134,7 @@ __device__ __forceinline__ int ppq_iapm(const Geo& G, const int g[3], const int3
 // lane rather than once per candidate that any of its lanes has in range.
 constexpr int PPL_T = 128;  // threads per block
 constexpr int PPL_H = 8;    // deferred pairs per thread
+constexpr int PPL_U = 4;    // candidates evaluated together
 
 __global__ void __launch_bounds__(PPL_T) k_ppq_light(Geo G, int64_t np, const int32_t* __restrict__ pcell,
                                                    const int64_t* __restrict__ cstart, const int32_t* __restrict__ ires,
@@ -165,25 +166,36 @@ __global__ void __launch_bounds__(PPL_T) k_ppq_light(Geo G, int64_t np, const in
           P.cand += (unsigned)(e - s);
           const float bx = (float)((P.l[0] + dx) * G.rcs), by = (float)((P.l[1] + dy) * G.rcs),
                       bz = (float)((P.l[2] + dz) * G.rcs);
-          for (int64_t q = s; q < e; ++q) {
-            const float4 p = pfin[q];
-            const float rv0 = __fsub_rn(__fadd_rn(bx, p.x), P.xf[0]);
-            const float rv1 = __fsub_rn(__fadd_rn(by, p.y), P.xf[1]);
-            const float rv2 = __fsub_rn(__fadd_rn(bz, p.z), P.xf[2]);
-            const float r2 = sumsq3(rv0, rv1, rv2);
-            if (r2 > 0.f && r2 < P.range2) {
-              if (nh == PPL_H) {
-#pragma unroll 1
-                for (int h = 0; h < PPL_H; ++h) {
-                  const float4 r = hb[h][threadIdx.x];
-                  P.accum(r.x, r.y, r.z, r.w, G.app);
-                }
-                nh = 0;
-              }
-              hb[nh][threadIdx.x] = make_float4(rv0, rv1, rv2, r2);
-              ++nh;
-              ++P.pairs;
+          for (int64_t q0 = s; q0 < e; q0 += PPL_U) {
+            // PPL_U candidates as independent chains (loads in flight together, the tail
+            // predicated off), their pairs then recorded in candidate order
+            float rv[PPL_U][3], r2[PPL_U];
+            bool hit[PPL_U];
+#pragma unroll
+            for (int u = 0; u < PPL_U; ++u) {
+              const bool valid = q0 + u < e;
+              const float4 p = pfin[valid ? q0 + u : q0];
+              rv[u][0] = __fsub_rn(__fadd_rn(bx, p.x), P.xf[0]);
+              rv[u][1] = __fsub_rn(__fadd_rn(by, p.y), P.xf[1]);
+              rv[u][2] = __fsub_rn(__fadd_rn(bz, p.z), P.xf[2]);
+              r2[u] = sumsq3(rv[u][0], rv[u][1], rv[u][2]);
+              hit[u] = valid && r2[u] > 0.f && r2[u] < P.range2;
             }
+#pragma unroll
+            for (int u = 0; u < PPL_U; ++u)
+              if (hit[u]) {
+                if (nh == PPL_H) {
+#pragma unroll 1
+                  for (int h = 0; h < PPL_H; ++h) {
+                    const float4 r = hb[h][threadIdx.x];
+                    P.accum(r.x, r.y, r.z, r.w, G.app);
+                  }
+                  nh = 0;
+                }
+                hb[nh][threadIdx.x] = make_float4(rv[u][0], rv[u][1], rv[u][2], r2[u]);
+                ++nh;
+                ++P.pairs;
+              }
           }
         }
 #pragma unroll 1
@@ -402,20 +414,29 @@ __global__ void k_ppq_heavy(Geo G, const int32_t* __restrict__ hlist, const int*
             __syncthreads();
             if (__any_sync(0xffffffffu, need))  // warp-uniform
             for (int k0 = 0; k0 < cnt; k0 += PPH_U) {
-              const int kn = min(cnt, k0 + PPH_U);
-              if (need)
-                for (int k = k0; k < kn; ++k) {
-                  const float4 p = sj[k];
-                  const float rv0 = __fsub_rn(__fadd_rn(bx, p.x), P.xf[0]);
-                  const float rv1 = __fsub_rn(__fadd_rn(by, p.y), P.xf[1]);
-                  const float rv2 = __fsub_rn(__fadd_rn(bz, p.z), P.xf[2]);
-                  const float r2 = sumsq3(rv0, rv1, rv2);
-                  if (r2 > 0.f && r2 < P.range2) {
-                    hb[nh * B + threadIdx.x] = make_float4(rv0, rv1, rv2, r2);
+              if (need) {
+                // PPH_U candidates as independent chains (the tail predicated off), their
+                // pairs then recorded in candidate order
+                float rv[PPH_U][3], r2[PPH_U];
+                bool hit[PPH_U];
+#pragma unroll
+                for (int q = 0; q < PPH_U; ++q) {
+                  const bool valid = k0 + q < cnt;
+                  const float4 p = sj[valid ? k0 + q : k0];
+                  rv[q][0] = __fsub_rn(__fadd_rn(bx, p.x), P.xf[0]);
+                  rv[q][1] = __fsub_rn(__fadd_rn(by, p.y), P.xf[1]);
+                  rv[q][2] = __fsub_rn(__fadd_rn(bz, p.z), P.xf[2]);
+                  r2[q] = sumsq3(rv[q][0], rv[q][1], rv[q][2]);
+                  hit[q] = valid && r2[q] > 0.f && r2[q] < P.range2;
+                }
+#pragma unroll
+                for (int q = 0; q < PPH_U; ++q)
+                  if (hit[q]) {
+                    hb[nh * B + threadIdx.x] = make_float4(rv[q][0], rv[q][1], rv[q][2], r2[q]);
                     ++nh;
                     ++P.pairs;
                   }
-                }
+              }
               if (__any_sync(0xffffffffu, nh > PPH_H - PPH_U)) flush();
             }
           }
