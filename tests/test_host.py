@@ -137,3 +137,23 @@ def test_timestep_snaps_to_the_checkpoint():
     st.dt_pm1 = st.dt_pm2 = st.dt_pm3 = st.dt_pp = st.dt_vmax = 0.05
     cosmology.timestep(bg, st, [49.0, 10.0, 5.0])
     assert st.checkpoint_step and not st.final_step
+
+
+def test_expansion_table_matches_the_reference_recursion():
+    """The rows t and a of the expansion table against the reference's own recursion
+    (neutrinos/Pk.py:263-277, executed by tests/golden/make_expansion_golden.py with the same
+    analytic H(a) standing in for CAMB): bit for bit, sampled entries and the SHA-256 of all."""
+    import hashlib
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "expansion_table_ref.npz"))
+    p = Params()
+    tab = cosmology.expansion_table(float(g["h0"]), float(g["omega_m"]), float(g["omega_r"]))
+    n = int(g["n"])
+    a = np.ascontiguousarray(tab[1][:n])
+    assert a[n - 1] <= 1.0 / 301 < a[n - 2]  # the table stops where Pk.py's loop does
+    idx = g["idx"]
+    assert np.array_equal(a[idx], g["a_sample"])
+    assert np.array_equal(tab[0][idx], g["t_sample"])
+    assert hashlib.sha256(a.tobytes()).hexdigest() == str(g["a_sha256"])
+    assert p.h0 == float(g["h0"]) and p.omega_m == float(g["omega_m"])
