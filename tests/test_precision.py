@@ -41,10 +41,10 @@ def _params(fixed):
     return p
 
 
-def _schedule(p):
+def _schedule(p, nsteps=NSTEPS, z_end=Z_END):
     tab = cosmology.expansion_table(p.h0, p.omega_m, p.omega_r)
     bg = cosmology.Background.from_table(tab)
-    return cosmology.fixed_steps(bg, 1 / (1 + Z_START), 1 / (1 + Z_END), NSTEPS)
+    return cosmology.fixed_steps(bg, 1 / (1 + Z_START), 1 / (1 + z_end), nsteps)
 
 
 def _positions(p, xp, rhoc):
@@ -104,8 +104,9 @@ def _power(p, st, nw):
     return xi
 
 
-@pytest.fixture(scope="module")
-def runs(oracle_lib):
+def make_runs(oracle_lib, nsteps=NSTEPS, z_end=Z_END):
+    """Every arm's run from the same device ICs: the GPU in both forms, the oracle in FP32
+    and FP64 (also used by tests/precision_run.py for whole runs)."""
     from cube_nu_b200 import ic
     from cube_nu_b200._lib import Context
 
@@ -114,7 +115,7 @@ def runs(oracle_lib):
     with Context(p) as ctx:
         d = ic.zeldovich_device(ctx, p, z_i=Z_START, seed=1)
         st0 = ctx.download()
-    sched = _schedule(p)
+    sched = _schedule(p, nsteps, z_end)
     res = {"p": p, "st0": st0, "sched": sched}
     for name, fixed in (("gpu_fixed", True), ("gpu_plain", False)):
         q = _params(fixed)
@@ -124,6 +125,11 @@ def runs(oracle_lib):
     res["oracle32"] = _run_oracle(oracle_lib, p, st0, sched, d["vz_max"], fp64=False)
     res["oracle64"] = _run_oracle(oracle_lib, p, st0, sched, d["vz_max"], fp64=True)
     return res
+
+
+@pytest.fixture(scope="module")
+def runs(oracle_lib):
+    return make_runs(oracle_lib)
 
 
 def _pos_vel_errors(p, st, ref):
