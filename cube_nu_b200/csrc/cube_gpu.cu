@@ -1019,6 +1019,8 @@ static int alloc_particles(cube_ctx* c, int64_t np) {
 // empty at the new size.
 static int grow_particles(cube_ctx* c, int64_t need) {
   if (need <= c->cap) return 0;
+  if (c->P.pp_queue && need > INT32_MAX)  // the heavy-cell index array holds 32-bit indices
+    return fail(CUBE_E_CAPACITY, "pp_queue indexes particles in 32 bits: at most 2^31 - 1 per context");
   drop_graphs(c);
   if (c->ckpt_pending) cudaEventSynchronize(c->ev_ckpt);
   CK(cudaStreamSynchronize(c->s));
