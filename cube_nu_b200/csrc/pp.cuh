@@ -6,15 +6,18 @@
 // cells of its subtile's class), cells in the order dz, dy, dx and particles in storage
 // order within a cell.  The work is split by the occupancy of the particle's own cell:
 //   * light cells (at most T particles): one thread per particle (k_ppq_light);
-//   * heavy cells: items of B particles of one cell, pulled from a device queue by a
-//     persistent kernel (k_ppq_heavy) whose block stages the candidate cells' particles in
-//     shared memory in chunks of J and tests its B particles against each chunk.  The
-//     queue is ordered by occupancy, largest first (log2 buckets), so the long items start
-//     first and the tail is short.
+//   * heavy cells: their particles counted-sorted by the set of neighbour cells they reach
+//     (k_ppq_sort_codes), then cut into items of B particles of one cell, pulled from a
+//     device queue by a persistent kernel (k_ppq_heavy) whose block stages the candidate
+//     cells' particles in shared memory in chunks of J and tests its B particles against
+//     each chunk.  The queue is ordered by occupancy, largest first (log2 buckets), so the
+//     long items start first and the tail is short.
 // Both paths read the candidates' in-cell offsets, decoded once per step into a float4
-// array (k_ppq_prep), and accumulate each particle's pairs with the same operations in
-// the same order, so the force does not depend on (T, B, J): the autotuner
-// (cube_gpu.cu, pp_tune) picks the fastest shape per occupancy class freely.
+// array (k_ppq_prep), test candidates four at a time as independent chains, defer the
+// pairs in range to a per-thread shared-memory column and add them in candidate order,
+// so each particle's pairs are summed with the same operations in the same order and the
+// force does not depend on (T, B, J): the autotuner (cube_gpu.cu, pp_tune) picks the
+// fastest shape per occupancy class freely.
 #pragma once
 #include "kernels.cuh"
 
