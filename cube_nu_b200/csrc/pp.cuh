@@ -6,7 +6,7 @@
 // cells of its subtile's class), cells in the order dz, dy, dx and particles in storage
 // order within a cell.  The work is split by the occupancy of the particle's own cell:
 //   * light cells (at most T particles): one thread per particle (k_ppq_light);
-//   * heavy cells: their particles counted-sorted by the set of neighbour cells they reach
+//   * heavy cells: their particles counting-sorted by the set of neighbour cells they reach
 //     (k_ppq_sort_codes), then cut into items of B particles of one cell, pulled from a
 //     device queue by a persistent kernel (k_ppq_heavy) whose block stages the candidate
 //     cells' particles in shared memory in chunks of J and tests its B particles against
