@@ -59,3 +59,28 @@ def test_single_process_is_the_identity():
 
     assert bench.over_ranks([3.0, 4.0], "max") == [3.0, 4.0]
     assert bench.job_rate(10, 3, 2.0) == 15.0
+
+
+def test_roofline_numerators():
+    """The algorithmic bytes bench.py divides by kernel time: the owner PM3 deposit writes
+    every cell of every class-2 box once as float and reads each position code once; the
+    PM3 FFT passes move the float mesh and the half spectrum once each way."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from cube_nu_b200.params import config_512
+
+    p = config_512()
+    n = p.npglobal
+    napm = [0, 0, p.ns3, 0, 0, 0]
+    nft = p.nft(2)
+    assert bench.kernel_bytes(p, "deposit_pm3", n, napm, True) == p.ns3 * nft ** 3 * 4 + n * 3 * p.izipx
+    nh = nft * nft * (nft // 2 + 1) * p.ns3
+    assert bench.kernel_bytes(p, "fft_x_pm3", n, napm, True) == p.ns3 * nft ** 3 * 4 + nh * 8
+    assert bench.kernel_bytes(p, "fft_c2r_pm3", n, napm, True) == nh * 8 + p.ns3 * nft ** 3 * 4
+    assert bench.kernel_bytes(p, "fft_y_pm3", n, napm, True) == 2 * 2 * nh * 8
+    for name in ("deposit_pm1", "deposit_pm2", "interp_pm1", "interp_pm2", "interp_pm3", "pp", "drift_dest",
+                 "drift_gather", "fft_x_pm2", "fft_z_green_pm3"):
+        b = bench.kernel_bytes(p, name, n, napm, True)
+        assert isinstance(b, int) and b > 0, name
+    assert bench.kernel_bytes(p, "momentum", n, napm, True) is None
+    assert bench.job_rate(4 * n, 20, 2.0) == 4 * n * 10
