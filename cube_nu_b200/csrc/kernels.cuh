@@ -1581,14 +1581,24 @@ __global__ void __launch_bounds__(1024) k_build_lists(const int32_t* __restrict_
 // coarse cells its range can reach; equivalent to the reference's PP-cell lists
 // (the PP cell 4/rsf fine cells is wider than the range 3.5/rsf).
 // =================================================================================
-__device__ __forceinline__ float F_ra(float r, float apm) {
+// The softened force law's coefficient (1/35)/apm^2, a constant of apm.
+__device__ __forceinline__ float F_ra_coef(float apm) { return __fdiv_rn(__fdiv_rn(1.f, 35.f), __fmul_rn(apm, apm)); }
+
+// F_ra with its coefficient c = F_ra_coef(apm) passed in, for callers that evaluate it for
+// one apm many times; the same operations as F_ra.
+__device__ __forceinline__ float F_ra_c(float r, float apm, float c) {
   const float ep = __fdiv_rn(2.f * r, apm);
   if (apm == 0.f || ep > 2.f) return __fdiv_rn(1.f, __fmul_rn(r, r));
-  const float c = __fdiv_rn(__fdiv_rn(1.f, 35.f), __fmul_rn(apm, apm));
   const float e2 = ep * ep, e3 = e2 * ep, e4 = e3 * ep, e5 = e4 * ep, e6 = e5 * ep;
   if (ep > 1.f) return c * (12.f * (1.f / e2) - 224.f + 896.f * ep - 840.f * e2 + 224.f * e3 + 70.f * e4 - 48.f * e5 + 7.f * e6);
   if (ep > 0.f) return c * (224.f * ep - 224.f * e3 + 70.f * e4 + 48.f * e5 - 21.f * e6);
   return 0.f;
+}
+
+__device__ __forceinline__ float F_ra(float r, float apm) {
+  const float ep = __fdiv_rn(2.f * r, apm);
+  if (apm == 0.f || ep > 2.f) return __fdiv_rn(1.f, __fmul_rn(r, r));
+  return F_ra_c(r, apm, F_ra_coef(apm));
 }
 
 // Candidate coordinate (xq in kick.f90:424): ((lq + (u+0.5)*x_res) * ratio_cs) rounded to

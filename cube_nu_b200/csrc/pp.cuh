@@ -41,7 +41,7 @@ __global__ void k_ppq_prep(Geo G, int64_t np, const void* __restrict__ xp, float
 struct PPi {
   float xf[3];
   int l[3], lo[3], hi[3];
-  float range, range2;
+  float range, range2, coef_range, coef_app;  // range and F_ra_coef of range and app
   float acc[3];
   unsigned pairs, cand;  // of this particle (item): well below 2^32
 
@@ -49,6 +49,8 @@ struct PPi {
     const float fi[3] = {fin.x, fin.y, fin.z};
     range = __fdiv_rn(3.5f, (float)rsf_of(iapm));  // apm3(iapm)
     range2 = __fmul_rn(range, range);
+    coef_range = F_ra_coef(range);
+    coef_app = F_ra_coef(G.app);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       l[d] = g[d] % G.nt;
@@ -68,7 +70,7 @@ struct PPi {
   // that defer their pairs call it in candidate order, so the sums are k_pp's.
   __device__ __forceinline__ void accum(float rv0, float rv1, float rv2, float r2, float app) {
     const float rm = __fsqrt_rn(r2);
-    const float sc = __fsub_rn(F_ra(rm, app), F_ra(rm, range));
+    const float sc = __fsub_rn(F_ra_c(rm, app, coef_app), F_ra_c(rm, range, coef_range));
     acc[0] = __fadd_rn(acc[0], __fmul_rn(__fdiv_rn(rv0, rm), sc));
     acc[1] = __fadd_rn(acc[1], __fmul_rn(__fdiv_rn(rv1, rm), sc));
     acc[2] = __fadd_rn(acc[2], __fmul_rn(__fdiv_rn(rv2, rm), sc));
